@@ -1,0 +1,197 @@
+/*
+ * mxm_dg.h -- C ABI of the B200 nodal-DG right-hand-side library.
+ *
+ * Drop-in for mojoxm's hot path: the 3D `Solver[PhysT, P]` stage kernel,
+ * SSPRK3 stepping and Barth-Jespersen/Venkatakrishnan cell limiter on
+ * periodic/bounded Kuhn tetrahedral meshes, and the 2D per-physics stage
+ * kernels on Kuhn triangle meshes.  Conventions follow the reference's only
+ * native shim, src/mpi_shim.c: plain C functions, `int` return codes (0 = OK,
+ * negative = MXM_DG_E*), opaque `void*` handles, caller-owned host arrays, no
+ * structs with implementation-defined layout.  A Mojo binding wraps each call
+ * as `external_call["mxm_dg_...", c_int](...)` and raises on rc != 0, as
+ * src/mpi.mojo:33-43 does for the MPI shim.
+ *
+ * State layout (identical to the reference, src/solver.mojo:17-22):
+ *   q[(e * NP + i) * NC + c]   element-major, node, then component,
+ * elements numbered cell * 6 + tet (3D, cell = i + Nx*(j + Ny*k)) or
+ * cell * 2 + tri (2D, cell = j*Nx + i), nodes in the reference's equispaced
+ * Lagrange order (src/reference.mojo:136-200, src/reference.mojo:203-237).
+ *
+ * Threading: one host thread per handle (MPI_THREAD_FUNNELED model of
+ * src/mpi_shim.c:44).  All work is enqueued on the handle's own CUDA stream;
+ * mxm_dg_synchronize() blocks.  Errors raised asynchronously on the device
+ * are reported by the next call that synchronizes.
+ */
+#ifndef MXM_DG_H
+#define MXM_DG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MXM_DG_VERSION 10000 /* 1.0.0 */
+
+/* Return codes (mpi_shim.c returns the MPI error code; we use negatives). */
+#define MXM_DG_OK 0
+#define MXM_DG_EINVAL (-1)     /* bad argument, unsupported P/physics/flux   */
+#define MXM_DG_ENOMEM (-2)     /* device allocation failed / over budget     */
+#define MXM_DG_ECUDA (-3)      /* CUDA runtime error (message in last_error) */
+#define MXM_DG_ENONFINITE (-4) /* non-finite value detected in a reduction   */
+#define MXM_DG_ETIMEDOUT (-5)  /* bounded device wait gave up                */
+#define MXM_DG_ENOTREADY (-6)  /* request not finished yet (serving poll)    */
+
+/* Physics kinds: src/advection.mojo, src/euler.mojo, src/maxwell.mojo,
+ * src/shallow_water.mojo. */
+#define MXM_DG_PHYS_ADVECTION 0
+#define MXM_DG_PHYS_EULER 1
+#define MXM_DG_PHYS_MAXWELL 2
+#define MXM_DG_PHYS_SHALLOW_WATER 3
+
+/* Numerical fluxes.  3D Euler: FLUX_RUSANOV..FLUX_HLLEC (euler.mojo:33-36).
+ * 2D Euler: RUSANOV (|v|+c speed, local_mesh_2d_gpu_euler.mojo:220-337),
+ * HLLC (:392-545) or HLLE (3D HLLE on the w=0, n_z=0 embedding).
+ * 2D shallow water: RUSANOV or HLL (local_mesh_2d_gpu_sw.mojo:178,308).
+ * Maxwell and advection have a single flux each and ignore this field. */
+#define MXM_DG_FLUX_RUSANOV 0
+#define MXM_DG_FLUX_ROE 1
+#define MXM_DG_FLUX_HLLE 2
+#define MXM_DG_FLUX_HLLEC 3
+#define MXM_DG_FLUX_HLLC 4
+#define MXM_DG_FLUX_HLL 5
+
+/* Boundary-condition codes, src/boundary.mojo:310-313.  BC_INTERIOR on an
+ * axis means periodic. */
+#define MXM_DG_BC_INTERIOR 0
+#define MXM_DG_BC_WALL 1
+#define MXM_DG_BC_OUTFLOW 2
+#define MXM_DG_BC_INFLOW 3
+
+/* Arithmetic of a handle. */
+#define MXM_DG_PREC_F64 0   /* state, geometry and all arithmetic in FP64       */
+#define MXM_DG_PREC_F32 1   /* FP32 state and arithmetic (the reference's path) */
+#define MXM_DG_PREC_MIXED 2 /* FP32 state/flux, split-BF16 tensor-core contractions */
+
+/* Physics parameters, `p[]` in the field order of the Mojo structs:
+ *  ADVECTION (advection.mojo:192-199): p = {vx, vy, vz, inflow_q}
+ *  EULER (euler.mojo:534-554): p = {gamma, min_density, min_pressure, gx, gy,
+ *        gz, inflow_rho, inflow_rhou, inflow_rhov, inflow_rhow, inflow_E};
+ *        flux_type and entropy_fix are the integer fields below.  In 2D the
+ *        inflow state is {rho, rhou, rhov, E} = p[6], p[7], p[8], p[10].
+ *  MAXWELL (maxwell.mojo:55-74): p = {c, Jx, Jy, Jz, Mx, My, Mz, inflow_Ex,
+ *        inflow_Ey, inflow_Ez, inflow_Bx, inflow_By, inflow_Bz}
+ *  SHALLOW_WATER (shallow_water.mojo:34-40): p = {g, h_min, inflow_h,
+ *        inflow_hu, inflow_hv} */
+typedef struct mxm_dg_physics_desc {
+  int32_t kind;
+  int32_t flux_type;
+  int32_t entropy_fix;
+  int32_t reserved;
+  double p[16];
+} mxm_dg_physics_desc;
+
+/* Mesh: dim 3 -> Nx*Ny*Nz cubes x 6 Kuhn tets on [0,Lx]x[0,Ly]x[0,Lz]
+ * (src/local_mesh.mojo:1241-1485); dim 2 -> Nx*Ny cells x 2 triangles
+ * (src/local_mesh_2d.mojo:106-395, nz/Lz ignored).  bc[] = {x_lo, x_hi,
+ * y_lo, y_hi, z_lo, z_hi} (boundary.mojo:328-333; 2D uses the first four). */
+typedef struct mxm_dg_mesh_desc {
+  int32_t dim;
+  int32_t nx, ny, nz;
+  double lx, ly, lz;
+  int32_t bc[6];
+} mxm_dg_mesh_desc;
+
+/* ---- lifetime ----------------------------------------------------------- */
+int mxm_dg_version(void);
+/* Replaces Solver.__init__(ctx, mesh, halo, physics, D_ref, Lift_ref,
+ * node_weights) (src/solver.mojo:595-643) and Mesh[P](...) (mesh.mojo:362):
+ * builds operators (host FP64) and mesh tables for order P (1..5), allocates
+ * q/q1/q2 zero-filled on the current CUDA device. */
+int mxm_dg_create(const mxm_dg_mesh_desc* mesh, const mxm_dg_physics_desc* phys, int P, int precision, void** handle);
+int mxm_dg_destroy(void* handle);
+/* num_elements, NP, NFP (nodes per face), NC, bytes per state value. */
+int mxm_dg_sizes(void* handle, int64_t* num_elements, int32_t* np, int32_t* nfp, int32_t* nc, int32_t* real_bytes);
+/* Solver.dof_count (solver.mojo:757-763): num_elements * NP * NC. */
+int mxm_dg_dof_count(void* handle, int64_t* dof);
+/* Solver.state_bytes_per_step (solver.mojo:804-824): 8 buffer touches per step. */
+int mxm_dg_state_bytes_per_step(void* handle, int64_t* bytes);
+
+/* ---- state access ------------------------------------------------------- */
+/* Device pointer to d_q (which=0), d_q1 (1) or d_q2 (2), for caller IC
+ * kernels (the reference's drivers write solver.d_q directly). */
+int mxm_dg_state_ptr(void* handle, int which, void** dptr);
+/* Device pointer to node coordinates, float32 [Ne*NP*dim], the reference's
+ * elem_node_xyz (local_mesh.mojo:777-845; 2D: local_mesh_2d.mojo:163-180). */
+int mxm_dg_node_xyz_ptr(void* handle, void** dptr);
+/* Host copies of node coordinates in FP64 [Ne*NP*dim]. */
+int mxm_dg_node_xyz(void* handle, double* host);
+/* Copy a whole state buffer from/to caller-owned host memory; `nbytes` must
+ * equal Ne*NP*NC*real_bytes.  Synchronous. */
+int mxm_dg_upload_state(void* handle, int which, const void* host, size_t nbytes);
+int mxm_dg_download_state(void* handle, int which, void* host, size_t nbytes);
+/* Solver.download_owned_component (solver.mojo:711-729): component c of d_q
+ * for all elements, Float32 [Ne*NP] (as the reference) or FP64. */
+int mxm_dg_download_component(void* handle, int c, float* host);
+int mxm_dg_download_component_f64(void* handle, int c, double* host);
+
+/* ---- stepping ------------------------------------------------------------ */
+/* Solver.enable_cell_limiter (solver.mojo:741-755).  3D: theta over all
+ * components; 2D: theta from component 0, BC self-neighbours excluded
+ * (local_mesh_2d_gpu_limiter.mojo:74-133).  Default off, eps 0.1. */
+int mxm_dg_enable_limiter(void* handle, int on, double venkat_eps);
+/* Solver.step_ssprk3 (solver.mojo:1071-1092) / ssprk3_stage_plans. */
+int mxm_dg_step_ssprk3(void* handle, double dt);
+/* Advance `nsteps` SSPRK3 steps (one enqueue, no host sync). */
+int mxm_dg_step_n(void* handle, double dt, int nsteps);
+/* One Shu-Osher stage s in {0,1,2} (q->q1, (q,q1)->q2, (q,q2)->q) incl. the
+ * limiter when enabled. */
+int mxm_dg_rk_stage(void* handle, int stage, double dt);
+/* Semi-discrete RHS L(q) of device buffer q_dev into rhs_dev (both
+ * Ne*NP*NC values of the handle's real type); no RK combine, no floors. */
+int mxm_dg_eval_rhs(void* handle, const void* q_dev, void* rhs_dev);
+/* Apply the cell limiter once to state buffer `which`. */
+int mxm_dg_limit(void* handle, int which);
+/* Host-buffer entry: upload q_host into d_q, take `nsteps` SSPRK3 steps and
+ * download d_q into q_out_host (the same layout).  Pinned host memory gives
+ * asynchronous copies; pageable memory works too. */
+int mxm_dg_advance_host(void* handle, const void* q_host, void* q_out_host, int nsteps, double dt);
+
+/* ---- diagnostics (FP64 device reductions) -------------------------------- */
+/* Max over all face nodes of the signal speed numerical_flux/boundary_flux
+ * return (discarded by the reference, solver.mojo:266-268), on d_q. */
+int mxm_dg_max_wavespeed(void* handle, double* out);
+/* kind 0: integral of q_c over the domain (sum_e V_e sum_i w_i q);
+ * kind 1: integral of q_c^2 (nodal quadrature); kind 2: max |q_c|.
+ * Reductions accumulate in FP64 on the device in a fixed order. */
+int mxm_dg_reduce_conserved(void* handle, int which, int c, int kind, double* out);
+
+/* ---- misc ---------------------------------------------------------------- */
+/* Make `device` the current CUDA device of the calling thread; handles are
+ * created on the thread's current device (one process per GPU). */
+int mxm_dg_set_device(int device);
+/* Page-locked host buffers for asynchronous state transfers. */
+int mxm_dg_host_alloc(size_t nbytes, void** host);
+int mxm_dg_host_free(void* host);
+int mxm_dg_synchronize(void* handle);
+/* Time `nsteps` SSPRK3 steps with CUDA events on the handle's stream; the
+ * device time in milliseconds goes to *ms. */
+int mxm_dg_time_steps(void* handle, double dt, int nsteps, double* ms);
+/* Number of kernel launches the handle issues per SSPRK3 step. */
+int mxm_dg_launches_per_step(void* handle, int32_t* n);
+/* Copies the handle's last error message (NUL-terminated). handle may be NULL
+ * for errors raised by mxm_dg_create. */
+int mxm_dg_last_error(void* handle, char* buf, int len);
+/* Device operator blocks for inspection: the per-tet-type fused
+ * [Dx|Dy|Dz|-Lift] matrices in FP64, type-major [ntypes][NP][K]
+ * (K = 3*NP + 4*NFP in 3D, 2*NP + 3*(P+1) in 2D).  `count` in/out. */
+int mxm_dg_operator(void* handle, double* host, int64_t* count);
+/* Reference operators the library built (host FP64): D [dim*NP*NP],
+ * Lift [nfaces*NP*NFP] in the reference's face-local order, w [NP]. */
+int mxm_dg_reference_operators(int dim, int P, double* D, double* Lift, double* w);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MXM_DG_H */

@@ -1,0 +1,427 @@
+"""mojoxm_b200 -- B200 (sm_100a) nodal DG right-hand side, SSPRK3 stage and
+slope limiter for Kuhn tetrahedral (3D) and triangular (2D) meshes.
+
+Python front end over the C ABI in include/mxm_dg.h (libmxm_dg.so, built in
+this directory by build.py).  The names mirror mojoxm's host API:
+
+    physics = Euler(gamma=1.4, min_density=1e-6, min_pressure=1e-6,
+                    flux_type=FLUX_HLLEC, entropy_fix=True)
+    solver = Solver(Mesh(nx, ny, nz, L, BoundaryConditions.periodic()),
+                    physics, P=2, precision="f64")
+    solver.upload_state(q0)                    # or write solver.d_q on the device
+    solver.step_ssprk3(dt)
+    rho = solver.download_owned_component(0)
+
+(src/solver.mojo:538-1092, src/euler.mojo:556-584, src/boundary.mojo:326-362).
+There is no CPU execution path: constructing a Solver without the CUDA
+library or without a GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmxm_dg.so")
+
+# include/mxm_dg.h constants
+OK, EINVAL, ENOMEM, ECUDA, ENONFINITE, ETIMEDOUT, ENOTREADY = 0, -1, -2, -3, -4, -5, -6
+PHYS_ADVECTION, PHYS_EULER, PHYS_MAXWELL, PHYS_SHALLOW_WATER = 0, 1, 2, 3
+FLUX_RUSANOV, FLUX_ROE, FLUX_HLLE, FLUX_HLLEC, FLUX_HLLC, FLUX_HLL = 0, 1, 2, 3, 4, 5
+BC_INTERIOR, BC_WALL, BC_OUTFLOW, BC_INFLOW = 0, 1, 2, 3
+PREC = {"f64": 0, "f32": 1, "mixed": 2}
+
+EXPORTED = [
+    "mxm_dg_version", "mxm_dg_create", "mxm_dg_destroy", "mxm_dg_sizes", "mxm_dg_dof_count",
+    "mxm_dg_state_bytes_per_step", "mxm_dg_state_ptr", "mxm_dg_node_xyz_ptr", "mxm_dg_node_xyz",
+    "mxm_dg_upload_state", "mxm_dg_download_state", "mxm_dg_download_component", "mxm_dg_download_component_f64",
+    "mxm_dg_enable_limiter", "mxm_dg_step_ssprk3", "mxm_dg_step_n", "mxm_dg_rk_stage", "mxm_dg_eval_rhs",
+    "mxm_dg_limit", "mxm_dg_advance_host", "mxm_dg_max_wavespeed", "mxm_dg_reduce_conserved",
+    "mxm_dg_synchronize", "mxm_dg_time_steps", "mxm_dg_launches_per_step", "mxm_dg_last_error",
+    "mxm_dg_operator", "mxm_dg_reference_operators", "mxm_dg_set_device", "mxm_dg_host_alloc", "mxm_dg_host_free",
+]
+
+
+class DGError(RuntimeError):
+    def __init__(self, rc, msg):
+        super().__init__(f"mxm_dg error {rc}: {msg}")
+        self.rc = rc
+
+
+class _PhysDesc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("flux_type", ctypes.c_int32), ("entropy_fix", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("p", ctypes.c_double * 16)]
+
+
+class _MeshDesc(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int32), ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+                ("bc", ctypes.c_int32 * 6)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libmxm_dg.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python mojoxm_b200/build.py` (nvcc, sm_100a)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i64p, i32p, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32), \
+            ctypes.POINTER(ctypes.c_double)
+        L.mxm_dg_create.argtypes = [ctypes.POINTER(_MeshDesc), ctypes.POINTER(_PhysDesc), ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_void_p)]
+        L.mxm_dg_destroy.argtypes = [vp]
+        L.mxm_dg_sizes.argtypes = [vp, i64p, i32p, i32p, i32p, i32p]
+        L.mxm_dg_dof_count.argtypes = [vp, i64p]
+        L.mxm_dg_state_bytes_per_step.argtypes = [vp, i64p]
+        L.mxm_dg_state_ptr.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.mxm_dg_node_xyz_ptr.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
+        L.mxm_dg_node_xyz.argtypes = [vp, dp]
+        L.mxm_dg_upload_state.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t]
+        L.mxm_dg_download_state.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t]
+        L.mxm_dg_download_component.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+        L.mxm_dg_download_component_f64.argtypes = [vp, ctypes.c_int, dp]
+        L.mxm_dg_enable_limiter.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+        L.mxm_dg_step_ssprk3.argtypes = [vp, ctypes.c_double]
+        L.mxm_dg_step_n.argtypes = [vp, ctypes.c_double, ctypes.c_int]
+        L.mxm_dg_rk_stage.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+        L.mxm_dg_eval_rhs.argtypes = [vp, vp, vp]
+        L.mxm_dg_limit.argtypes = [vp, ctypes.c_int]
+        L.mxm_dg_advance_host.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double]
+        L.mxm_dg_max_wavespeed.argtypes = [vp, dp]
+        L.mxm_dg_reduce_conserved.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
+        L.mxm_dg_synchronize.argtypes = [vp]
+        L.mxm_dg_time_steps.argtypes = [vp, ctypes.c_double, ctypes.c_int, dp]
+        L.mxm_dg_launches_per_step.argtypes = [vp, i32p]
+        L.mxm_dg_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+        L.mxm_dg_operator.argtypes = [vp, dp, i64p]
+        L.mxm_dg_reference_operators.argtypes = [ctypes.c_int, ctypes.c_int, dp, dp, dp]
+        L.mxm_dg_set_device.argtypes = [ctypes.c_int]
+        L.mxm_dg_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
+        L.mxm_dg_host_free.argtypes = [vp]
+        _lib = L
+    return _lib
+
+
+def set_device(device: int):
+    _check(lib().mxm_dg_set_device(device))
+
+
+class PinnedArray:
+    """numpy view over page-locked host memory (mxm_dg_host_alloc)."""
+
+    def __init__(self, shape, dtype):
+        n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        p = ctypes.c_void_p()
+        _check(lib().mxm_dg_host_alloc(n, ctypes.byref(p)))
+        self.ptr = p
+        buf = (ctypes.c_char * n).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    def free(self):
+        if self.ptr:
+            self.array = None
+            lib().mxm_dg_host_free(self.ptr)
+            self.ptr = None
+
+
+def _err(h=None):
+    buf = ctypes.create_string_buffer(1024)
+    lib().mxm_dg_last_error(h, buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def _check(rc, h=None):
+    if rc != OK:
+        raise DGError(rc, _err(h))
+
+
+# ------------------------------------------------------------------ physics
+@dataclass
+class Advection:  # src/advection.mojo:187-205
+    vx: float
+    vy: float
+    vz: float = 0.0
+    inflow_q: float = 0.0
+    kind: int = field(default=PHYS_ADVECTION, init=False)
+    flux_type: int = field(default=0, init=False)
+    entropy_fix: bool = field(default=False, init=False)
+
+    def params(self):
+        return [self.vx, self.vy, self.vz, self.inflow_q]
+
+
+@dataclass
+class Euler:  # src/euler.mojo:531-584
+    gamma: float = 1.4
+    min_density: float = 1e-6
+    min_pressure: float = 1e-6
+    flux_type: int = FLUX_HLLEC
+    entropy_fix: bool = False
+    gx: float = 0.0
+    gy: float = 0.0
+    gz: float = 0.0
+    inflow_rho: float = 0.0
+    inflow_rhou: float = 0.0
+    inflow_rhov: float = 0.0
+    inflow_rhow: float = 0.0
+    inflow_E: float = 0.0
+    kind: int = field(default=PHYS_EULER, init=False)
+
+    def params(self):
+        return [self.gamma, self.min_density, self.min_pressure, self.gx, self.gy, self.gz, self.inflow_rho,
+                self.inflow_rhou, self.inflow_rhov, self.inflow_rhow, self.inflow_E]
+
+
+@dataclass
+class Maxwell:  # src/maxwell.mojo:48-104
+    c: float = 1.0
+    Jx: float = 0.0
+    Jy: float = 0.0
+    Jz: float = 0.0
+    Mx: float = 0.0
+    My: float = 0.0
+    Mz: float = 0.0
+    inflow_Ex: float = 0.0
+    inflow_Ey: float = 0.0
+    inflow_Ez: float = 0.0
+    inflow_Bx: float = 0.0
+    inflow_By: float = 0.0
+    inflow_Bz: float = 0.0
+    kind: int = field(default=PHYS_MAXWELL, init=False)
+    flux_type: int = field(default=0, init=False)
+    entropy_fix: bool = field(default=False, init=False)
+
+    def params(self):
+        return [self.c, self.Jx, self.Jy, self.Jz, self.Mx, self.My, self.Mz, self.inflow_Ex, self.inflow_Ey,
+                self.inflow_Ez, self.inflow_Bx, self.inflow_By, self.inflow_Bz]
+
+
+@dataclass
+class ShallowWater:  # src/shallow_water.mojo:31-47
+    g: float = 9.81
+    h_min: float = 1e-6
+    inflow_h: float = 0.0
+    inflow_hu: float = 0.0
+    inflow_hv: float = 0.0
+    flux_type: int = FLUX_RUSANOV
+    kind: int = field(default=PHYS_SHALLOW_WATER, init=False)
+    entropy_fix: bool = field(default=False, init=False)
+
+    def params(self):
+        return [self.g, self.h_min, self.inflow_h, self.inflow_hu, self.inflow_hv]
+
+
+def physics_dict(ph):
+    """Flat descriptor {kind, flux, entropy_fix, p} shared with the oracle."""
+    return dict(kind=ph.kind, flux=ph.flux_type, entropy_fix=int(ph.entropy_fix), p=list(ph.params()))
+
+
+@dataclass
+class BoundaryConditions:  # src/boundary.mojo:326-343 ([-x, +x, -y, +y, -z, +z])
+    bc_x_lo: int = BC_INTERIOR
+    bc_x_hi: int = BC_INTERIOR
+    bc_y_lo: int = BC_INTERIOR
+    bc_y_hi: int = BC_INTERIOR
+    bc_z_lo: int = BC_INTERIOR
+    bc_z_hi: int = BC_INTERIOR
+
+    @staticmethod
+    def periodic():
+        return BoundaryConditions()
+
+    def all_periodic(self):
+        return all(b == BC_INTERIOR for b in self.as_list())
+
+    def as_list(self):
+        return [self.bc_x_lo, self.bc_x_hi, self.bc_y_lo, self.bc_y_hi, self.bc_z_lo, self.bc_z_hi]
+
+
+@dataclass
+class Mesh:
+    """Kuhn mesh: dim 3 -> nx*ny*nz cubes x 6 tets; dim 2 -> nx*ny cells x 2 triangles."""
+    nx: int
+    ny: int
+    nz: int = 1
+    lx: float = 1.0
+    ly: float = 1.0
+    lz: float = 1.0
+    bcs: BoundaryConditions = field(default_factory=BoundaryConditions.periodic)
+    dim: int = 3
+
+    def desc(self):
+        d = _MeshDesc()
+        d.dim, d.nx, d.ny, d.nz = self.dim, self.nx, self.ny, self.nz
+        d.lx, d.ly, d.lz = self.lx, self.ly, self.lz
+        for k, b in enumerate(self.bcs.as_list()):
+            d.bc[k] = b
+        return d
+
+
+class Solver:
+    """Solver[PhysT, P] over the C ABI: device state q/q1/q2, SSPRK3, limiter."""
+
+    def __init__(self, mesh: Mesh, physics, P: int = 2, precision: str = "f64"):
+        L = lib()
+        pd = _PhysDesc()
+        pd.kind, pd.flux_type, pd.entropy_fix = physics.kind, physics.flux_type, int(physics.entropy_fix)
+        for k, v in enumerate(physics.params()):
+            pd.p[k] = v
+        md = mesh.desc()
+        h = ctypes.c_void_p()
+        _check(L.mxm_dg_create(ctypes.byref(md), ctypes.byref(pd), P, PREC[precision], ctypes.byref(h)))
+        self.h = h
+        self.mesh, self.physics, self.P, self.precision = mesh, physics, P, precision
+        ne, np_, nfp, nc, rb = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        _check(L.mxm_dg_sizes(h, ctypes.byref(ne), ctypes.byref(np_), ctypes.byref(nfp), ctypes.byref(nc),
+                              ctypes.byref(rb)), h)
+        self.num_elements, self.NP, self.NFP, self.NC = ne.value, np_.value, nfp.value, nc.value
+        self.dtype = np.float64 if rb.value == 8 else np.float32
+        self.shape = (self.num_elements, self.NP, self.NC)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mxm_dg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc):
+        _check(rc, self.h)
+
+    # -- state
+    def state_ptr(self, which=0):
+        p = ctypes.c_void_p()
+        self._c(lib().mxm_dg_state_ptr(self.h, which, ctypes.byref(p)))
+        return p.value
+
+    @property
+    def d_q(self):
+        return self.state_ptr(0)
+
+    def node_xyz(self):
+        out = np.zeros((self.num_elements, self.NP, self.mesh.dim))
+        self._c(lib().mxm_dg_node_xyz(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    def node_xyz_ptr(self):
+        p = ctypes.c_void_p()
+        self._c(lib().mxm_dg_node_xyz_ptr(self.h, ctypes.byref(p)))
+        return p.value
+
+    def upload_state(self, q, which=0):
+        a = np.ascontiguousarray(q, dtype=self.dtype).reshape(-1)
+        assert a.size == self.num_elements * self.NP * self.NC, "state size mismatch"
+        self._c(lib().mxm_dg_upload_state(self.h, which, a.ctypes.data, a.nbytes))
+
+    def download_state(self, which=0):
+        out = np.empty(self.shape, dtype=self.dtype)
+        self._c(lib().mxm_dg_download_state(self.h, which, out.ctypes.data, out.nbytes))
+        return out
+
+    def download_owned_component(self, c):  # solver.mojo:711-729 (Float32 as the reference)
+        out = np.empty(self.num_elements * self.NP, dtype=np.float32)
+        self._c(lib().mxm_dg_download_component(self.h, c, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    # -- stepping
+    def enable_cell_limiter(self, enabled=True, venkat_eps=0.1):
+        self._c(lib().mxm_dg_enable_limiter(self.h, int(enabled), venkat_eps))
+
+    def step_ssprk3(self, dt):
+        self._c(lib().mxm_dg_step_ssprk3(self.h, dt))
+
+    def step_n(self, dt, nsteps):
+        self._c(lib().mxm_dg_step_n(self.h, dt, nsteps))
+
+    def rk_stage(self, stage, dt):
+        self._c(lib().mxm_dg_rk_stage(self.h, stage, dt))
+
+    def limit(self, which=0):
+        self._c(lib().mxm_dg_limit(self.h, which))
+
+    def rhs(self, q):
+        """Semi-discrete RHS L(q) of a host array (uses q1 as scratch, q2 as output)."""
+        self.upload_state(q, 1)
+        self._c(lib().mxm_dg_eval_rhs(self.h, self.state_ptr(1), self.state_ptr(2)))
+        return self.download_state(2)
+
+    def advance_host(self, q_host, nsteps, dt, out=None):
+        a = np.ascontiguousarray(q_host, dtype=self.dtype)
+        out = np.empty_like(a) if out is None else out
+        self._c(lib().mxm_dg_advance_host(self.h, a.ctypes.data, out.ctypes.data, nsteps, dt))
+        return out
+
+    def synchronize(self):
+        self._c(lib().mxm_dg_synchronize(self.h))
+
+    # -- diagnostics
+    def max_wavespeed(self):
+        v = ctypes.c_double()
+        self._c(lib().mxm_dg_max_wavespeed(self.h, ctypes.byref(v)))
+        return v.value
+
+    def integral(self, c, which=0, kind=0):
+        v = ctypes.c_double()
+        self._c(lib().mxm_dg_reduce_conserved(self.h, which, c, kind, ctypes.byref(v)))
+        return v.value
+
+    def dof_count(self):  # solver.mojo:757-763
+        v = ctypes.c_int64()
+        self._c(lib().mxm_dg_dof_count(self.h, ctypes.byref(v)))
+        return v.value
+
+    def state_bytes_per_step(self):  # solver.mojo:804-824
+        v = ctypes.c_int64()
+        self._c(lib().mxm_dg_state_bytes_per_step(self.h, ctypes.byref(v)))
+        return v.value
+
+    def launches_per_step(self):
+        v = ctypes.c_int32()
+        self._c(lib().mxm_dg_launches_per_step(self.h, ctypes.byref(v)))
+        return v.value
+
+    def time_steps(self, dt, nsteps):
+        ms = ctypes.c_double()
+        self._c(lib().mxm_dg_time_steps(self.h, dt, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def bench_step_loop(self, dt, warmup_steps=5, measure_steps=50):
+        """solver.mojo:765-802: warm up, then time `measure_steps` steps (CUDA events)."""
+        self.step_n(dt, warmup_steps)
+        self.synchronize()
+        ms = self.time_steps(dt, measure_steps)
+        dof = self.dof_count()
+        return dict(steps=measure_steps, seconds=ms * 1e-3, dof_per_step=dof,
+                    dof_stage_per_s=3 * dof * measure_steps / (ms * 1e-3),
+                    state_gbs=self.state_bytes_per_step() * measure_steps / (ms * 1e-3) / 1e9)
+
+    def operator(self):
+        n = ctypes.c_int64(0)
+        self._c(lib().mxm_dg_operator(self.h, None, ctypes.byref(n)))
+        out = np.zeros(n.value)
+        self._c(lib().mxm_dg_operator(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(n)))
+        return out
+
+
+def reference_operators(dim, P):
+    """Host FP64 operators the library builds: D [dim,NP,NP], Lift [nf,NP,NFP] (reference face order), w [NP]."""
+    NP = (P + 1) * (P + 2) * (P + 3) // 6 if dim == 3 else (P + 1) * (P + 2) // 2
+    NFP = (P + 1) * (P + 2) // 2 if dim == 3 else P + 1
+    nf = dim + 1
+    D = np.zeros(dim * NP * NP)
+    Lf = np.zeros(nf * NP * NFP)
+    w = np.zeros(NP)
+    dp = ctypes.POINTER(ctypes.c_double)
+    _check(lib().mxm_dg_reference_operators(dim, P, D.ctypes.data_as(dp), Lf.ctypes.data_as(dp), w.ctypes.data_as(dp)))
+    return D.reshape(dim, NP, NP), Lf.reshape(nf, NP, NFP), w

@@ -1,0 +1,83 @@
+"""Build libmxm_dg.so in place (sm_100a) from mojoxm_b200/csrc.
+
+Every translation unit is compiled by nvcc for `-gencode
+arch=compute_100a,code=sm_100a` into mojoxm_b200/_build/, in parallel, and
+linked with the static CUDA runtime into mojoxm_b200/libmxm_dg.so.  A unit is
+rebuilt when it or any header in csrc/ or include/ is newer than its object.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libmxm_dg.so")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+              "-I" + os.path.join(ROOT, "include")]
+
+
+def _nvcc() -> str:
+    for c in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def _headers_mtime() -> float:
+    hs = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) + \
+        glob.glob(os.path.join(ROOT, "include", "*.h"))
+    return max(os.path.getmtime(h) for h in hs)
+
+
+def _compile(src: str, obj: str, verbose: bool) -> str:
+    if src.endswith(".cpp"):  # host-only units (binary128 operator construction) go to the host compiler
+        cmd = [shutil.which("g++") or "g++", "-O2", "-std=c++17", "-fPIC", "-I" + os.path.join(ROOT, "include"),
+               "-c", src, "-o", obj]
+    else:
+        cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-c", src, "-o", obj]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {os.path.basename(src)}:\n{r.stderr[-6000:]}")
+    return r.stderr
+
+
+def build(verbose: bool = False, jobs: int | None = None) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
+    hdr = _headers_mtime()
+    todo, objs = [], []
+    for s in srcs:
+        o = os.path.join(BUILD, os.path.basename(s) + ".o")
+        objs.append(o)
+        if not os.path.exists(o) or os.path.getmtime(o) < max(hdr, os.path.getmtime(s)):
+            todo.append((s, o))
+    if todo:
+        jobs = jobs or min(len(todo), os.cpu_count() or 4)
+        with cf.ThreadPoolExecutor(jobs) as ex:
+            futs = {ex.submit(_compile, s, o, verbose): s for s, o in todo}
+            for f in cf.as_completed(futs):
+                log = f.result()
+                if verbose and log:
+                    sys.stderr.write(log)
+    if todo or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+        tmp = LIB + ".tmp"
+        cmd = [_nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n" + r.stderr[-4000:])
+        os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

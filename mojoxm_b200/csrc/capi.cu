@@ -1,0 +1,870 @@
+// C ABI of the B200 DG library (include/mxm_dg.h): host-side Solver that owns
+// device state, operators and scratch, and dispatches the sm_100a kernels.
+// Mirrors the reference's Solver[PhysT, P] (src/solver.mojo:538-1092) and
+// the 2D stage helpers (src/local_mesh_2d_gpu_*.mojo, src/ssprk3.mojo:56-78).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/mxm_dg.h"
+#include "dg_common.cuh"
+#include "physics.cuh"
+#include "physics2d.cuh"
+#include "refops.hpp"
+
+namespace mxm {
+
+struct CudaError : std::exception {
+  cudaError_t e;
+  std::string msg;
+  CudaError(cudaError_t e_, const char* where) : e(e_), msg(std::string(where) + ": " + cudaGetErrorString(e_)) {}
+  const char* what() const noexcept override { return msg.c_str(); }
+};
+struct ArgError : std::exception {
+  std::string msg;
+  explicit ArgError(std::string m) : msg(std::move(m)) {}
+  const char* what() const noexcept override { return msg.c_str(); }
+};
+#define CK(x)                                            \
+  do {                                                   \
+    cudaError_t _e = (x);                                \
+    if (_e != cudaSuccess) throw ::mxm::CudaError(_e, #x); \
+  } while (0)
+
+struct Handle {
+  int dim = 3, P = 1, prec = MXM_DG_PREC_F64, NP = 0, NFP = 0, NC = 0, ntypes = 6, K = 0;
+  mxm_dg_physics_desc phys{};
+  int nx = 1, ny = 1, nz = 1;
+  double lx = 1, ly = 1, lz = 1;
+  int bc[6] = {0, 0, 0, 0, 0, 0};
+  int64_t ncell = 0, ne = 0;
+  size_t rbytes = 8;
+  int device = 0, nsm = 148;
+  cudaStream_t stream = nullptr;
+  void* q[3] = {nullptr, nullptr, nullptr};
+  void* A = nullptr;
+  void* w = nullptr;
+  void* avg = nullptr;
+  float* xyz = nullptr;
+  double* partial = nullptr;
+  double* dscalar = nullptr;
+  unsigned long long* uscalar = nullptr;
+  int npartial = 1024;
+  bool lim_on = false;
+  double lim_eps = 0.1;
+  RefOps ref;
+  Kuhn3D k3;
+  Kuhn2D k2;
+  std::vector<double> Ahost;
+  KuhnTab3<double> t3d{};
+  KuhnTab3<float> t3f{};
+  KuhnTab2<double> t2d{};
+  KuhnTab2<float> t2f{};
+  std::string err;
+  size_t qcount() const { return size_t(ne) * NP * NC; }
+  size_t qbytes() const { return qcount() * rbytes; }
+};
+
+static std::mutex g_err_mu;
+static std::string g_create_err;
+
+template <class R>
+KuhnTab3<R>& tab3(Handle* h);
+template <>
+KuhnTab3<double>& tab3<double>(Handle* h) { return h->t3d; }
+template <>
+KuhnTab3<float>& tab3<float>(Handle* h) { return h->t3f; }
+template <class R>
+KuhnTab2<R>& tab2(Handle* h);
+template <>
+KuhnTab2<double>& tab2<double>(Handle* h) { return h->t2d; }
+template <>
+KuhnTab2<float>& tab2<float>(Handle* h) { return h->t2f; }
+
+template <class R>
+void fill_tab3(Handle* h, KuhnTab3<R>& t) {
+  const Kuhn3D& k = h->k3;
+  std::memset(&t, 0, sizeof(t));
+  for (int a = 0; a < 6; ++a)
+    for (int lf = 0; lf < 4; ++lf) {
+      t.nb_t[a][lf] = int8_t(k.nb_t[a][lf]);
+      for (int d = 0; d < 3; ++d) t.off[a][lf][d] = int8_t(k.off[a][lf][d]);
+      t.side[a][lf] = int8_t(k.side[a][lf]);
+      t.axis[a][lf] = int8_t(k.axis[a][lf]);
+      t.dir[a][lf] = int8_t(k.dir[a][lf]);
+      for (int d = 0; d < 3; ++d) t.normal[a][lf][d] = R(k.normal[a][lf][d]);
+      for (int m = 0; m < h->NFP; ++m) t.nb_node[a][lf][m] = uint8_t(k.nb_node[(a * 4 + lf) * h->NFP + m]);
+    }
+  for (int lf = 0; lf < 4; ++lf)
+    for (int m = 0; m < h->NFP; ++m) t.own_node[lf][m] = uint8_t(h->ref.face_nodes[lf * h->NFP + m]);
+}
+
+template <class R>
+void fill_tab2(Handle* h, KuhnTab2<R>& t) {
+  const Kuhn2D& k = h->k2;
+  std::memset(&t, 0, sizeof(t));
+  for (int a = 0; a < 2; ++a)
+    for (int lf = 0; lf < 3; ++lf) {
+      t.nb_t[a][lf] = int8_t(k.nb_t[a][lf]);
+      for (int d = 0; d < 2; ++d) t.off[a][lf][d] = int8_t(k.off[a][lf][d]);
+      t.side[a][lf] = int8_t(k.side[a][lf]);
+      t.axis[a][lf] = int8_t(k.axis[a][lf]);
+      t.dir[a][lf] = int8_t(k.dir[a][lf]);
+      for (int d = 0; d < 2; ++d) t.normal[a][lf][d] = R(k.normal[a][lf][d]);
+      for (int m = 0; m < h->NFP; ++m) t.nb_node[a][lf][m] = uint8_t(k.nb_node[(a * 3 + lf) * h->NFP + m]);
+    }
+  for (int lf = 0; lf < 3; ++lf)
+    for (int m = 0; m < h->NFP; ++m) t.own_node[lf][m] = uint8_t(h->ref.face_nodes[((lf + 2) % 3) * h->NFP + m]);
+}
+
+// ---------------------------------------------------------------- dispatch
+template <class R>
+cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double a, double b,
+                         double c, double dt, int rhs_only) {
+  const double* p = h->phys.p;
+  const R cdt = R(c) * R(dt);
+  if (h->dim == 3) {
+    Stage3DArgs<R> ar;
+    ar.q_in = (const R*)qi;
+    ar.q_a = (const R*)qa;
+    ar.q_b = (const R*)qb;
+    ar.q_out = (R*)qo;
+    ar.A = (const R*)h->A;
+    ar.a = R(a);
+    ar.b = R(b);
+    ar.cdt = cdt;
+    ar.nx = h->nx;
+    ar.ny = h->ny;
+    ar.nz = h->nz;
+    ar.ncell = int(h->ncell);
+    for (int k = 0; k < 6; ++k) ar.bc[k] = h->bc[k];
+    ar.rhs_only = rhs_only;
+    const KuhnTab3<R>& t = tab3<R>(h);
+    switch (h->phys.kind) {
+      case MXM_DG_PHYS_ADVECTION: {
+        AdvectionD<R> ph{R(p[0]), R(p[1]), R(p[2]), R(p[3])};
+        return launch_stage3d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+      }
+      case MXM_DG_PHYS_EULER: {
+        auto mk = [&](auto ph) {
+          ph.gamma = R(p[0]); ph.rho_min = R(p[1]); ph.p_min = R(p[2]);
+          ph.gx = R(p[3]); ph.gy = R(p[4]); ph.gz = R(p[5]);
+          for (int k = 0; k < 5; ++k) ph.inflow[k] = R(p[6 + k]);
+          ph.entropy_fix = h->phys.entropy_fix;
+          return launch_stage3d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+        };
+        switch (h->phys.flux_type) {
+          case MXM_DG_FLUX_RUSANOV: return mk(EulerD<R, FLUX_RUSANOV>{});
+          case MXM_DG_FLUX_ROE: return mk(EulerD<R, FLUX_ROE>{});
+          case MXM_DG_FLUX_HLLE: return mk(EulerD<R, FLUX_HLLE>{});
+          case MXM_DG_FLUX_HLLEC: return mk(EulerD<R, FLUX_HLLEC>{});
+        }
+        return cudaErrorInvalidValue;
+      }
+      case MXM_DG_PHYS_MAXWELL: {
+        MaxwellD<R> ph;
+        ph.c = R(p[0]);
+        for (int k = 0; k < 3; ++k) { ph.J[k] = R(p[1 + k]); ph.M[k] = R(p[4 + k]); }
+        for (int k = 0; k < 6; ++k) ph.inflow[k] = R(p[7 + k]);
+        return launch_stage3d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+      }
+      case MXM_DG_PHYS_SHALLOW_WATER: {
+        ShallowWaterD<R> ph;
+        ph.g = R(p[0]); ph.h_min = R(p[1]);
+        for (int k = 0; k < 3; ++k) ph.inflow[k] = R(p[2 + k]);
+        return launch_stage3d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+      }
+    }
+    return cudaErrorInvalidValue;
+  }
+  Stage2DArgs<R> ar;
+  ar.q_in = (const R*)qi;
+  ar.q_a = (const R*)qa;
+  ar.q_b = (const R*)qb;
+  ar.q_out = (R*)qo;
+  ar.A = (const R*)h->A;
+  ar.a = R(a);
+  ar.b = R(b);
+  ar.cdt = cdt;
+  ar.nx = h->nx;
+  ar.ny = h->ny;
+  ar.ncell = int(h->ncell);
+  for (int k = 0; k < 4; ++k) ar.bc[k] = h->bc[k];
+  ar.rhs_only = rhs_only;
+  const KuhnTab2<R>& t = tab2<R>(h);
+  switch (h->phys.kind) {
+    case MXM_DG_PHYS_ADVECTION: {
+      Advection2D<R> ph{R(p[0]), R(p[1]), R(p[3])};
+      return launch_stage2d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+    }
+    case MXM_DG_PHYS_EULER: {
+      auto mk = [&](auto ph) {
+        ph.gamma = R(p[0]); ph.rho_min = R(p[1]); ph.p_min = R(p[2]);
+        ph.gx = R(p[3]); ph.gy = R(p[4]);
+        ph.inflow[0] = R(p[6]); ph.inflow[1] = R(p[7]); ph.inflow[2] = R(p[8]); ph.inflow[3] = R(p[10]);
+        ph.entropy_fix = h->phys.entropy_fix;
+        return launch_stage2d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+      };
+      switch (h->phys.flux_type) {
+        case MXM_DG_FLUX_RUSANOV: return mk(Euler2D<R, FLUX_RUSANOV>{});
+        case MXM_DG_FLUX_HLLC: return mk(Euler2D<R, FLUX_HLLC>{});
+        case MXM_DG_FLUX_HLLE: return mk(Euler2D<R, FLUX_HLLE>{});
+      }
+      return cudaErrorInvalidValue;
+    }
+    case MXM_DG_PHYS_SHALLOW_WATER: {
+      auto mk = [&](auto ph) {
+        ph.g = R(p[0]); ph.h_min = R(p[1]);
+        for (int k = 0; k < 3; ++k) ph.inflow[k] = R(p[2 + k]);
+        return launch_stage2d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+      };
+      if (h->phys.flux_type == MXM_DG_FLUX_HLL) return mk(ShallowWater2D<R, FLUX_HLL>{});
+      return mk(ShallowWater2D<R, FLUX_RUSANOV>{});
+    }
+    case MXM_DG_PHYS_MAXWELL: {
+      Maxwell2D<R> ph;
+      ph.c = R(p[0]);
+      for (int k = 0; k < 3; ++k) { ph.J[k] = R(p[1 + k]); ph.M[k] = R(p[4 + k]); }
+      for (int k = 0; k < 6; ++k) ph.inflow[k] = R(p[7 + k]);
+      return launch_stage2d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class R>
+cudaError_t wavespeed_launch(Handle* h, const void* qi, unsigned long long* out) {
+  const double* p = h->phys.p;
+  if (h->dim == 3) {
+    Stage3DArgs<R> ar{};
+    ar.q_in = (const R*)qi;
+    ar.nx = h->nx;
+    ar.ny = h->ny;
+    ar.nz = h->nz;
+    ar.ncell = int(h->ncell);
+    for (int k = 0; k < 6; ++k) ar.bc[k] = h->bc[k];
+    const KuhnTab3<R>& t = tab3<R>(h);
+    switch (h->phys.kind) {
+      case MXM_DG_PHYS_ADVECTION: {
+        AdvectionD<R> ph{R(p[0]), R(p[1]), R(p[2]), R(p[3])};
+        return launch_wavespeed3d<R>(h->P, ar, t, ph, out, h->stream);
+      }
+      case MXM_DG_PHYS_EULER: {
+        auto mk = [&](auto ph) {
+          ph.gamma = R(p[0]); ph.rho_min = R(p[1]); ph.p_min = R(p[2]);
+          ph.gx = R(p[3]); ph.gy = R(p[4]); ph.gz = R(p[5]);
+          for (int k = 0; k < 5; ++k) ph.inflow[k] = R(p[6 + k]);
+          ph.entropy_fix = h->phys.entropy_fix;
+          return launch_wavespeed3d<R>(h->P, ar, t, ph, out, h->stream);
+        };
+        switch (h->phys.flux_type) {
+          case MXM_DG_FLUX_RUSANOV: return mk(EulerD<R, FLUX_RUSANOV>{});
+          case MXM_DG_FLUX_ROE: return mk(EulerD<R, FLUX_ROE>{});
+          case MXM_DG_FLUX_HLLE: return mk(EulerD<R, FLUX_HLLE>{});
+          case MXM_DG_FLUX_HLLEC: return mk(EulerD<R, FLUX_HLLEC>{});
+        }
+        return cudaErrorInvalidValue;
+      }
+      case MXM_DG_PHYS_MAXWELL: {
+        MaxwellD<R> ph;
+        ph.c = R(p[0]);
+        for (int k = 0; k < 3; ++k) { ph.J[k] = R(p[1 + k]); ph.M[k] = R(p[4 + k]); }
+        for (int k = 0; k < 6; ++k) ph.inflow[k] = R(p[7 + k]);
+        return launch_wavespeed3d<R>(h->P, ar, t, ph, out, h->stream);
+      }
+      case MXM_DG_PHYS_SHALLOW_WATER: {
+        ShallowWaterD<R> ph;
+        ph.g = R(p[0]); ph.h_min = R(p[1]);
+        for (int k = 0; k < 3; ++k) ph.inflow[k] = R(p[2 + k]);
+        return launch_wavespeed3d<R>(h->P, ar, t, ph, out, h->stream);
+      }
+    }
+    return cudaErrorInvalidValue;
+  }
+  const int64_t nn = h->ne * h->NP;
+  switch (h->phys.kind) {
+    case MXM_DG_PHYS_ADVECTION: {
+      Advection2D<R> ph{R(p[0]), R(p[1]), R(p[3])};
+      return launch_wavespeed2d<R>((const R*)qi, nn, ph, out, h->stream);
+    }
+    case MXM_DG_PHYS_EULER: {
+      Euler2D<R, FLUX_RUSANOV> ph{};
+      ph.gamma = R(p[0]); ph.rho_min = R(p[1]); ph.p_min = R(p[2]);
+      return launch_wavespeed2d<R>((const R*)qi, nn, ph, out, h->stream);
+    }
+    case MXM_DG_PHYS_SHALLOW_WATER: {
+      ShallowWater2D<R, FLUX_RUSANOV> ph{};
+      ph.g = R(p[0]); ph.h_min = R(p[1]);
+      return launch_wavespeed2d<R>((const R*)qi, nn, ph, out, h->stream);
+    }
+    case MXM_DG_PHYS_MAXWELL: {
+      Maxwell2D<R> ph{};
+      ph.c = R(p[0]);
+      return launch_wavespeed2d<R>((const R*)qi, nn, ph, out, h->stream);
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
+void stage(Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double a, double b, double c, double dt,
+           int rhs_only) {
+  cudaError_t e = h->rbytes == 8 ? stage_launch<double>(h, qi, qa, qb, qo, a, b, c, dt, rhs_only)
+                                 : stage_launch<float>(h, qi, qa, qb, qo, a, b, c, dt, rhs_only);
+  if (e != cudaSuccess) throw CudaError(e, "stage kernel launch");
+}
+
+void limit_buf(Handle* h, void* qv) {
+  cudaError_t e;
+  if (h->rbytes == 8) {
+    LimArgs<double> a;
+    a.q = (double*)qv;
+    a.avg = (double*)h->avg;
+    a.w = (const double*)h->w;
+    a.ne = h->ne;
+    a.nx = h->nx; a.ny = h->ny; a.nz = h->dim == 3 ? h->nz : 1;
+    for (int k = 0; k < 6; ++k) a.bc[k] = h->bc[k];
+    a.eps2 = h->lim_eps * h->lim_eps;
+    e = launch_limiter<double>(h->dim, h->P, h->NC, a, h->t3d, h->t2d, h->stream);
+  } else {
+    LimArgs<float> a;
+    a.q = (float*)qv;
+    a.avg = (float*)h->avg;
+    a.w = (const float*)h->w;
+    a.ne = h->ne;
+    a.nx = h->nx; a.ny = h->ny; a.nz = h->dim == 3 ? h->nz : 1;
+    for (int k = 0; k < 6; ++k) a.bc[k] = h->bc[k];
+    const float ef = float(h->lim_eps);  // reference: venkat_eps Float32, eps2 = eps*eps in Float32
+    a.eps2 = ef * ef;
+    e = launch_limiter<float>(h->dim, h->P, h->NC, a, h->t3f, h->t2f, h->stream);
+  }
+  if (e != cudaSuccess) throw CudaError(e, "limiter launch");
+}
+
+// Shu-Osher stage s of SSPRK3 (solver.mojo:1071-1092; ssprk3.mojo:56-78).
+void rk_stage(Handle* h, int s, double dt) {
+  void *q0 = h->q[0], *q1 = h->q[1], *q2 = h->q[2];
+  if (s == 0) stage(h, q0, q0, q0, q1, 1.0, 0.0, 1.0, dt, 0);
+  else if (s == 1) stage(h, q1, q0, q1, q2, 0.75, 0.25, 0.25, dt, 0);
+  else stage(h, q2, q0, q2, q0, 1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0, dt, 0);
+  if (h->lim_on) limit_buf(h, s == 0 ? q1 : (s == 1 ? q2 : q0));
+}
+
+void step_n(Handle* h, double dt, int n) {
+  for (int k = 0; k < n; ++k)
+    for (int s = 0; s < 3; ++s) rk_stage(h, s, dt);
+}
+
+// Float32 node coordinates exactly as the reference builds elem_node_xyz.
+void build_xyz(Handle* h) {
+  std::vector<float> x(size_t(h->ne) * h->NP * h->dim);
+  if (h->dim == 3) {
+    // local_mesh.mojo:568-580 (rel coords in Float32) and :814-827
+    const float dx = float(h->lx / h->nx), dy = float(h->ly / h->ny), dz = float(h->lz / h->nz);
+    const float Pf = float(h->P);
+    std::vector<float> rel(6 * h->NP * 3);
+    for (int t = 0; t < 6; ++t)
+      for (int n = 0; n < h->NP; ++n)
+        for (int d = 0; d < 3; ++d) {
+          float s = 0.0f;
+          for (int v = 0; v < 4; ++v) s = s + (float(h->ref.nodes[n].a[v]) / Pf) * float(h->k3.vert[t][v][d]);
+          rel[(t * h->NP + n) * 3 + d] = s;
+        }
+    for (int64_t e = 0; e < h->ne; ++e) {
+      const int t = int(e % 6);
+      const int64_t cell = e / 6;
+      const int k = int(cell / (int64_t(h->nx) * h->ny));
+      const int64_t rem = cell - int64_t(k) * h->nx * h->ny;
+      const int j = int(rem / h->nx), i = int(rem - int64_t(j) * h->nx);
+      const float o[3] = {float(i) * dx, float(j) * dy, float(k) * dz}, hh[3] = {dx, dy, dz};
+      for (int n = 0; n < h->NP; ++n)
+        for (int d = 0; d < 3; ++d) x[(e * h->NP + n) * 3 + d] = o[d] + rel[(t * h->NP + n) * 3 + d] * hh[d];
+    }
+  } else {
+    // local_mesh_2d.mojo:125-180: FP64 on the host, uploaded as Float32
+    const double dx = h->lx / h->nx, dy = h->ly / h->ny;
+    for (int64_t e = 0; e < h->ne; ++e) {
+      const int t = int(e % 2);
+      const int64_t cell = e / 2;
+      const int j = int(cell / h->nx), i = int(cell - int64_t(j) * h->nx);
+      const double bx = i * dx, by = j * dy;
+      double v[3][2];
+      for (int a = 0; a < 3; ++a) {
+        v[a][0] = bx + h->k2.vert[t][a][0] * dx;
+        v[a][1] = by + h->k2.vert[t][a][1] * dy;
+      }
+      for (int n = 0; n < h->NP; ++n) {
+        const double r = double(h->ref.nodes[n].a[1]) / h->P, s = double(h->ref.nodes[n].a[2]) / h->P;
+        const double l0 = 1.0 - r - s;
+        x[(e * h->NP + n) * 2 + 0] = float(l0 * v[0][0] + r * v[1][0] + s * v[2][0]);
+        x[(e * h->NP + n) * 2 + 1] = float(l0 * v[0][1] + r * v[1][1] + s * v[2][1]);
+      }
+    }
+  }
+  CK(cudaMalloc(&h->xyz, x.size() * sizeof(float)));
+  CK(cudaMemcpy(h->xyz, x.data(), x.size() * sizeof(float), cudaMemcpyHostToDevice));
+}
+
+void destroy(Handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (auto& b : h->q) cudaFree(b);
+  cudaFree(h->A);
+  cudaFree(h->w);
+  cudaFree(h->avg);
+  cudaFree(h->xyz);
+  cudaFree(h->partial);
+  cudaFree(h->dscalar);
+  cudaFree(h->uscalar);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, int prec) {
+  if (!m || !ph) throw ArgError("null descriptor");
+  if (m->dim != 2 && m->dim != 3) throw ArgError("mesh dim must be 2 or 3");
+  if (P < 1 || P > 5) throw ArgError("order P must be in 1..5");
+  if (prec != MXM_DG_PREC_F64 && prec != MXM_DG_PREC_F32)
+    throw ArgError("precision must be MXM_DG_PREC_F64 or MXM_DG_PREC_F32 for a single-solve handle");
+  if (ph->kind < 0 || ph->kind > 3) throw ArgError("unknown physics kind");
+  if (m->nx < 1 || m->ny < 1 || (m->dim == 3 && m->nz < 1)) throw ArgError("cell counts must be >= 1");
+  for (int k = 0; k < 2 * m->dim; ++k)
+    if (m->bc[k] < 0 || m->bc[k] > 3) throw ArgError("bc codes must be 0..3");
+  if (ph->kind == MXM_DG_PHYS_EULER) {
+    const int f = ph->flux_type;
+    const bool ok = m->dim == 3 ? (f >= 0 && f <= 3) : (f == MXM_DG_FLUX_RUSANOV || f == MXM_DG_FLUX_HLLC || f == MXM_DG_FLUX_HLLE);
+    if (!ok) throw ArgError(m->dim == 3 ? "3D Euler flux must be RUSANOV, ROE, HLLE or HLLEC" : "2D Euler flux must be RUSANOV, HLLC or HLLE");
+  }
+  if (m->dim == 2 && ph->kind == MXM_DG_PHYS_SHALLOW_WATER && ph->flux_type != MXM_DG_FLUX_RUSANOV &&
+      ph->flux_type != MXM_DG_FLUX_HLL)
+    throw ArgError("2D shallow-water flux must be RUSANOV or HLL");
+  std::unique_ptr<Handle> h(new Handle);
+  h->dim = m->dim;
+  h->P = P;
+  h->prec = prec;
+  h->phys = *ph;
+  h->nx = m->nx;
+  h->ny = m->ny;
+  h->nz = m->dim == 3 ? m->nz : 1;
+  h->lx = m->lx;
+  h->ly = m->ly;
+  h->lz = m->lz;
+  for (int k = 0; k < 2 * m->dim; ++k) h->bc[k] = m->bc[k];
+  h->NC = ph->kind == MXM_DG_PHYS_ADVECTION ? 1
+        : ph->kind == MXM_DG_PHYS_EULER     ? (m->dim == 3 ? 5 : 4)
+        : ph->kind == MXM_DG_PHYS_MAXWELL   ? 6
+                                            : 3;
+  h->ntypes = m->dim == 3 ? 6 : 2;
+  h->ncell = int64_t(h->nx) * h->ny * h->nz;
+  h->ne = h->ncell * h->ntypes;
+  if (h->ne > (int64_t(1) << 31) / 64) throw ArgError("mesh too large for 32-bit cell indexing");
+  h->rbytes = prec == MXM_DG_PREC_F64 ? 8 : 4;
+  h->ref = build_refops(h->dim, P);
+  h->NP = h->ref.NP;
+  h->NFP = h->ref.NFP;
+  if (h->dim == 3) {
+    h->k3 = build_kuhn3d(h->ref, h->lx / h->nx, h->ly / h->ny, h->lz / h->nz);
+    h->Ahost = fused_operator_3d(h->ref, h->k3);
+    h->K = 3 * h->NP + 4 * h->NFP;
+    fill_tab3<double>(h.get(), h->t3d);
+    fill_tab3<float>(h.get(), h->t3f);
+  } else {
+    h->k2 = build_kuhn2d(h->ref, h->lx / h->nx, h->ly / h->ny);
+    h->Ahost = fused_operator_2d(h->ref, h->k2);
+    h->K = 2 * h->NP + 3 * h->NFP;
+    fill_tab2<double>(h.get(), h->t2d);
+    fill_tab2<float>(h.get(), h->t2f);
+  }
+  CK(cudaGetDevice(&h->device));
+  CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
+  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  Handle* raw = h.get();
+  try {
+    for (auto& b : raw->q) {
+      cudaError_t e = cudaMalloc(&b, raw->qbytes());
+      if (e != cudaSuccess) throw CudaError(e, "cudaMalloc(state)");
+      CK(cudaMemsetAsync(b, 0, raw->qbytes(), raw->stream));
+    }
+    // fused operators, k-major per type, in the handle's real type
+    std::vector<double> At(size_t(raw->ntypes) * raw->K * raw->NP);
+    for (int t = 0; t < raw->ntypes; ++t)
+      for (int i = 0; i < raw->NP; ++i)
+        for (int k = 0; k < raw->K; ++k)
+          At[(size_t(t) * raw->K + k) * raw->NP + i] = raw->Ahost[(size_t(t) * raw->NP + i) * raw->K + k];
+    auto upload = [&](void** dst, const std::vector<double>& src) {
+      CK(cudaMalloc(dst, src.size() * raw->rbytes));
+      if (raw->rbytes == 8) {
+        CK(cudaMemcpy(*dst, src.data(), src.size() * 8, cudaMemcpyHostToDevice));
+      } else {
+        std::vector<float> f(src.begin(), src.end());
+        CK(cudaMemcpy(*dst, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+      }
+    };
+    upload(&raw->A, At);
+    upload(&raw->w, raw->ref.w);
+    CK(cudaMalloc(&raw->avg, size_t(raw->ne) * raw->NC * raw->rbytes));
+    CK(cudaMalloc(&raw->partial, raw->npartial * sizeof(double)));
+    CK(cudaMalloc(&raw->dscalar, 4 * sizeof(double)));
+    CK(cudaMalloc(&raw->uscalar, 4 * sizeof(unsigned long long)));
+    CK(cudaStreamSynchronize(raw->stream));
+  } catch (...) {
+    h.release();
+    destroy(raw);
+    throw;
+  }
+  return h.release();
+}
+
+}  // namespace mxm
+
+using mxm::Handle;
+
+#define API_BEGIN                      \
+  Handle* h = (Handle*)handle;         \
+  if (!h) return MXM_DG_EINVAL;        \
+  try {                                \
+    cudaSetDevice(h->device);
+#define API_END                                         \
+  return MXM_DG_OK;                                     \
+  }                                                     \
+  catch (mxm::CudaError & ex) {                         \
+    h->err = ex.what();                                 \
+    return ex.e == cudaErrorMemoryAllocation ? MXM_DG_ENOMEM : MXM_DG_ECUDA; \
+  }                                                     \
+  catch (mxm::ArgError & ex) {                          \
+    h->err = ex.what();                                 \
+    return MXM_DG_EINVAL;                               \
+  }                                                     \
+  catch (std::exception & ex) {                         \
+    h->err = ex.what();                                 \
+    return MXM_DG_EINVAL;                               \
+  }
+
+extern "C" {
+
+int mxm_dg_version(void) { return MXM_DG_VERSION; }
+
+int mxm_dg_create(const mxm_dg_mesh_desc* mesh, const mxm_dg_physics_desc* phys, int P, int precision, void** out) {
+  if (!out) return MXM_DG_EINVAL;
+  *out = nullptr;
+  try {
+    *out = mxm::create(mesh, phys, P, precision);
+    return MXM_DG_OK;
+  } catch (mxm::CudaError& ex) {
+    std::lock_guard<std::mutex> g(mxm::g_err_mu);
+    mxm::g_create_err = ex.what();
+    return ex.e == cudaErrorMemoryAllocation ? MXM_DG_ENOMEM : MXM_DG_ECUDA;
+  } catch (std::exception& ex) {
+    std::lock_guard<std::mutex> g(mxm::g_err_mu);
+    mxm::g_create_err = ex.what();
+    return MXM_DG_EINVAL;
+  }
+}
+
+int mxm_dg_destroy(void* handle) {
+  mxm::destroy((Handle*)handle);
+  return MXM_DG_OK;
+}
+
+int mxm_dg_sizes(void* handle, int64_t* ne, int32_t* np, int32_t* nfp, int32_t* nc, int32_t* rb) {
+  API_BEGIN
+  if (ne) *ne = h->ne;
+  if (np) *np = h->NP;
+  if (nfp) *nfp = h->NFP;
+  if (nc) *nc = h->NC;
+  if (rb) *rb = int32_t(h->rbytes);
+  API_END
+}
+
+int mxm_dg_dof_count(void* handle, int64_t* dof) {
+  API_BEGIN
+  *dof = h->ne * h->NP * h->NC;
+  API_END
+}
+
+int mxm_dg_state_bytes_per_step(void* handle, int64_t* bytes) {
+  API_BEGIN
+  *bytes = int64_t(8) * int64_t(h->qbytes());
+  API_END
+}
+
+int mxm_dg_state_ptr(void* handle, int which, void** dptr) {
+  API_BEGIN
+  if (which < 0 || which > 2 || !dptr) throw mxm::ArgError("which must be 0, 1 or 2");
+  *dptr = h->q[which];
+  API_END
+}
+
+int mxm_dg_node_xyz_ptr(void* handle, void** dptr) {
+  API_BEGIN
+  if (!h->xyz) mxm::build_xyz(h);
+  *dptr = h->xyz;
+  API_END
+}
+
+int mxm_dg_node_xyz(void* handle, double* out) {
+  API_BEGIN
+  const int dim = h->dim, NP = h->NP;
+  if (dim == 3) {
+    const double hh[3] = {h->lx / h->nx, h->ly / h->ny, h->lz / h->nz};
+    for (int64_t e = 0; e < h->ne; ++e) {
+      const int t = int(e % 6);
+      const int64_t cell = e / 6;
+      const int k = int(cell / (int64_t(h->nx) * h->ny));
+      const int64_t rem = cell - int64_t(k) * h->nx * h->ny;
+      const int j = int(rem / h->nx), i = int(rem - int64_t(j) * h->nx);
+      const int c[3] = {i, j, k};
+      for (int n = 0; n < NP; ++n)
+        for (int d = 0; d < 3; ++d) out[(e * NP + n) * 3 + d] = (c[d] + h->k3.rel_xyz[(t * NP + n) * 3 + d]) * hh[d];
+    }
+  } else {
+    const double hh[2] = {h->lx / h->nx, h->ly / h->ny};
+    for (int64_t e = 0; e < h->ne; ++e) {
+      const int t = int(e % 2);
+      const int64_t cell = e / 2;
+      const int j = int(cell / h->nx), i = int(cell - int64_t(j) * h->nx);
+      const int c[2] = {i, j};
+      for (int n = 0; n < NP; ++n)
+        for (int d = 0; d < 2; ++d) out[(e * NP + n) * 2 + d] = (c[d] + h->k2.rel_xy[(t * NP + n) * 2 + d]) * hh[d];
+    }
+  }
+  API_END
+}
+
+int mxm_dg_upload_state(void* handle, int which, const void* host, size_t nbytes) {
+  API_BEGIN
+  if (which < 0 || which > 2 || !host) throw mxm::ArgError("which must be 0..2 and host non-null");
+  if (nbytes != h->qbytes()) throw mxm::ArgError("nbytes must equal Ne*NP*NC*real_bytes");
+  CK(cudaMemcpyAsync(h->q[which], host, nbytes, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  API_END
+}
+
+int mxm_dg_download_state(void* handle, int which, void* host, size_t nbytes) {
+  API_BEGIN
+  if (which < 0 || which > 2 || !host) throw mxm::ArgError("which must be 0..2 and host non-null");
+  if (nbytes != h->qbytes()) throw mxm::ArgError("nbytes must equal Ne*NP*NC*real_bytes");
+  CK(cudaMemcpyAsync(host, h->q[which], nbytes, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  API_END
+}
+
+static void download_component(Handle* h, int c, float* f32, double* f64) {
+  if (c < 0 || c >= h->NC) throw mxm::ArgError("component out of range");
+  std::vector<unsigned char> buf(h->qbytes());
+  CK(cudaMemcpyAsync(buf.data(), h->q[0], h->qbytes(), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const size_t nn = size_t(h->ne) * h->NP;
+  for (size_t k = 0; k < nn; ++k) {
+    const double v = h->rbytes == 8 ? ((const double*)buf.data())[k * h->NC + c] : ((const float*)buf.data())[k * h->NC + c];
+    if (f32) f32[k] = float(v);
+    if (f64) f64[k] = v;
+  }
+}
+
+int mxm_dg_download_component(void* handle, int c, float* host) {
+  API_BEGIN
+  download_component(h, c, host, nullptr);
+  API_END
+}
+
+int mxm_dg_download_component_f64(void* handle, int c, double* host) {
+  API_BEGIN
+  download_component(h, c, nullptr, host);
+  API_END
+}
+
+int mxm_dg_enable_limiter(void* handle, int on, double eps) {
+  API_BEGIN
+  h->lim_on = on != 0;
+  h->lim_eps = eps;
+  API_END
+}
+
+int mxm_dg_step_ssprk3(void* handle, double dt) {
+  API_BEGIN
+  mxm::step_n(h, dt, 1);
+  API_END
+}
+
+int mxm_dg_step_n(void* handle, double dt, int nsteps) {
+  API_BEGIN
+  if (nsteps < 0) throw mxm::ArgError("nsteps must be >= 0");
+  mxm::step_n(h, dt, nsteps);
+  API_END
+}
+
+int mxm_dg_rk_stage(void* handle, int s, double dt) {
+  API_BEGIN
+  if (s < 0 || s > 2) throw mxm::ArgError("stage must be 0, 1 or 2");
+  mxm::rk_stage(h, s, dt);
+  API_END
+}
+
+int mxm_dg_eval_rhs(void* handle, const void* q_dev, void* rhs_dev) {
+  API_BEGIN
+  if (!q_dev || !rhs_dev || q_dev == rhs_dev) throw mxm::ArgError("q and rhs must be distinct device buffers");
+  mxm::stage(h, q_dev, q_dev, q_dev, rhs_dev, 0.0, 0.0, 0.0, 0.0, 1);
+  CK(cudaStreamSynchronize(h->stream));
+  API_END
+}
+
+int mxm_dg_limit(void* handle, int which) {
+  API_BEGIN
+  if (which < 0 || which > 2) throw mxm::ArgError("which must be 0..2");
+  mxm::limit_buf(h, h->q[which]);
+  API_END
+}
+
+int mxm_dg_advance_host(void* handle, const void* q_host, void* q_out_host, int nsteps, double dt) {
+  API_BEGIN
+  if (!q_host || !q_out_host || nsteps < 0) throw mxm::ArgError("host buffers must be non-null, nsteps >= 0");
+  CK(cudaMemcpyAsync(h->q[0], q_host, h->qbytes(), cudaMemcpyHostToDevice, h->stream));
+  mxm::step_n(h, dt, nsteps);
+  CK(cudaMemcpyAsync(q_out_host, h->q[0], h->qbytes(), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  API_END
+}
+
+int mxm_dg_max_wavespeed(void* handle, double* out) {
+  API_BEGIN
+  CK(cudaMemsetAsync(h->uscalar, 0, sizeof(unsigned long long), h->stream));
+  cudaError_t e = h->rbytes == 8 ? mxm::wavespeed_launch<double>(h, h->q[0], h->uscalar)
+                                 : mxm::wavespeed_launch<float>(h, h->q[0], h->uscalar);
+  if (e != cudaSuccess) throw mxm::CudaError(e, "wavespeed launch");
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, h->uscalar, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  std::memcpy(out, &bits, sizeof(double));
+  if (!(*out < 1.0e300)) {
+    h->err = "non-finite wave speed";
+    return MXM_DG_ENONFINITE;
+  }
+  API_END
+}
+
+int mxm_dg_reduce_conserved(void* handle, int which, int c, int kind, double* out) {
+  API_BEGIN
+  if (which < 0 || which > 2 || c < 0 || c >= h->NC || kind < 0 || kind > 2)
+    throw mxm::ArgError("which 0..2, component in range, kind 0..2");
+  const double vol = h->dim == 3 ? (h->lx / h->nx) * (h->ly / h->ny) * (h->lz / h->nz) / 6.0
+                                 : (h->lx / h->nx) * (h->ly / h->ny) / 2.0;
+  const double scale = kind == 2 ? 1.0 : vol;
+  cudaError_t e = h->rbytes == 8
+                      ? mxm::launch_reduce<double>(h->P, h->dim, h->NC, (const double*)h->q[which], (const double*)h->w,
+                                                   h->ne, c, kind, scale, h->partial, h->npartial, h->dscalar, h->stream)
+                      : mxm::launch_reduce<float>(h->P, h->dim, h->NC, (const float*)h->q[which], (const float*)h->w,
+                                                  h->ne, c, kind, scale, h->partial, h->npartial, h->dscalar, h->stream);
+  if (e != cudaSuccess) throw mxm::CudaError(e, "reduction launch");
+  CK(cudaMemcpyAsync(out, h->dscalar, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (!(*out == *out) || *out > 1.0e300 || *out < -1.0e300) {
+    h->err = "non-finite reduction result";
+    return MXM_DG_ENONFINITE;
+  }
+  API_END
+}
+
+int mxm_dg_set_device(int device) {
+  if (cudaSetDevice(device) != cudaSuccess) {
+    std::lock_guard<std::mutex> g(mxm::g_err_mu);
+    mxm::g_create_err = "cudaSetDevice failed";
+    return MXM_DG_ECUDA;
+  }
+  return MXM_DG_OK;
+}
+
+int mxm_dg_host_alloc(size_t nbytes, void** host) {
+  if (!host) return MXM_DG_EINVAL;
+  *host = nullptr;
+  if (cudaMallocHost(host, nbytes) != cudaSuccess) {
+    std::lock_guard<std::mutex> g(mxm::g_err_mu);
+    mxm::g_create_err = "cudaMallocHost failed";
+    return MXM_DG_ENOMEM;
+  }
+  return MXM_DG_OK;
+}
+
+int mxm_dg_host_free(void* host) {
+  if (host) cudaFreeHost(host);
+  return MXM_DG_OK;
+}
+
+int mxm_dg_synchronize(void* handle) {
+  API_BEGIN
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaGetLastError());
+  API_END
+}
+
+int mxm_dg_time_steps(void* handle, double dt, int nsteps, double* ms) {
+  API_BEGIN
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(a, h->stream));
+  mxm::step_n(h, dt, nsteps);
+  CK(cudaEventRecord(b, h->stream));
+  CK(cudaEventSynchronize(b));
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = f;
+  API_END
+}
+
+int mxm_dg_launches_per_step(void* handle, int32_t* n) {
+  API_BEGIN
+  *n = 3 * (1 + (h->lim_on ? 2 : 0));
+  API_END
+}
+
+int mxm_dg_last_error(void* handle, char* buf, int len) {
+  if (!buf || len <= 0) return MXM_DG_EINVAL;
+  std::string s;
+  if (handle) s = ((Handle*)handle)->err;
+  else {
+    std::lock_guard<std::mutex> g(mxm::g_err_mu);
+    s = mxm::g_create_err;
+  }
+  std::snprintf(buf, size_t(len), "%s", s.c_str());
+  return MXM_DG_OK;
+}
+
+int mxm_dg_operator(void* handle, double* host, int64_t* count) {
+  API_BEGIN
+  const int64_t n = int64_t(h->Ahost.size());
+  if (host && *count >= n) std::memcpy(host, h->Ahost.data(), size_t(n) * sizeof(double));
+  *count = n;
+  API_END
+}
+
+int mxm_dg_reference_operators(int dim, int P, double* D, double* Lift, double* w) {
+  try {
+    mxm::RefOps r = mxm::build_refops(dim, P);
+    auto ord = mxm::reference_face_order(dim, P, r);
+    const int NP = r.NP, NFP = r.NFP, NF = r.NF;
+    if (D) std::memcpy(D, r.D.data(), r.D.size() * sizeof(double));
+    if (w) std::memcpy(w, r.w.data(), r.w.size() * sizeof(double));
+    if (Lift)
+      for (int f = 0; f < NF; ++f) {
+        const int fo = dim == 2 ? (f + 2) % 3 : f;  // reference face f (2D: edge (f, f+1))
+        for (int i = 0; i < NP; ++i)
+          for (int m = 0; m < NFP; ++m) Lift[(f * NP + i) * NFP + m] = r.Lift[(fo * NP + i) * NFP + ord[f * NFP + m]];
+      }
+    return MXM_DG_OK;
+  } catch (std::exception& ex) {
+    std::lock_guard<std::mutex> g(mxm::g_err_mu);
+    mxm::g_create_err = ex.what();
+    return MXM_DG_EINVAL;
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,136 @@
+// Shared device-side definitions of the B200 DG kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mxm {
+
+__host__ __device__ constexpr int ntet(int P) { return (P + 1) * (P + 2) * (P + 3) / 6; }
+__host__ __device__ constexpr int ntri(int P) { return (P + 1) * (P + 2) / 2; }
+constexpr int kMaxNFP3 = 21;  // P = 5 tet face
+constexpr int kMaxNFP2 = 6;   // P = 5 triangle edge
+
+enum : int { BC_INTERIOR = 0, BC_WALL = 1, BC_OUTFLOW = 2, BC_INFLOW = 3 };
+enum : int { FLUX_RUSANOV = 0, FLUX_ROE = 1, FLUX_HLLE = 2, FLUX_HLLEC = 3, FLUX_HLLC = 4, FLUX_HLL = 5 };
+
+// Kuhn topology of one tet type's faces, passed by value as a kernel
+// parameter (lives in the constant bank; ~1.7 KB).
+template <class R>
+struct KuhnTab3 {
+  int8_t nb_t[6][4];
+  int8_t off[6][4][3];
+  int8_t side[6][4];
+  int8_t axis[6][4];
+  int8_t dir[6][4];
+  uint8_t own_node[4][kMaxNFP3];
+  uint8_t nb_node[6][4][kMaxNFP3];
+  R normal[6][4][3];
+};
+
+template <class R>
+struct KuhnTab2 {
+  int8_t nb_t[2][3];
+  int8_t off[2][3][2];
+  int8_t side[2][3];
+  int8_t axis[2][3];
+  int8_t dir[2][3];
+  uint8_t own_node[3][kMaxNFP2];
+  uint8_t nb_node[2][3][kMaxNFP2];
+  R normal[2][3][2];
+};
+
+// Face treatment for an element's face, resolved from the cell position and
+// the six BC codes exactly as mojoxm's BC overlay resolves it
+// (src/local_mesh.mojo:946-1187): the +axis cube face of the last cell
+// layer becomes a boundary face when bc_hi != 0; the -axis face of the first
+// layer gets its own one-sided boundary face when bc_lo != 0; with bc_lo ==
+// 0 but bc_hi != 0 the first layer still reads the shared face, whose flux
+// is the boundary flux of the last layer's state.
+enum : int { FACE_INTERIOR = 0, FACE_BC_HI = 1, FACE_BC_LO = 2, FACE_MIXED = 3 };
+
+__device__ __forceinline__ int face_mode(int axis, int dir, int cpos, int ncell_axis, const int* bc, int& code) {
+  code = 0;
+  if (axis < 0) return FACE_INTERIOR;
+  const int lo = bc[2 * axis], hi = bc[2 * axis + 1];
+  if (dir > 0) {
+    if (cpos == ncell_axis - 1 && hi != 0) {
+      code = hi;
+      return FACE_BC_HI;
+    }
+    return FACE_INTERIOR;
+  }
+  if (cpos == 0) {
+    if (lo != 0) {
+      code = lo;
+      return FACE_BC_LO;
+    }
+    if (hi != 0) {
+      code = hi;
+      return FACE_MIXED;
+    }
+  }
+  return FACE_INTERIOR;
+}
+
+__device__ __forceinline__ int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+// Kernel argument blocks (by value).
+template <class R>
+struct Stage3DArgs {
+  const R* q_in;
+  const R* q_a;
+  const R* q_b;
+  R* q_out;
+  const R* A;  // [6][K][NP] fused operators, k-major (transposed)
+  R a, b, cdt;
+  int nx, ny, nz;
+  int ncell;
+  int bc[6];
+  int rhs_only;
+};
+
+template <class R>
+struct Stage2DArgs {
+  const R* q_in;
+  const R* q_a;
+  const R* q_b;
+  R* q_out;
+  const R* A;  // [2][K][NP] k-major
+  R a, b, cdt;
+  int nx, ny;
+  int ncell;
+  int bc[4];
+  int rhs_only;
+};
+
+template <class R>
+struct LimArgs {
+  R* q;
+  R* avg;          // [Ne][NC]
+  const R* w;      // [NP] node weights
+  int64_t ne;
+  int nx, ny, nz;  // cells (nz = 1 in 2D)
+  int bc[6];
+  R eps2;
+};
+
+// Host launchers; each is explicitly instantiated next to its kernels.
+template <class R, class Phys>
+cudaError_t launch_stage3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phys& ph, int nsm,
+                           cudaStream_t st);
+template <class R, class Phys>
+cudaError_t launch_wavespeed3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phys& ph,
+                               unsigned long long* out, cudaStream_t st);
+template <class R, class Phys>
+cudaError_t launch_stage2d(int P, const Stage2DArgs<R>& a, const KuhnTab2<R>& tab, const Phys& ph, int nsm,
+                           cudaStream_t st);
+template <class R, class Phys>
+cudaError_t launch_wavespeed2d(const R* q, int64_t nnodes, const Phys& ph, unsigned long long* out, cudaStream_t st);
+template <class R>
+cudaError_t launch_limiter(int dim, int P, int NC, const LimArgs<R>& a, const KuhnTab3<R>& t3, const KuhnTab2<R>& t2,
+                           cudaStream_t st);
+template <class R>
+cudaError_t launch_reduce(int P, int dim, int NC, const R* q, const R* w, int64_t ne, int c, int kind, double scale,
+                          double* partial, int npartial, double* out, cudaStream_t st);
+
+}  // namespace mxm

@@ -1,0 +1,161 @@
+// Barth-Jespersen / Venkatakrishnan cell limiter and FP64 diagnostics.
+//
+// Reference: compute_cell_averages_kernel, bj_limiter_compute_theta_kernel,
+// bj_limiter_apply_kernel (src/solver.mojo:384-530) for 3D -- theta over
+// every node and component, neighbour set = self + 4 face neighbours with BC
+// faces resolving to self; and cell_mean_kernel_2d +
+// bj_limit_{compute_theta,apply}_kernel_2d (src/local_mesh_2d_gpu.mojo:180-198,
+// src/local_mesh_2d_gpu_limiter.mojo:74-153) for 2D -- theta from component 0
+// only, BC self-neighbours skipped, applied to every component.
+//
+// B200 form: pass 1 computes cell means with one thread per (element,
+// component) over coalesced loads; pass 2 stages a group of elements' nodal
+// values in shared memory with contiguous loads, reduces theta per element
+// with warp shuffles, and writes the limited values back contiguously only
+// for elements with theta < 1.
+#pragma once
+#include "dg_common.cuh"
+
+namespace mxm {
+
+template <class R, int NP, int NC>
+__global__ void cell_avg_kernel(LimArgs<R> a) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (tid >= a.ne * NC) return;
+  const int64_t e = tid / NC;
+  const int c = int(tid - e * NC);
+  const R* q = a.q + e * NP * NC + c;
+  R s = R(0);
+#pragma unroll
+  for (int n = 0; n < NP; ++n) s += __ldg(&a.w[n]) * q[n * NC];
+  a.avg[tid] = s;
+}
+
+// One warp per element; EPB elements per block of 32*EPB threads.
+template <class R, int DIM, int NP, int NC, int EPB>
+__global__ void __launch_bounds__(32 * EPB) theta_apply_kernel(LimArgs<R> a, KuhnTab3<R> t3, KuhnTab2<R> t2) {
+  constexpr int NTYPE = DIM == 3 ? 6 : 2, NFACE = DIM + 1, VALS = NP * NC;
+  __shared__ R sq[EPB][VALS];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t e = int64_t(blockIdx.x) * EPB + warp;
+  const bool valid = e < a.ne;
+  // contiguous block load of the EPB elements
+  const int64_t base = int64_t(blockIdx.x) * EPB * VALS;
+  const int64_t nvals = (a.ne - int64_t(blockIdx.x) * EPB) * VALS;
+  for (int idx = threadIdx.x; idx < EPB * VALS; idx += 32 * EPB)
+    if (idx < nvals) (&sq[0][0])[idx] = a.q[base + idx];
+  __syncthreads();
+  if (!valid) return;
+  const int t = int(e % NTYPE);
+  const int64_t cell = e / NTYPE;
+  int cpos[3];
+  if (DIM == 3) {
+    const int64_t nxy = int64_t(a.nx) * a.ny;
+    cpos[2] = int(cell / nxy);
+    const int64_t rem = cell - int64_t(cpos[2]) * nxy;
+    cpos[1] = int(rem / a.nx);
+    cpos[0] = int(rem - int64_t(cpos[1]) * a.nx);
+  } else {
+    cpos[1] = int(cell / a.nx);
+    cpos[0] = int(cell - int64_t(cpos[1]) * a.nx);
+    cpos[2] = 0;
+  }
+  const int ncells[3] = {a.nx, a.ny, a.nz};
+  // neighbour cell means: lanes 0..NFACE-1 each resolve one face
+  int64_t nb = e;
+  if (lane < NFACE) {
+    const int lf = lane;
+    const int ax = DIM == 3 ? t3.axis[t][lf] : t2.axis[t][lf];
+    const int dir = DIM == 3 ? t3.dir[t][lf] : t2.dir[t][lf];
+    int code;
+    const int mode = face_mode(ax, dir, ax >= 0 ? cpos[ax] : 0, ax >= 0 ? ncells[ax] : 1, a.bc, code);
+    if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
+      if (DIM == 3) {
+        const int ni = wrapi(cpos[0] + t3.off[t][lf][0], a.nx), nj = wrapi(cpos[1] + t3.off[t][lf][1], a.ny),
+                  nk = wrapi(cpos[2] + t3.off[t][lf][2], a.nz);
+        nb = (int64_t(ni) + int64_t(a.nx) * (nj + int64_t(a.ny) * nk)) * 6 + t3.nb_t[t][lf];
+      } else {
+        const int ni = wrapi(cpos[0] + t2.off[t][lf][0], a.nx), nj = wrapi(cpos[1] + t2.off[t][lf][1], a.ny);
+        nb = (int64_t(nj) * a.nx + ni) * 2 + t2.nb_t[t][lf];
+      }
+    }
+  }
+  constexpr int NCT = DIM == 3 ? NC : 1;  // components entering theta
+  R own[NCT], lo[NCT], hi[NCT];
+#pragma unroll
+  for (int c = 0; c < NCT; ++c) own[c] = lo[c] = hi[c] = a.avg[e * NC + c];
+#pragma unroll
+  for (int lf = 0; lf < NFACE; ++lf) {
+    const int64_t n = __shfl_sync(0xffffffffu, nb, lf);
+    if (DIM == 2 && n == e) continue;  // 2D: BC faces do not constrain
+#pragma unroll
+    for (int c = 0; c < NCT; ++c) {
+      const R v = a.avg[n * NC + c];
+      if (v < lo[c]) lo[c] = v;
+      if (v > hi[c]) hi[c] = v;
+    }
+  }
+  R th = R(1);
+  const R tiny = R(1.0e-30);
+  for (int idx = lane; idx < NP * NCT; idx += 32) {
+    const int n = idx / NCT, c = idx - n * NCT;
+    const R dl = sq[warp][n * NC + c] - own[c];
+    const R da = dl >= R(0) ? dl : -dl;
+    if (da <= tiny) continue;
+    R pD = hi[c] - own[c];
+    if (pD < R(0)) pD = R(0);
+    R nD = own[c] - lo[c];
+    if (nD < R(0)) nD = R(0);
+    const R D = dl > R(0) ? pD : nD;
+    const R D2 = D * D, d2 = da * da, Dd = D * da;
+    const R al = (D2 + R(2) * Dd + a.eps2) / (D2 + R(2) * d2 + Dd + a.eps2);
+    if (al < th) th = al;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const R v = __shfl_xor_sync(0xffffffffu, th, o);
+    th = v < th ? v : th;
+  }
+  if (!(th < R(1))) return;
+  R* qe = a.q + e * VALS;
+  for (int idx = lane; idx < VALS; idx += 32) {
+    const int c = idx % NC;
+    const R bm = a.avg[e * NC + c];
+    qe[idx] = bm + th * (sq[warp][idx] - bm);
+  }
+}
+
+// ---- FP64 reductions: per-block partial sums, then a fixed-order final sum.
+template <class R, int NP, int NC>
+__global__ void reduce_partial_kernel(const R* q, const R* w, int64_t ne, int c, int kind, double* partial) {
+  __shared__ double red[32];
+  double acc = kind == 2 ? 0.0 : 0.0;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < ne; e += int64_t(gridDim.x) * blockDim.x) {
+    const R* qe = q + e * NP * NC + c;
+    double s = 0.0;
+#pragma unroll
+    for (int n = 0; n < NP; ++n) {
+      const double v = double(qe[n * NC]);
+      if (kind == 0) s += double(__ldg(&w[n])) * v;
+      else if (kind == 1) s += double(__ldg(&w[n])) * v * v;
+      else s = fmax(s, fabs(v));
+    }
+    if (kind == 2) acc = fmax(acc, s);
+    else acc += s;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double v = __shfl_xor_sync(0xffffffffu, acc, o);
+    acc = kind == 2 ? fmax(acc, v) : acc + v;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int k = 0; k < int(blockDim.x >> 5); ++k) s = kind == 2 ? fmax(s, red[k]) : s + red[k];
+    partial[blockIdx.x] = s;
+  }
+}
+
+__global__ void reduce_final_kernel(const double* partial, int n, int kind, double scale, double* out);
+
+}  // namespace mxm

@@ -1,0 +1,365 @@
+// Device physics for the 3D stage kernel: pointwise flux, numerical flux,
+// boundary flux (ghost-state), source and positivity floor of mojoxm's
+// `Physics` implementations (trait: src/solver.mojo:97-145).
+//   Advection     src/advection.mojo:187-286
+//   Euler         src/euler.mojo:44-792 (Rusanov/Roe/HLLE/HLLEC, Harten-Hyman fix)
+//   Maxwell       src/maxwell.mojo:48-255
+//   ShallowWater  src/shallow_water.mojo:31-167
+// Each formula keeps the reference's operation order; comparisons that the
+// reference writes as `not (x > floor)` stay NaN-catching.
+#pragma once
+#include "dg_common.cuh"
+
+namespace mxm {
+
+template <class R>
+__device__ __forceinline__ R rmax(R a, R b) { return a > b ? a : b; }
+template <class R>
+__device__ __forceinline__ R rmin(R a, R b) { return a < b ? a : b; }
+template <class R>
+__device__ __forceinline__ R rabs(R a) { return a >= R(0) ? a : -a; }
+
+// ------------------------------------------------------------------ advection
+template <class R>
+struct AdvectionD {
+  static constexpr int NC = 1;
+  static constexpr bool kSource = false, kLimit = false;
+  R vx, vy, vz, inflow_q;
+  __device__ void flux(const R* q, R* F) const {  // F[d*NC + c]
+    F[0] = vx * q[0];
+    F[1] = vy * q[0];
+    F[2] = vz * q[0];
+  }
+  __device__ R num_flux(const R* ql, const R* qr, R nx, R ny, R nz, R* f) const {
+    R nc = vx * nx + vy * ny + vz * nz;
+    R a = rabs(nc);
+    f[0] = R(0.5) * ((nc + a) * ql[0] + (nc - a) * qr[0]);
+    return a;
+  }
+  __device__ R bnd_flux(const R* q, int bc, R nx, R ny, R nz, R* f) const {
+    R nc = vx * nx + vy * ny + vz * nz;
+    R a = rabs(nc);
+    R g = (bc == BC_INFLOW) ? inflow_q : R(0);
+    f[0] = R(0.5) * ((nc + a) * q[0] + (nc - a) * g);
+    return a;
+  }
+  __device__ void source(const R*, R* s) const { s[0] = R(0); }
+  __device__ void limit(R*) const {}
+};
+
+// ---------------------------------------------------------------------- euler
+template <class R, int FLUX>
+struct EulerD {
+  static constexpr int NC = 5;
+  static constexpr bool kSource = true, kLimit = true;
+  R gamma, rho_min, p_min, gx, gy, gz;
+  R inflow[5];
+  int entropy_fix;
+
+  __device__ __forceinline__ R rho_f(const R* q) const { return q[0] > rho_min ? q[0] : rho_min; }
+  __device__ __forceinline__ R p_f(const R* q, R rho) const {
+    R ke = R(0.5) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) / rho;
+    R p = (gamma - R(1)) * (q[4] - ke);
+    return p > p_min ? p : p_min;
+  }
+  __device__ void flux(const R* q, R* F) const {  // euler.mojo:597-621
+    R rho = rho_f(q), p = p_f(q, rho);
+    R u = q[1] / rho, v = q[2] / rho, w = q[3] / rho;
+    F[0] = q[1]; F[1] = q[1] * u + p; F[2] = q[1] * v; F[3] = q[1] * w; F[4] = u * (q[4] + p);
+    F[5] = q[2]; F[6] = q[2] * u; F[7] = q[2] * v + p; F[8] = q[2] * w; F[9] = v * (q[4] + p);
+    F[10] = q[3]; F[11] = q[3] * u; F[12] = q[3] * v; F[13] = q[3] * w + p; F[14] = w * (q[4] + p);
+  }
+  __device__ void flux1d(const R* q, R* f) const {  // euler.mojo:64-72
+    R rho = rho_f(q), p = p_f(q, rho);
+    R u = q[1] / rho;
+    f[0] = q[1]; f[1] = q[1] * u + p; f[2] = q[2] * u; f[3] = q[3] * u; f[4] = u * (q[4] + p);
+  }
+  __device__ void roe_avg(const R* ql, const R* qr, R pl, R pr, R& u, R& v, R& w, R& enth, R& a) const {
+    R sl = sqrt(rho_f(ql)), sr = sqrt(rho_f(qr)), s = sl + sr;  // euler.mojo:161-176
+    u = (ql[1] / sl + qr[1] / sr) / s;
+    v = (ql[2] / sl + qr[2] / sr) / s;
+    w = (ql[3] / sl + qr[3] / sr) / s;
+    enth = ((ql[4] + pl) / sl + (qr[4] + pr) / sr) / s;
+    R aa2 = rmax((gamma - R(1)) * (enth - R(0.5) * (u * u + v * v + w * w)), R(0));
+    a = sqrt(aa2);
+  }
+  __device__ void fluct(const R* s, const R* wv, R* amdq, R* apdq) const {  // euler.mojo:184-199
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      R am = R(0), ap = R(0);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        R t = s[k] * wv[m * 3 + k];
+        if (s[k] < R(0)) am += t; else ap += t;
+      }
+      amdq[m] = am;
+      apdq[m] = ap;
+    }
+  }
+  __device__ void hh_fix(const R* ql, const R* qr, const R* s, const R* wv, R* amdq, R* apdq) const {  // euler.mojo:207-288
+    R rl = rho_f(ql), pl = p_f(ql, rl);
+    R s0 = ql[1] / rl - sqrt(gamma * pl / rl);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) amdq[m] = R(0);
+    if (!(s0 > R(0) && s[0] > R(0))) {
+      R q10 = rmax(ql[0] + wv[0], rho_min);
+      R q11 = ql[1] + wv[3], q12 = ql[2] + wv[6], q13 = ql[3] + wv[9], q14 = ql[4] + wv[12];
+      R ke1 = R(0.5) * (q11 * q11 + q12 * q12 + q13 * q13) / q10;
+      R p1 = rmax((gamma - R(1)) * (q14 - ke1), p_min);
+      R s1 = q11 / q10 - sqrt(gamma * p1 / q10);
+      R sf = (s0 < R(0) && s1 > R(0)) ? s0 * (s1 - s[0]) / (s1 - s0) : (s[0] < R(0) ? s[0] : R(0));
+#pragma unroll
+      for (int m = 0; m < 5; ++m) amdq[m] = sf * wv[m * 3 + 0];
+      if (s[1] < R(0)) {
+#pragma unroll
+        for (int m = 0; m < 5; ++m) amdq[m] += s[1] * wv[m * 3 + 1];
+        R rr = rho_f(qr), pr = p_f(qr, rr);
+        R s3 = qr[1] / rr + sqrt(gamma * pr / rr);
+        R q20 = rmax(qr[0] - wv[2], rho_min);
+        R q21 = qr[1] - wv[5], q22 = qr[2] - wv[8], q23 = qr[3] - wv[11], q24 = qr[4] - wv[14];
+        R ke2 = R(0.5) * (q21 * q21 + q22 * q22 + q23 * q23) / q20;
+        R p2 = rmax((gamma - R(1)) * (q24 - ke2), p_min);
+        R s2 = q21 / q20 + sqrt(gamma * p2 / q20);
+        R sf2 = (s2 < R(0) && s3 > R(0)) ? s2 * (s3 - s[2]) / (s3 - s2) : (s[2] < R(0) ? s[2] : R(0));
+#pragma unroll
+        for (int m = 0; m < 5; ++m) amdq[m] += sf2 * wv[m * 3 + 2];
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      R d = R(0);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) d += s[k] * wv[m * 3 + k];
+      apdq[m] = d - amdq[m];
+    }
+  }
+  // 1D Riemann problem in the face frame (rotated states): numerical flux rf.
+  __device__ R solve1d(const R* ql, const R* qr, R* rf) const {
+    if (FLUX == FLUX_RUSANOV) {  // euler.mojo:649-668
+      R rhol = rho_f(ql), rhor = rho_f(qr), pl = p_f(ql, rhol), pr = p_f(qr, rhor);
+      R cl = sqrt(gamma * pl / rhol), cr = sqrt(gamma * pr / rhor);
+      R uxl = ql[1] / rhol, uxr = qr[1] / rhor;
+      R cmax = rmax(rabs(uxl) + cl, rabs(uxr) + cr);
+      rf[0] = R(0.5) * (ql[1] + qr[1] + cmax * (rhol - rhor));
+      rf[1] = R(0.5) * (ql[1] * uxl + pl + qr[1] * uxr + pr + cmax * (ql[1] - qr[1]));
+      rf[2] = R(0.5) * (ql[2] * uxl + qr[2] * uxr + cmax * (ql[2] - qr[2]));
+      rf[3] = R(0.5) * (ql[3] * uxl + qr[3] * uxr + cmax * (ql[3] - qr[3]));
+      rf[4] = R(0.5) * ((ql[4] + pl) * uxl + (qr[4] + pr) * uxr + cmax * (ql[4] - qr[4]));
+      return cmax;
+    } else {
+      R s[3], wv[15], amdq[5], apdq[5];
+      R pl = p_f(ql, rho_f(ql)), pr = p_f(qr, rho_f(qr));
+      R u, v, w, enth, a;
+      roe_avg(ql, qr, pl, pr, u, v, w, enth, a);
+      if (FLUX == FLUX_ROE) {  // euler.mojo:296-361
+        R g1 = gamma - R(1);
+        R d0 = qr[0] - ql[0], d1 = qr[1] - ql[1], d2 = qr[2] - ql[2], d3 = qr[3] - ql[3], d4 = qr[4] - ql[4];
+        R q2 = u * u + v * v + w * w;
+        R g1a2 = g1 / (a * a);
+        R euv = enth - q2;
+        R a4 = g1a2 * (euv * d0 + u * d1 + v * d2 + w * d3 - d4);
+        R a2 = d2 - v * d0, a3 = d3 - w * d0;
+        R a5 = (d1 + (a - u) * d0 - a * a4) / (R(2) * a);
+        R a1 = d0 - a4 - a5;
+        wv[0] = a1; wv[3] = a1 * (u - a); wv[6] = a1 * v; wv[9] = a1 * w; wv[12] = a1 * (enth - u * a);
+        wv[1] = a4; wv[4] = a4 * u; wv[7] = a4 * v + a2; wv[10] = a4 * w + a3;
+        wv[13] = a4 * R(0.5) * q2 + a2 * v + a3 * w;
+        wv[2] = a5; wv[5] = a5 * (u + a); wv[8] = a5 * v; wv[11] = a5 * w; wv[14] = a5 * (enth + u * a);
+        s[0] = u - a; s[1] = u; s[2] = u + a;
+      } else {
+        R rl = rho_f(ql), al = sqrt(gamma * pl / rl), ul = ql[1] / rl;
+        R rr = rho_f(qr), ar = sqrt(gamma * pr / rr), ur = qr[1] / rr;
+        s[0] = rmin(ul - al, u - a);
+        s[2] = rmax(ur + ar, u + a);
+        if (FLUX == FLUX_HLLE) {  // euler.mojo:364-412
+          s[1] = R(0);
+          R fl[5], fr[5];
+          flux1d(ql, fl);
+          flux1d(qr, fr);
+          R den = s[0] - s[2];
+#pragma unroll
+          for (int m = 0; m < 5; ++m) {
+            R qh = (fr[m] - fl[m] - s[2] * qr[m] + s[0] * ql[m]) / den;
+            wv[m * 3 + 0] = qh - ql[m];
+            wv[m * 3 + 1] = R(0);
+            wv[m * 3 + 2] = qr[m] - qh;
+          }
+        } else {  // HLLEC  euler.mojo:415-485
+          s[1] = (pr - pl + rl * ul * (s[0] - ul) - rr * ur * (s[2] - ur)) / (rl * (s[0] - ul) - rr * (s[2] - ur));
+          R lm = rl * (s[0] - ul) / (s[0] - s[1]);
+          R hL[5] = {lm, lm * s[1], lm * ql[2] / rl, lm * ql[3] / rl,
+                     lm * (ql[4] / rl + (s[1] - ul) * (s[1] + pl / (rl * (s[0] - ul))))};
+          R rm = rr * (s[2] - ur) / (s[2] - s[1]);
+          R hR[5] = {rm, rm * s[1], rm * qr[2] / rr, rm * qr[3] / rr,
+                     rm * (qr[4] / rr + (s[1] - ur) * (s[1] + pr / (rr * (s[2] - ur))))};
+#pragma unroll
+          for (int m = 0; m < 5; ++m) {
+            wv[m * 3 + 0] = hL[m] - ql[m];
+            wv[m * 3 + 1] = hR[m] - hL[m];
+            wv[m * 3 + 2] = qr[m] - hR[m];
+          }
+        }
+      }
+      if (entropy_fix) hh_fix(ql, qr, s, wv, amdq, apdq);
+      else fluct(s, wv, amdq, apdq);
+      R fl[5], fr[5];  // euler_flux_from_fluctuations  euler.mojo:495-520
+      flux1d(ql, fl);
+      flux1d(qr, fr);
+#pragma unroll
+      for (int m = 0; m < 5; ++m) rf[m] = R(0.5) * (fl[m] + fr[m]) - R(0.5) * (apdq[m] - amdq[m]);
+      return rmax(rmax(rabs(s[0]), rabs(s[1])), rabs(s[2]));
+    }
+  }
+  __device__ R num_flux(const R* q_l, const R* q_r, R nx, R ny, R nz, R* flux) const {  // euler.mojo:626-691
+    // tangent/binormal (euler.mojo:94-118)
+    R ax = nx, ay = ny, az = nz;
+    if (rabs(nx) >= R(0.9)) ay += R(1); else ax += R(1);
+    R pro = nx * ax + ny * ay + nz * az;
+    ax -= nx * pro; ay -= ny * pro; az -= nz * pro;
+    R mag = sqrt(ax * ax + ay * ay + az * az);
+    R tx = ax / mag, ty = ay / mag, tz = az / mag;
+    R bx = ny * tz - nz * ty, by = nz * tx - nx * tz, bz = nx * ty - ny * tx;
+    R ql[5], qr[5], rf[5];
+    ql[0] = q_l[0]; ql[4] = q_l[4];
+    ql[1] = nx * q_l[1] + ny * q_l[2] + nz * q_l[3];
+    ql[2] = tx * q_l[1] + ty * q_l[2] + tz * q_l[3];
+    ql[3] = bx * q_l[1] + by * q_l[2] + bz * q_l[3];
+    qr[0] = q_r[0]; qr[4] = q_r[4];
+    qr[1] = nx * q_r[1] + ny * q_r[2] + nz * q_r[3];
+    qr[2] = tx * q_r[1] + ty * q_r[2] + tz * q_r[3];
+    qr[3] = bx * q_r[1] + by * q_r[2] + bz * q_r[3];
+    R vmax = solve1d(ql, qr, rf);
+    flux[0] = rf[0]; flux[4] = rf[4];
+    flux[1] = nx * rf[1] + tx * rf[2] + bx * rf[3];
+    flux[2] = ny * rf[1] + ty * rf[2] + by * rf[3];
+    flux[3] = nz * rf[1] + tz * rf[2] + bz * rf[3];
+    return vmax;
+  }
+  __device__ R bnd_flux(const R* q, int bc, R nx, R ny, R nz, R* f) const {  // euler.mojo:705-730
+    R g[5];
+    if (bc == BC_WALL) {
+      R mn = q[1] * nx + q[2] * ny + q[3] * nz;
+      g[0] = q[0]; g[4] = q[4];
+      g[1] = q[1] - R(2) * mn * nx; g[2] = q[2] - R(2) * mn * ny; g[3] = q[3] - R(2) * mn * nz;
+    } else if (bc == BC_INFLOW) {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) g[c] = inflow[c];
+    } else {
+#pragma unroll
+      for (int c = 0; c < 5; ++c) g[c] = q[c];
+    }
+    return num_flux(q, g, nx, ny, nz, f);
+  }
+  __device__ void source(const R* q, R* s) const {  // euler.mojo:738-747
+    s[0] = R(0);
+    s[1] = q[0] * gx;
+    s[2] = q[0] * gy;
+    s[3] = q[0] * gz;
+    s[4] = q[1] * gx + q[2] * gy + q[3] * gz;
+  }
+  __device__ void limit(R* q) const {  // euler.mojo:758-792
+    R rho = q[0];
+    if (!(rho > rho_min)) {
+      q[0] = rho_min; q[1] = R(0); q[2] = R(0); q[3] = R(0);
+      q[4] = p_min / (gamma - R(1));
+      return;
+    }
+    R m2 = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+    if (!(m2 >= R(0))) {
+      q[1] = R(0); q[2] = R(0); q[3] = R(0);
+      q[4] = p_min / (gamma - R(1));
+      return;
+    }
+    R ke = R(0.5) * m2 / rho;
+    R p = (gamma - R(1)) * (q[4] - ke);
+    if (!(p > p_min)) q[4] = ke + p_min / (gamma - R(1));
+  }
+};
+
+// -------------------------------------------------------------------- maxwell
+template <class R>
+struct MaxwellD {
+  static constexpr int NC = 6;
+  static constexpr bool kSource = true, kLimit = false;
+  R c, J[3], M[3], inflow[6];
+  __device__ void flux(const R* q, R* F) const {  // maxwell.mojo:127-156
+    R c2 = c * c;
+    F[0] = R(0); F[1] = c2 * q[5]; F[2] = -c2 * q[4]; F[3] = R(0); F[4] = -q[2]; F[5] = q[1];
+    F[6] = -c2 * q[5]; F[7] = R(0); F[8] = c2 * q[3]; F[9] = q[2]; F[10] = R(0); F[11] = -q[0];
+    F[12] = c2 * q[4]; F[13] = -c2 * q[3]; F[14] = R(0); F[15] = -q[1]; F[16] = q[0]; F[17] = R(0);
+  }
+  __device__ R num_flux(const R* l, const R* r, R nx, R ny, R nz, R* f) const {  // maxwell.mojo:161-207
+    R c2 = c * c, h = R(0.5);
+    f[0] = h * (c2 * (l[4] * nz - l[5] * ny) + c2 * (r[4] * nz - r[5] * ny)) - h * c * (r[0] - l[0]);
+    f[1] = h * (c2 * (l[5] * nx - l[3] * nz) + c2 * (r[5] * nx - r[3] * nz)) - h * c * (r[1] - l[1]);
+    f[2] = h * (c2 * (l[3] * ny - l[4] * nx) + c2 * (r[3] * ny - r[4] * nx)) - h * c * (r[2] - l[2]);
+    f[3] = h * ((ny * l[2] - nz * l[1]) + (ny * r[2] - nz * r[1])) - h * c * (r[3] - l[3]);
+    f[4] = h * ((nz * l[0] - nx * l[2]) + (nz * r[0] - nx * r[2])) - h * c * (r[4] - l[4]);
+    f[5] = h * ((nx * l[1] - ny * l[0]) + (nx * r[1] - ny * r[0])) - h * c * (r[5] - l[5]);
+    return c;
+  }
+  __device__ R bnd_flux(const R* q, int bc, R nx, R ny, R nz, R* f) const {  // maxwell.mojo:213-240
+    R g[6];
+    if (bc == BC_WALL) {
+      R En = q[0] * nx + q[1] * ny + q[2] * nz, Bn = q[3] * nx + q[4] * ny + q[5] * nz;
+      g[0] = R(2) * En * nx - q[0]; g[1] = R(2) * En * ny - q[1]; g[2] = R(2) * En * nz - q[2];
+      g[3] = q[3] - R(2) * Bn * nx; g[4] = q[4] - R(2) * Bn * ny; g[5] = q[5] - R(2) * Bn * nz;
+    } else if (bc == BC_INFLOW) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) g[k] = inflow[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) g[k] = q[k];
+    }
+    return num_flux(q, g, nx, ny, nz, f);
+  }
+  __device__ void source(const R*, R* s) const {  // maxwell.mojo:245-252
+    R c2 = c * c;
+    s[0] = -c2 * J[0]; s[1] = -c2 * J[1]; s[2] = -c2 * J[2];
+    s[3] = -M[0]; s[4] = -M[1]; s[5] = -M[2];
+  }
+  __device__ void limit(R*) const {}
+};
+
+// -------------------------------------------------------------- shallow water
+template <class R>
+struct ShallowWaterD {
+  static constexpr int NC = 3;
+  static constexpr bool kSource = false, kLimit = false;
+  R g, h_min, inflow[3];
+  __device__ void flux(const R* q, R* F) const {  // shallow_water.mojo:63-86
+    R h = q[0] > h_min ? q[0] : h_min;
+    R u = q[1] / h, v = q[2] / h, gh = R(0.5) * g * h * h;
+    F[0] = q[1]; F[1] = q[1] * u + gh; F[2] = q[1] * v;
+    F[3] = q[2]; F[4] = q[1] * v; F[5] = q[2] * v + gh;
+    F[6] = R(0); F[7] = R(0); F[8] = R(0);
+  }
+  __device__ R num_flux(const R* l, const R* r, R nx, R ny, R, R* f) const {  // shallow_water.mojo:90-134
+    R hl = l[0] > h_min ? l[0] : h_min, hr = r[0] > h_min ? r[0] : h_min;
+    R ul = l[1] / hl, vl = l[2] / hl, ur = r[1] / hr, vr = r[2] / hr;
+    R unl = ul * nx + vl * ny, unr = ur * nx + vr * ny;
+    R cl = sqrt(g * hl), cr = sqrt(g * hr);
+    R gl = R(0.5) * g * hl * hl, gr = R(0.5) * g * hr * hr;
+    R al = rmax(rabs(unl) + cl, rabs(unr) + cr), h = R(0.5);
+    f[0] = h * ((l[1] * nx + l[2] * ny) + (r[1] * nx + r[2] * ny)) - h * al * (r[0] - l[0]);
+    f[1] = h * ((l[1] * unl + gl * nx) + (r[1] * unr + gr * nx)) - h * al * (r[1] - l[1]);
+    f[2] = h * ((l[2] * unl + gl * ny) + (r[2] * unr + gr * ny)) - h * al * (r[2] - l[2]);
+    return al;
+  }
+  __device__ R bnd_flux(const R* q, int bc, R nx, R ny, R nz, R* f) const {  // shallow_water.mojo:138-156
+    R gs[3];
+    if (bc == BC_WALL) {
+      R mn = q[1] * nx + q[2] * ny;
+      gs[0] = q[0]; gs[1] = q[1] - R(2) * mn * nx; gs[2] = q[2] - R(2) * mn * ny;
+    } else if (bc == BC_INFLOW) {
+      gs[0] = inflow[0]; gs[1] = inflow[1]; gs[2] = inflow[2];
+    } else {
+      gs[0] = q[0]; gs[1] = q[1]; gs[2] = q[2];
+    }
+    return num_flux(q, gs, nx, ny, nz, f);
+  }
+  __device__ void source(const R*, R* s) const { s[0] = s[1] = s[2] = R(0); }
+  __device__ void limit(R*) const {}
+};
+
+}  // namespace mxm

@@ -1,0 +1,79 @@
+// Launch configuration of the 3D stage kernel per (real type, P, NC).
+#pragma once
+#include "stage3d.cuh"
+
+namespace mxm {
+
+template <class R, int P, int NC>
+struct Cfg3 {
+  using S = Stage3DShape<P, NC, R>;
+  static constexpr int NP = S::NP;
+  // rows per thread: a divisor of NP
+  static constexpr int RI = P <= 2 ? 2 : (P == 4 ? 5 : 4);
+  // stage A_t in shared memory when it takes <= 64 KB
+  static constexpr bool ASMEM = sizeof(R) * S::K * S::NP <= 64 * 1024;
+  static constexpr size_t kBudget = 110 * 1024;
+  static constexpr size_t kA = ASMEM ? sizeof(R) * S::K * S::NP : 0;
+  static constexpr size_t kPerEl = sizeof(R) * (size_t(S::NP) * NC + S::BSTR);
+  static constexpr int EB_RAW = int((kBudget - kA) / kPerEl);
+  static constexpr int EB = EB_RAW > 64 ? 64 : (EB_RAW < 1 ? 1 : EB_RAW);
+  static constexpr int NT = 128;
+  static constexpr size_t kSmem = stage3d_smem_bytes<R, P, NC, EB, ASMEM>();
+};
+
+template <class R, class Phys, int P>
+cudaError_t launch3_p(const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phys& ph, int nsm, cudaStream_t st) {
+  using C = Cfg3<R, P, Phys::NC>;
+  auto kern = stage3d_kernel<R, Phys, P, C::RI, C::EB, C::NT, C::ASMEM>;
+  static int bps = -1;
+  if (bps < 0) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(C::kSmem));
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, C::NT, C::kSmem);
+    if (e != cudaSuccess) return e;
+    if (bps < 1) bps = 1;
+  }
+  const int ngroups = (a.ncell + C::EB - 1) / C::EB;
+  int per_type = (nsm * bps + 5) / 6;
+  if (per_type > ngroups) per_type = ngroups;
+  if (per_type < 1) per_type = 1;
+  kern<<<6 * per_type, C::NT, C::kSmem, st>>>(a, tab, ph);
+  return cudaGetLastError();
+}
+
+template <class R, class Phys>
+cudaError_t launch_stage3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phys& ph, int nsm,
+                           cudaStream_t st) {
+  switch (P) {
+    case 1: return launch3_p<R, Phys, 1>(a, tab, ph, nsm, st);
+    case 2: return launch3_p<R, Phys, 2>(a, tab, ph, nsm, st);
+    case 3: return launch3_p<R, Phys, 3>(a, tab, ph, nsm, st);
+    case 4: return launch3_p<R, Phys, 4>(a, tab, ph, nsm, st);
+    case 5: return launch3_p<R, Phys, 5>(a, tab, ph, nsm, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class R, class Phys>
+cudaError_t launch_wavespeed3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phys& ph,
+                               unsigned long long* out, cudaStream_t st) {
+  const int64_t n = int64_t(a.ncell) * 6 * 4 * ntri(P);
+  const int nb = int((n + 255) / 256);
+  switch (P) {
+    case 1: wavespeed3d_kernel<R, Phys, 1><<<nb, 256, 0, st>>>(a, tab, ph, out); break;
+    case 2: wavespeed3d_kernel<R, Phys, 2><<<nb, 256, 0, st>>>(a, tab, ph, out); break;
+    case 3: wavespeed3d_kernel<R, Phys, 3><<<nb, 256, 0, st>>>(a, tab, ph, out); break;
+    case 4: wavespeed3d_kernel<R, Phys, 4><<<nb, 256, 0, st>>>(a, tab, ph, out); break;
+    case 5: wavespeed3d_kernel<R, Phys, 5><<<nb, 256, 0, st>>>(a, tab, ph, out); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+#define MXM_INSTANTIATE_STAGE3D(R, PHYS)                                                                          \
+  template cudaError_t launch_stage3d<R, PHYS>(int, const Stage3DArgs<R>&, const KuhnTab3<R>&, const PHYS&, int, \
+                                               cudaStream_t);                                                     \
+  template cudaError_t launch_wavespeed3d<R, PHYS>(int, const Stage3DArgs<R>&, const KuhnTab3<R>&, const PHYS&,  \
+                                                   unsigned long long*, cudaStream_t);
+
+}  // namespace mxm

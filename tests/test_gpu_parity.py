@@ -1,0 +1,141 @@
+"""CUDA path vs the CPU oracle on identical seeded inputs (through the C ABI).
+
+Element-wise RHS parity for every (physics, flux, entropy-fix, P, BC arm),
+full SSPRK3 steps with and without the cell limiter, 2D kernels, node
+coordinates, FP64 reductions and the max wave speed.  Meshes are small and
+anisotropic (dx != dy != dz) so permutation and scaling mistakes show.
+"""
+import numpy as np
+import pytest
+
+import mojoxm_b200 as M
+from tests import dgcases as C
+
+pytestmark = pytest.mark.gpu
+
+
+def make_pair(oracle, phys, P, n, L, bcs, prec="f64", dim=3):
+    bc = M.BoundaryConditions(*bcs) if dim == 3 else M.BoundaryConditions(*bcs, 0, 0)
+    mesh = M.Mesh(*n, *L, bcs=bc, dim=dim) if dim == 3 else M.Mesh(n[0], n[1], 1, L[0], L[1], 1.0, bcs=bc, dim=2)
+    s = M.Solver(mesh, phys, P=P, precision=prec)
+    real = "f64" if prec == "f64" else "f32"
+    if dim == 3:
+        o = oracle.Oracle3D(P, n, L, M.physics_dict(phys), bcs=bcs, real=real)
+    else:
+        o = oracle.Oracle2D(P, n, L, M.physics_dict(phys), bcs=bcs, real=real)
+    return s, o
+
+
+N3, L3 = (3, 4, 2), (1.0, 1.3, 0.7)
+N2, L2 = (4, 3), (1.0, 0.8)
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("name", list(C.PHYSICS_3D))
+def test_rhs3d_f64_periodic(oracle_mod, name, P):
+    phys = C.PHYSICS_3D[name]()
+    s, o = make_pair(oracle_mod, phys, P, N3, L3, C.BCS_3D["periodic"])
+    q = C.random_state(s.shape, phys, seed=100 + P)
+    r_gpu, r_cpu = s.rhs(q), o.rhs(q)
+    assert C.rel_err(r_gpu, r_cpu) <= C.TOL_F64_3D[P]
+
+
+@pytest.mark.parametrize("bcname", [b for b in C.BCS_3D if b != "periodic"])
+@pytest.mark.parametrize("name", ["advection", "euler_hllec_fix", "euler_rusanov", "maxwell", "shallow_water"])
+@pytest.mark.parametrize("P", [2, 3])
+def test_rhs3d_f64_boundaries(oracle_mod, name, bcname, P):
+    phys = C.PHYSICS_3D[name]()
+    s, o = make_pair(oracle_mod, phys, P, N3, L3, C.BCS_3D[bcname])
+    q = C.random_state(s.shape, phys, seed=7)
+    assert C.rel_err(s.rhs(q), o.rhs(q)) <= C.TOL_F64_3D[P]
+
+
+@pytest.mark.parametrize("name", ["euler_hllec", "euler_roe_fix", "maxwell", "advection", "shallow_water"])
+@pytest.mark.parametrize("P", [1, 3, 5])
+def test_rhs3d_f32(oracle_mod, name, P):
+    phys = C.PHYSICS_3D[name]()
+    s, o = make_pair(oracle_mod, phys, P, N3, L3, C.BCS_3D["walls"], prec="f32")
+    q = C.random_state(s.shape, phys, seed=11)
+    qf = q.astype(np.float32).astype(np.float64)
+    assert C.rel_err(s.rhs(qf), o.rhs(qf)) <= C.TOL_F32
+
+
+@pytest.mark.parametrize("limiter", [False, True])
+@pytest.mark.parametrize("P", [2, 4])
+def test_ssprk3_steps_f64(oracle_mod, P, limiter):
+    phys = C.PHYSICS_3D["euler_hllec_fix"]()
+    s, o = make_pair(oracle_mod, phys, P, N3, L3, C.BCS_3D["outflow_x_wall_yz"])
+    q = C.random_state(s.shape, phys, seed=3)
+    s.upload_state(q)
+    o.set(q)
+    if limiter:
+        s.enable_cell_limiter(True, 0.05)
+        o.enable_limiter(True, 0.05)
+    dt = 2e-3
+    s.step_n(dt, 3)
+    o.step(dt, 3)
+    assert C.rel_err(s.download_state(0), o.get(0)) <= 50 * C.TOL_F64_3D[P]
+
+
+@pytest.mark.parametrize("P", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("name", list(C.PHYSICS_2D))
+def test_rhs2d_f64(oracle_mod, name, P):
+    phys = C.PHYSICS_2D[name]()
+    for bcname in ("periodic", "inflow_outflow"):
+        s, o = make_pair(oracle_mod, phys, P, N2, L2, C.BCS_2D[bcname], dim=2)
+        q = C.random_state(s.shape, phys, seed=21 + P)
+        assert C.rel_err(s.rhs(q), o.rhs(q)) <= C.TOL_F64_2D[P], bcname
+
+
+@pytest.mark.parametrize("P", [2, 3])
+@pytest.mark.parametrize("bcname", list(C.BCS_2D))
+def test_ssprk3_2d_limited(oracle_mod, bcname, P):
+    phys = C.PHYSICS_2D["euler_hllc"]()
+    s, o = make_pair(oracle_mod, phys, P, N2, L2, C.BCS_2D[bcname], dim=2)
+    q = C.random_state(s.shape, phys, seed=5)
+    s.upload_state(q)
+    o.set(q)
+    s.enable_cell_limiter(True, 0.02)
+    o.enable_limiter(True, 0.02)
+    s.step_n(1e-3, 2)
+    o.step(1e-3, 2)
+    assert C.rel_err(s.download_state(0), o.get(0)) <= 50 * C.TOL_F64_2D[P]
+
+
+def test_limiter_alone_3d(oracle_mod):
+    phys = C.PHYSICS_3D["euler_hllec"]()
+    s, o = make_pair(oracle_mod, phys, 3, N3, L3, C.BCS_3D["walls"])
+    q = C.random_state(s.shape, phys, seed=9)
+    s.upload_state(q)
+    o.set(q)
+    s.enable_cell_limiter(True, 0.01)
+    o.enable_limiter(True, 0.01)
+    s.limit(0)
+    o.limit(0)
+    out = s.download_state(0)
+    assert C.rel_err(out, o.get(0)) <= 1e-13
+    assert np.abs(out - q).max() > 1e-3  # the limiter fired
+
+
+def test_node_xyz(oracle_mod):
+    for dim, n, L in ((3, N3, L3), (2, N2, L2)):
+        phys = M.Advection(1.0, 0.5, 0.0)
+        s, o = make_pair(oracle_mod, phys, 3, n, L, (0,) * (2 * dim), dim=dim)
+        x_gpu = s.node_xyz()
+        x_cpu = o.node_xyz() if dim == 3 else o.node_xy()
+        assert np.abs(x_gpu - x_cpu).max() < 1e-14
+
+
+def test_reductions_and_wavespeed(oracle_mod):
+    phys = C.PHYSICS_3D["euler_hllec"]()
+    s, o = make_pair(oracle_mod, phys, 3, N3, L3, C.BCS_3D["inflow_outflow"])
+    q = C.random_state(s.shape, phys, seed=13)
+    s.upload_state(q)
+    o.set(q)
+    w = oracle_mod.refelem3d(3)["w"]
+    vol = (L3[0] / N3[0]) * (L3[1] / N3[1]) * (L3[2] / N3[2]) / 6.0
+    for c in range(5):
+        want = vol * float((q[..., c] * w[None, :]).sum())
+        assert abs(s.integral(c) - want) <= 1e-13 * abs(want)
+        assert abs(s.integral(c, kind=2) - np.abs(q[..., c]).max()) == 0.0
+    assert abs(s.max_wavespeed() - o.max_face_speed()) <= 1e-13 * o.max_face_speed()
