@@ -45,9 +45,40 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=32, help="cubes per axis")
     ap.add_argument("--P", type=int, default=3)
-    ap.add_argument("--precision", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32", "mixed"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--l2-steps", type=int, default=100,
+                    help="SSPRK3 steps of the accuracy check vs the FP64 path (0 = skip)")
     return ap.parse_args()
+
+
+def accuracy_check(M, a, q0, dt):
+    """L2 error of the benchmarked precision after `l2_steps` SSPRK3 steps,
+    relative to the FP64 kernels (parity-checked against the FP64 oracle)
+    and to the exact translated wave."""
+    mesh = M.Mesh(a.n, a.n, a.n, 1.0, 1.0, 1.0)
+    phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_RUSANOV, False)
+    ref = M.Solver(mesh, phys, P=a.P, precision="f64")
+    ref.upload_state(q0)
+    ref.step_n(dt, a.l2_steps)
+    q64 = ref.download_state(0)
+    xyz = ref.node_xyz()
+    ref.close()
+    out = {"steps": a.l2_steps}
+    if a.precision != "f64":
+        s = M.Solver(mesh, phys, P=a.P, precision=a.precision)
+        s.upload_state(q0)
+        s.step_n(dt, a.l2_steps)
+        qp = s.download_state(0).astype(np.float64)
+        s.close()
+        out["rel_l2_vs_f64"] = float(np.sqrt(((qp - q64) ** 2).sum() / (q64 ** 2).sum()))
+    else:
+        qp = q64
+    t = a.l2_steps * dt
+    exact = smooth_wave_state(xyz - t)  # translation with u = (1,1,1)
+    out["rel_l2_vs_exact"] = float(np.sqrt(((qp - exact) ** 2).sum() / (exact ** 2).sum()))
+    out["rel_l2_f64_vs_exact"] = float(np.sqrt(((q64 - exact) ** 2).sum() / (exact ** 2).sum()))
+    return out
 
 
 def smooth_wave_state(xyz):
@@ -68,7 +99,11 @@ def dt_for(n, P, cfl=0.1):
 
 def workload_name(a):
     return (f"3D Euler smooth density wave, periodic [0,1]^3 Kuhn mesh {a.n}^3x6 = {6 * a.n ** 3} tets, "
-            f"P={a.P}, Rusanov, {a.precision.upper()}")
+            f"P={a.P}, Rusanov, " + {"f64": "FP64", "f32": "FP32",
+                                     "mixed": "FP32 state + split-BF16 tcgen05 contraction"}[a.precision])
+
+
+DTYPE = {"f64": "f64", "f32": "f32", "mixed": "f32+bf16x3"}
 
 
 class ClockSampler:
@@ -173,7 +208,8 @@ def run_reference(a, rank, world):
     cb = cpu_baseline(a, a.cpu_seconds)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": a.precision, "data": "synthetic", "config": {"workload": workload_name(a), "sample": cb["sample"]},
+            "dtype": DTYPE[a.precision], "data": "synthetic",
+            "config": {"workload": workload_name(a), "sample": cb["sample"]},
             "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -257,18 +293,21 @@ def main():
         achieved = alg_bytes / avg_launch_s / 1e9
         nsm_flops = 2 * (3 * s.NP + 4 * s.NFP) * dof  # contraction flops per stage
         cb = cpu_baseline(a, a.cpu_seconds)
+        acc = accuracy_check(M, a, q0, dt) if a.l2_steps > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": a.precision, "data": "synthetic",
+            "dtype": DTYPE[a.precision], "data": "synthetic",
             "config": {"workload": workload_name(a), "elements": s.num_elements, "NP": s.NP, "NC": s.NC,
+                       "accuracy": acc,
                        "dof_per_stage": dof, "dt": dt, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2: 3 state buffers of "
                              f"{qbytes / 1e6:.0f} MB each (L2 126 MB), no flush"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic_per_launch(a),
                          "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                         "kernel": "stage3d_kernel", "alg_bytes_per_launch": alg_bytes,
+                         "kernel": "stage3d_tc_kernel" if a.precision == "mixed" else "stage3d_kernel",
+                         "alg_bytes_per_launch": alg_bytes,
                          "contraction_tflops": nsm_flops / avg_launch_s / 1e12},
             "cpu_baseline": cb,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": qbytes,

@@ -10,6 +10,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/mxm_dg.h"
@@ -17,6 +18,7 @@
 #include "physics.cuh"
 #include "physics2d.cuh"
 #include "refops.hpp"
+#include "tc.cuh"
 
 namespace mxm {
 
@@ -55,6 +57,9 @@ struct Handle {
   double* partial = nullptr;
   double* dscalar = nullptr;
   unsigned long long* uscalar = nullptr;
+  int* derr = nullptr;  // device error word written by bounded waits
+  bool use_tc = false;  // MIXED precision: tensor-core contraction
+  void* tcimg = nullptr;  // operator image (bf16 hi | lo) in the UMMA layout
   int npartial = 1024;
   bool lim_on = false;
   double lim_eps = 0.1;
@@ -73,6 +78,40 @@ struct Handle {
 
 static std::mutex g_err_mu;
 static std::string g_create_err;
+
+// round-to-nearest-even float -> bfloat16 bits (finite inputs)
+static uint16_t bf16_bits(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return uint16_t(u >> 16);
+}
+static float bf16_value(uint16_t b) {
+  uint32_t u = uint32_t(b) << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+// Shared operator A (NP x K, row-major, FP64) as the tensor-core B operand:
+// N = NP rounded up to 16 rows, K rounded up to 16, K-major no-swizzle
+// core-matrix layout, split into a bfloat16 hi image followed by a lo image
+// (a = hi + lo); padding entries are zero.
+static std::vector<unsigned char> tc_operator_image(const std::vector<double>& A, int NP, int K) {
+  const int NN = (NP + 15) / 16 * 16, KP = (K + 15) / 16 * 16;
+  const size_t half = size_t(NN) * KP * 2;
+  std::vector<unsigned char> img(2 * half, 0);
+  for (int i = 0; i < NN; ++i)
+    for (int k = 0; k < KP; ++k) {
+      const double v = (i < NP && k < K) ? A[size_t(i) * K + k] : 0.0;
+      const uint16_t hi = bf16_bits(float(v));
+      const uint16_t lo = bf16_bits(float(v - double(bf16_value(hi))));
+      const size_t off = umma_tile_offset(i, k, NN);
+      std::memcpy(&img[off], &hi, 2);
+      std::memcpy(&img[half + off], &lo, 2);
+    }
+  return img;
+}
 
 template <class R>
 KuhnTab3<R>& tab3(Handle* h);
@@ -99,10 +138,13 @@ void fill_tab3(Handle* h, KuhnTab3<R>& t) {
       t.axis[a][lf] = int8_t(k.axis[a][lf]);
       t.dir[a][lf] = int8_t(k.dir[a][lf]);
       for (int d = 0; d < 3; ++d) t.normal[a][lf][d] = R(k.normal[a][lf][d]);
+      t.fscale[a][lf] = R((k.side[a][lf] == 0 ? 1.0 : -1.0) * k.area[a][lf] * k.inv6V[a]);
       for (int m = 0; m < h->NFP; ++m) t.nb_node[a][lf][m] = uint8_t(k.nb_node[(a * 4 + lf) * h->NFP + m]);
     }
   for (int lf = 0; lf < 4; ++lf)
     for (int m = 0; m < h->NFP; ++m) t.own_node[lf][m] = uint8_t(h->ref.face_nodes[lf * h->NFP + m]);
+  for (int a = 0; a < 6; ++a)
+    for (int q = 0; q < 9; ++q) t.invJ[a][q] = R(k.invJ[a][q]);
 }
 
 template <class R>
@@ -117,10 +159,13 @@ void fill_tab2(Handle* h, KuhnTab2<R>& t) {
       t.axis[a][lf] = int8_t(k.axis[a][lf]);
       t.dir[a][lf] = int8_t(k.dir[a][lf]);
       for (int d = 0; d < 2; ++d) t.normal[a][lf][d] = R(k.normal[a][lf][d]);
+      t.fscale[a][lf] = R((k.side[a][lf] == 0 ? 1.0 : -1.0) * k.length[a][lf] * k.inv2A[a]);
       for (int m = 0; m < h->NFP; ++m) t.nb_node[a][lf][m] = uint8_t(k.nb_node[(a * 3 + lf) * h->NFP + m]);
     }
   for (int lf = 0; lf < 3; ++lf)
     for (int m = 0; m < h->NFP; ++m) t.own_node[lf][m] = uint8_t(h->ref.face_nodes[((lf + 2) % 3) * h->NFP + m]);
+  for (int a = 0; a < 2; ++a)
+    for (int q = 0; q < 4; ++q) t.invJ[a][q] = R(k.invJ[a][q]);
 }
 
 // ---------------------------------------------------------------- dispatch
@@ -145,11 +190,20 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
     ar.ncell = int(h->ncell);
     for (int k = 0; k < 6; ++k) ar.bc[k] = h->bc[k];
     ar.rhs_only = rhs_only;
+    ar.err = h->derr;
     const KuhnTab3<R>& t = tab3<R>(h);
+    // MIXED precision routes the 3D stage through the tensor-core kernel
+    auto go = [&](const auto& ph) -> cudaError_t {
+      if constexpr (std::is_same<R, float>::value) {
+        if (h->use_tc)
+          return launch_stage3d_tc(h->P, ar, t, ph, (const unsigned char*)h->tcimg, h->nsm, h->stream);
+      }
+      return launch_stage3d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+    };
     switch (h->phys.kind) {
       case MXM_DG_PHYS_ADVECTION: {
         AdvectionD<R> ph{R(p[0]), R(p[1]), R(p[2]), R(p[3])};
-        return launch_stage3d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+        return go(ph);
       }
       case MXM_DG_PHYS_EULER: {
         auto mk = [&](auto ph) {
@@ -157,7 +211,7 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
           ph.gx = R(p[3]); ph.gy = R(p[4]); ph.gz = R(p[5]);
           for (int k = 0; k < 5; ++k) ph.inflow[k] = R(p[6 + k]);
           ph.entropy_fix = h->phys.entropy_fix;
-          return launch_stage3d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+          return go(ph);
         };
         switch (h->phys.flux_type) {
           case MXM_DG_FLUX_RUSANOV: return mk(EulerD<R, FLUX_RUSANOV>{});
@@ -172,13 +226,13 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
         ph.c = R(p[0]);
         for (int k = 0; k < 3; ++k) { ph.J[k] = R(p[1 + k]); ph.M[k] = R(p[4 + k]); }
         for (int k = 0; k < 6; ++k) ph.inflow[k] = R(p[7 + k]);
-        return launch_stage3d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+        return go(ph);
       }
       case MXM_DG_PHYS_SHALLOW_WATER: {
         ShallowWaterD<R> ph;
         ph.g = R(p[0]); ph.h_min = R(p[1]);
         for (int k = 0; k < 3; ++k) ph.inflow[k] = R(p[2 + k]);
-        return launch_stage3d<R>(h->P, ar, t, ph, h->nsm, h->stream);
+        return go(ph);
       }
     }
     return cudaErrorInvalidValue;
@@ -197,6 +251,7 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
   ar.ncell = int(h->ncell);
   for (int k = 0; k < 4; ++k) ar.bc[k] = h->bc[k];
   ar.rhs_only = rhs_only;
+  ar.err = h->derr;
   const KuhnTab2<R>& t = tab2<R>(h);
   switch (h->phys.kind) {
     case MXM_DG_PHYS_ADVECTION: {
@@ -422,6 +477,8 @@ void destroy(Handle* h) {
   cudaFree(h->partial);
   cudaFree(h->dscalar);
   cudaFree(h->uscalar);
+  cudaFree(h->derr);
+  cudaFree(h->tcimg);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -430,8 +487,8 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   if (!m || !ph) throw ArgError("null descriptor");
   if (m->dim != 2 && m->dim != 3) throw ArgError("mesh dim must be 2 or 3");
   if (P < 1 || P > 5) throw ArgError("order P must be in 1..5");
-  if (prec != MXM_DG_PREC_F64 && prec != MXM_DG_PREC_F32)
-    throw ArgError("precision must be MXM_DG_PREC_F64 or MXM_DG_PREC_F32 for a single-solve handle");
+  if (prec != MXM_DG_PREC_F64 && prec != MXM_DG_PREC_F32 && prec != MXM_DG_PREC_MIXED)
+    throw ArgError("precision must be MXM_DG_PREC_F64, MXM_DG_PREC_F32 or MXM_DG_PREC_MIXED");
   if (ph->kind < 0 || ph->kind > 3) throw ArgError("unknown physics kind");
   if (m->nx < 1 || m->ny < 1 || (m->dim == 3 && m->nz < 1)) throw ArgError("cell counts must be >= 1");
   for (int k = 0; k < 2 * m->dim; ++k)
@@ -465,18 +522,20 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   h->ne = h->ncell * h->ntypes;
   if (h->ne > (int64_t(1) << 31) / 64) throw ArgError("mesh too large for 32-bit cell indexing");
   h->rbytes = prec == MXM_DG_PREC_F64 ? 8 : 4;
+  // split-BF16 tensor-core contraction for the 3D orders it is built for
+  h->use_tc = prec == MXM_DG_PREC_MIXED && m->dim == 3 && P >= 2 && P <= 4;
   h->ref = build_refops(h->dim, P);
   h->NP = h->ref.NP;
   h->NFP = h->ref.NFP;
   if (h->dim == 3) {
     h->k3 = build_kuhn3d(h->ref, h->lx / h->nx, h->ly / h->ny, h->lz / h->nz);
-    h->Ahost = fused_operator_3d(h->ref, h->k3);
+    h->Ahost = shared_operator(h->ref);
     h->K = 3 * h->NP + 4 * h->NFP;
     fill_tab3<double>(h.get(), h->t3d);
     fill_tab3<float>(h.get(), h->t3f);
   } else {
     h->k2 = build_kuhn2d(h->ref, h->lx / h->nx, h->ly / h->ny);
-    h->Ahost = fused_operator_2d(h->ref, h->k2);
+    h->Ahost = shared_operator(h->ref);
     h->K = 2 * h->NP + 3 * h->NFP;
     fill_tab2<double>(h.get(), h->t2d);
     fill_tab2<float>(h.get(), h->t2f);
@@ -492,11 +551,9 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
       CK(cudaMemsetAsync(b, 0, raw->qbytes(), raw->stream));
     }
     // fused operators, k-major per type, in the handle's real type
-    std::vector<double> At(size_t(raw->ntypes) * raw->K * raw->NP);
-    for (int t = 0; t < raw->ntypes; ++t)
-      for (int i = 0; i < raw->NP; ++i)
-        for (int k = 0; k < raw->K; ++k)
-          At[(size_t(t) * raw->K + k) * raw->NP + i] = raw->Ahost[(size_t(t) * raw->NP + i) * raw->K + k];
+    std::vector<double> At(size_t(raw->K) * raw->NP);  // k-major copy of the shared operator
+    for (int i = 0; i < raw->NP; ++i)
+      for (int k = 0; k < raw->K; ++k) At[size_t(k) * raw->NP + i] = raw->Ahost[size_t(i) * raw->K + k];
     auto upload = [&](void** dst, const std::vector<double>& src) {
       CK(cudaMalloc(dst, src.size() * raw->rbytes));
       if (raw->rbytes == 8) {
@@ -508,10 +565,17 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
     };
     upload(&raw->A, At);
     upload(&raw->w, raw->ref.w);
+    if (raw->use_tc) {
+      auto img = tc_operator_image(raw->Ahost, raw->NP, raw->K);
+      CK(cudaMalloc(&raw->tcimg, img.size()));
+      CK(cudaMemcpy(raw->tcimg, img.data(), img.size(), cudaMemcpyHostToDevice));
+    }
     CK(cudaMalloc(&raw->avg, size_t(raw->ne) * raw->NC * raw->rbytes));
     CK(cudaMalloc(&raw->partial, raw->npartial * sizeof(double)));
     CK(cudaMalloc(&raw->dscalar, 4 * sizeof(double)));
     CK(cudaMalloc(&raw->uscalar, 4 * sizeof(unsigned long long)));
+    CK(cudaMalloc(&raw->derr, sizeof(int)));
+    CK(cudaMemsetAsync(raw->derr, 0, sizeof(int), raw->stream));
     CK(cudaStreamSynchronize(raw->stream));
   } catch (...) {
     h.release();
@@ -800,6 +864,13 @@ int mxm_dg_synchronize(void* handle) {
   API_BEGIN
   CK(cudaStreamSynchronize(h->stream));
   CK(cudaGetLastError());
+  int derr = 0;
+  CK(cudaMemcpy(&derr, h->derr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (derr) {
+    CK(cudaMemset(h->derr, 0, sizeof(int)));
+    h->err = "a stage kernel's bounded wait for its state tile gave up";
+    return MXM_DG_ETIMEDOUT;
+  }
   API_END
 }
 

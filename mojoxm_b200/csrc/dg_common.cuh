@@ -17,6 +17,9 @@ enum : int { FLUX_RUSANOV = 0, FLUX_ROE = 1, FLUX_HLLE = 2, FLUX_HLLEC = 3, FLUX
 // parameter (lives in the constant bank; ~1.7 KB).
 template <class R>
 struct KuhnTab3 {
+  R normal[6][4][3];  // unit normal, side 0 -> side 1
+  R invJ[6][9];       // d(r,s,t)/d(x,y,z) per tet type, [k][d]
+  R fscale[6][4];     // side_sign * face area / (6 V)
   int8_t nb_t[6][4];
   int8_t off[6][4][3];
   int8_t side[6][4];
@@ -24,11 +27,13 @@ struct KuhnTab3 {
   int8_t dir[6][4];
   uint8_t own_node[4][kMaxNFP3];
   uint8_t nb_node[6][4][kMaxNFP3];
-  R normal[6][4][3];
 };
 
 template <class R>
 struct KuhnTab2 {
+  R normal[2][3][2];
+  R invJ[2][4];    // d(r,s)/d(x,y) per triangle type, [k][d]
+  R fscale[2][3];  // side_sign * edge length / (2 A)
   int8_t nb_t[2][3];
   int8_t off[2][3][2];
   int8_t side[2][3];
@@ -36,7 +41,6 @@ struct KuhnTab2 {
   int8_t dir[2][3];
   uint8_t own_node[3][kMaxNFP2];
   uint8_t nb_node[2][3][kMaxNFP2];
-  R normal[2][3][2];
 };
 
 // Face treatment for an element's face, resolved from the cell position and
@@ -51,7 +55,9 @@ enum : int { FACE_INTERIOR = 0, FACE_BC_HI = 1, FACE_BC_LO = 2, FACE_MIXED = 3 }
 __device__ __forceinline__ int face_mode(int axis, int dir, int cpos, int ncell_axis, const int* bc, int& code) {
   code = 0;
   if (axis < 0) return FACE_INTERIOR;
-  const int lo = bc[2 * axis], hi = bc[2 * axis + 1];
+  // constant indices keep a by-value bc[] in the parameter bank (no local copy)
+  const int lo = axis == 0 ? bc[0] : (axis == 1 ? bc[2] : bc[4]);
+  const int hi = axis == 0 ? bc[1] : (axis == 1 ? bc[3] : bc[5]);
   if (dir > 0) {
     if (cpos == ncell_axis - 1 && hi != 0) {
       code = hi;
@@ -81,12 +87,13 @@ struct Stage3DArgs {
   const R* q_a;
   const R* q_b;
   R* q_out;
-  const R* A;  // [6][K][NP] fused operators, k-major (transposed)
+  const R* A;  // [K][NP] shared operator [D_r|D_s|D_t|-Lift_0..3], k-major
   R a, b, cdt;
   int nx, ny, nz;
   int ncell;
   int bc[6];
   int rhs_only;
+  int* err;  // device error word (bounded waits that gave up set bit 0)
 };
 
 template <class R>
@@ -95,12 +102,13 @@ struct Stage2DArgs {
   const R* q_a;
   const R* q_b;
   R* q_out;
-  const R* A;  // [2][K][NP] k-major
+  const R* A;  // [K][NP] shared operator [D_r|D_s|-Lift_0..2], k-major
   R a, b, cdt;
   int nx, ny;
   int ncell;
   int bc[4];
   int rhs_only;
+  int* err;
 };
 
 template <class R>
@@ -121,6 +129,11 @@ cudaError_t launch_stage3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& ta
 template <class R, class Phys>
 cudaError_t launch_wavespeed3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phys& ph,
                                unsigned long long* out, cudaStream_t st);
+// Tensor-core (split-BF16 tcgen05) 3D stage for FP32 state, P = 2..4;
+// `img` is the operator image built by tc_operator_image().
+template <class Phys>
+cudaError_t launch_stage3d_tc(int P, const Stage3DArgs<float>& a, const KuhnTab3<float>& tab, const Phys& ph,
+                              const unsigned char* img, int nsm, cudaStream_t st);
 template <class R, class Phys>
 cudaError_t launch_stage2d(int P, const Stage2DArgs<R>& a, const KuhnTab2<R>& tab, const Phys& ph, int nsm,
                            cudaStream_t st);

@@ -306,44 +306,21 @@ Kuhn2D build_kuhn2d(const RefOps& r, double dx, double dy) {
   return k;
 }
 
-std::vector<double> fused_operator_3d(const RefOps& r, const Kuhn3D& k) {
-  const int NP = r.NP, NFP = r.NFP, K = 3 * NP + 4 * NFP;
-  std::vector<double> A(6 * NP * K, 0.0);
-  for (int t = 0; t < 6; ++t)
-    for (int i = 0; i < NP; ++i) {
-      double* row = &A[(t * NP + i) * K];
-      for (int d = 0; d < 3; ++d)
-        for (int j = 0; j < NP; ++j) {
-          double s = 0.0;
-          for (int kk = 0; kk < 3; ++kk) s += k.invJ[t][kk * 3 + d] * r.D[(kk * NP + i) * NP + j];
-          row[d * NP + j] = s;
-        }
-      for (int lf = 0; lf < 4; ++lf) {
-        const double sc = (k.side[t][lf] == 0 ? 1.0 : -1.0) * k.area[t][lf] * k.inv6V[t];
-        for (int m = 0; m < NFP; ++m) row[3 * NP + lf * NFP + m] = -sc * r.Lift[(lf * NP + i) * NFP + m];
-      }
+std::vector<double> shared_operator(const RefOps& r) {
+  // [D_0 | .. | D_{dim-1} | -Lift_0 | .. | -Lift_{nf-1}]  (NP x K), one
+  // operator for every element type.  2D local edge lf joins vertices
+  // (lf, lf+1), i.e. RefOps face (lf+2)%3.
+  const int NP = r.NP, NFP = r.NFP, dim = r.dim, nf = r.NF, K = dim * NP + nf * NFP;
+  std::vector<double> A(size_t(NP) * K, 0.0);
+  for (int i = 0; i < NP; ++i) {
+    double* row = &A[size_t(i) * K];
+    for (int d = 0; d < dim; ++d)
+      for (int j = 0; j < NP; ++j) row[d * NP + j] = r.D[(d * NP + i) * NP + j];
+    for (int lf = 0; lf < nf; ++lf) {
+      const int fo = dim == 2 ? (lf + 2) % 3 : lf;
+      for (int m = 0; m < NFP; ++m) row[dim * NP + lf * NFP + m] = -r.Lift[(fo * NP + i) * NFP + m];
     }
-  return A;
-}
-
-std::vector<double> fused_operator_2d(const RefOps& r, const Kuhn2D& k) {
-  const int NP = r.NP, NFP = r.NFP, K = 2 * NP + 3 * NFP;
-  std::vector<double> A(2 * NP * K, 0.0);
-  for (int t = 0; t < 2; ++t)
-    for (int i = 0; i < NP; ++i) {
-      double* row = &A[(t * NP + i) * K];
-      for (int d = 0; d < 2; ++d)
-        for (int j = 0; j < NP; ++j) {
-          double s = 0.0;
-          for (int kk = 0; kk < 2; ++kk) s += k.invJ[t][kk * 2 + d] * r.D[(kk * NP + i) * NP + j];
-          row[d * NP + j] = s;
-        }
-      for (int lf = 0; lf < 3; ++lf) {
-        const int fo = (lf + 2) % 3;
-        const double sc = (k.side[t][lf] == 0 ? 1.0 : -1.0) * k.length[t][lf] * k.inv2A[t];
-        for (int m = 0; m < NFP; ++m) row[2 * NP + lf * NFP + m] = -sc * r.Lift[(fo * NP + i) * NFP + m];
-      }
-    }
+  }
   return A;
 }
 

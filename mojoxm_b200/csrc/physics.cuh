@@ -36,12 +36,12 @@ struct AdvectionD {
     f[0] = R(0.5) * ((nc + a) * ql[0] + (nc - a) * qr[0]);
     return a;
   }
+  // ghost state of a boundary face: the BC flux is num_flux(q, ghost)
+  __device__ void ghost(const R*, int bc, R, R, R, R* g) const { g[0] = (bc == BC_INFLOW) ? inflow_q : R(0); }
   __device__ R bnd_flux(const R* q, int bc, R nx, R ny, R nz, R* f) const {
-    R nc = vx * nx + vy * ny + vz * nz;
-    R a = rabs(nc);
-    R g = (bc == BC_INFLOW) ? inflow_q : R(0);
-    f[0] = R(0.5) * ((nc + a) * q[0] + (nc - a) * g);
-    return a;
+    R g[1];
+    ghost(q, bc, nx, ny, nz, g);
+    return num_flux(q, g, nx, ny, nz, f);
   }
   __device__ void source(const R*, R* s) const { s[0] = R(0); }
   __device__ void limit(R*) const {}
@@ -237,6 +237,10 @@ struct EulerD {
   }
   __device__ R bnd_flux(const R* q, int bc, R nx, R ny, R nz, R* f) const {  // euler.mojo:705-730
     R g[5];
+    ghost(q, bc, nx, ny, nz, g);
+    return num_flux(q, g, nx, ny, nz, f);
+  }
+  __device__ void ghost(const R* q, int bc, R nx, R ny, R nz, R* g) const {
     if (bc == BC_WALL) {
       R mn = q[1] * nx + q[2] * ny + q[3] * nz;
       g[0] = q[0]; g[4] = q[4];
@@ -248,7 +252,6 @@ struct EulerD {
 #pragma unroll
       for (int c = 0; c < 5; ++c) g[c] = q[c];
     }
-    return num_flux(q, g, nx, ny, nz, f);
   }
   __device__ void source(const R* q, R* s) const {  // euler.mojo:738-747
     s[0] = R(0);
@@ -300,6 +303,10 @@ struct MaxwellD {
   }
   __device__ R bnd_flux(const R* q, int bc, R nx, R ny, R nz, R* f) const {  // maxwell.mojo:213-240
     R g[6];
+    ghost(q, bc, nx, ny, nz, g);
+    return num_flux(q, g, nx, ny, nz, f);
+  }
+  __device__ void ghost(const R* q, int bc, R nx, R ny, R nz, R* g) const {
     if (bc == BC_WALL) {
       R En = q[0] * nx + q[1] * ny + q[2] * nz, Bn = q[3] * nx + q[4] * ny + q[5] * nz;
       g[0] = R(2) * En * nx - q[0]; g[1] = R(2) * En * ny - q[1]; g[2] = R(2) * En * nz - q[2];
@@ -311,7 +318,6 @@ struct MaxwellD {
 #pragma unroll
       for (int k = 0; k < 6; ++k) g[k] = q[k];
     }
-    return num_flux(q, g, nx, ny, nz, f);
   }
   __device__ void source(const R*, R* s) const {  // maxwell.mojo:245-252
     R c2 = c * c;
@@ -348,6 +354,10 @@ struct ShallowWaterD {
   }
   __device__ R bnd_flux(const R* q, int bc, R nx, R ny, R nz, R* f) const {  // shallow_water.mojo:138-156
     R gs[3];
+    ghost(q, bc, nx, ny, nz, gs);
+    return num_flux(q, gs, nx, ny, nz, f);
+  }
+  __device__ void ghost(const R* q, int bc, R nx, R ny, R, R* gs) const {
     if (bc == BC_WALL) {
       R mn = q[1] * nx + q[2] * ny;
       gs[0] = q[0]; gs[1] = q[1] - R(2) * mn * nx; gs[2] = q[2] - R(2) * mn * ny;
@@ -356,7 +366,6 @@ struct ShallowWaterD {
     } else {
       gs[0] = q[0]; gs[1] = q[1]; gs[2] = q[2];
     }
-    return num_flux(q, gs, nx, ny, nz, f);
   }
   __device__ void source(const R*, R* s) const { s[0] = s[1] = s[2] = R(0); }
   __device__ void limit(R*) const {}

@@ -68,11 +68,11 @@ struct Kuhn2D {
 };
 Kuhn2D build_kuhn2d(const RefOps& r, double dx, double dy);
 
-// Fused per-type operator A_t = [D_x | D_y (| D_z) | -Lift_scaled]
-// ([ntypes][NP][K]) with D_phys = sum_k invJ[k][d] D_k and
-// Lift_scaled = side_sign * area * 1/(6V) * Lift (3D) or
-// side_sign * length * 1/(2A) * Lift (2D).
-std::vector<double> fused_operator_3d(const RefOps& r, const Kuhn3D& k);
-std::vector<double> fused_operator_2d(const RefOps& r, const Kuhn2D& k);
+// Operator shared by every element type, row-major NP x K:
+// A = [D_r | D_s (| D_t) | -Lift_0 | ... ] with lift columns in face_nodes
+// order (2D: local edge lf = RefOps face (lf+2)%3).  The kernels apply the
+// per-type invJ to nodal fluxes and side*area/(6V) (3D) or
+// side*length/(2A) (2D) to f*.
+std::vector<double> shared_operator(const RefOps& r);
 
 }  // namespace mxm

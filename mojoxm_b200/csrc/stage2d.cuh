@@ -3,14 +3,18 @@
 // Replaces the reference's two launches per stage -- *_face_flux_kernel_2d
 // (one thread per (face, slot) writing fstar to global memory) and
 // *_vol_lift_combine_rk_kernel_2d (src/local_mesh_2d_gpu_euler.mojo:33-144
-// and siblings) -- with one kernel: a block owns one triangle type (2 per
-// cell), stages the fused operator A_t = [D_x | D_y | -Lift_t] once, and per
-// element evaluates volume fluxes and its 3 edges' numerical fluxes into a
-// shared B tile, then rhs = A_t B + source and the RK combine.  Face traces
-// never touch global memory; connectivity is implicit in (cell, type).
+// and siblings) -- with one kernel.  A block owns EC whole cells (2
+// triangles each, one contiguous span of q, bulk-copied into a
+// double-buffered shared tile), keeps one shared operator
+// A = [D_r | D_s | -Lift_0..2] for both triangle types (invJ applied to the
+// nodal flux, side*length/(2A) to f*), evaluates volume fluxes and its
+// edges' numerical fluxes into a shared B tile (the diagonal's neighbour
+// trace comes from the tile), then rhs = A B + source and the RK combine.
+// Face traces never touch global memory; connectivity is implicit.
 #pragma once
 #include "dg_common.cuh"
 #include "physics2d.cuh"
+#include "tma.cuh"
 
 namespace mxm {
 
@@ -22,84 +26,125 @@ struct Stage2DShape {
   static constexpr int BSTR = BSTR_RAW + ((1 - BSTR_RAW % BMOD) + BMOD) % BMOD;
 };
 
-template <class R, class Phys, int P, int RI, int EB, int NT>
-__global__ void __launch_bounds__(NT) stage2d_kernel(Stage2DArgs<R> args, KuhnTab2<R> tab, Phys ph) {
+constexpr uint64_t kWaitLimitNs2 = 2000000000ull;
+
+template <class R, class Phys, int P, int EC, int RI, int NT>
+__global__ void __launch_bounds__(NT) stage2d_kernel(Stage2DArgs<R> args, KuhnTab2<R> tabp, Phys ph) {
   constexpr int NC = Phys::NC;
   using S = Stage2DShape<P, NC, R>;
   constexpr int NP = S::NP, NFP = S::NFP, K = S::K, BSTR = S::BSTR;
-  constexpr int G = NP / RI;
+  constexpr int EB = 2 * EC, G = NP / RI, QV = EB * NP * NC;
+  constexpr bool BULK = (2 * NP * NC * sizeof(R)) % 16 == 0;
   static_assert(NP % RI == 0, "row tile must divide NP");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* sA = reinterpret_cast<R*>(smem_raw);  // [K][NP]
-  R* sQ = sA + K * NP;                     // [EB][NP][NC]
-  R* sB = sQ + EB * NP * NC;               // [EB][BSTR]
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
+  KuhnTab2<R>* tab = reinterpret_cast<KuhnTab2<R>*>(smem_raw + 16);
+  constexpr size_t kTabBytes = (sizeof(KuhnTab2<R>) + 15) / 16 * 16;
+  R* sQ = reinterpret_cast<R*>(smem_raw + 16 + kTabBytes);  // [2][QV]
+  R* sB = sQ + 2 * QV;                                      // [EB][BSTR]
+  R* sA = sB + EB * BSTR;                                   // [K][NP]
   const int tid = threadIdx.x;
-  const int t = blockIdx.x & 1;
-  const int nblk_t = gridDim.x >> 1;
-  const int ngroups = (args.ncell + EB - 1) / EB;
-  const R* gA = args.A + size_t(t) * K * NP;
-  for (int idx = tid; idx < NP * K; idx += NT) sA[idx] = gA[idx];
+  const int ngroups = (args.ncell + EC - 1) / EC;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  {
+    const int* src = reinterpret_cast<const int*>(&tabp);
+    int* dst = reinterpret_cast<int*>(tab);
+    for (int k = tid; k < int(sizeof(KuhnTab2<R>) / 4); k += NT) dst[k] = src[k];
+  }
+  for (int idx = tid; idx < NP * K; idx += NT) sA[idx] = args.A[idx];
+  __syncthreads();
+  auto issue = [&](int grp, int buf) {
+    const int c0 = grp * EC, nc = min(EC, args.ncell - c0);
+    const uint32_t bytes = uint32_t(nc) * 2u * NP * NC * sizeof(R);
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&bar[buf], bytes);
+    bulk_g2s(sQ + buf * QV, args.q_in + size_t(c0) * 2 * NP * NC, bytes, &bar[buf]);
+  };
+  uint32_t parity[2] = {0u, 0u};
+  int buf = 0;
+  if (BULK && tid == 0 && int(blockIdx.x) < ngroups) issue(blockIdx.x, 0);
 
-  for (int grp = blockIdx.x >> 1; grp < ngroups; grp += nblk_t) {
-    const int cell0 = grp * EB;
-    const int nhere = min(EB, args.ncell - cell0);
-    __syncthreads();
-    for (int idx = tid; idx < EB * NP * NC; idx += NT) {
-      const int el = idx / (NP * NC), r = idx - el * NP * NC;
-      if (el < nhere) sQ[idx] = args.q_in[(size_t(cell0 + el) * 2 + t) * (NP * NC) + r];
+  for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x, buf ^= 1) {
+    const int cell0 = grp * EC;
+    const int ne_here = 2 * min(EC, args.ncell - cell0);
+    R* q = sQ + buf * QV;
+    if (BULK) {
+      const bool ok = mbar_wait_bounded(&bar[buf], parity[buf], kWaitLimitNs2);
+      parity[buf] ^= 1u;
+      if (!__syncthreads_and(ok)) {
+        if (tid == 0 && args.err) atomicOr(args.err, 1);
+        return;
+      }
+      if (tid == 0 && grp + int(gridDim.x) < ngroups) issue(grp + gridDim.x, buf ^ 1);
+    } else {
+      const R* src = args.q_in + size_t(cell0) * 2 * NP * NC;
+      for (int idx = tid; idx < ne_here * NP * NC; idx += NT) q[idx] = src[idx];
+      __syncthreads();
     }
-    __syncthreads();
-    for (int idx = tid; idx < EB * NP; idx += NT) {
-      const int el = idx / NP, j = idx - el * NP;
-      if (el >= nhere) continue;
+    for (int idx = tid; idx < ne_here * NP; idx += NT) {
+      const int el = idx / NP, j = idx - el * NP, t = el & 1;
       R Fx[NC], Fy[NC];
-      ph.flux(&sQ[(el * NP + j) * NC], Fx, Fy);
-      R* b = &sB[el * BSTR];
+      ph.flux(&q[(el * NP + j) * NC], Fx, Fy);
+      const R* iJ = tab->invJ[t];
+      R* b = &sB[el * BSTR + j * NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        b[j * NC + c] = Fx[c];
-        b[(NP + j) * NC + c] = Fy[c];
+        b[c] = iJ[0] * Fx[c] + iJ[1] * Fy[c];
+        b[NP * NC + c] = iJ[2] * Fx[c] + iJ[3] * Fy[c];
       }
     }
-    for (int idx = tid; idx < EB * 3 * NFP; idx += NT) {
+    for (int idx = tid; idx < ne_here * 3 * NFP; idx += NT) {
       const int el = idx / (3 * NFP), fm = idx - el * 3 * NFP;
-      if (el >= nhere) continue;
-      const int lf = fm / NFP, m = fm - lf * NFP;
-      const int cell = cell0 + el;
+      const int lf = fm / NFP, m = fm - lf * NFP, t = el & 1, cl = el >> 1;
+      const int cell = cell0 + cl;
       const int cj = cell / args.nx, ci = cell - cj * args.nx;
-      const int ax = tab.axis[t][lf], dir = tab.dir[t][lf];
-      const int cpos = ax == 0 ? ci : cj;
-      const int nax = ax == 0 ? args.nx : args.ny;
+      const int ax = tab->axis[t][lf], dir = tab->dir[t][lf];
       int code;
-      const int mode = face_mode(ax, dir, cpos, nax, args.bc, code);
-      const R* qo = &sQ[(el * NP + tab.own_node[lf][m]) * NC];
-      const R nx = tab.normal[t][lf][0], ny = tab.normal[t][lf][1];
-      R f[NC];
-      if (mode == FACE_BC_HI) {
-        ph.face(qo, qo, code, nx, ny, f);
-      } else if (mode == FACE_BC_LO) {
-        ph.face(qo, qo, code, -nx, -ny, f);
+      const int mode = face_mode(ax, dir, ax == 0 ? ci : cj, ax == 0 ? args.nx : args.ny, args.bc, code);
+      const R* qo = &q[(el * NP + tab->own_node[lf][m]) * NC];
+      R nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1];
+      R scale = tab->fscale[t][lf];
+      // one face-flux call per face node (the 2D face functions build the
+      // BC ghost state themselves from the left state and the BC code)
+      R qn[NC];
+      if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
+        const int nbt = tab->nb_t[t][lf], nbn = tab->nb_node[t][lf][m];
+        if (ax < 0) {
 #pragma unroll
-        for (int c = 0; c < NC; ++c) f[c] = -f[c];
+          for (int c = 0; c < NC; ++c) qn[c] = q[((cl * 2 + nbt) * NP + nbn) * NC + c];
+        } else {
+          const int ni = wrapi(ci + tab->off[t][lf][0], args.nx), nj = wrapi(cj + tab->off[t][lf][1], args.ny);
+          const R* gq = args.q_in + ((size_t(nj) * args.nx + ni) * 2 * NP + size_t(nbt) * NP + nbn) * NC;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) qn[c] = __ldg(gq + c);
+        }
       } else {
-        const int ni = wrapi(ci + tab.off[t][lf][0], args.nx), nj = wrapi(cj + tab.off[t][lf][1], args.ny);
-        const size_t enb = (size_t(nj) * args.nx + ni) * 2 + tab.nb_t[t][lf];
-        const R* gq = args.q_in + (enb * NP + tab.nb_node[t][lf][m]) * NC;
-        R qn[NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) qn[c] = gq[c];
-        if (mode == FACE_MIXED) ph.face(qn, qn, code, nx, ny, f);
-        else if (tab.side[t][lf] == 0) ph.face(qo, qn, BC_INTERIOR, nx, ny, f);
-        else ph.face(qn, qo, BC_INTERIOR, nx, ny, f);
+        for (int c = 0; c < NC; ++c) qn[c] = qo[c];
       }
+      if (mode == FACE_BC_LO) {
+        nx = -nx;
+        ny = -ny;
+        scale = -scale;
+      }
+      const bool bcf = mode != FACE_INTERIOR;
+      const bool own_left = tab->side[t][lf] == 0;
+      const R* L = bcf ? qn : (own_left ? qo : qn);
+      const R* Rr = bcf ? qn : (own_left ? qn : qo);
+      R f[NC];
+      ph.face(L, Rr, bcf ? code : int(BC_INTERIOR), nx, ny, f);
       R* b = &sB[el * BSTR + (2 * NP + fm) * NC];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) b[c] = f[c];
+      for (int c = 0; c < NC; ++c) b[c] = scale * f[c];
     }
     __syncthreads();
-    for (int w = tid; w < EB * G; w += NT) {
+    const bool a_in = args.q_a == args.q_in, b_in = args.q_b == args.q_in;
+    for (int w = tid; w < ne_here * G; w += NT) {
       const int el = w / G, g = w - el * G;
-      if (el >= nhere) continue;
       const int i0 = g * RI;
       R acc[RI][NC];
 #pragma unroll
@@ -119,18 +164,20 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(Stage2DArgs<R> args, KuhnTa
 #pragma unroll
           for (int c = 0; c < NC; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
       }
-      const size_t e = size_t(cell0 + el) * 2 + t;
+      const size_t e = size_t(cell0) * 2 + el;
 #pragma unroll
       for (int r = 0; r < RI; ++r) {
         const int i = i0 + r;
         const size_t base = (e * NP + i) * NC;
+        const R* ql = &q[(el * NP + i) * NC];
         R src[NC];
-        if (Phys::kSource) ph.source(&sQ[(el * NP + i) * NC], src);
+        if (Phys::kSource) ph.source(ql, src);
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           const R rhs = Phys::kSource ? acc[r][c] + src[c] : acc[r][c];
-          args.q_out[base + c] =
-              args.rhs_only ? rhs : args.a * args.q_a[base + c] + args.b * args.q_b[base + c] + args.cdt * rhs;
+          const R va = a_in ? ql[c] : args.q_a[base + c];
+          const R vb = b_in ? ql[c] : args.q_b[base + c];
+          args.q_out[base + c] = args.rhs_only ? rhs : args.a * va + args.b * vb + args.cdt * rhs;
         }
       }
     }
@@ -142,18 +189,18 @@ struct Cfg2 {
   using S = Stage2DShape<P, NC, R>;
   static constexpr int NP = S::NP;
   static constexpr int RI = P == 1 ? 3 : (P == 2 ? 2 : (P == 3 ? 5 : (P == 4 ? 5 : 3)));  // divisors of 3,6,10,15,21
-  static constexpr size_t kA = sizeof(R) * S::K * S::NP;
-  static constexpr size_t kPerEl = sizeof(R) * (size_t(S::NP) * NC + S::BSTR);
-  static constexpr int EB_RAW = int((96 * 1024 - kA) / kPerEl);
-  static constexpr int EB = EB_RAW > 128 ? 128 : (EB_RAW < 1 ? 1 : EB_RAW);
-  static constexpr int NT = 128;
-  static constexpr size_t kSmem = kA + sizeof(R) * (size_t(EB) * S::NP * NC + size_t(EB) * S::BSTR);
+  static constexpr size_t kFixed = 16 + (sizeof(KuhnTab2<R>) + 15) / 16 * 16 + sizeof(R) * S::K * S::NP;
+  static constexpr size_t kPerCell = 2 * sizeof(R) * (2 * size_t(S::NP) * NC + S::BSTR);
+  static constexpr int EC_RAW = int((100 * 1024 - kFixed) / kPerCell);
+  static constexpr int EC = EC_RAW > 64 ? 64 : (EC_RAW < 1 ? 1 : EC_RAW);
+  static constexpr int NT = 256;
+  static constexpr size_t kSmem = kFixed + sizeof(R) * (2 * size_t(2 * EC) * S::NP * NC + size_t(2 * EC) * S::BSTR);
 };
 
 template <class R, class Phys, int P>
 cudaError_t launch2_p(const Stage2DArgs<R>& a, const KuhnTab2<R>& tab, const Phys& ph, int nsm, cudaStream_t st) {
   using C = Cfg2<R, P, Phys::NC>;
-  auto kern = stage2d_kernel<R, Phys, P, C::RI, C::EB, C::NT>;
+  auto kern = stage2d_kernel<R, Phys, P, C::EC, C::RI, C::NT>;
   static int bps = -1;
   if (bps < 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(C::kSmem));
@@ -162,11 +209,11 @@ cudaError_t launch2_p(const Stage2DArgs<R>& a, const KuhnTab2<R>& tab, const Phy
     if (e != cudaSuccess) return e;
     if (bps < 1) bps = 1;
   }
-  const int ngroups = (a.ncell + C::EB - 1) / C::EB;
-  int per_type = (nsm * bps + 1) / 2;
-  if (per_type > ngroups) per_type = ngroups;
-  if (per_type < 1) per_type = 1;
-  kern<<<2 * per_type, C::NT, C::kSmem, st>>>(a, tab, ph);
+  const int ngroups = (a.ncell + C::EC - 1) / C::EC;
+  int nblk = nsm * bps;
+  if (nblk > ngroups) nblk = ngroups;
+  if (nblk < 1) nblk = 1;
+  kern<<<nblk, C::NT, C::kSmem, st>>>(a, tab, ph);
   return cudaGetLastError();
 }
 

@@ -7,121 +7,171 @@
 // the positivity floor.
 //
 // B200 design:
-//  * A block owns one tet type t (6 per cube) and walks groups of EB cubes,
-//    so it stages ONE fused operator A_t = [D_x|D_y|D_z|-Lift_t] (physical
-//    derivatives with invJ folded in, lift pre-scaled by side*area/(6V)) in
-//    shared memory once, and every element's RHS is a small GEMM
-//    rhs[i][c] = sum_k A_t[i][k] B[k][c] with B = [F_x; F_y; F_z; f*].
-//  * Connectivity is not read from memory: neighbour element and node of
-//    every face node follow from (cube, type) and a 1.7 KB table in the
-//    constant bank (Kuhn meshes are translation invariant); only q moves.
-//  * Element state is staged in shared memory with contiguous loads; the RK
-//    combine reads q_a/q_b and writes q_out per node (NC contiguous values).
+//  * A block owns EC whole cubes (EB = 6*EC consecutive elements, one
+//    contiguous span of q) per iteration of a persistent loop.  The span
+//    arrives by a 1D bulk copy (TMA engine) into a double-buffered shared
+//    tile, prefetched one iteration ahead, completion tracked by an mbarrier
+//    with a bounded wait.
+//  * One operator serves all six tet types: A = [D_r|D_s|D_t|-Lift_0..3]
+//    (NP x K, K = 3NP + 4NFP) lives in shared memory for the block's life;
+//    the per-type invJ is applied to the nodal flux and the per-face scale
+//    side*area/(6V) to f*, so every element's RHS is rhs = A B with
+//    B = [Fr; Fs; Ft; f*] (K x NC) in shared memory.
+//  * Connectivity is never read from memory: neighbour element and node
+//    follow from (cube, type) and a 1.7 KB topology table copied to shared
+//    memory.  Faces between tets of the same cube read both traces from the
+//    shared tile; only cube-boundary faces gather from global memory.
+//  * q_a / q_b equal to q_in (SSPRK3 stages 1-3) are read from the tile, so
+//    each stage moves the algorithmic minimum of state bytes.
 #pragma once
 #include "dg_common.cuh"
 #include "physics.cuh"
+#include "tma.cuh"
 
 namespace mxm {
 
 template <int P, int NC, class R>
 struct Stage3DShape {
   static constexpr int NP = ntet(P), NFP = ntri(P), K = 3 * NP + 4 * NFP;
-  // element stride of the B tile, padded so that up to 16 (FP64) / 32 (FP32)
-  // elements read in the same warp land in distinct banks
+  // element stride of the B tile, padded so that elements read in the same
+  // warp land in distinct banks
   static constexpr int BSTR_RAW = K * NC;
   static constexpr int BMOD = sizeof(R) == 8 ? 16 : 32;
   static constexpr int BSTR = BSTR_RAW + ((1 - BSTR_RAW % BMOD) + BMOD) % BMOD;
 };
 
-template <class R, class Phys, int P, int RI, int EB, int NT, bool ASMEM>
-__global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTab3<R> tab, Phys ph) {
+template <class R, class Phys, int P, int EC, int RI, int NT, bool ASMEM>
+__global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTab3<R> tabp, Phys ph) {
   constexpr int NC = Phys::NC;
   using S = Stage3DShape<P, NC, R>;
   constexpr int NP = S::NP, NFP = S::NFP, K = S::K, BSTR = S::BSTR;
-  constexpr int G = NP / RI;
+  constexpr int EB = 6 * EC, G = NP / RI, QV = EB * NP * NC;
+  constexpr bool BULK = (6 * NP * NC * sizeof(R)) % 16 == 0;
   static_assert(NP % RI == 0, "row tile must divide NP");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* sAbuf = reinterpret_cast<R*>(smem_raw);  // [K][NP] when staged
-  R* sQ = sAbuf + (ASMEM ? K * NP : 0);          // [EB][NP][NC]
-  R* sB = sQ + EB * NP * NC;               // [EB][BSTR]
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);                       // [2]
+  KuhnTab3<R>* tab = reinterpret_cast<KuhnTab3<R>*>(smem_raw + 16);            // topology
+  constexpr size_t kTabBytes = (sizeof(KuhnTab3<R>) + 15) / 16 * 16;
+  R* sQ = reinterpret_cast<R*>(smem_raw + 16 + kTabBytes);                     // [2][QV]
+  R* sB = sQ + 2 * QV;                                                         // [EB][BSTR]
+  R* sA = sB + EB * BSTR;                                                      // [K][NP] (ASMEM)
+  const R* Aop = ASMEM ? sA : args.A;
 
   const int tid = threadIdx.x;
-  const int t = blockIdx.x % 6;
-  const int nblk_t = gridDim.x / 6;
-  const int ngroups = (args.ncell + EB - 1) / EB;
-
-  // Stage A_t (k-major) once per block, or read it through L1 when it
-  // does not fit next to the element tiles.
-  const R* gA = args.A + size_t(t) * K * NP;
+  const int ngroups = (args.ncell + EC - 1) / EC;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  {
+    const int* src = reinterpret_cast<const int*>(&tabp);
+    int* dst = reinterpret_cast<int*>(tab);
+    for (int k = tid; k < int(sizeof(KuhnTab3<R>) / 4); k += NT) dst[k] = src[k];
+  }
   if (ASMEM)
-    for (int idx = tid; idx < NP * K; idx += NT) sAbuf[idx] = gA[idx];
-  const R* sA = ASMEM ? sAbuf : gA;
+    for (int idx = tid; idx < NP * K; idx += NT) sA[idx] = args.A[idx];
+  __syncthreads();
+
+  auto issue = [&](int grp, int buf) {
+    const int c0 = grp * EC, nc = min(EC, args.ncell - c0);
+    const uint32_t bytes = uint32_t(nc) * 6u * NP * NC * sizeof(R);
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&bar[buf], bytes);
+    bulk_g2s(sQ + buf * QV, args.q_in + size_t(c0) * 6 * NP * NC, bytes, &bar[buf]);
+  };
+  uint32_t parity[2] = {0u, 0u};
+  int buf = 0;
+  if (BULK && tid == 0 && int(blockIdx.x) < ngroups) issue(blockIdx.x, 0);
 
   const int nxy = args.nx * args.ny;
-  for (int grp = blockIdx.x / 6; grp < ngroups; grp += nblk_t) {
-    const int cell0 = grp * EB;
-    const int ncell_here = min(EB, args.ncell - cell0);
-    __syncthreads();  // previous group done with sQ / sB (and sA staged)
-    // ---- stage q_in of the EB elements of type t
-    for (int idx = tid; idx < EB * NP * NC; idx += NT) {
-      const int el = idx / (NP * NC), r = idx - el * NP * NC;
-      if (el < ncell_here) sQ[idx] = args.q_in[(size_t(cell0 + el) * 6 + t) * (NP * NC) + r];
-    }
-    __syncthreads();
-    // ---- volume fluxes F_j -> B rows d*NP + j
-    for (int idx = tid; idx < EB * NP; idx += NT) {
-      const int el = idx / NP, j = idx - el * NP;
-      if (el >= ncell_here) continue;
-      R F[3 * NC];
-      ph.flux(&sQ[(el * NP + j) * NC], F);
-      R* b = &sB[el * BSTR];
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int c = 0; c < NC; ++c) b[(d * NP + j) * NC + c] = F[d * NC + c];
-    }
-    // ---- face numerical fluxes -> B rows 3NP + lf*NFP + m
-    for (int idx = tid; idx < EB * 4 * NFP; idx += NT) {
-      const int el = idx / (4 * NFP), fm = idx - el * 4 * NFP;
-      if (el >= ncell_here) continue;
-      const int lf = fm / NFP, m = fm - lf * NFP;
-      const int cell = cell0 + el;
-      const int ck = cell / nxy, rem = cell - ck * nxy, cj = rem / args.nx, ci = rem - cj * args.nx;
-      const int ax = tab.axis[t][lf], dir = tab.dir[t][lf];
-      const int cpos = ax == 0 ? ci : (ax == 1 ? cj : ck);
-      const int nax = ax == 0 ? args.nx : (ax == 1 ? args.ny : args.nz);
-      int code;
-      const int mode = face_mode(ax, dir, cpos, nax, args.bc, code);
-      const R* qo = &sQ[(el * NP + tab.own_node[lf][m]) * NC];
-      R nx = tab.normal[t][lf][0], ny = tab.normal[t][lf][1], nz = tab.normal[t][lf][2];
-      R f[NC];
-      if (mode == FACE_BC_HI) {
-        ph.bnd_flux(qo, code, nx, ny, nz, f);
-      } else if (mode == FACE_BC_LO) {
-        ph.bnd_flux(qo, code, -nx, -ny, -nz, f);
-#pragma unroll
-        for (int c = 0; c < NC; ++c) f[c] = -f[c];  // one-sided face: element on side 0
-      } else {
-        const int ni = wrapi(ci + tab.off[t][lf][0], args.nx), nj = wrapi(cj + tab.off[t][lf][1], args.ny),
-                  nk = wrapi(ck + tab.off[t][lf][2], args.nz);
-        const size_t enb = (size_t(ni) + size_t(args.nx) * (nj + size_t(args.ny) * nk)) * 6 + tab.nb_t[t][lf];
-        const R* gq = args.q_in + (enb * NP + tab.nb_node[t][lf][m]) * NC;
-        R qn[NC];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) qn[c] = gq[c];
-        if (mode == FACE_MIXED) ph.bnd_flux(qn, code, nx, ny, nz, f);
-        else if (tab.side[t][lf] == 0) ph.num_flux(qo, qn, nx, ny, nz, f);
-        else ph.num_flux(qn, qo, nx, ny, nz, f);
+  for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x, buf ^= 1) {
+    const int cell0 = grp * EC;
+    const int nhere = min(EC, args.ncell - cell0);
+    const int ne_here = 6 * nhere;
+    R* q = sQ + buf * QV;
+    if (BULK) {
+      const bool ok = mbar_wait_bounded(&bar[buf], parity[buf], kWaitLimitNs);
+      parity[buf] ^= 1u;
+      if (!__syncthreads_and(ok)) {
+        if (tid == 0 && args.err) atomicOr(args.err, 1);
+        return;
       }
+      if (tid == 0 && grp + int(gridDim.x) < ngroups) issue(grp + gridDim.x, buf ^ 1);
+    } else {
+      const R* src = args.q_in + size_t(cell0) * 6 * NP * NC;
+      for (int idx = tid; idx < ne_here * NP * NC; idx += NT) q[idx] = src[idx];
+      __syncthreads();
+    }
+    // ---- volume fluxes in reference coordinates -> B rows k*NP + j
+    for (int idx = tid; idx < ne_here * NP; idx += NT) {
+      const int el = idx / NP, j = idx - el * NP, t = el % 6;
+      R F[3 * NC];
+      ph.flux(&q[(el * NP + j) * NC], F);
+      const R* iJ = tab->invJ[t];
+      R* b = &sB[el * BSTR + j * NC];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+          b[k * NP * NC + c] = iJ[k * 3 + 0] * F[c] + iJ[k * 3 + 1] * F[NC + c] + iJ[k * 3 + 2] * F[2 * NC + c];
+    }
+    // ---- face numerical fluxes, scaled by side*area/(6V) -> B rows 3NP + lf*NFP + m
+    for (int idx = tid; idx < ne_here * 4 * NFP; idx += NT) {
+      const int el = idx / (4 * NFP), fm = idx - el * 4 * NFP;
+      const int lf = fm / NFP, m = fm - lf * NFP, t = el % 6, cl = el / 6;
+      const int cell = cell0 + cl;
+      const int ck = cell / nxy, rem = cell - ck * nxy, cj = rem / args.nx, ci = rem - cj * args.nx;
+      const int ax = tab->axis[t][lf], dir = tab->dir[t][lf];
+      int code;
+      const int mode = face_mode(ax, dir, ax == 0 ? ci : (ax == 1 ? cj : ck),
+                                 ax == 0 ? args.nx : (ax == 1 ? args.ny : args.nz), args.bc, code);
+      const R* qo = &q[(el * NP + tab->own_node[lf][m]) * NC];
+      R nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1], nz = tab->normal[t][lf][2];
+      R scale = tab->fscale[t][lf];
+      // Resolve the face to (left, right, normal) and call the Riemann
+      // solver once: BC faces use the ghost state (boundary_flux ==
+      // numerical_flux(q_int, ghost)), interior faces keep side-0 on the left.
+      R qn[NC], qg[NC];
+      if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
+        const int nbt = tab->nb_t[t][lf], nbn = tab->nb_node[t][lf][m];
+        if (ax < 0) {  // face inside the cube: neighbour trace is in the tile
+#pragma unroll
+          for (int c = 0; c < NC; ++c) qn[c] = q[((cl * 6 + nbt) * NP + nbn) * NC + c];
+        } else {
+          const int ni = wrapi(ci + tab->off[t][lf][0], args.nx), nj = wrapi(cj + tab->off[t][lf][1], args.ny),
+                    nk = wrapi(ck + tab->off[t][lf][2], args.nz);
+          const size_t enb = (size_t(ni) + size_t(args.nx) * (nj + size_t(args.ny) * nk)) * 6 + nbt;
+          const R* gq = args.q_in + (enb * NP + nbn) * NC;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) qn[c] = __ldg(gq + c);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) qn[c] = qo[c];
+      }
+      if (mode == FACE_BC_LO) {  // one-sided face: the element is its side 0, outward normal -n
+        nx = -nx;
+        ny = -ny;
+        nz = -nz;
+        scale = -scale;
+      }
+      const bool bcf = mode != FACE_INTERIOR;
+      if (bcf) ph.ghost(qn, code, nx, ny, nz, qg);  // BC_HI/BC_LO: qn = own trace; MIXED: neighbour's
+      const bool own_left = bcf ? (mode != FACE_MIXED) : (tab->side[t][lf] == 0);
+      const R* L = bcf ? qn : (own_left ? qo : qn);
+      const R* Rr = bcf ? qg : (own_left ? qn : qo);
+      R f[NC];
+      ph.num_flux(L, Rr, nx, ny, nz, f);
       R* b = &sB[el * BSTR + (3 * NP + fm) * NC];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) b[c] = f[c];
+      for (int c = 0; c < NC; ++c) b[c] = scale * f[c];
     }
     __syncthreads();
-    // ---- contraction rhs = A_t B, source, RK combine, floor, store
-    for (int w = tid; w < EB * G; w += NT) {
+    // ---- contraction rhs = A B, source, RK combine, floor, store
+    const bool a_in = args.q_a == args.q_in, b_in = args.q_b == args.q_in;
+    for (int w = tid; w < ne_here * G; w += NT) {
       const int el = w / G, g = w - el * G;
-      if (el >= ncell_here) continue;
       const int i0 = g * RI;
       R acc[RI][NC];
 #pragma unroll
@@ -133,7 +183,7 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
       for (int k = 0; k < K; ++k) {
         R av[RI], bv[NC];
 #pragma unroll
-        for (int r = 0; r < RI; ++r) av[r] = ASMEM ? sA[k * NP + i0 + r] : __ldg(&sA[k * NP + i0 + r]);
+        for (int r = 0; r < RI; ++r) av[r] = ASMEM ? Aop[k * NP + i0 + r] : __ldg(&Aop[k * NP + i0 + r]);
 #pragma unroll
         for (int c = 0; c < NC; ++c) bv[c] = b[k * NC + c];
 #pragma unroll
@@ -141,18 +191,25 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
 #pragma unroll
           for (int c = 0; c < NC; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
       }
-      const size_t e = size_t(cell0 + el) * 6 + t;
+      const size_t e = size_t(cell0) * 6 + el;
 #pragma unroll
       for (int r = 0; r < RI; ++r) {
         const int i = i0 + r;
         const size_t base = (e * NP + i) * NC;
+        const R* ql = &q[(el * NP + i) * NC];
         R src[NC];
-        if (Phys::kSource) ph.source(&sQ[(el * NP + i) * NC], src);
+        if (Phys::kSource) ph.source(ql, src);
         R out[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           const R rhs = Phys::kSource ? acc[r][c] + src[c] : acc[r][c];
-          out[c] = args.rhs_only ? rhs : args.a * args.q_a[base + c] + args.b * args.q_b[base + c] + args.cdt * rhs;
+          if (args.rhs_only) {
+            out[c] = rhs;
+          } else {
+            const R va = a_in ? ql[c] : args.q_a[base + c];
+            const R vb = b_in ? ql[c] : args.q_b[base + c];
+            out[c] = args.a * va + args.b * vb + args.cdt * rhs;
+          }
         }
         if (Phys::kLimit && !args.rhs_only) ph.limit(out);
 #pragma unroll
@@ -179,10 +236,9 @@ __global__ void wavespeed3d_kernel(Stage3DArgs<R> args, KuhnTab3<R> tab, Phys ph
     const int cell = int(e / 6), nxy = args.nx * args.ny;
     const int ck = cell / nxy, rem = cell - ck * nxy, cj = rem / args.nx, ci = rem - cj * args.nx;
     const int ax = tab.axis[t][lf], dir = tab.dir[t][lf];
-    const int cpos = ax == 0 ? ci : (ax == 1 ? cj : ck);
-    const int nax = ax == 0 ? args.nx : (ax == 1 ? args.ny : args.nz);
     int code;
-    const int mode = face_mode(ax, dir, cpos, nax, args.bc, code);
+    const int mode = face_mode(ax, dir, ax == 0 ? ci : (ax == 1 ? cj : ck),
+                               ax == 0 ? args.nx : (ax == 1 ? args.ny : args.nz), args.bc, code);
     const R* qo = args.q_in + (e * NP + tab.own_node[lf][m]) * NC;
     R nx = tab.normal[t][lf][0], ny = tab.normal[t][lf][1], nz = tab.normal[t][lf][2];
     R f[NC], s;
@@ -204,10 +260,11 @@ __global__ void wavespeed3d_kernel(Stage3DArgs<R> args, KuhnTab3<R> tab, Phys ph
   if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(best));
 }
 
-template <class R, int P, int NC, int EB, bool ASMEM>
+template <class R, int P, int NC, int EC, bool ASMEM>
 constexpr size_t stage3d_smem_bytes() {
   using S = Stage3DShape<P, NC, R>;
-  return sizeof(R) * ((ASMEM ? size_t(S::K) * S::NP : 0) + size_t(EB) * S::NP * NC + size_t(EB) * S::BSTR);
+  return 16 + (sizeof(KuhnTab3<R>) + 15) / 16 * 16 +
+         sizeof(R) * (2 * size_t(6 * EC) * S::NP * NC + size_t(6 * EC) * S::BSTR + (ASMEM ? size_t(S::K) * S::NP : 0));
 }
 
 }  // namespace mxm

@@ -9,22 +9,23 @@ struct Cfg3 {
   using S = Stage3DShape<P, NC, R>;
   static constexpr int NP = S::NP;
   // rows per thread: a divisor of NP
-  static constexpr int RI = P <= 2 ? 2 : (P == 4 ? 5 : 4);
-  // stage A_t in shared memory when it takes <= 64 KB
+  static constexpr int RI = sizeof(R) == 8 ? (P <= 3 ? 2 : (P == 4 ? 5 : 4))
+                                           : (P == 1 ? 4 : (P == 2 ? 5 : (P == 3 ? 4 : (P == 4 ? 5 : 8))));
+  // keep the shared operator in shared memory when it takes <= 64 KB
   static constexpr bool ASMEM = sizeof(R) * S::K * S::NP <= 64 * 1024;
-  static constexpr size_t kBudget = 110 * 1024;
-  static constexpr size_t kA = ASMEM ? sizeof(R) * S::K * S::NP : 0;
-  static constexpr size_t kPerEl = sizeof(R) * (size_t(S::NP) * NC + S::BSTR);
-  static constexpr int EB_RAW = int((kBudget - kA) / kPerEl);
-  static constexpr int EB = EB_RAW > 64 ? 64 : (EB_RAW < 1 ? 1 : EB_RAW);
-  static constexpr int NT = 128;
-  static constexpr size_t kSmem = stage3d_smem_bytes<R, P, NC, EB, ASMEM>();
+  static constexpr size_t kBudget = 110 * 1024;  // two blocks per SM
+  static constexpr size_t kFixed = 16 + (sizeof(KuhnTab3<R>) + 15) / 16 * 16 + (ASMEM ? sizeof(R) * S::K * S::NP : 0);
+  static constexpr size_t kPerCube = 6 * sizeof(R) * (2 * size_t(S::NP) * NC + S::BSTR);
+  static constexpr int EC_RAW = kBudget > kFixed ? int((kBudget - kFixed) / kPerCube) : 1;
+  static constexpr int EC = EC_RAW > 16 ? 16 : (EC_RAW < 1 ? 1 : EC_RAW);
+  static constexpr int NT = 256;
+  static constexpr size_t kSmem = stage3d_smem_bytes<R, P, NC, EC, ASMEM>();
 };
 
 template <class R, class Phys, int P>
 cudaError_t launch3_p(const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phys& ph, int nsm, cudaStream_t st) {
   using C = Cfg3<R, P, Phys::NC>;
-  auto kern = stage3d_kernel<R, Phys, P, C::RI, C::EB, C::NT, C::ASMEM>;
+  auto kern = stage3d_kernel<R, Phys, P, C::EC, C::RI, C::NT, C::ASMEM>;
   static int bps = -1;
   if (bps < 0) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(C::kSmem));
@@ -33,11 +34,11 @@ cudaError_t launch3_p(const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phy
     if (e != cudaSuccess) return e;
     if (bps < 1) bps = 1;
   }
-  const int ngroups = (a.ncell + C::EB - 1) / C::EB;
-  int per_type = (nsm * bps + 5) / 6;
-  if (per_type > ngroups) per_type = ngroups;
-  if (per_type < 1) per_type = 1;
-  kern<<<6 * per_type, C::NT, C::kSmem, st>>>(a, tab, ph);
+  const int ngroups = (a.ncell + C::EC - 1) / C::EC;
+  int nblk = nsm * bps;
+  if (nblk > ngroups) nblk = ngroups;
+  if (nblk < 1) nblk = 1;
+  kern<<<nblk, C::NT, C::kSmem, st>>>(a, tab, ph);
   return cudaGetLastError();
 }
 

@@ -1,0 +1,278 @@
+// Mixed-precision 3D stage kernel: FP32 state, fluxes and Riemann solves,
+// the volume + lift contraction on the 5th-generation tensor cores
+// (tcgen05.mma, split-BF16 operands, FP32 accumulation in tensor memory).
+//
+// Same dataflow as stage3d_kernel (whole cubes per tile, bulk-copied
+// double-buffered state, implicit connectivity), with the contraction
+// written in the transposed form
+//     RHS^T[(el,c), i] = sum_k  B^T[(el,c), k] * A[i, k]
+// so one MMA tile covers up to 128 (element, component) rows against the
+// shared operator A (N = NP rounded up to 16, K = 3NP + 4NFP rounded up to
+// 16).  Every operand x is split x = hi + lo in bfloat16 and the product is
+// hi*hi + hi*lo + lo*hi (three MMAs into one FP32 accumulator), about 16
+// significant bits per product.  One thread issues the MMAs; completion is
+// tracked by tcgen05.commit on an mbarrier with a bounded wait; warps 0-3
+// read the accumulator back with tcgen05.ld for the FP32 epilogue
+// (source, RK combine, positivity floor).
+#pragma once
+#include "dg_common.cuh"
+#include "physics.cuh"
+#include "tc.cuh"
+
+namespace mxm {
+
+__host__ __device__ constexpr int rup16(int x) { return (x + 15) / 16 * 16; }
+__host__ __device__ constexpr int tmem_cols_for(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : (n <= 128 ? 128 : 256)); }
+
+template <int P, int NC>
+struct TcShape {
+  static constexpr int NP = ntet(P), NFP = ntri(P), K = 3 * NP + 4 * NFP;
+  static constexpr int KP = rup16(K), NN = rup16(NP), M = 128;
+  static constexpr int EC = M / (6 * NC), EB = 6 * EC, ROWS = EB * NC;
+  static constexpr int NCOLS = tmem_cols_for(NN);
+  static constexpr size_t A_BYTES = size_t(NN) * KP * 2;  // one of hi / lo
+  static constexpr size_t B_BYTES = size_t(M) * KP * 2;
+  static constexpr size_t Q_BYTES = size_t(EB) * NP * NC * 4;
+  static constexpr size_t HDR = 128;
+  static constexpr size_t TAB = (sizeof(KuhnTab3<float>) + 127) / 128 * 128;
+  static constexpr size_t OFF_A = HDR + TAB;
+  static constexpr size_t OFF_B = OFF_A + 2 * A_BYTES;
+  static constexpr size_t OFF_Q = OFF_B + 2 * B_BYTES;
+  static constexpr size_t OFF_O = OFF_Q + 2 * Q_BYTES;
+  static constexpr size_t SMEM = OFF_O + Q_BYTES;
+  static constexpr bool BULK = (6 * NP * NC * 4) % 16 == 0;
+};
+
+template <class Phys, int P, int NT>
+__global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args, KuhnTab3<float> tabp, Phys ph,
+                                                         const unsigned char* __restrict__ a_image) {
+  constexpr int NC = Phys::NC;
+  using S = TcShape<P, NC>;
+  constexpr int NP = S::NP, NFP = S::NFP, K = S::K, KP = S::KP, NN = S::NN, M = S::M;
+  constexpr int EC = S::EC, EB = S::EB, QV = EB * NP * NC;
+  constexpr uint32_t LBO_A = NN * 16, LBO_B = M * 16, SBO = 128;
+  constexpr uint32_t IDESC = umma_idesc_bf16_f32(M, NN);
+  static_assert(NN % 16 == 0 && NN <= 256 && KP % 16 == 0, "UMMA shape");
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);  // [0..1] q tiles, [2] mma, [3] A image
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 32);
+  KuhnTab3<float>* tab = reinterpret_cast<KuhnTab3<float>*>(smem + S::HDR);
+  unsigned char* sAhi = smem + S::OFF_A;
+  unsigned char* sAlo = sAhi + S::A_BYTES;
+  unsigned char* sBhi = smem + S::OFF_B;
+  unsigned char* sBlo = sBhi + S::B_BYTES;
+  float* sQ = reinterpret_cast<float*>(smem + S::OFF_Q);
+  float* sO = reinterpret_cast<float*>(smem + S::OFF_O);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ngroups = (args.ncell + EC - 1) / EC;
+  if (tid == 0) {
+    for (int k = 0; k < 4; ++k) mbar_init(&bar[k], 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(tslot, S::NCOLS);
+    tmem_relinquish();
+  }
+  {
+    const int* src = reinterpret_cast<const int*>(&tabp);
+    int* dst = reinterpret_cast<int*>(tab);
+    for (int k = tid; k < int(sizeof(KuhnTab3<float>) / 4); k += NT) dst[k] = src[k];
+  }
+  // zero the flux tiles once: padding rows / k columns stay zero for good
+  for (int k = tid; k < int(2 * S::B_BYTES / 16); k += NT) reinterpret_cast<uint4*>(sBhi)[k] = make_uint4(0, 0, 0, 0);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  if (tid == 0) {  // operator image (hi | lo), already in the UMMA layout
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&bar[3], uint32_t(2 * S::A_BYTES));
+    bulk_g2s(sAhi, a_image, uint32_t(2 * S::A_BYTES), &bar[3]);
+  }
+  auto issue = [&](int grp, int buf) {
+    const int c0 = grp * EC, nc = min(EC, args.ncell - c0);
+    const uint32_t bytes = uint32_t(nc) * 6u * NP * NC * 4u;
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&bar[buf], bytes);
+    bulk_g2s(sQ + buf * QV, args.q_in + size_t(c0) * 6 * NP * NC, bytes, &bar[buf]);
+  };
+  uint32_t parity[2] = {0u, 0u}, mma_parity = 0u;
+  bool q_pending[2] = {false, false}, mma_pending = false;
+  int buf = 0;
+  bool failed = !__syncthreads_and(mbar_wait_bounded(&bar[3], 0, kWaitLimitNs));
+  if (S::BULK && int(blockIdx.x) < ngroups && !failed) {
+    if (tid == 0) issue(blockIdx.x, 0);
+    q_pending[0] = true;
+  }
+  const int nxy = args.nx * args.ny;
+
+  for (int grp = blockIdx.x; grp < ngroups && !failed; grp += gridDim.x, buf ^= 1) {
+    const int cell0 = grp * EC;
+    const int ne_here = 6 * min(EC, args.ncell - cell0);
+    float* q = sQ + buf * QV;
+    if (S::BULK) {
+      const bool ok = mbar_wait_bounded(&bar[buf], parity[buf], kWaitLimitNs);
+      if (!__syncthreads_and(ok)) {
+        failed = true;
+        break;
+      }
+      parity[buf] ^= 1u;
+      q_pending[buf] = false;
+      if (grp + int(gridDim.x) < ngroups) {
+        if (tid == 0) issue(grp + gridDim.x, buf ^ 1);
+        q_pending[buf ^ 1] = true;
+      }
+    } else {
+      const float* src = args.q_in + size_t(cell0) * 6 * NP * NC;
+      for (int idx = tid; idx < ne_here * NP * NC; idx += NT) q[idx] = src[idx];
+      __syncthreads();
+    }
+    // ---- volume fluxes in reference coordinates -> rows (el,c), k = d*NP + j
+    for (int idx = tid; idx < ne_here * NP; idx += NT) {
+      const int el = idx / NP, j = idx - el * NP, t = el % 6;
+      float F[3 * NC];
+      ph.flux(&q[(el * NP + j) * NC], F);
+      const float* iJ = tab->invJ[t];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const float v = iJ[d * 3 + 0] * F[c] + iJ[d * 3 + 1] * F[NC + c] + iJ[d * 3 + 2] * F[2 * NC + c];
+          __nv_bfloat16 h, l;
+          split_bf16(v, h, l);
+          const uint32_t off = umma_tile_offset(el * NC + c, d * NP + j, M);
+          *reinterpret_cast<__nv_bfloat16*>(sBhi + off) = h;
+          *reinterpret_cast<__nv_bfloat16*>(sBlo + off) = l;
+        }
+    }
+    // ---- face fluxes scaled by side*area/(6V) -> k = 3NP + lf*NFP + m
+    for (int idx = tid; idx < ne_here * 4 * NFP; idx += NT) {
+      const int el = idx / (4 * NFP), fm = idx - el * 4 * NFP;
+      const int lf = fm / NFP, m = fm - lf * NFP, t = el % 6, cl = el / 6;
+      const int cell = cell0 + cl;
+      const int ck = cell / nxy, rem = cell - ck * nxy, cj = rem / args.nx, ci = rem - cj * args.nx;
+      const int ax = tab->axis[t][lf], dir = tab->dir[t][lf];
+      int code;
+      const int mode = face_mode(ax, dir, ax == 0 ? ci : (ax == 1 ? cj : ck),
+                                 ax == 0 ? args.nx : (ax == 1 ? args.ny : args.nz), args.bc, code);
+      const float* qo = &q[(el * NP + tab->own_node[lf][m]) * NC];
+      float nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1], nz = tab->normal[t][lf][2];
+      float scale = tab->fscale[t][lf];
+      float qn[NC], qg[NC];
+      if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
+        const int nbt = tab->nb_t[t][lf], nbn = tab->nb_node[t][lf][m];
+        if (ax < 0) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) qn[c] = q[((cl * 6 + nbt) * NP + nbn) * NC + c];
+        } else {
+          const int ni = wrapi(ci + tab->off[t][lf][0], args.nx), nj = wrapi(cj + tab->off[t][lf][1], args.ny),
+                    nk = wrapi(ck + tab->off[t][lf][2], args.nz);
+          const size_t enb = (size_t(ni) + size_t(args.nx) * (nj + size_t(args.ny) * nk)) * 6 + nbt;
+          const float* gq = args.q_in + (enb * NP + nbn) * NC;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) qn[c] = __ldg(gq + c);
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) qn[c] = qo[c];
+      }
+      if (mode == FACE_BC_LO) {
+        nx = -nx;
+        ny = -ny;
+        nz = -nz;
+        scale = -scale;
+      }
+      const bool bcf = mode != FACE_INTERIOR;
+      if (bcf) ph.ghost(qn, code, nx, ny, nz, qg);
+      const bool own_left = tab->side[t][lf] == 0;
+      const float* L = bcf ? qn : (own_left ? qo : qn);
+      const float* Rr = bcf ? qg : (own_left ? qn : qo);
+      float f[NC];
+      ph.num_flux(L, Rr, nx, ny, nz, f);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        __nv_bfloat16 h, l;
+        split_bf16(scale * f[c], h, l);
+        const uint32_t off = umma_tile_offset(el * NC + c, 3 * NP + fm, M);
+        *reinterpret_cast<__nv_bfloat16*>(sBhi + off) = h;
+        *reinterpret_cast<__nv_bfloat16*>(sBlo + off) = l;
+      }
+    }
+    // make the generic-proxy tile writes visible to the tensor-core (async) proxy
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t ah = smem_u32(sAhi), al = smem_u32(sAlo), bh = smem_u32(sBhi), bl = smem_u32(sBlo);
+#pragma unroll 1
+      for (int ks = 0; ks < KP / 16; ++ks) {
+        const uint64_t dAh = umma_desc(ah + ks * 2 * LBO_A, LBO_A, SBO), dAl = umma_desc(al + ks * 2 * LBO_A, LBO_A, SBO);
+        const uint64_t dBh = umma_desc(bh + ks * 2 * LBO_B, LBO_B, SBO), dBl = umma_desc(bl + ks * 2 * LBO_B, LBO_B, SBO);
+        tc_mma_bf16(tmem, dBh, dAh, IDESC, ks > 0 ? 1u : 0u);
+        tc_mma_bf16(tmem, dBh, dAl, IDESC, 1u);
+        tc_mma_bf16(tmem, dBl, dAh, IDESC, 1u);
+      }
+      tc_commit(&bar[2]);
+    }
+    mma_pending = true;
+    const bool mok = mbar_wait_bounded(&bar[2], mma_parity, kWaitLimitNs);
+    if (!__syncthreads_and(mok)) {
+      failed = true;
+      break;
+    }
+    mma_parity ^= 1u;
+    mma_pending = false;
+    tc_fence_after();
+    if (warp < 4) {  // warp w reads TMEM lanes [32w, 32w+32): rows (el, c)
+      const int row = warp * 32 + lane;
+      float v[NN];
+#pragma unroll
+      for (int c0 = 0; c0 < NN; c0 += 16) tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + c0, v + c0);
+      tmem_ld_wait();
+      if (row < ne_here * NC) {
+        const int el = row / NC, c = row - el * NC;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) sO[(el * NP + i) * NC + c] = v[i];
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+    // ---- epilogue per node: source, RK combine, floor, store
+    const bool a_in = args.q_a == args.q_in, b_in = args.q_b == args.q_in;
+    for (int idx = tid; idx < ne_here * NP; idx += NT) {
+      const size_t base = (size_t(cell0) * 6 * NP + idx) * NC;
+      const float* ql = &q[idx * NC];
+      float src[NC], out[NC];
+      if (Phys::kSource) ph.source(ql, src);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float rhs = Phys::kSource ? sO[idx * NC + c] + src[c] : sO[idx * NC + c];
+        if (args.rhs_only) {
+          out[c] = rhs;
+        } else {
+          const float va = a_in ? ql[c] : args.q_a[base + c];
+          const float vb = b_in ? ql[c] : args.q_b[base + c];
+          out[c] = args.a * va + args.b * vb + args.cdt * rhs;
+        }
+      }
+      if (Phys::kLimit && !args.rhs_only) ph.limit(out);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) args.q_out[base + c] = out[c];
+    }
+  }
+  if (failed) {
+    if (tid == 0 && args.err) atomicOr(args.err, 2);
+    // let copies and the MMA batch still in flight land before the shared
+    // tiles and the accumulator are released (each wait bounded)
+    for (int b = 0; b < 2; ++b)
+      if (q_pending[b]) mbar_wait_bounded(&bar[b], parity[b], kWaitLimitNs);
+    if (mma_pending) mbar_wait_bounded(&bar[2], mma_parity, kWaitLimitNs);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, S::NCOLS);
+}
+
+}  // namespace mxm

@@ -139,3 +139,35 @@ def test_reductions_and_wavespeed(oracle_mod):
         assert abs(s.integral(c) - want) <= 1e-13 * abs(want)
         assert abs(s.integral(c, kind=2) - np.abs(q[..., c]).max()) == 0.0
     assert abs(s.max_wavespeed() - o.max_face_speed()) <= 1e-13 * o.max_face_speed()
+
+
+# Mixed precision (FP32 state, split-BF16 tcgen05 contraction) vs the FP64
+# oracle: element-wise RHS error relative to max |RHS|.  Split-BF16 products
+# carry ~16 significant bits; the bound leaves room for the cancellation in
+# the derivative/lift sums.
+TOL_MIXED = 5e-4
+
+
+@pytest.mark.parametrize("P", [2, 3, 4])
+@pytest.mark.parametrize("name", ["euler_rusanov", "euler_hllec_fix", "maxwell", "advection", "shallow_water"])
+def test_rhs3d_mixed_vs_f64(oracle_mod, name, P):
+    phys = C.PHYSICS_3D[name]()
+    s, o = make_pair(oracle_mod, phys, P, N3, L3, C.BCS_3D["outflow_x_wall_yz"], prec="mixed")
+    q = C.random_state(s.shape, phys, seed=31)
+    qf = q.astype(np.float32).astype(np.float64)
+    o64 = oracle_mod.Oracle3D(P, N3, L3, M.physics_dict(phys), bcs=C.BCS_3D["outflow_x_wall_yz"], real="f64")
+    err = C.rel_err(s.rhs(qf), o64.rhs(qf))
+    print(f"mixed {name} P={P}: rel err vs FP64 oracle {err:.2e}")
+    assert err <= TOL_MIXED
+
+
+def test_mixed_large_mesh_vs_f32(oracle_mod):
+    """Many tiles, partial last tile, mixed vs the FP32 SIMT kernel."""
+    phys = C.PHYSICS_3D["euler_hllec"]()
+    n, L = (7, 5, 3), (1.0, 1.0, 1.0)
+    sm = M.Solver(M.Mesh(*n, *L), phys, P=3, precision="mixed")
+    sf = M.Solver(M.Mesh(*n, *L), phys, P=3, precision="f32")
+    q = C.random_state(sm.shape, phys, seed=41)
+    err = C.rel_err(sm.rhs(q), sf.rhs(q))
+    print(f"mixed vs f32 on {n}: {err:.2e}")
+    assert err <= TOL_MIXED
