@@ -145,6 +145,20 @@ void fill_tab3(Handle* h, KuhnTab3<R>& t) {
     for (int m = 0; m < h->NFP; ++m) t.own_node[lf][m] = uint8_t(h->ref.face_nodes[lf * h->NFP + m]);
   for (int a = 0; a < 6; ++a)
     for (int q = 0; q < 9; ++q) t.invJ[a][q] = R(k.invJ[a][q]);
+  // neighbour's face and face-local index of each face node (node pairing
+  // expressed in the neighbour's own face order)
+  for (int a = 0; a < 6; ++a)
+    for (int lf = 0; lf < 4; ++lf) {
+      const int nlf = k.nb_lf[a][lf];
+      t.nb_lf[a][lf] = uint8_t(nlf);
+      for (int m = 0; m < h->NFP; ++m) {
+        const int nbn = k.nb_node[(a * 4 + lf) * h->NFP + m];
+        int mm = 0;
+        while (mm < h->NFP && h->ref.face_nodes[nlf * h->NFP + mm] != nbn) ++mm;
+        if (mm == h->NFP) throw ArgError("internal: neighbour face node not found");
+        t.nb_m[a][lf][m] = uint8_t(mm);
+      }
+    }
 }
 
 template <class R>

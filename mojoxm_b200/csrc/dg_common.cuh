@@ -27,6 +27,8 @@ struct KuhnTab3 {
   int8_t dir[6][4];
   uint8_t own_node[4][kMaxNFP3];
   uint8_t nb_node[6][4][kMaxNFP3];
+  uint8_t nb_lf[6][4];             // neighbour's local face
+  uint8_t nb_m[6][4][kMaxNFP3];    // neighbour's face-local index of face node m
 };
 
 template <class R>
@@ -79,6 +81,39 @@ __device__ __forceinline__ int face_mode(int axis, int dir, int cpos, int ncell_
 }
 
 __device__ __forceinline__ int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+// Per-tile face descriptor, resolved once per (element, local face) at the
+// start of a tile so the face-node loops do no integer division:
+//   x = mode | code << 8,  y = neighbour element (global index), z = neighbour
+//   element inside the tile (-1 when outside)
+struct FaceInfo {
+  int x, y, z;
+};
+
+// Fill info[el*4 + lf] for the ne_here elements of a tile of whole cubes
+// starting at cell0 (3D Kuhn meshes).
+template <class Tab, class Args>
+__device__ __forceinline__ void setup_faces3(const Tab* tab, const Args& args, int cell0, int ne_here, FaceInfo* info,
+                                             int tid, int nt) {
+  const int nxy = args.nx * args.ny;
+  for (int idx = tid; idx < ne_here * 4; idx += nt) {
+    const int el = idx >> 2, lf = idx & 3, t = el % 6, cl = el / 6;
+    const int cell = cell0 + cl;
+    const int ck = cell / nxy, rem = cell - ck * nxy, cj = rem / args.nx, ci = rem - cj * args.nx;
+    const int ax = tab->axis[t][lf];
+    int code;
+    const int mode = face_mode(ax, tab->dir[t][lf], ax == 0 ? ci : (ax == 1 ? cj : ck),
+                               ax == 0 ? args.nx : (ax == 1 ? args.ny : args.nz), args.bc, code);
+    const int nbt = tab->nb_t[t][lf];
+    const int ni = wrapi(ci + tab->off[t][lf][0], args.nx), nj = wrapi(cj + tab->off[t][lf][1], args.ny),
+              nk = wrapi(ck + tab->off[t][lf][2], args.nz);
+    FaceInfo f;
+    f.x = mode | (code << 8);
+    f.y = (ni + args.nx * (nj + args.ny * nk)) * 6 + nbt;
+    f.z = ax < 0 ? cl * 6 + nbt : -1;
+    info[idx] = f;
+  }
+}
 
 // Kernel argument blocks (by value).
 template <class R>

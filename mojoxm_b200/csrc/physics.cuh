@@ -211,6 +211,23 @@ struct EulerD {
     }
   }
   __device__ R num_flux(const R* q_l, const R* q_r, R nx, R ny, R nz, R* flux) const {  // euler.mojo:626-691
+    if (FLUX == FLUX_RUSANOV) {
+      // euler.mojo:649-668 evaluated in the world frame: with the orthonormal
+      // frame (n, t, b), anti-rotating the face-frame Rusanov flux gives
+      // 0.5 (m_L un_L + m_R un_R + (p_L + p_R) n + cmax (m_L - m_R)) for the
+      // momentum, so the rotation pair and the tangent construction drop out.
+      const R rl = rho_f(q_l), rr = rho_f(q_r), pl = p_f(q_l, rl), pr = p_f(q_r, rr);
+      const R mnl = nx * q_l[1] + ny * q_l[2] + nz * q_l[3], mnr = nx * q_r[1] + ny * q_r[2] + nz * q_r[3];
+      const R ul = mnl / rl, ur = mnr / rr;
+      const R cmax = rmax(rabs(ul) + sqrt(gamma * pl / rl), rabs(ur) + sqrt(gamma * pr / rr));
+      const R h = R(0.5), ps = pl + pr;
+      flux[0] = h * (mnl + mnr + cmax * (rl - rr));
+      flux[1] = h * (q_l[1] * ul + q_r[1] * ur + ps * nx + cmax * (q_l[1] - q_r[1]));
+      flux[2] = h * (q_l[2] * ul + q_r[2] * ur + ps * ny + cmax * (q_l[2] - q_r[2]));
+      flux[3] = h * (q_l[3] * ul + q_r[3] * ur + ps * nz + cmax * (q_l[3] - q_r[3]));
+      flux[4] = h * ((q_l[4] + pl) * ul + (q_r[4] + pr) * ur + cmax * (q_l[4] - q_r[4]));
+      return cmax;
+    }
     // tangent/binormal (euler.mojo:94-118)
     R ax = nx, ay = ny, az = nz;
     if (rabs(nx) >= R(0.9)) ay += R(1); else ax += R(1);

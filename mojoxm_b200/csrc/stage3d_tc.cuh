@@ -3,17 +3,28 @@
 // (tcgen05.mma, split-BF16 operands, FP32 accumulation in tensor memory).
 //
 // Same dataflow as stage3d_kernel (whole cubes per tile, bulk-copied
-// double-buffered state, implicit connectivity), with the contraction
-// written in the transposed form
-//     RHS^T[(el,c), i] = sum_k  B^T[(el,c), k] * A[i, k]
-// so one MMA tile covers up to 128 (element, component) rows against the
-// shared operator A (N = NP rounded up to 16, K = 3NP + 4NFP rounded up to
-// 16).  Every operand x is split x = hi + lo in bfloat16 and the product is
-// hi*hi + hi*lo + lo*hi (three MMAs into one FP32 accumulator), about 16
-// significant bits per product.  One thread issues the MMAs; completion is
-// tracked by tcgen05.commit on an mbarrier with a bounded wait; warps 0-3
-// read the accumulator back with tcgen05.ld for the FP32 epilogue
-// (source, RK combine, positivity floor).
+// double-buffered state, implicit connectivity), with the contraction in
+// the transposed form
+//     RHS^T[(c,el), i] = sum_k  B^T[(c,el), k] * A[i, k]
+// so one 128-row MMA tile covers the (component, element) pairs of a tile
+// against the shared operator A (N = NP rounded up to 16, K = 3NP + 4NFP
+// rounded up to 16).  Operands are split x = hi + lo in bfloat16 and the
+// product is hi*hi + hi*lo + lo*hi (three MMAs into one FP32 accumulator).
+//
+// Accuracy: before splitting, every element subtracts its own constant flux
+// Fbar = F(q at node 0) from its volume fluxes and Fbar.n from its face
+// fluxes.  The weak-form operator maps a constant flux to zero
+// (sum_j D_k[i,j] = lift of the constant normal flux), so the RHS is
+// unchanged in exact arithmetic while the operands -- and with them the
+// cancellation error of the O(|F|/h) terms -- shrink to the flux variation
+// across the element.
+//
+// Layout: the (c,el) x K operand is MN-major (8 consecutive rows of one k in
+// 16 bytes), so threads that own consecutive nodes write disjoint banks.
+// Faces inside a cube are evaluated once, by their side-0 tet, which writes
+// both tets' rows.  One thread issues the MMAs; completion is tracked by
+// tcgen05.commit on an mbarrier with a bounded wait; warps 0-3 read the
+// accumulator with tcgen05.ld for the FP32 epilogue (source, RK, floor).
 #pragma once
 #include "dg_common.cuh"
 #include "physics.cuh"
@@ -24,22 +35,35 @@ namespace mxm {
 __host__ __device__ constexpr int rup16(int x) { return (x + 15) / 16 * 16; }
 __host__ __device__ constexpr int tmem_cols_for(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : (n <= 128 ? 128 : 256)); }
 
+// MN-major, no-swizzle operand tile of `rows` x KP bf16:
+// byte (k/8)*(rows*16) + (row/8)*128 + (k%8)*16 + (row%8)*2
+__host__ __device__ constexpr uint32_t umma_mn_offset(int row, int k, int rows) {
+  return uint32_t((k >> 3) * rows * 16 + (row >> 3) * 128 + (k & 7) * 16 + (row & 7) * 2);
+}
+
+__host__ __device__ constexpr uint32_t umma_idesc_bf16_f32_amn(int M, int N) {
+  return umma_idesc_bf16_f32(M, N) | (1u << 15);  // A operand MN-major
+}
+
 template <int P, int NC>
 struct TcShape {
   static constexpr int NP = ntet(P), NFP = ntri(P), K = 3 * NP + 4 * NFP;
   static constexpr int KP = rup16(K), NN = rup16(NP), M = 128;
-  static constexpr int EC = M / (6 * NC), EB = 6 * EC, ROWS = EB * NC;
+  static constexpr int EBP = (M / NC) / 8 * 8;      // element slots per component (multiple of 8)
+  static constexpr int EC = EBP / 6, EB = 6 * EC;   // whole cubes in a tile
   static constexpr int NCOLS = tmem_cols_for(NN);
   static constexpr size_t A_BYTES = size_t(NN) * KP * 2;  // one of hi / lo
   static constexpr size_t B_BYTES = size_t(M) * KP * 2;
   static constexpr size_t Q_BYTES = size_t(EB) * NP * NC * 4;
+  static constexpr size_t FB_BYTES = size_t(EB) * 3 * NC * 4;
   static constexpr size_t HDR = 128;
   static constexpr size_t TAB = (sizeof(KuhnTab3<float>) + 127) / 128 * 128;
   static constexpr size_t OFF_A = HDR + TAB;
   static constexpr size_t OFF_B = OFF_A + 2 * A_BYTES;
   static constexpr size_t OFF_Q = OFF_B + 2 * B_BYTES;
   static constexpr size_t OFF_O = OFF_Q + 2 * Q_BYTES;
-  static constexpr size_t SMEM = OFF_O + Q_BYTES;
+  static constexpr size_t OFF_F = OFF_O + Q_BYTES;
+  static constexpr size_t SMEM = OFF_F + FB_BYTES;
   static constexpr bool BULK = (6 * NP * NC * 4) % 16 == 0;
 };
 
@@ -48,11 +72,11 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
                                                          const unsigned char* __restrict__ a_image) {
   constexpr int NC = Phys::NC;
   using S = TcShape<P, NC>;
-  constexpr int NP = S::NP, NFP = S::NFP, K = S::K, KP = S::KP, NN = S::NN, M = S::M;
-  constexpr int EC = S::EC, EB = S::EB, QV = EB * NP * NC;
+  constexpr int NP = S::NP, NFP = S::NFP, KP = S::KP, NN = S::NN, M = S::M;
+  constexpr int EC = S::EC, EB = S::EB, EBP = S::EBP, QV = EB * NP * NC;
   constexpr uint32_t LBO_A = NN * 16, LBO_B = M * 16, SBO = 128;
-  constexpr uint32_t IDESC = umma_idesc_bf16_f32(M, NN);
-  static_assert(NN % 16 == 0 && NN <= 256 && KP % 16 == 0, "UMMA shape");
+  constexpr uint32_t IDESC = umma_idesc_bf16_f32_amn(M, NN);
+  static_assert(NN % 16 == 0 && NN <= 256 && KP % 16 == 0 && EC >= 1 && EBP * NC <= M, "UMMA shape");
   extern __shared__ __align__(1024) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);  // [0..1] q tiles, [2] mma, [3] A image
   uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 32);
@@ -63,6 +87,7 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
   unsigned char* sBlo = sBhi + S::B_BYTES;
   float* sQ = reinterpret_cast<float*>(smem + S::OFF_Q);
   float* sO = reinterpret_cast<float*>(smem + S::OFF_O);
+  float* sF = reinterpret_cast<float*>(smem + S::OFF_F);  // [EB][3][NC] element flux Fbar
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ngroups = (args.ncell + EC - 1) / EC;
@@ -85,7 +110,7 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  if (tid == 0) {  // operator image (hi | lo), already in the UMMA layout
+  if (tid == 0) {  // operator image (hi | lo), already in the K-major UMMA layout
     fence_proxy_async();
     mbar_arrive_expect_tx(&bar[3], uint32_t(2 * S::A_BYTES));
     bulk_g2s(sAhi, a_image, uint32_t(2 * S::A_BYTES), &bar[3]);
@@ -96,6 +121,14 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
     fence_proxy_async();
     mbar_arrive_expect_tx(&bar[buf], bytes);
     bulk_g2s(sQ + buf * QV, args.q_in + size_t(c0) * 6 * NP * NC, bytes, &bar[buf]);
+  };
+  // store one operand value (row (c, el), column k) as bf16 hi / lo
+  auto put = [&](int el, int c, int k, float v) {
+    __nv_bfloat16 h, l;
+    split_bf16(v, h, l);
+    const uint32_t off = umma_mn_offset(c * EBP + el, k, M);
+    *reinterpret_cast<__nv_bfloat16*>(sBhi + off) = h;
+    *reinterpret_cast<__nv_bfloat16*>(sBlo + off) = l;
   };
   uint32_t parity[2] = {0u, 0u}, mma_parity = 0u;
   bool q_pending[2] = {false, false}, mma_pending = false;
@@ -128,40 +161,43 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
       for (int idx = tid; idx < ne_here * NP * NC; idx += NT) q[idx] = src[idx];
       __syncthreads();
     }
-    // ---- volume fluxes in reference coordinates -> rows (el,c), k = d*NP + j
+    // ---- per-element constant flux Fbar = F(q at node 0)
+    for (int el = tid; el < ne_here; el += NT) ph.flux(&q[el * NP * NC], &sF[el * 3 * NC]);
+    __syncthreads();
+    // ---- volume fluxes (F - Fbar) in reference coordinates -> k = d*NP + j
     for (int idx = tid; idx < ne_here * NP; idx += NT) {
       const int el = idx / NP, j = idx - el * NP, t = el % 6;
       float F[3 * NC];
       ph.flux(&q[(el * NP + j) * NC], F);
+      const float* Fb = &sF[el * 3 * NC];
+#pragma unroll
+      for (int k = 0; k < 3 * NC; ++k) F[k] -= Fb[k];
       const float* iJ = tab->invJ[t];
 #pragma unroll
       for (int d = 0; d < 3; ++d)
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          const float v = iJ[d * 3 + 0] * F[c] + iJ[d * 3 + 1] * F[NC + c] + iJ[d * 3 + 2] * F[2 * NC + c];
-          __nv_bfloat16 h, l;
-          split_bf16(v, h, l);
-          const uint32_t off = umma_tile_offset(el * NC + c, d * NP + j, M);
-          *reinterpret_cast<__nv_bfloat16*>(sBhi + off) = h;
-          *reinterpret_cast<__nv_bfloat16*>(sBlo + off) = l;
-        }
+        for (int c = 0; c < NC; ++c)
+          put(el, c, d * NP + j, iJ[d * 3 + 0] * F[c] + iJ[d * 3 + 1] * F[NC + c] + iJ[d * 3 + 2] * F[2 * NC + c]);
     }
-    // ---- face fluxes scaled by side*area/(6V) -> k = 3NP + lf*NFP + m
+    // ---- face fluxes: (f - Fbar.n) * side*area/(6V) -> k = 3NP + lf*NFP + m
     for (int idx = tid; idx < ne_here * 4 * NFP; idx += NT) {
       const int el = idx / (4 * NFP), fm = idx - el * 4 * NFP;
       const int lf = fm / NFP, m = fm - lf * NFP, t = el % 6, cl = el / 6;
+      const int ax = tab->axis[t][lf];
+      const bool own_left = tab->side[t][lf] == 0;
+      if (ax < 0 && !own_left) continue;  // inside the cube: the side-0 tet writes both rows
       const int cell = cell0 + cl;
       const int ck = cell / nxy, rem = cell - ck * nxy, cj = rem / args.nx, ci = rem - cj * args.nx;
-      const int ax = tab->axis[t][lf], dir = tab->dir[t][lf];
       int code;
-      const int mode = face_mode(ax, dir, ax == 0 ? ci : (ax == 1 ? cj : ck),
+      const int mode = face_mode(ax, tab->dir[t][lf], ax == 0 ? ci : (ax == 1 ? cj : ck),
                                  ax == 0 ? args.nx : (ax == 1 ? args.ny : args.nz), args.bc, code);
       const float* qo = &q[(el * NP + tab->own_node[lf][m]) * NC];
       float nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1], nz = tab->normal[t][lf][2];
       float scale = tab->fscale[t][lf];
       float qn[NC], qg[NC];
+      const int nbt = tab->nb_t[t][lf];
       if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
-        const int nbt = tab->nb_t[t][lf], nbn = tab->nb_node[t][lf][m];
+        const int nbn = tab->nb_node[t][lf][m];
         if (ax < 0) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) qn[c] = q[((cl * 6 + nbt) * NP + nbn) * NC + c];
@@ -185,18 +221,20 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
       }
       const bool bcf = mode != FACE_INTERIOR;
       if (bcf) ph.ghost(qn, code, nx, ny, nz, qg);
-      const bool own_left = tab->side[t][lf] == 0;
       const float* L = bcf ? qn : (own_left ? qo : qn);
       const float* Rr = bcf ? qg : (own_left ? qn : qo);
       float f[NC];
       ph.num_flux(L, Rr, nx, ny, nz, f);
+      const float* Fb = &sF[el * 3 * NC];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        __nv_bfloat16 h, l;
-        split_bf16(scale * f[c], h, l);
-        const uint32_t off = umma_tile_offset(el * NC + c, 3 * NP + fm, M);
-        *reinterpret_cast<__nv_bfloat16*>(sBhi + off) = h;
-        *reinterpret_cast<__nv_bfloat16*>(sBlo + off) = l;
+      for (int c = 0; c < NC; ++c) put(el, c, 3 * NP + fm, scale * (f[c] - (Fb[c] * nx + Fb[NC + c] * ny + Fb[2 * NC + c] * nz)));
+      if (ax < 0) {  // the other tet of this cube face: same flux, its own scale and Fbar
+        const int el2 = cl * 6 + nbt, lf2 = tab->nb_lf[t][lf];
+        const float s2 = tab->fscale[nbt][lf2];
+        const float* Fb2 = &sF[el2 * 3 * NC];
+        const int k2 = 3 * NP + lf2 * NFP + tab->nb_m[t][lf][m];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) put(el2, c, k2, s2 * (f[c] - (Fb2[c] * nx + Fb2[NC + c] * ny + Fb2[2 * NC + c] * nz)));
       }
     }
     // make the generic-proxy tile writes visible to the tensor-core (async) proxy
@@ -225,14 +263,14 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
     mma_parity ^= 1u;
     mma_pending = false;
     tc_fence_after();
-    if (warp < 4) {  // warp w reads TMEM lanes [32w, 32w+32): rows (el, c)
+    if (warp < 4) {  // warp w reads TMEM lanes [32w, 32w+32): rows (c, el)
       const int row = warp * 32 + lane;
       float v[NN];
 #pragma unroll
       for (int c0 = 0; c0 < NN; c0 += 16) tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + c0, v + c0);
       tmem_ld_wait();
-      if (row < ne_here * NC) {
-        const int el = row / NC, c = row - el * NC;
+      const int c = row / EBP, el = row - c * EBP;
+      if (c < NC && el < ne_here) {
 #pragma unroll
         for (int i = 0; i < NP; ++i) sO[(el * NP + i) * NC + c] = v[i];
       }
