@@ -166,6 +166,17 @@ int mxm_dg_max_wavespeed(void* handle, double* out);
  * kind 1: integral of q_c^2 (nodal quadrature); kind 2: max |q_c|.
  * Reductions accumulate in FP64 on the device in a fixed order. */
 int mxm_dg_reduce_conserved(void* handle, int which, int c, int kind, double* out);
+/* The same reduction without any device allocation; it has no counterpart
+ * in the reference.  Its scratch is a static device array of the library
+ * (4096 first-pass partials plus the result slot), so `nblocks`, the number
+ * of first-pass blocks, must lie in 0..4096 (0 picks the same count as
+ * mxm_dg_reduce_conserved, which makes the two results bit-identical);
+ * larger values return MXM_DG_EINVAL with a message.  The first call on a
+ * device looks the scratch up (one-time set-up), so make it before any
+ * stream capture.  Nothing in the scratch needs to start at zero.  The
+ * scratch is shared by all handles on a device: calls whose work overlaps
+ * on one device (other host threads, other streams) race on it. */
+int mxm_dg_reduce_conserved_noalloc(void* handle, int which, int c, int kind, int nblocks, double* out);
 
 /* ---- misc ---------------------------------------------------------------- */
 /* Make `device` the current CUDA device of the calling thread; handles are

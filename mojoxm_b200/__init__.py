@@ -42,6 +42,7 @@ EXPORTED = [
     "mxm_dg_limit", "mxm_dg_advance_host", "mxm_dg_max_wavespeed", "mxm_dg_reduce_conserved",
     "mxm_dg_synchronize", "mxm_dg_time_steps", "mxm_dg_launches_per_step", "mxm_dg_last_error",
     "mxm_dg_operator", "mxm_dg_reference_operators", "mxm_dg_set_device", "mxm_dg_host_alloc", "mxm_dg_host_free",
+    "mxm_dg_reduce_conserved_noalloc",
 ]
 
 
@@ -96,6 +97,7 @@ def lib():
         L.mxm_dg_advance_host.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double]
         L.mxm_dg_max_wavespeed.argtypes = [vp, dp]
         L.mxm_dg_reduce_conserved.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
+        L.mxm_dg_reduce_conserved_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
         L.mxm_dg_synchronize.argtypes = [vp]
         L.mxm_dg_time_steps.argtypes = [vp, ctypes.c_double, ctypes.c_int, dp]
         L.mxm_dg_launches_per_step.argtypes = [vp, i32p]

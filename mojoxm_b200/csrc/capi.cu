@@ -849,6 +849,57 @@ int mxm_dg_reduce_conserved(void* handle, int which, int c, int kind, double* ou
   API_END
 }
 
+// Allocation-free variant of mxm_dg_reduce_conserved.  Callers that cannot
+// let the library allocate: a host driver that runs its conservation
+// diagnostics after device memory has been exhausted (an ENOMEM from
+// create or admission), where a fresh cudaMalloc would fail, and a server
+// that admits solves against a fixed HBM budget and counts every byte of
+// device memory up front, where a hidden per-call buffer would break the
+// count.  Its scratch is a fixed-size static device array of the library
+// module; the first call on a device looks that array's address up (module
+// set-up), later calls only launch.
+namespace {
+std::mutex g_static_mu;
+double* g_static_scratch[64] = {};
+}  // namespace
+
+int mxm_dg_reduce_conserved_noalloc(void* handle, int which, int c, int kind, int nblocks, double* out) {
+  API_BEGIN
+  if (which < 0 || which > 2 || c < 0 || c >= h->NC || kind < 0 || kind > 2 || !out)
+    throw mxm::ArgError("which 0..2, component in range, kind 0..2, out non-null");
+  if (nblocks < 0 || nblocks > mxm::kStaticPartials)
+    throw mxm::ArgError("nblocks " + std::to_string(nblocks) + " is outside 0.." +
+                        std::to_string(mxm::kStaticPartials) + ", the size of the static reduction scratch");
+  if (h->device < 0 || h->device >= 64) throw mxm::ArgError("device ordinal beyond the static scratch table");
+  double* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_static_mu);
+    if (!g_static_scratch[h->device]) {
+      CK(mxm::static_reduce_scratch(&g_static_scratch[h->device]));
+    }
+    scratch = g_static_scratch[h->device];
+  }
+  const int64_t want = (h->ne + 255) / 256;
+  const int nb = nblocks > 0 ? nblocks : int(want < h->npartial ? want : h->npartial);
+  const double vol = h->dim == 3 ? (h->lx / h->nx) * (h->ly / h->ny) * (h->lz / h->nz) / 6.0
+                                 : (h->lx / h->nx) * (h->ly / h->ny) / 2.0;
+  const double scale = kind == 2 ? 1.0 : vol;
+  double* result = scratch + mxm::kStaticPartials;
+  cudaError_t e = h->rbytes == 8
+                      ? mxm::launch_reduce<double>(h->P, h->dim, h->NC, (const double*)h->q[which], (const double*)h->w,
+                                                   h->ne, c, kind, scale, scratch, nb, result, h->stream)
+                      : mxm::launch_reduce<float>(h->P, h->dim, h->NC, (const float*)h->q[which], (const float*)h->w,
+                                                  h->ne, c, kind, scale, scratch, nb, result, h->stream);
+  if (e != cudaSuccess) throw mxm::CudaError(e, "reduction launch");
+  CK(cudaMemcpyAsync(out, result, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (!(*out == *out) || *out > 1.0e300 || *out < -1.0e300) {
+    h->err = "non-finite reduction result";
+    return MXM_DG_ENONFINITE;
+  }
+  API_END
+}
+
 int mxm_dg_set_device(int device) {
   if (cudaSetDevice(device) != cudaSuccess) {
     std::lock_guard<std::mutex> g(mxm::g_err_mu);

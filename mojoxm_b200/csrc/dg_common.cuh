@@ -180,5 +180,10 @@ cudaError_t launch_limiter(int dim, int P, int NC, const LimArgs<R>& a, const Ku
 template <class R>
 cudaError_t launch_reduce(int P, int dim, int NC, const R* q, const R* w, int64_t ne, int c, int kind, double scale,
                           double* partial, int npartial, double* out, cudaStream_t st);
+// Static (module-resident) scratch of the allocation-free reduction: the
+// address of kStaticPartials partial slots followed by the result slot, on
+// the calling thread's current device.
+constexpr int kStaticPartials = 4096;
+cudaError_t static_reduce_scratch(double** ptr);
 
 }  // namespace mxm

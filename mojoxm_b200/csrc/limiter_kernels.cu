@@ -101,6 +101,18 @@ cudaError_t launch_reduce(int P, int dim, int NC, const R* q, const R* w, int64_
   return cudaErrorInvalidValue;
 }
 
+// Scratch of the allocation-free reduction: kStaticPartials first-pass
+// partial sums followed by one result slot, in the module's own static
+// device memory.  The first pass writes every partial it launches a block
+// for and the second pass writes the result slot, so nothing here has to
+// start at zero.  The array is shared by every caller on a device: two
+// reductions in flight at once on one device race on it.
+static __device__ __align__(256) double g_static_reduce_scratch[kStaticPartials + 32];
+
+cudaError_t static_reduce_scratch(double** ptr) {
+  return cudaGetSymbolAddress((void**)ptr, g_static_reduce_scratch);
+}
+
 template cudaError_t launch_limiter<double>(int, int, int, const LimArgs<double>&, const KuhnTab3<double>&,
                                             const KuhnTab2<double>&, cudaStream_t);
 template cudaError_t launch_limiter<float>(int, int, int, const LimArgs<float>&, const KuhnTab3<float>&,
