@@ -3,9 +3,12 @@
 
 Workload (default): 3D Euler smooth density wave rho = 1 + 0.2 sin(2 pi (x+y+z)),
 u = (1,1,1), p = 1 on the periodic [0,1]^3 Kuhn mesh of 32^3 cubes x 6 =
-196,608 tets, order P = 3 (NP = 20), Rusanov flux, plain FP64.  A step is one
-SSPRK3 step = 3 fused stage kernels over the whole mesh; the metric counts
-Ne*NP*NC DOF per stage (Solver.dof_count, src/solver.mojo:757-763).
+196,608 tets, order P = 3 (NP = 20), Rusanov flux; FP32 state with the
+volume/lift contraction as split-BF16 tcgen05 products (--precision mixed,
+the default), beside the plain FP64 kernels on the same workload
+(`plain_f64` in the JSON line).  A step is one SSPRK3 step = 3 fused stage
+kernels over the whole mesh; the metric counts Ne*NP*NC DOF per stage
+(Solver.dof_count, src/solver.mojo:757-763).
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -45,7 +48,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=32, help="cubes per axis")
     ap.add_argument("--P", type=int, default=3)
-    ap.add_argument("--precision", default="f64", choices=["f64", "f32", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["f64", "f32", "mixed"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--l2-steps", type=int, default=100,
                     help="SSPRK3 steps of the accuracy check vs the FP64 path (0 = skip)")
@@ -104,6 +107,66 @@ def workload_name(a):
 
 
 DTYPE = {"f64": "f64", "f32": "f32", "mixed": "f32+bf16x3"}
+
+
+class NvmlClockSampler:
+    """SM clock and clock-event reasons sampled through NVML every 2 ms while
+    the timed region runs (short timed regions still get samples)."""
+
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
+
+    def __init__(self, device):
+        import pynvml
+
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        idx = device
+        if vis:
+            parts = [p.strip() for p in vis.split(",")]
+            if device < len(parts) and parts[device].isdigit():
+                idx = int(parts[device])
+        self.h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+        self.samples, self.reasons, self.stop = [], set(), threading.Event()
+        self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+
+    def _run(self):
+        nv = self.nv
+        while True:
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                get = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                    nv.nvmlDeviceGetCurrentClocksThrottleReasons
+                r = int(get(self.h))
+                for name, bit in self.BITS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            if self.stop.wait(0.002):
+                break
+
+    def __enter__(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.t.join(timeout=2)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples), "source": "nvml"}
+
+
+def clock_sampler(device):
+    try:
+        return NvmlClockSampler(device)
+    except Exception:
+        return ClockSampler(device)
 
 
 class ClockSampler:
@@ -208,7 +271,7 @@ def run_reference(a, rank, world):
     cb = cpu_baseline(a, a.cpu_seconds)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": DTYPE[a.precision], "data": "synthetic",
+            "dtype": "f64" if a.precision == "f64" else "f32", "data": "synthetic",
             "config": {"workload": workload_name(a), "sample": cb["sample"]},
             "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
@@ -250,7 +313,7 @@ def main():
     # warm-up (>= 3 SSPRK3 steps)
     s.step_n(dt, max(3, a.warmup))
     barrier()
-    with ClockSampler(local) as clk:
+    with clock_sampler(local) as clk:
         ms = s.time_steps(dt, a.steps)  # CUDA events on the solver's stream
     barrier()
     ms_max = ms
@@ -285,6 +348,25 @@ def main():
     pin_in.free()
     pin_out.free()
 
+    # the plain FP64 kernels on the same workload (the ratio's denominator)
+    plain = None
+    if a.precision != "f64":
+        s64 = M.Solver(M.Mesh(a.n, a.n, a.n, 1.0, 1.0, 1.0), phys, P=a.P, precision="f64")
+        s64.upload_state(q0)
+        s64.step_n(dt, max(3, a.warmup))
+        barrier()
+        ms64 = s64.time_steps(dt, a.steps)
+        barrier()
+        if dist:
+            import torch
+
+            t = torch.tensor([ms64], dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms64 = float(t.item())
+        s64.close()
+        v64 = world * 3 * dof * a.steps / (ms64 * 1e-3)
+        plain = {"value": v64, "ms_per_step": ms64 / a.steps, "speedup": value / v64}
+
     if rank == 0:
         peak, peak_kind = peaks()
         launches = s.launches_per_step()
@@ -310,6 +392,7 @@ def main():
                          "alg_bytes_per_launch": alg_bytes,
                          "contraction_tflops": nsm_flops / avg_launch_s / 1e12},
             "cpu_baseline": cb,
+            "plain_f64": plain,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": qbytes,
                     "entry": "mxm_dg_advance_host (pinned host state in/out, 1 SSPRK3 step per call)"},
             "gpu_launches": launches * a.steps,

@@ -202,6 +202,92 @@ int mxm_dg_operator(void* handle, double* host, int64_t* count);
  * Lift [nfaces*NP*NFP] in the reference's face-local order, w [NP]. */
 int mxm_dg_reference_operators(int dim, int P, double* D, double* Lift, double* w);
 
+/* ---- initial conditions on the device ------------------------------------
+ * Fill state buffer `which` from node coordinates computed on the device
+ * (the role of the reference's IC kernels, e.g. examples/euler_vortex.mojo:
+ * 87-129).  params (nparams <= 16):
+ *   CONSTANT    NC state values
+ *   SINE_WAVE   Euler: rho0, amp, u, v, w, p, kx, ky, kz:
+ *               rho = rho0 + amp sin(2 pi (kx x + ky y + kz z)), uniform u, p
+ *   VORTEX      Euler isentropic vortex: beta, x0, y0, u, v, w, periodic(0/1)
+ *               (nearest periodic image when 1); gamma from the physics
+ *   SOD         Euler tanh-smoothed tube along x: rhoL, pL, rhoR, pR, x0, width
+ *   DAM_BREAK   shallow water at rest: hL, hR, x0, width
+ *   CAVITY      Maxwell: mx, my, amp: E_z = amp sin(mx pi x/Lx) sin(my pi y/Ly)
+ *   PLANE_WAVE  Maxwell: amp, k: E_z = amp sin(2 pi k x/Lx), B_y = -E_z/c */
+#define MXM_DG_IC_CONSTANT 0
+#define MXM_DG_IC_SINE_WAVE 1
+#define MXM_DG_IC_VORTEX 2
+#define MXM_DG_IC_SOD 3
+#define MXM_DG_IC_DAM_BREAK 4
+#define MXM_DG_IC_CAVITY 5
+#define MXM_DG_IC_PLANE_WAVE 6
+int mxm_dg_fill_ic(void* handle, int which, int kind, const double* params, int nparams);
+
+/* ---- batched engine (no reference counterpart: the reference runs each
+ * 2D solve through its own driver loop, examples/euler_sod_2d_gpu.mojo +
+ * src/ssprk3.mojo:56-78) ----------------------------------------------------
+ * A batch advances many independent 2D solves of uneven mesh size, order P
+ * and physics together: per SSPRK3 stage one persistent stage launch per
+ * physics group (solves whose physics descriptors are identical) plus the
+ * two limiter passes for groups with limited solves, the whole step captured
+ * once in a CUDA graph and replayed.  Members are ordinary solver handles
+ * (2D, one precision per batch); their state stays in their own buffers and
+ * each advances with its own dt.  Enable limiters and upload states before
+ * the first batch step; adding a solve re-plans the batch.  Synchronize the
+ * batch before reading a member's state; destroy the batch before its
+ * members. */
+int mxm_dg_batch_create(void** batch);
+int mxm_dg_batch_destroy(void* batch);
+int mxm_dg_batch_add(void* batch, void* solver, double dt, int32_t* index);
+/* Pick the cells per tile of every (physics group, P) by timing the batched
+ * stage kernel on the batch's own solves; runs by itself on the first step
+ * when not called. */
+int mxm_dg_batch_autotune(void* batch);
+/* The tuned cells per tile used for member `member`. */
+int mxm_dg_batch_tile_cells(void* batch, int member, int32_t* cells);
+/* `nsteps` SSPRK3 steps of every member (one graph replay per step). */
+int mxm_dg_batch_step(void* batch, int nsteps);
+/* As mxm_dg_batch_step, timed with CUDA events on the batch stream. */
+int mxm_dg_batch_time_steps(void* batch, int nsteps, double* ms);
+int mxm_dg_batch_synchronize(void* batch);
+/* Sum over members of Ne*NP*NC. */
+int mxm_dg_batch_dof_count(void* batch, int64_t* dof);
+/* Kernel launches per batched SSPRK3 step. */
+int mxm_dg_batch_launches_per_step(void* batch, int32_t* n);
+/* Last error message of the batch (batch may be NULL for create errors). */
+int mxm_dg_batch_last_error(void* batch, char* buf, int len);
+
+/* ---- serving loop (no reference counterpart) -----------------------------
+ * Continuous batching of independent solves on the calling thread's device:
+ * a scheduler thread admits submitted requests in arrival order while their
+ * device footprint (three state buffers, limiter means, operator) fits
+ * `hbm_budget_bytes` and fewer than `max_active` are running, builds each on
+ * its own stream (handle + device IC fill, see mxm_dg_fill_ic) and feeds
+ * every running solve chunks of `steps_per_chunk` SSPRK3 steps, so requests
+ * that arrive while others run are admitted as memory frees up and their
+ * kernels overlap.  A finished solve's state (buffer q, Ne*NP*NC values of
+ * its real type) is copied to `out_host` (caller-owned, may be NULL) and its
+ * memory released; latency = submit -> result on the host.  Each solve's
+ * arithmetic is that of a single solve on its own buffers.  All calls are
+ * thread-safe. */
+int mxm_dg_server_create(double hbm_budget_bytes, int max_active, int steps_per_chunk, void** server);
+/* Stops the scheduler: queued requests fail, running ones are drained. */
+int mxm_dg_server_destroy(void* server);
+int mxm_dg_server_submit(void* server, const mxm_dg_mesh_desc* mesh, const mxm_dg_physics_desc* phys, int P,
+                         int precision, int ic_kind, const double* ic_params, int nparams, int limiter,
+                         double venkat_eps, double dt, int nsteps, void* out_host, int64_t* request_id);
+/* MXM_DG_OK when finished, MXM_DG_ENOTREADY while queued or running. */
+int mxm_dg_server_poll(void* server, int64_t request_id, double* latency_ms);
+/* Block until finished or `timeout_s` passes (MXM_DG_ETIMEDOUT). */
+int mxm_dg_server_wait(void* server, int64_t request_id, double timeout_s, double* latency_ms);
+/* out[0] completed, [1] failed, [2] p50 ms, [3] p99 ms, [4] mean ms,
+ * [5] solves/s and [6] DOF·stage/s from the first submit to the last
+ * completion, [7] peak admitted bytes, [8] peak concurrent solves,
+ * [9] queued now, [10] running now. */
+int mxm_dg_server_stats(void* server, double* out, int n);
+int mxm_dg_server_last_error(void* server, char* buf, int len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,7 +43,15 @@ EXPORTED = [
     "mxm_dg_synchronize", "mxm_dg_time_steps", "mxm_dg_launches_per_step", "mxm_dg_last_error",
     "mxm_dg_operator", "mxm_dg_reference_operators", "mxm_dg_set_device", "mxm_dg_host_alloc", "mxm_dg_host_free",
     "mxm_dg_reduce_conserved_noalloc",
+    "mxm_dg_batch_create", "mxm_dg_batch_destroy", "mxm_dg_batch_add", "mxm_dg_batch_autotune",
+    "mxm_dg_batch_tile_cells", "mxm_dg_batch_step", "mxm_dg_batch_time_steps", "mxm_dg_batch_synchronize",
+    "mxm_dg_batch_dof_count", "mxm_dg_batch_launches_per_step", "mxm_dg_batch_last_error",
+    "mxm_dg_fill_ic",
+    "mxm_dg_server_create", "mxm_dg_server_destroy", "mxm_dg_server_submit", "mxm_dg_server_poll",
+    "mxm_dg_server_wait", "mxm_dg_server_stats", "mxm_dg_server_last_error",
 ]
+
+IC_CONSTANT, IC_SINE_WAVE, IC_VORTEX, IC_SOD, IC_DAM_BREAK, IC_CAVITY, IC_PLANE_WAVE = range(7)
 
 
 class DGError(RuntimeError):
@@ -107,6 +115,27 @@ def lib():
         L.mxm_dg_set_device.argtypes = [ctypes.c_int]
         L.mxm_dg_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
         L.mxm_dg_host_free.argtypes = [vp]
+        L.mxm_dg_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p)]
+        L.mxm_dg_batch_destroy.argtypes = [vp]
+        L.mxm_dg_batch_add.argtypes = [vp, vp, ctypes.c_double, i32p]
+        L.mxm_dg_batch_autotune.argtypes = [vp]
+        L.mxm_dg_batch_tile_cells.argtypes = [vp, ctypes.c_int, i32p]
+        L.mxm_dg_batch_step.argtypes = [vp, ctypes.c_int]
+        L.mxm_dg_batch_time_steps.argtypes = [vp, ctypes.c_int, dp]
+        L.mxm_dg_batch_synchronize.argtypes = [vp]
+        L.mxm_dg_batch_dof_count.argtypes = [vp, i64p]
+        L.mxm_dg_batch_launches_per_step.argtypes = [vp, i32p]
+        L.mxm_dg_batch_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+        L.mxm_dg_fill_ic.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
+        L.mxm_dg_server_create.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.mxm_dg_server_destroy.argtypes = [vp]
+        L.mxm_dg_server_submit.argtypes = [vp, ctypes.POINTER(_MeshDesc), ctypes.POINTER(_PhysDesc), ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, dp, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_int, vp, i64p]
+        L.mxm_dg_server_poll.argtypes = [vp, ctypes.c_int64, dp]
+        L.mxm_dg_server_wait.argtypes = [vp, ctypes.c_int64, ctypes.c_double, dp]
+        L.mxm_dg_server_stats.argtypes = [vp, dp, ctypes.c_int]
+        L.mxm_dg_server_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -321,6 +350,11 @@ class Solver:
         self._c(lib().mxm_dg_node_xyz_ptr(self.h, ctypes.byref(p)))
         return p.value
 
+    def fill_ic(self, kind, params, which=0):
+        """Device initial condition (mxm_dg_fill_ic) from node coordinates."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        self._c(lib().mxm_dg_fill_ic(self.h, which, kind, p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), p.size))
+
     def upload_state(self, q, which=0):
         a = np.ascontiguousarray(q, dtype=self.dtype).reshape(-1)
         assert a.size == self.num_elements * self.NP * self.NC, "state size mismatch"
@@ -414,6 +448,165 @@ class Solver:
         out = np.zeros(n.value)
         self._c(lib().mxm_dg_operator(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(n)))
         return out
+
+
+class Batch:
+    """Many independent 2D solves advanced together (mxm_dg_batch_*): one
+    persistent stage launch per physics group and stage, the SSPRK3 step
+    captured as a CUDA graph, tile sizes autotuned per (group, P)."""
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        rc = lib().mxm_dg_batch_create(ctypes.byref(h))
+        if rc != OK:
+            raise DGError(rc, self._err(None))
+        self.h = h
+        self.members = []
+
+    @staticmethod
+    def _err(h):
+        buf = ctypes.create_string_buffer(1024)
+        lib().mxm_dg_batch_last_error(h, buf, 1024)
+        return buf.value.decode(errors="replace")
+
+    def _c(self, rc):
+        if rc != OK:
+            raise DGError(rc, self._err(self.h))
+
+    def add(self, solver: Solver, dt: float) -> int:
+        i = ctypes.c_int32()
+        self._c(lib().mxm_dg_batch_add(self.h, solver.h, dt, ctypes.byref(i)))
+        self.members.append(solver)
+        return i.value
+
+    def autotune(self):
+        self._c(lib().mxm_dg_batch_autotune(self.h))
+
+    def tile_cells(self, member):
+        v = ctypes.c_int32()
+        self._c(lib().mxm_dg_batch_tile_cells(self.h, member, ctypes.byref(v)))
+        return v.value
+
+    def step(self, nsteps=1):
+        self._c(lib().mxm_dg_batch_step(self.h, nsteps))
+
+    def time_steps(self, nsteps):
+        ms = ctypes.c_double()
+        self._c(lib().mxm_dg_batch_time_steps(self.h, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def synchronize(self):
+        self._c(lib().mxm_dg_batch_synchronize(self.h))
+
+    def dof_count(self):
+        v = ctypes.c_int64()
+        self._c(lib().mxm_dg_batch_dof_count(self.h, ctypes.byref(v)))
+        return v.value
+
+    def launches_per_step(self):
+        v = ctypes.c_int32()
+        self._c(lib().mxm_dg_batch_launches_per_step(self.h, ctypes.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mxm_dg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _phys_desc(physics):
+    pd = _PhysDesc()
+    pd.kind, pd.flux_type, pd.entropy_fix = physics.kind, physics.flux_type, int(physics.entropy_fix)
+    for k, v in enumerate(physics.params()):
+        pd.p[k] = v
+    return pd
+
+
+def state_shape(mesh: Mesh, physics, P: int):
+    """(Ne, NP, NC) of a solve on `mesh` with `physics` at order P."""
+    dim = mesh.dim
+    ne = mesh.nx * mesh.ny * (mesh.nz if dim == 3 else 1) * (6 if dim == 3 else 2)
+    NP = (P + 1) * (P + 2) * (P + 3) // 6 if dim == 3 else (P + 1) * (P + 2) // 2
+    NC = {PHYS_ADVECTION: 1, PHYS_EULER: 5 if dim == 3 else 4, PHYS_MAXWELL: 6, PHYS_SHALLOW_WATER: 3}[physics.kind]
+    return ne, NP, NC
+
+
+class Server:
+    """Continuous-batching serving loop (mxm_dg_server_*): requests are
+    admitted by HBM budget, run concurrently on their own streams, and their
+    final states land in host arrays."""
+
+    def __init__(self, hbm_budget_bytes=150e9, max_active=64, steps_per_chunk=10):
+        h = ctypes.c_void_p()
+        _check(lib().mxm_dg_server_create(hbm_budget_bytes, max_active, steps_per_chunk, ctypes.byref(h)))
+        self.h = h
+        self._out = {}
+
+    def _errmsg(self):
+        buf = ctypes.create_string_buffer(1024)
+        lib().mxm_dg_server_last_error(self.h, buf, 1024)
+        return buf.value.decode(errors="replace")
+
+    def submit(self, mesh: Mesh, physics, P, precision, ic_kind, ic_params, dt, nsteps, limiter_eps=None):
+        shape = state_shape(mesh, physics, P)
+        out = np.empty(shape, dtype=np.float64 if precision == "f64" else np.float32)
+        p = np.ascontiguousarray(ic_params, dtype=np.float64)
+        md, pd = mesh.desc(), _phys_desc(physics)
+        rid = ctypes.c_int64()
+        rc = lib().mxm_dg_server_submit(self.h, ctypes.byref(md), ctypes.byref(pd), P, PREC[precision], ic_kind,
+                                        p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), p.size,
+                                        0 if limiter_eps is None else 1,
+                                        0.1 if limiter_eps is None else limiter_eps, dt, nsteps,
+                                        out.ctypes.data, ctypes.byref(rid))
+        if rc != OK:
+            raise DGError(rc, self._errmsg())
+        self._out[rid.value] = out
+        return rid.value
+
+    def poll(self, rid):
+        lat = ctypes.c_double()
+        rc = lib().mxm_dg_server_poll(self.h, rid, ctypes.byref(lat))
+        if rc == ENOTREADY:
+            return None
+        if rc != OK:
+            raise DGError(rc, self._errmsg())
+        return lat.value
+
+    def wait(self, rid, timeout_s=600.0):
+        """Latency in ms once the request finished."""
+        lat = ctypes.c_double()
+        rc = lib().mxm_dg_server_wait(self.h, rid, timeout_s, ctypes.byref(lat))
+        if rc != OK:
+            raise DGError(rc, self._errmsg())
+        return lat.value
+
+    def result(self, rid):
+        self.wait(rid)
+        return self._out[rid]
+
+    def stats(self):
+        v = np.zeros(11)
+        _check(lib().mxm_dg_server_stats(self.h, v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 11))
+        keys = ["completed", "failed", "p50_ms", "p99_ms", "mean_ms", "solves_per_s", "dof_stage_per_s",
+                "peak_bytes", "peak_concurrent", "queued", "running"]
+        return dict(zip(keys, v.tolist()))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mxm_dg_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def reference_operators(dim, P):

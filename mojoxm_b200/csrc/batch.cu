@@ -1,0 +1,506 @@
+// Batched engine of the C ABI (mxm_dg_batch_*): many independent 2D solves
+// of uneven mesh size and order advanced together, one persistent stage
+// launch per physics group and stage, the whole SSPRK3 step (counter resets,
+// stage kernels, limiter passes) captured once in a CUDA graph and replayed.
+// Tile sizes (cells per tile) per (group, P) come from an autotuner that
+// times the batched stage kernel on the batch's own solves.
+//
+// The reference has no batching: each 2D solve runs its own driver loop
+// (examples/euler_sod_2d_gpu.mojo, src/ssprk3.mojo:56-78).  Member solves are
+// ordinary solver handles; their state stays in their own buffers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "batch2d.cuh"
+#include "batch2d_launch.hpp"
+#include "handle.hpp"
+
+namespace mxm {
+
+struct BatchGroup {
+  mxm_dg_physics_desc phys{};
+  int NC = 0;
+  std::vector<int> members;  // indices into Batch::members
+  int ec[6] = {0, 0, 0, 0, 0, 0};
+  int4* d_items = nullptr;
+  int nitems = 0;
+  int4* d_litems = nullptr;  // limiter chunks of the limited members
+  int nlitems = 0;
+  int* d_counter = nullptr;  // [3]: one work counter per stage
+  size_t smem = 0;
+  int grid = 0;
+  int qv = 0, a_len = 0, aoff[6] = {0, 0, 0, 0, 0, 0};
+  const void* A[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+struct Batch {
+  int device = 0, nsm = 148;
+  cudaStream_t stream = nullptr;
+  size_t rbytes = 0;
+  std::vector<Handle*> members;
+  std::vector<double> dt;
+  std::vector<BatchGroup> groups;
+  void* d_solves = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool built = false, tuned = false;
+  int* derr = nullptr;
+  std::string err;
+};
+
+namespace {
+
+constexpr int kLimChunk = 128;      // elements per limiter block
+constexpr size_t kSmemCap = 200 * 1024;
+const int kEcCandidates[] = {1, 2, 4, 8, 16, 32, 64};
+
+size_t tab_bytes(size_t rb) {
+  return rb == 8 ? (sizeof(KuhnTab2<double>) + 15) / 16 * 16 : (sizeof(KuhnTab2<float>) + 15) / 16 * 16;
+}
+int ntri_h(int P) { return (P + 1) * (P + 2) / 2; }
+int klen2d(int P) { return 2 * ntri_h(P) + 3 * (P + 1); }
+
+void release_graph(Batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->built = false;
+}
+
+void free_group(BatchGroup& g) {
+  cudaFree(g.d_items);
+  cudaFree(g.d_litems);
+  cudaFree(g.d_counter);
+  g.d_items = g.d_litems = nullptr;
+  g.d_counter = nullptr;
+}
+
+template <class R>
+void upload_solves(Batch* b) {
+  std::vector<SolveDesc2<R>> sd(b->members.size());
+  for (size_t i = 0; i < b->members.size(); ++i) {
+    const Handle* h = b->members[i];
+    SolveDesc2<R>& d = sd[i];
+    std::memset(&d, 0, sizeof(d));
+    d.tab = h->rbytes == 8 ? reinterpret_cast<const KuhnTab2<R>&>(h->t2d) : reinterpret_cast<const KuhnTab2<R>&>(h->t2f);
+    for (int k = 0; k < 3; ++k) d.q[k] = (R*)h->q[k];
+    d.avg = (R*)h->avg;
+    d.w = (const R*)h->w;
+    d.dt = R(b->dt[i]);
+    if (sizeof(R) == 4) {
+      const float ef = float(h->lim_eps);  // as the single-solve limiter: eps2 = eps*eps in FP32
+      d.eps2 = R(ef * ef);
+    } else {
+      d.eps2 = R(h->lim_eps * h->lim_eps);
+    }
+    d.P = h->P;
+    d.nx = h->nx;
+    d.ny = h->ny;
+    d.ncell = int(h->ncell);
+    for (int k = 0; k < 4; ++k) d.bc[k] = h->bc[k];
+    d.limiter = h->lim_on ? 1 : 0;
+  }
+  cudaFree(b->d_solves);
+  b->d_solves = nullptr;
+  CK(cudaMalloc(&b->d_solves, sd.size() * sizeof(SolveDesc2<R>)));
+  CK(cudaMemcpy(b->d_solves, sd.data(), sd.size() * sizeof(SolveDesc2<R>), cudaMemcpyHostToDevice));
+}
+
+// tile items {solve, first cell, cells, P} of the group's members whose order
+// is in `onlyP` (0 = all), heaviest P first
+std::vector<int4> make_items(const Batch* b, const BatchGroup& g, const int* ec, int onlyP) {
+  std::vector<int4> it;
+  for (int P = 5; P >= 1; --P) {
+    if (onlyP && P != onlyP) continue;
+    for (int m : g.members) {
+      const Handle* h = b->members[m];
+      if (h->P != P) continue;
+      const int E = ec[P];
+      for (int c0 = 0; c0 < int(h->ncell); c0 += E) it.push_back(make_int4(m, c0, std::min(E, int(h->ncell) - c0), P));
+    }
+  }
+  return it;
+}
+
+// shared-memory layout of the group's stage kernel for tile sizes ec[]
+void layout(const Batch* b, BatchGroup& g, const int* ec) {
+  bool present[6] = {false, false, false, false, false, false};
+  for (int m : g.members) present[b->members[m]->P] = true;
+  int off = 0, qv = 0, bmax = 0;
+  for (int P = 1; P <= 5; ++P) {
+    g.aoff[P] = 0;
+    g.A[P] = nullptr;
+    if (!present[P]) continue;
+    g.aoff[P] = off;
+    off += klen2d(P) * ntri_h(P);
+    for (int m : g.members)
+      if (b->members[m]->P == P) {
+        g.A[P] = b->members[m]->A;
+        break;
+      }
+    qv = std::max(qv, 2 * ec[P] * ntri_h(P) * g.NC);
+    bmax = std::max(bmax, 2 * ec[P] * bstr2d(P, g.NC, b->rbytes));
+  }
+  g.a_len = (off + 3) / 4 * 4;
+  g.qv = (qv + 3) / 4 * 4;
+  g.smem = 32 + 2 * tab_bytes(b->rbytes) + size_t(g.a_len + 2 * g.qv + bmax) * b->rbytes;
+}
+
+template <class R>
+Batch2DArgs<R> stage_args(const Batch* b, const BatchGroup& g, const int4* items, int nitems, int stage) {
+  Batch2DArgs<R> a;
+  std::memset(&a, 0, sizeof(a));
+  a.solves = (const SolveDesc2<R>*)b->d_solves;
+  a.items = items;
+  a.nitems = nitems;
+  a.counter = g.d_counter + stage;
+  a.stage = stage;
+  for (int P = 0; P < 6; ++P) {
+    a.A[P] = (const R*)g.A[P];
+    a.aoff[P] = g.aoff[P];
+  }
+  a.a_len = g.a_len;
+  a.qv = g.qv;
+  a.err = b->derr;
+  return a;
+}
+
+template <class R>
+cudaError_t launch_group_stage(const Batch* b, const BatchGroup& g, const int4* items, int nitems, int stage,
+                               int grid, size_t smem) {
+  const Batch2DArgs<R> a = stage_args<R>(b, g, items, nitems, stage);
+  return launch_stage2d_batch<R>(g.phys, a, grid, smem, b->stream);
+}
+
+template <class R>
+int grid_for(const Batch* b, const BatchGroup& g, size_t smem, int nitems) {
+  int bps = 1;
+  CK(stage2d_batch_blocks_per_sm<R>(g.phys, smem, &bps));
+  int grid = b->nsm * bps;
+  if (grid > nitems) grid = nitems;
+  return grid < 1 ? 1 : grid;
+}
+
+// Autotune the cells per tile of every (group, P): time stage 0 of the
+// group's members of that order (it writes only their q1 buffers) for each
+// candidate that fits the shared-memory cap, keep the fastest.
+template <class R>
+void autotune(Batch* b) {
+  upload_solves<R>(b);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  for (auto& g : b->groups) {
+    if (!g.d_counter) CK(cudaMalloc(&g.d_counter, 3 * sizeof(int)));
+    for (int P = 1; P <= 5; ++P) {
+      bool any = false;
+      for (int m : g.members) any = any || b->members[m]->P == P;
+      if (!any) continue;
+      double best = 1e30;
+      int best_ec = 1;
+      for (int E : kEcCandidates) {
+        int ec[6] = {0, 0, 0, 0, 0, 0};
+        ec[P] = E;
+        BatchGroup t = g;  // shallow copy for the layout of this trial
+        t.d_items = nullptr;
+        layout(b, t, ec);
+        if (t.smem > kSmemCap) continue;
+        std::vector<int4> items = make_items(b, t, ec, P);
+        int4* d_items = nullptr;
+        CK(cudaMalloc(&d_items, items.size() * sizeof(int4)));
+        CK(cudaMemcpy(d_items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        const int grid = grid_for<R>(b, t, t.smem, int(items.size()));
+        float tot = 0.f;
+        for (int rep = 0; rep < 4; ++rep) {
+          CK(cudaMemsetAsync(g.d_counter, 0, 3 * sizeof(int), b->stream));
+          CK(cudaEventRecord(e0, b->stream));
+          CK(launch_group_stage<R>(b, t, d_items, int(items.size()), 0, grid, t.smem));
+          CK(cudaEventRecord(e1, b->stream));
+          CK(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          CK(cudaEventElapsedTime(&ms, e0, e1));
+          if (rep > 0) tot += ms;  // first launch warms up
+        }
+        cudaFree(d_items);
+        if (tot < best) {
+          best = tot;
+          best_ec = E;
+        }
+      }
+      g.ec[P] = best_ec;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->tuned = true;
+}
+
+template <class R>
+void build(Batch* b) {
+  release_graph(b);
+  upload_solves<R>(b);
+  for (auto& g : b->groups) {
+    free_group(g);
+    layout(b, g, g.ec);
+    std::vector<int4> items = make_items(b, g, g.ec, 0);
+    g.nitems = int(items.size());
+    CK(cudaMalloc(&g.d_items, std::max<size_t>(1, items.size()) * sizeof(int4)));
+    CK(cudaMemcpy(g.d_items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    std::vector<int4> lit;
+    for (int m : g.members) {
+      const Handle* h = b->members[m];
+      if (!h->lim_on) continue;
+      for (int64_t e0 = 0; e0 < h->ne; e0 += kLimChunk)
+        lit.push_back(make_int4(m, int(e0), int(std::min<int64_t>(kLimChunk, h->ne - e0)), h->P));
+    }
+    g.nlitems = int(lit.size());
+    if (!lit.empty()) {
+      CK(cudaMalloc(&g.d_litems, lit.size() * sizeof(int4)));
+      CK(cudaMemcpy(g.d_litems, lit.data(), lit.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMalloc(&g.d_counter, 3 * sizeof(int)));
+    g.grid = grid_for<R>(b, g, g.smem, g.nitems);
+  }
+  // one SSPRK3 step as a graph
+  CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t cap = cudaSuccess;
+  for (auto& g : b->groups)
+    if (cap == cudaSuccess) cap = cudaMemsetAsync(g.d_counter, 0, 3 * sizeof(int), b->stream);
+  for (int s = 0; s < 3 && cap == cudaSuccess; ++s) {
+    for (auto& g : b->groups) {
+      if (cap != cudaSuccess) break;
+      cap = launch_group_stage<R>(b, g, g.d_items, g.nitems, s, g.grid, g.smem);
+    }
+    for (auto& g : b->groups) {
+      if (cap != cudaSuccess || g.nlitems == 0) continue;
+      LimBatch2DArgs<R> la;
+      la.solves = (const SolveDesc2<R>*)b->d_solves;
+      la.items = g.d_litems;
+      la.nitems = g.nlitems;
+      la.which = s == 0 ? 1 : (s == 1 ? 2 : 0);
+      cap = launch_lim2d_batch<R>(g.NC, la, b->stream);
+    }
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(b->stream, &graph);
+  if (cap != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    throw CudaError(cap, "batched step capture");
+  }
+  CK(end);
+  b->graph = graph;
+  CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  b->built = true;
+}
+
+void ensure_built(Batch* b) {
+  if (b->built) return;
+  if (b->members.empty()) throw ArgError("the batch has no solves");
+  // members must be idle before the batch stream uses their buffers
+  for (Handle* h : b->members) CK(cudaStreamSynchronize(h->stream));
+  if (b->rbytes == 8) {
+    if (!b->tuned) autotune<double>(b);
+    build<double>(b);
+  } else {
+    if (!b->tuned) autotune<float>(b);
+    build<float>(b);
+  }
+}
+
+void run_steps(Batch* b, int n) {
+  for (int k = 0; k < n; ++k) CK(cudaGraphLaunch(b->exec, b->stream));
+}
+
+}  // namespace
+}  // namespace mxm
+
+using mxm::Batch;
+
+#define BATCH_BEGIN                 \
+  Batch* b = (Batch*)batch;         \
+  if (!b) return MXM_DG_EINVAL;     \
+  try {                             \
+    cudaSetDevice(b->device);
+#define BATCH_END                                                                \
+  return MXM_DG_OK;                                                              \
+  }                                                                              \
+  catch (mxm::CudaError & ex) {                                                  \
+    b->err = ex.what();                                                          \
+    return ex.e == cudaErrorMemoryAllocation ? MXM_DG_ENOMEM : MXM_DG_ECUDA;     \
+  }                                                                              \
+  catch (std::exception & ex) {                                                  \
+    b->err = ex.what();                                                          \
+    return MXM_DG_EINVAL;                                                        \
+  }
+
+extern "C" {
+
+int mxm_dg_batch_create(void** batch) {
+  if (!batch) return MXM_DG_EINVAL;
+  *batch = nullptr;
+  std::unique_ptr<Batch> b(new Batch);
+  if (cudaGetDevice(&b->device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&b->derr, sizeof(int)) != cudaSuccess || cudaMemset(b->derr, 0, sizeof(int)) != cudaSuccess) {
+    std::lock_guard<std::mutex> g(mxm::g_err_mu);
+    mxm::g_create_err = "batch create: CUDA setup failed";
+    if (b->stream) cudaStreamDestroy(b->stream);
+    cudaFree(b->derr);
+    return MXM_DG_ECUDA;
+  }
+  *batch = b.release();
+  return MXM_DG_OK;
+}
+
+int mxm_dg_batch_destroy(void* batch) {
+  Batch* b = (Batch*)batch;
+  if (!b) return MXM_DG_OK;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  mxm::release_graph(b);
+  for (auto& g : b->groups) mxm::free_group(g);
+  cudaFree(b->d_solves);
+  cudaFree(b->derr);
+  cudaStreamDestroy(b->stream);
+  delete b;
+  return MXM_DG_OK;
+}
+
+int mxm_dg_batch_add(void* batch, void* solver, double dt, int32_t* index) {
+  BATCH_BEGIN
+  mxm::Handle* h = (mxm::Handle*)solver;
+  if (!h) throw mxm::ArgError("null solver handle");
+  if (h->dim != 2) throw mxm::ArgError("batched solves are 2D (triangle meshes)");
+  if (h->device != b->device) throw mxm::ArgError("solver lives on another device than the batch");
+  if (!(dt > 0.0)) throw mxm::ArgError("dt must be positive");
+  if (b->rbytes && h->rbytes != b->rbytes) throw mxm::ArgError("all solves of a batch share one precision");
+  for (mxm::Handle* m : b->members)
+    if (m == h) throw mxm::ArgError("solver already in the batch");
+  b->rbytes = h->rbytes;
+  const int id = int(b->members.size());
+  b->members.push_back(h);
+  b->dt.push_back(dt);
+  int gi = -1;
+  for (size_t k = 0; k < b->groups.size(); ++k)
+    if (std::memcmp(&b->groups[k].phys, &h->phys, sizeof(h->phys)) == 0) gi = int(k);
+  if (gi < 0) {
+    b->groups.emplace_back();
+    b->groups.back().phys = h->phys;
+    b->groups.back().NC = h->NC;
+    gi = int(b->groups.size()) - 1;
+  }
+  b->groups[gi].members.push_back(id);
+  mxm::release_graph(b);
+  b->tuned = false;
+  if (index) *index = id;
+  BATCH_END
+}
+
+int mxm_dg_batch_autotune(void* batch) {
+  BATCH_BEGIN
+  if (b->members.empty()) throw mxm::ArgError("the batch has no solves");
+  for (mxm::Handle* h : b->members) CK(cudaStreamSynchronize(h->stream));
+  mxm::release_graph(b);
+  if (b->rbytes == 8) mxm::autotune<double>(b);
+  else mxm::autotune<float>(b);
+  CK(cudaStreamSynchronize(b->stream));
+  BATCH_END
+}
+
+int mxm_dg_batch_tile_cells(void* batch, int member, int32_t* cells) {
+  BATCH_BEGIN
+  if (member < 0 || member >= int(b->members.size()) || !cells) throw mxm::ArgError("member index out of range");
+  mxm::ensure_built(b);
+  for (auto& g : b->groups)
+    for (int m : g.members)
+      if (m == member) *cells = g.ec[b->members[m]->P];
+  BATCH_END
+}
+
+int mxm_dg_batch_step(void* batch, int nsteps) {
+  BATCH_BEGIN
+  if (nsteps < 0) throw mxm::ArgError("nsteps >= 0");
+  mxm::ensure_built(b);
+  mxm::run_steps(b, nsteps);
+  BATCH_END
+}
+
+int mxm_dg_batch_time_steps(void* batch, int nsteps, double* ms) {
+  BATCH_BEGIN
+  if (nsteps < 0 || !ms) throw mxm::ArgError("nsteps >= 0, ms non-null");
+  mxm::ensure_built(b);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, b->stream));
+  mxm::run_steps(b, nsteps);
+  CK(cudaEventRecord(e1, b->stream));
+  CK(cudaEventSynchronize(e1));
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = f;
+  BATCH_END
+}
+
+int mxm_dg_batch_synchronize(void* batch) {
+  BATCH_BEGIN
+  CK(cudaStreamSynchronize(b->stream));
+  CK(cudaGetLastError());
+  int derr = 0;
+  CK(cudaMemcpy(&derr, b->derr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (derr) {
+    CK(cudaMemset(b->derr, 0, sizeof(int)));
+    b->err = "a batched stage kernel's bounded wait for its state tile gave up";
+    return MXM_DG_ETIMEDOUT;
+  }
+  BATCH_END
+}
+
+int mxm_dg_batch_dof_count(void* batch, int64_t* dof) {
+  BATCH_BEGIN
+  if (!dof) throw mxm::ArgError("dof non-null");
+  int64_t n = 0;
+  for (mxm::Handle* h : b->members) n += h->ne * h->NP * h->NC;
+  *dof = n;
+  BATCH_END
+}
+
+int mxm_dg_batch_launches_per_step(void* batch, int32_t* n) {
+  BATCH_BEGIN
+  if (!n) throw mxm::ArgError("n non-null");
+  // per stage: one stage kernel per group, plus the two limiter passes of a
+  // group with limited members
+  int k = 0;
+  for (auto& g : b->groups) {
+    bool lim = false;
+    for (int m : g.members) lim = lim || b->members[m]->lim_on;
+    k += 3 * (lim ? 3 : 1);
+  }
+  *n = k;
+  BATCH_END
+}
+
+int mxm_dg_batch_last_error(void* batch, char* buf, int len) {
+  if (!buf || len <= 0) return MXM_DG_EINVAL;
+  std::string s;
+  if (batch) s = ((Batch*)batch)->err;
+  else {
+    std::lock_guard<std::mutex> g(mxm::g_err_mu);
+    s = mxm::g_create_err;
+  }
+  std::strncpy(buf, s.c_str(), size_t(len) - 1);
+  buf[len - 1] = '\0';
+  return MXM_DG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,297 @@
+// Batched 2D DG: many independent solves of uneven mesh size and order P in
+// one persistent stage launch.
+//
+// Work is a list of items (solve, first cell, cells, P), one tile of whole
+// cells each; the tile size per P comes from the autotuner.  Blocks take
+// items from a global counter (dynamic scheduling, so big-P tiles do not
+// leave blocks idle at the end), prefetch the next item's state span with a
+// bulk copy into the other half of a double-buffered shared tile, and run the
+// same per-tile code as the single-solve kernel (stage2d_tile) instantiated
+// for P = 1..5 behind a switch.  The five shared operators live in shared
+// memory for the launch.  Each solve carries its own topology/metric table,
+// state buffers, time step and boundary codes (SolveDesc2).
+//
+// The SSPRK3 routing is the reference's (src/ssprk3.mojo:56-78): stage 0
+// q -> q1 (1, 0, 1), stage 1 q1 -> q2 (3/4, 1/4, 1/4), stage 2 q2 -> q
+// (1/3, 2/3, 2/3).  The limiter passes (cell means, theta + apply, as in
+// src/local_mesh_2d_gpu_limiter.mojo:74-210 and
+// src/local_mesh_2d_gpu.mojo:180-198) run over the limited solves' element
+// chunks, one block per chunk.
+#pragma once
+#include "stage2d.cuh"
+
+namespace mxm {
+
+template <class R>
+struct SolveDesc2 {
+  KuhnTab2<R> tab;
+  R* q[3];
+  R* avg;
+  const R* w;
+  R dt, eps2;
+  int P, nx, ny, ncell;
+  int bc[4];
+  int limiter;
+  int pad;
+};
+
+template <class R>
+struct Batch2DArgs {
+  const SolveDesc2<R>* solves;
+  const int4* items;  // {solve, first cell, cells, P}
+  int nitems;
+  int* counter;       // work counter, zero before the launch
+  int stage;          // SSPRK3 stage 0..2
+  const R* A[6];      // shared operator [K][NP] per P (index P)
+  int aoff[6];        // element offset of each P's operator in the shared copy
+  int a_len;          // values of all operators, a multiple of 4
+  int qv;             // values per tile buffer, a multiple of 4
+  int* err;
+};
+
+template <int P, int NC, class R>
+__host__ __device__ constexpr bool bulk2d_ok() {
+  return (2 * ntri(P) * NC * sizeof(R)) % 16 == 0;
+}
+
+template <class R, int NC>
+__device__ __forceinline__ bool bulk2d(int P) {
+  switch (P) {
+    case 1: return bulk2d_ok<1, NC, R>();
+    case 2: return bulk2d_ok<2, NC, R>();
+    case 3: return bulk2d_ok<3, NC, R>();
+    case 4: return bulk2d_ok<4, NC, R>();
+    default: return bulk2d_ok<5, NC, R>();
+  }
+}
+
+template <class R>
+__device__ __forceinline__ void ssprk3_route(int stage, R* const* q, const R*& qi, const R*& qa, const R*& qb,
+                                             R*& qo, R& a, R& b, R& c) {
+  if (stage == 0) {
+    qi = q[0]; qa = q[0]; qb = q[0]; qo = q[1];
+    a = R(1); b = R(0); c = R(1);
+  } else if (stage == 1) {
+    qi = q[1]; qa = q[0]; qb = q[1]; qo = q[2];
+    a = R(0.75); b = R(0.25); c = R(0.25);
+  } else {
+    qi = q[2]; qa = q[0]; qb = q[2]; qo = q[0];
+    a = R(1.0 / 3.0); b = R(2.0 / 3.0); c = R(2.0 / 3.0);
+  }
+}
+
+template <class R, class Phys, int NT>
+__global__ void __launch_bounds__(NT) stage2d_batch_kernel(Batch2DArgs<R> ba, Phys ph) {
+  constexpr int NC = Phys::NC;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);          // [2]
+  int* sIt = reinterpret_cast<int*>(smem_raw + 16);               // [2] item of each tile buffer
+  constexpr size_t kTabBytes = (sizeof(KuhnTab2<R>) + 15) / 16 * 16;
+  KuhnTab2<R>* tabs = reinterpret_cast<KuhnTab2<R>*>(smem_raw + 32);  // [2]
+  R* sA = reinterpret_cast<R*>(smem_raw + 32 + 2 * kTabBytes);  // operators of P = 1..5
+  R* sQ = sA + ba.a_len;                                          // [2][qv], 16-byte aligned
+  R* sB = sQ + 2 * size_t(ba.qv);
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  for (int P = 1; P <= 5; ++P) {
+    const int n = (2 * ntri(P) + 3 * (P + 1)) * ntri(P);
+    if (ba.A[P])
+      for (int idx = tid; idx < n; idx += NT) sA[ba.aoff[P] + idx] = ba.A[P][idx];
+  }
+  auto issue = [&](int it, int b) {
+    const int4 item = ba.items[it];
+    const int np = ntri(item.w);
+    const uint32_t bytes = uint32_t(item.z) * 2u * np * NC * sizeof(R);
+    const R* src = ba.solves[item.x].q[ba.stage] + size_t(item.y) * 2 * np * NC;  // stage s reads q_s
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&bar[b], bytes);
+    bulk_g2s(sQ + size_t(b) * ba.qv, src, bytes, &bar[b]);
+  };
+  if (tid == 0) {
+    const int it = atomicAdd(ba.counter, 1);
+    sIt[0] = it;
+    if (it < ba.nitems && bulk2d<R, NC>(ba.items[it].w)) issue(it, 0);
+  }
+  __syncthreads();
+  uint32_t par = 0u;  // bit b: phase parity of tile buffer b
+  int buf = 0;
+  while (true) {
+    const int it = sIt[buf];
+    if (it >= ba.nitems) break;
+    const int4 item = ba.items[it];
+    const SolveDesc2<R>* sd = &ba.solves[item.x];
+    const int P = item.w, np = ntri(P);
+    {  // this solve's table into the buffer's table slot
+      const int* src = reinterpret_cast<const int*>(&sd->tab);
+      int* dst = reinterpret_cast<int*>(&tabs[buf]);
+      for (int k = tid; k < int(sizeof(KuhnTab2<R>) / 4); k += NT) dst[k] = src[k];
+    }
+    R* q = sQ + size_t(buf) * ba.qv;
+    const bool bulk = bulk2d<R, NC>(P);
+    if (bulk) {
+      if (!block_wait_bounded(&bar[buf], (par >> buf) & 1u, kWaitLimitNs2)) {
+        if (tid == 0) {
+          if (ba.err) atomicOr(ba.err, 1);
+          mbar_wait_bounded(&bar[buf], (par >> buf) & 1u, kWaitLimitNs2);
+        }
+        return;
+      }
+      par ^= 1u << buf;
+    } else {
+      const R* src = sd->q[ba.stage] + size_t(item.y) * 2 * np * NC;
+      for (int idx = tid; idx < item.z * 2 * np * NC; idx += NT) q[idx] = src[idx];
+      __syncthreads();
+    }
+    if (tid == 0) {  // next item into the other buffer (its previous tile is finished)
+      const int nx = atomicAdd(ba.counter, 1);
+      sIt[buf ^ 1] = nx;
+      if (nx < ba.nitems && bulk2d<R, NC>(ba.items[nx].w)) issue(nx, buf ^ 1);
+    }
+    Stage2DArgs<R> args;
+    R a, b, c;
+    ssprk3_route(ba.stage, sd->q, args.q_in, args.q_a, args.q_b, args.q_out, a, b, c);
+    args.A = nullptr;
+    args.a = a;
+    args.b = b;
+    args.cdt = c * sd->dt;
+    args.nx = sd->nx;
+    args.ny = sd->ny;
+    args.ncell = sd->ncell;
+    for (int k = 0; k < 4; ++k) args.bc[k] = sd->bc[k];
+    args.rhs_only = 0;
+    args.err = ba.err;
+    const int ne_here = 2 * item.z;
+    switch (P) {
+      case 1: stage2d_tile<R, Phys, 1, NT>(args, &tabs[buf], ph, q, sB, sA + ba.aoff[1], item.y, ne_here); break;
+      case 2: stage2d_tile<R, Phys, 2, NT>(args, &tabs[buf], ph, q, sB, sA + ba.aoff[2], item.y, ne_here); break;
+      case 3: stage2d_tile<R, Phys, 3, NT>(args, &tabs[buf], ph, q, sB, sA + ba.aoff[3], item.y, ne_here); break;
+      case 4: stage2d_tile<R, Phys, 4, NT>(args, &tabs[buf], ph, q, sB, sA + ba.aoff[4], item.y, ne_here); break;
+      default: stage2d_tile<R, Phys, 5, NT>(args, &tabs[buf], ph, q, sB, sA + ba.aoff[5], item.y, ne_here); break;
+    }
+    buf ^= 1;
+  }
+}
+
+// ---- batched limiter passes over element chunks of the limited solves
+template <class R>
+struct LimBatch2DArgs {
+  const SolveDesc2<R>* solves;
+  const int4* items;  // {solve, first element, elements, P}
+  int nitems;
+  int which;          // state buffer to limit (0..2)
+};
+
+template <class R, int NP, int NC>
+__device__ __forceinline__ void avg_chunk(const SolveDesc2<R>* sd, int which, int e0, int ne) {
+  const R* qb = sd->q[which];
+  for (int idx = threadIdx.x; idx < ne * NC; idx += blockDim.x) {
+    const int64_t e = e0 + idx / NC;
+    const int c = idx % NC;
+    const R* q = qb + e * NP * NC + c;
+    R s = R(0);
+#pragma unroll
+    for (int n = 0; n < NP; ++n) s += __ldg(&sd->w[n]) * q[n * NC];
+    sd->avg[e * NC + c] = s;
+  }
+}
+
+template <class R, int NC>
+__global__ void avg_batch_kernel(LimBatch2DArgs<R> la) {
+  const int4 item = la.items[blockIdx.x];
+  const SolveDesc2<R>* sd = &la.solves[item.x];
+  switch (item.w) {
+    case 1: avg_chunk<R, ntri(1), NC>(sd, la.which, item.y, item.z); break;
+    case 2: avg_chunk<R, ntri(2), NC>(sd, la.which, item.y, item.z); break;
+    case 3: avg_chunk<R, ntri(3), NC>(sd, la.which, item.y, item.z); break;
+    case 4: avg_chunk<R, ntri(4), NC>(sd, la.which, item.y, item.z); break;
+    default: avg_chunk<R, ntri(5), NC>(sd, la.which, item.y, item.z); break;
+  }
+}
+
+// One warp per element (8 warps per block, striding over the chunk): theta
+// from component 0 against the face neighbours' means (BC faces do not
+// constrain), applied to every component when theta < 1.
+template <class R, int NP, int NC>
+__device__ __forceinline__ void theta_chunk(const SolveDesc2<R>* sd, int which, int e0, int ne, R* sq) {
+  constexpr int VALS = NP * NC;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  R* mine = sq + warp * VALS;
+  R* qb = sd->q[which];
+  for (int el = warp; el < ne; el += nw) {
+    const int64_t e = e0 + el;
+    for (int idx = lane; idx < VALS; idx += 32) mine[idx] = qb[e * VALS + idx];
+    __syncwarp();
+    const int t = int(e & 1);
+    const int cell = int(e >> 1);
+    const int cj = cell / sd->nx, ci = cell - cj * sd->nx;
+    int64_t nb = e;
+    if (lane < 3) {
+      const int lf = lane;
+      const int ax = sd->tab.axis[t][lf], dir = sd->tab.dir[t][lf];
+      int code;
+      const int mode = face_mode(ax, dir, ax == 0 ? ci : cj, ax == 0 ? sd->nx : sd->ny, sd->bc, code);
+      if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
+        const int ni = wrapi(ci + sd->tab.off[t][lf][0], sd->nx), nj = wrapi(cj + sd->tab.off[t][lf][1], sd->ny);
+        nb = (int64_t(nj) * sd->nx + ni) * 2 + sd->tab.nb_t[t][lf];
+      }
+    }
+    const R own = sd->avg[e * NC];
+    R lo = own, hi = own;
+#pragma unroll
+    for (int lf = 0; lf < 3; ++lf) {
+      const int64_t n = __shfl_sync(0xffffffffu, nb, lf);
+      if (n == e) continue;
+      const R v = sd->avg[n * NC];
+      if (v < lo) lo = v;
+      if (v > hi) hi = v;
+    }
+    R th = R(1);
+    const R tiny = R(1.0e-30);
+    for (int n = lane; n < NP; n += 32) {
+      const R dl = mine[n * NC] - own;
+      const R da = dl >= R(0) ? dl : -dl;
+      if (da <= tiny) continue;
+      R pD = hi - own;
+      if (pD < R(0)) pD = R(0);
+      R nD = own - lo;
+      if (nD < R(0)) nD = R(0);
+      const R D = dl > R(0) ? pD : nD;
+      const R D2 = D * D, d2 = da * da, Dd = D * da;
+      const R al = (D2 + R(2) * Dd + sd->eps2) / (D2 + R(2) * d2 + Dd + sd->eps2);
+      if (al < th) th = al;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const R v = __shfl_xor_sync(0xffffffffu, th, o);
+      th = v < th ? v : th;
+    }
+    if (th < R(1)) {
+      for (int idx = lane; idx < VALS; idx += 32) {
+        const int c = idx % NC;
+        const R bm = sd->avg[e * NC + c];
+        qb[e * VALS + idx] = bm + th * (mine[idx] - bm);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <class R, int NC>
+__global__ void __launch_bounds__(256) theta_batch_kernel(LimBatch2DArgs<R> la) {
+  __shared__ R sq[8 * 21 * NC];
+  const int4 item = la.items[blockIdx.x];
+  const SolveDesc2<R>* sd = &la.solves[item.x];
+  switch (item.w) {
+    case 1: theta_chunk<R, ntri(1), NC>(sd, la.which, item.y, item.z, sq); break;
+    case 2: theta_chunk<R, ntri(2), NC>(sd, la.which, item.y, item.z, sq); break;
+    case 3: theta_chunk<R, ntri(3), NC>(sd, la.which, item.y, item.z, sq); break;
+    case 4: theta_chunk<R, ntri(4), NC>(sd, la.which, item.y, item.z, sq); break;
+    default: theta_chunk<R, ntri(5), NC>(sd, la.which, item.y, item.z, sq); break;
+  }
+}
+
+}  // namespace mxm

@@ -15,6 +15,8 @@
 
 #include "../../include/mxm_dg.h"
 #include "dg_common.cuh"
+#include "handle.hpp"
+#include "ic.hpp"
 #include "physics.cuh"
 #include "physics2d.cuh"
 #include "refops.hpp"
@@ -22,62 +24,8 @@
 
 namespace mxm {
 
-struct CudaError : std::exception {
-  cudaError_t e;
-  std::string msg;
-  CudaError(cudaError_t e_, const char* where) : e(e_), msg(std::string(where) + ": " + cudaGetErrorString(e_)) {}
-  const char* what() const noexcept override { return msg.c_str(); }
-};
-struct ArgError : std::exception {
-  std::string msg;
-  explicit ArgError(std::string m) : msg(std::move(m)) {}
-  const char* what() const noexcept override { return msg.c_str(); }
-};
-#define CK(x)                                            \
-  do {                                                   \
-    cudaError_t _e = (x);                                \
-    if (_e != cudaSuccess) throw ::mxm::CudaError(_e, #x); \
-  } while (0)
-
-struct Handle {
-  int dim = 3, P = 1, prec = MXM_DG_PREC_F64, NP = 0, NFP = 0, NC = 0, ntypes = 6, K = 0;
-  mxm_dg_physics_desc phys{};
-  int nx = 1, ny = 1, nz = 1;
-  double lx = 1, ly = 1, lz = 1;
-  int bc[6] = {0, 0, 0, 0, 0, 0};
-  int64_t ncell = 0, ne = 0;
-  size_t rbytes = 8;
-  int device = 0, nsm = 148;
-  cudaStream_t stream = nullptr;
-  void* q[3] = {nullptr, nullptr, nullptr};
-  void* A = nullptr;
-  void* w = nullptr;
-  void* avg = nullptr;
-  float* xyz = nullptr;
-  double* partial = nullptr;
-  double* dscalar = nullptr;
-  unsigned long long* uscalar = nullptr;
-  int* derr = nullptr;  // device error word written by bounded waits
-  bool use_tc = false;  // MIXED precision: tensor-core contraction
-  void* tcimg = nullptr;  // operator image (bf16 hi | lo) in the UMMA layout
-  int npartial = 1024;
-  bool lim_on = false;
-  double lim_eps = 0.1;
-  RefOps ref;
-  Kuhn3D k3;
-  Kuhn2D k2;
-  std::vector<double> Ahost;
-  KuhnTab3<double> t3d{};
-  KuhnTab3<float> t3f{};
-  KuhnTab2<double> t2d{};
-  KuhnTab2<float> t2f{};
-  std::string err;
-  size_t qcount() const { return size_t(ne) * NP * NC; }
-  size_t qbytes() const { return qcount() * rbytes; }
-};
-
-static std::mutex g_err_mu;
-static std::string g_create_err;
+std::mutex g_err_mu;
+std::string g_create_err;
 
 // round-to-nearest-even float -> bfloat16 bits (finite inputs)
 static uint16_t bf16_bits(float x) {
@@ -158,6 +106,22 @@ void fill_tab3(Handle* h, KuhnTab3<R>& t) {
         if (mm == h->NFP) throw ArgError("internal: neighbour face node not found");
         t.nb_m[a][lf][m] = uint8_t(mm);
       }
+    }
+  // work list of faces a cube evaluates once; a cube-boundary face must lead
+  // to the adjacent cube along its axis (the kernels resolve it per cube)
+  t.n_face_work = 0;
+  for (int a = 0; a < 6; ++a)
+    for (int lf = 0; lf < 4; ++lf) {
+      const int ax = k.axis[a][lf];
+      if (ax >= 0) {
+        for (int d = 0; d < 3; ++d)
+          if (k.off[a][lf][d] != (d == ax ? k.dir[a][lf] : 0)) throw ArgError("internal: cube face offset");
+      } else {
+        for (int d = 0; d < 3; ++d)
+          if (k.off[a][lf][d] != 0) throw ArgError("internal: inner face offset");
+        if (k.side[a][lf] != 0) continue;
+      }
+      t.face_work[t.n_face_work++] = uint8_t(a * 4 + lf);
     }
 }
 
@@ -479,6 +443,48 @@ void build_xyz(Handle* h) {
   CK(cudaMemcpy(h->xyz, x.data(), x.size() * sizeof(float), cudaMemcpyHostToDevice));
 }
 
+// Device IC fill of state buffer `which` (asynchronous on the handle's stream).
+void fill_ic(Handle* h, int which, int kind, const double* params, int nparams) {
+  if (which < 0 || which > 2) throw ArgError("which must be 0..2");
+  if (kind < MXM_DG_IC_CONSTANT || kind > MXM_DG_IC_PLANE_WAVE) throw ArgError("unknown initial-condition kind");
+  if (nparams < 0 || nparams > 16 || (nparams > 0 && !params)) throw ArgError("nparams must be 0..16");
+  const int k = h->phys.kind;
+  const bool ok = kind == MXM_DG_IC_CONSTANT ||
+                  ((kind == MXM_DG_IC_SINE_WAVE || kind == MXM_DG_IC_VORTEX || kind == MXM_DG_IC_SOD) &&
+                   k == MXM_DG_PHYS_EULER) ||
+                  (kind == MXM_DG_IC_DAM_BREAK && k == MXM_DG_PHYS_SHALLOW_WATER) ||
+                  ((kind == MXM_DG_IC_CAVITY || kind == MXM_DG_IC_PLANE_WAVE) && k == MXM_DG_PHYS_MAXWELL);
+  if (!ok) throw ArgError("initial-condition kind does not match the physics");
+  IcArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.ne = h->ne;
+  a.dim = h->dim;
+  a.P = h->P;
+  a.NP = h->NP;
+  a.NC = h->NC;
+  a.nx = h->nx;
+  a.ny = h->ny;
+  a.nz = h->nz;
+  a.kind = kind;
+  a.h[0] = h->lx / h->nx;
+  a.h[1] = h->ly / h->ny;
+  a.h[2] = h->lz / h->nz;
+  a.L[0] = h->lx;
+  a.L[1] = h->ly;
+  a.L[2] = h->lz;
+  for (int i = 0; i < nparams; ++i) a.prm[i] = params[i];
+  a.gamma = h->phys.p[0];
+  a.c = h->phys.p[0];
+  const int ntypes = h->dim == 3 ? 6 : 2;
+  for (int t = 0; t < ntypes; ++t)
+    for (int v = 0; v < h->dim + 1; ++v)
+      for (int d = 0; d < h->dim; ++d)
+        a.vert[t][v][d] = int8_t(h->dim == 3 ? h->k3.vert[t][v][d] : h->k2.vert[t][v][d]);
+  for (int n = 0; n < h->NP; ++n)
+    for (int v = 0; v < 4; ++v) a.bary[n][v] = uint8_t(h->ref.nodes[n].a[v]);
+  CK(launch_ic(a, h->q[which], h->rbytes, h->stream));
+}
+
 void destroy(Handle* h) {
   if (!h) return;
   cudaSetDevice(h->device);
@@ -712,6 +718,13 @@ int mxm_dg_node_xyz(void* handle, double* out) {
         for (int d = 0; d < 2; ++d) out[(e * NP + n) * 2 + d] = (c[d] + h->k2.rel_xy[(t * NP + n) * 2 + d]) * hh[d];
     }
   }
+  API_END
+}
+
+int mxm_dg_fill_ic(void* handle, int which, int kind, const double* params, int nparams) {
+  API_BEGIN
+  mxm::fill_ic(h, which, kind, params, nparams);
+  CK(cudaStreamSynchronize(h->stream));
   API_END
 }
 

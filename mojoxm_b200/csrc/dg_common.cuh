@@ -29,6 +29,10 @@ struct KuhnTab3 {
   uint8_t nb_node[6][4][kMaxNFP3];
   uint8_t nb_lf[6][4];             // neighbour's local face
   uint8_t nb_m[6][4][kMaxNFP3];    // neighbour's face-local index of face node m
+  // faces a cube evaluates once: every cube-boundary face (axis >= 0) and
+  // the side-0 copy of every face inside the cube; entry = t * 4 + lf
+  uint8_t face_work[24];
+  int32_t n_face_work;
 };
 
 template <class R>
@@ -82,37 +86,47 @@ __device__ __forceinline__ int face_mode(int axis, int dir, int cpos, int ncell_
 
 __device__ __forceinline__ int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
-// Per-tile face descriptor, resolved once per (element, local face) at the
-// start of a tile so the face-node loops do no integer division:
-//   x = mode | code << 8,  y = neighbour element (global index), z = neighbour
-//   element inside the tile (-1 when outside)
-struct FaceInfo {
-  int x, y, z;
-};
+// Neighbour cube and face treatment of the six cube faces of one cube,
+// resolved once per tile so the face-node loops do no integer division.
+// Direction index dd = 2 * axis + (dir > 0).  nb[dd] = neighbour cube
+// (periodic wrap), md[dd] = face mode | BC code << 8.
+__device__ __forceinline__ void cube_dirs3(int cell, int nx, int ny, int nz, const int* bc, int* nb, int* md, int dd) {
+  const int nxy = nx * ny;
+  const int ck = cell / nxy, rem = cell - ck * nxy, cj = rem / nx, ci = rem - cj * nx;
+  const int ax = dd >> 1, dir = (dd & 1) ? 1 : -1;
+  int code;
+  const int mode = face_mode(ax, dir, ax == 0 ? ci : (ax == 1 ? cj : ck), ax == 0 ? nx : (ax == 1 ? ny : nz), bc, code);
+  const int ni = ax == 0 ? wrapi(ci + dir, nx) : ci, nj = ax == 1 ? wrapi(cj + dir, ny) : cj,
+            nk = ax == 2 ? wrapi(ck + dir, nz) : ck;
+  nb[dd] = ni + nx * (nj + ny * nk);
+  md[dd] = mode | (code << 8);
+}
 
-// Fill info[el*4 + lf] for the ne_here elements of a tile of whole cubes
-// starting at cell0 (3D Kuhn meshes).
-template <class Tab, class Args>
-__device__ __forceinline__ void setup_faces3(const Tab* tab, const Args& args, int cell0, int ne_here, FaceInfo* info,
-                                             int tid, int nt) {
-  const int nxy = args.nx * args.ny;
-  for (int idx = tid; idx < ne_here * 4; idx += nt) {
-    const int el = idx >> 2, lf = idx & 3, t = el % 6, cl = el / 6;
-    const int cell = cell0 + cl;
-    const int ck = cell / nxy, rem = cell - ck * nxy, cj = rem / args.nx, ci = rem - cj * args.nx;
-    const int ax = tab->axis[t][lf];
-    int code;
-    const int mode = face_mode(ax, tab->dir[t][lf], ax == 0 ? ci : (ax == 1 ? cj : ck),
-                               ax == 0 ? args.nx : (ax == 1 ? args.ny : args.nz), args.bc, code);
-    const int nbt = tab->nb_t[t][lf];
-    const int ni = wrapi(ci + tab->off[t][lf][0], args.nx), nj = wrapi(cj + tab->off[t][lf][1], args.ny),
-              nk = wrapi(ck + tab->off[t][lf][2], args.nz);
-    FaceInfo f;
-    f.x = mode | (code << 8);
-    f.y = (ni + args.nx * (nj + args.ny * nk)) * 6 + nbt;
-    f.z = ax < 0 ? cl * 6 + nbt : -1;
-    info[idx] = f;
-  }
+// Resident blocks per SM of a persistent kernel with `nt` threads and `smem`
+// bytes of dynamic shared memory: the shared-memory carveout is set to its
+// maximum first, then the count is the least of the shared-memory, thread
+// and register limits (what the occupancy calculator reports, computed here
+// from the device attributes so the carveout choice cannot lower it).
+inline cudaError_t persistent_blocks_per_sm(const void* kern, int nt, size_t smem, int* bps) {
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) return e;
+  int dev = 0, smem_sm = 0, resv = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev)) != cudaSuccess) return e;
+  cudaFuncAttributes fa;
+  if ((e = cudaFuncGetAttributes(&fa, kern)) != cudaSuccess) return e;
+  const size_t per_block = smem + size_t(fa.sharedSizeBytes) + size_t(resv);
+  int by_smem = int(size_t(smem_sm) / per_block);
+  int by_threads = 2048 / nt;
+  const int regs_warp = ((fa.numRegs > 0 ? fa.numRegs : 1) * 32 + 255) / 256 * 256;
+  int by_regs = 65536 / (regs_warp * ((nt + 31) / 32));
+  int n = by_smem < by_threads ? by_smem : by_threads;
+  n = n < by_regs ? n : by_regs;
+  *bps = n < 1 ? 1 : n;
+  return cudaSuccess;
 }
 
 // Kernel argument blocks (by value).

@@ -1,0 +1,82 @@
+// Host-side state of one solve (the C ABI's opaque handle) and the error
+// types of the library's host code; shared by capi.cu and batch.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <exception>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/mxm_dg.h"
+#include "dg_common.cuh"
+#include "refops.hpp"
+
+namespace mxm {
+
+struct CudaError : std::exception {
+  cudaError_t e;
+  std::string msg;
+  CudaError(cudaError_t e_, const char* where) : e(e_), msg(std::string(where) + ": " + cudaGetErrorString(e_)) {}
+  const char* what() const noexcept override { return msg.c_str(); }
+};
+struct ArgError : std::exception {
+  std::string msg;
+  explicit ArgError(std::string m) : msg(std::move(m)) {}
+  const char* what() const noexcept override { return msg.c_str(); }
+};
+#define CK(x)                                              \
+  do {                                                     \
+    cudaError_t _e = (x);                                  \
+    if (_e != cudaSuccess) throw ::mxm::CudaError(_e, #x); \
+  } while (0)
+
+struct Handle {
+  int dim = 3, P = 1, prec = MXM_DG_PREC_F64, NP = 0, NFP = 0, NC = 0, ntypes = 6, K = 0;
+  mxm_dg_physics_desc phys{};
+  int nx = 1, ny = 1, nz = 1;
+  double lx = 1, ly = 1, lz = 1;
+  int bc[6] = {0, 0, 0, 0, 0, 0};
+  int64_t ncell = 0, ne = 0;
+  size_t rbytes = 8;
+  int device = 0, nsm = 148;
+  cudaStream_t stream = nullptr;
+  void* q[3] = {nullptr, nullptr, nullptr};
+  void* A = nullptr;
+  void* w = nullptr;
+  void* avg = nullptr;
+  float* xyz = nullptr;
+  double* partial = nullptr;
+  double* dscalar = nullptr;
+  unsigned long long* uscalar = nullptr;
+  int* derr = nullptr;  // device error word written by bounded waits
+  bool use_tc = false;  // MIXED precision: tensor-core contraction
+  void* tcimg = nullptr;  // operator image (bf16 hi | lo) in the UMMA layout
+  int npartial = 1024;
+  bool lim_on = false;
+  double lim_eps = 0.1;
+  RefOps ref;
+  Kuhn3D k3;
+  Kuhn2D k2;
+  std::vector<double> Ahost;
+  KuhnTab3<double> t3d{};
+  KuhnTab3<float> t3f{};
+  KuhnTab2<double> t2d{};
+  KuhnTab2<float> t2f{};
+  std::string err;
+  size_t qcount() const { return size_t(ne) * NP * NC; }
+  size_t qbytes() const { return qcount() * rbytes; }
+};
+
+// error text of calls that have no handle yet (create, batch create)
+extern std::mutex g_err_mu;
+extern std::string g_create_err;
+
+// Solver operations shared by the C ABI, the batch and the server (capi.cu);
+// they throw CudaError / ArgError.
+Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, int prec);
+void destroy(Handle* h);
+void step_n(Handle* h, double dt, int n);
+void fill_ic(Handle* h, int which, int kind, const double* params, int nparams);
+
+}  // namespace mxm

@@ -1,0 +1,20 @@
+// Device initial-condition fill (ic_kernels.cu): arguments and launcher.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mxm {
+
+struct IcArgs {
+  int64_t ne;
+  int dim, P, NP, NC, nx, ny, nz, kind;
+  double h[3], L[3];
+  double prm[16];
+  double gamma, c;          // Euler gamma, Maxwell wave speed (from the physics)
+  int8_t vert[6][4][3];     // cube-/cell-corner coordinates of each element type's vertices
+  uint8_t bary[56][4];      // barycentric exponents of each node (sum P)
+};
+
+cudaError_t launch_ic(const IcArgs& a, void* q, size_t rbytes, cudaStream_t st);
+
+}  // namespace mxm

@@ -5,8 +5,11 @@
 //   Euler         src/euler.mojo:44-792 (Rusanov/Roe/HLLE/HLLEC, Harten-Hyman fix)
 //   Maxwell       src/maxwell.mojo:48-255
 //   ShallowWater  src/shallow_water.mojo:31-167
-// Each formula keeps the reference's operation order; comparisons that the
-// reference writes as `not (x > floor)` stay NaN-catching.
+// Each formula keeps the reference's operation order, except that the
+// pointwise Euler flux and the Rusanov flux divide by the density through one
+// reciprocal per state (a few ulp apart from the reference's quotients);
+// comparisons that the reference writes as `not (x > floor)` stay
+// NaN-catching.
 #pragma once
 #include "dg_common.cuh"
 
@@ -62,9 +65,15 @@ struct EulerD {
     R p = (gamma - R(1)) * (q[4] - ke);
     return p > p_min ? p : p_min;
   }
+  // pressure from the reciprocal density ri = 1/rho and the velocity
+  __device__ __forceinline__ R p_fi(const R* q, R u, R v, R w) const {
+    R p = (gamma - R(1)) * (q[4] - R(0.5) * (q[1] * u + q[2] * v + q[3] * w));
+    return p > p_min ? p : p_min;
+  }
   __device__ void flux(const R* q, R* F) const {  // euler.mojo:597-621
-    R rho = rho_f(q), p = p_f(q, rho);
-    R u = q[1] / rho, v = q[2] / rho, w = q[3] / rho;
+    const R ri = R(1) / rho_f(q);
+    const R u = q[1] * ri, v = q[2] * ri, w = q[3] * ri;
+    const R p = p_fi(q, u, v, w);
     F[0] = q[1]; F[1] = q[1] * u + p; F[2] = q[1] * v; F[3] = q[1] * w; F[4] = u * (q[4] + p);
     F[5] = q[2]; F[6] = q[2] * u; F[7] = q[2] * v + p; F[8] = q[2] * w; F[9] = v * (q[4] + p);
     F[10] = q[3]; F[11] = q[3] * u; F[12] = q[3] * v; F[13] = q[3] * w + p; F[14] = w * (q[4] + p);
@@ -216,10 +225,12 @@ struct EulerD {
       // frame (n, t, b), anti-rotating the face-frame Rusanov flux gives
       // 0.5 (m_L un_L + m_R un_R + (p_L + p_R) n + cmax (m_L - m_R)) for the
       // momentum, so the rotation pair and the tangent construction drop out.
-      const R rl = rho_f(q_l), rr = rho_f(q_r), pl = p_f(q_l, rl), pr = p_f(q_r, rr);
+      const R rl = rho_f(q_l), rr = rho_f(q_r), il = R(1) / rl, ir = R(1) / rr;
+      const R pl = p_fi(q_l, q_l[1] * il, q_l[2] * il, q_l[3] * il);
+      const R pr = p_fi(q_r, q_r[1] * ir, q_r[2] * ir, q_r[3] * ir);
       const R mnl = nx * q_l[1] + ny * q_l[2] + nz * q_l[3], mnr = nx * q_r[1] + ny * q_r[2] + nz * q_r[3];
-      const R ul = mnl / rl, ur = mnr / rr;
-      const R cmax = rmax(rabs(ul) + sqrt(gamma * pl / rl), rabs(ur) + sqrt(gamma * pr / rr));
+      const R ul = mnl * il, ur = mnr * ir;
+      const R cmax = rmax(rabs(ul) + sqrt(gamma * pl * il), rabs(ur) + sqrt(gamma * pr * ir));
       const R h = R(0.5), ps = pl + pr;
       flux[0] = h * (mnl + mnr + cmax * (rl - rr));
       flux[1] = h * (q_l[1] * ul + q_r[1] * ur + ps * nx + cmax * (q_l[1] - q_r[1]));

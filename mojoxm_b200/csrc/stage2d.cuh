@@ -11,6 +11,10 @@
 // edges' numerical fluxes into a shared B tile (the diagonal's neighbour
 // trace comes from the tile), then rhs = A B + source and the RK combine.
 // Face traces never touch global memory; connectivity is implicit.
+//
+// The per-tile work is the device function stage2d_tile, shared by the
+// single-solve kernel below and the batched multi-solve kernel
+// (batch2d.cuh).
 #pragma once
 #include "dg_common.cuh"
 #include "physics2d.cuh"
@@ -24,18 +28,137 @@ struct Stage2DShape {
   static constexpr int BSTR_RAW = K * NC;
   static constexpr int BMOD = sizeof(R) == 8 ? 16 : 32;
   static constexpr int BSTR = BSTR_RAW + ((1 - BSTR_RAW % BMOD) + BMOD) % BMOD;
+  // rows of the contraction per thread: a divisor of NP
+  static constexpr int RI = P == 1 ? 3 : (P == 2 ? 2 : (P == 3 ? 5 : (P == 4 ? 5 : 3)));
+  static constexpr size_t kPerCell = 2 * sizeof(R) * (2 * size_t(NP) * NC + BSTR);  // 2 q buffers + B rows
 };
 
 constexpr uint64_t kWaitLimitNs2 = 2000000000ull;
 
-template <class R, class Phys, int P, int EC, int RI, int NT>
+// One tile of whole cells starting at cell0 (ne_here triangles), its state
+// already in shared memory at q: volume and edge fluxes into sB, then
+// rhs = A B + source and the RK combine into args.q_out.  Contains one
+// block barrier; every thread of the block must call it.
+template <class R, class Phys, int P, int NT>
+__device__ __forceinline__ void stage2d_tile(const Stage2DArgs<R>& args, const KuhnTab2<R>* tab, const Phys& ph,
+                                             const R* q, R* sB, const R* sA, int cell0, int ne_here) {
+  constexpr int NC = Phys::NC;
+  using S = Stage2DShape<P, NC, R>;
+  constexpr int NP = S::NP, NFP = S::NFP, K = S::K, BSTR = S::BSTR, RI = S::RI, G = NP / RI;
+  static_assert(NP % RI == 0, "row tile must divide NP");
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < ne_here * NP; idx += NT) {
+    const int el = idx / NP, j = idx - el * NP, t = el & 1;
+    R Fx[NC], Fy[NC];
+    ph.flux(&q[(el * NP + j) * NC], Fx, Fy);
+    const R* iJ = tab->invJ[t];
+    R* b = &sB[el * BSTR + j * NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      b[c] = iJ[0] * Fx[c] + iJ[1] * Fy[c];
+      b[NP * NC + c] = iJ[2] * Fx[c] + iJ[3] * Fy[c];
+    }
+  }
+  for (int idx = tid; idx < ne_here * 3 * NFP; idx += NT) {
+    const int el = idx / (3 * NFP), fm = idx - el * 3 * NFP;
+    const int lf = fm / NFP, m = fm - lf * NFP, t = el & 1, cl = el >> 1;
+    const int cell = cell0 + cl;
+    const int cj = cell / args.nx, ci = cell - cj * args.nx;
+    const int ax = tab->axis[t][lf], dir = tab->dir[t][lf];
+    int code;
+    const int mode = face_mode(ax, dir, ax == 0 ? ci : cj, ax == 0 ? args.nx : args.ny, args.bc, code);
+    const R* qo = &q[(el * NP + tab->own_node[lf][m]) * NC];
+    R nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1];
+    R scale = tab->fscale[t][lf];
+    // one face-flux call per face node (the 2D face functions build the
+    // BC ghost state themselves from the left state and the BC code)
+    R qn[NC];
+    if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
+      const int nbt = tab->nb_t[t][lf], nbn = tab->nb_node[t][lf][m];
+      if (ax < 0) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) qn[c] = q[((cl * 2 + nbt) * NP + nbn) * NC + c];
+      } else {
+        const int ni = wrapi(ci + tab->off[t][lf][0], args.nx), nj = wrapi(cj + tab->off[t][lf][1], args.ny);
+        const R* gq = args.q_in + ((size_t(nj) * args.nx + ni) * 2 * NP + size_t(nbt) * NP + nbn) * NC;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) qn[c] = __ldg(gq + c);
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) qn[c] = qo[c];
+    }
+    if (mode == FACE_BC_LO) {
+      nx = -nx;
+      ny = -ny;
+      scale = -scale;
+    }
+    const bool bcf = mode != FACE_INTERIOR;
+    const bool own_left = tab->side[t][lf] == 0;
+    // left/right states by value (selecting between pointers would force
+    // the register arrays into local memory)
+    R L[NC], Rr[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const R o = qo[c];
+      L[c] = bcf ? qn[c] : (own_left ? o : qn[c]);
+      Rr[c] = bcf ? qn[c] : (own_left ? qn[c] : o);
+    }
+    R f[NC];
+    ph.face(L, Rr, bcf ? code : int(BC_INTERIOR), nx, ny, f);
+    R* b = &sB[el * BSTR + (2 * NP + fm) * NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) b[c] = scale * f[c];
+  }
+  __syncthreads();
+  const bool a_in = args.q_a == args.q_in, b_in = args.q_b == args.q_in;
+  for (int w = tid; w < ne_here * G; w += NT) {
+    const int el = w / G, g = w - el * G;
+    const int i0 = g * RI;
+    R acc[RI][NC];
+#pragma unroll
+    for (int r = 0; r < RI; ++r)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[r][c] = R(0);
+    const R* b = &sB[el * BSTR];
+#pragma unroll 4
+    for (int k = 0; k < K; ++k) {
+      R av[RI], bv[NC];
+#pragma unroll
+      for (int r = 0; r < RI; ++r) av[r] = sA[k * NP + i0 + r];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) bv[c] = b[k * NC + c];
+#pragma unroll
+      for (int r = 0; r < RI; ++r)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
+    }
+    const size_t e = size_t(cell0) * 2 + el;
+#pragma unroll
+    for (int r = 0; r < RI; ++r) {
+      const int i = i0 + r;
+      const size_t base = (e * NP + i) * NC;
+      const R* ql = &q[(el * NP + i) * NC];
+      R src[NC];
+      if (Phys::kSource) ph.source(ql, src);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const R rhs = Phys::kSource ? acc[r][c] + src[c] : acc[r][c];
+        const R va = a_in ? ql[c] : args.q_a[base + c];
+        const R vb = b_in ? ql[c] : args.q_b[base + c];
+        args.q_out[base + c] = args.rhs_only ? rhs : args.a * va + args.b * vb + args.cdt * rhs;
+      }
+    }
+  }
+}
+
+template <class R, class Phys, int P, int EC, int NT>
 __global__ void __launch_bounds__(NT) stage2d_kernel(Stage2DArgs<R> args, KuhnTab2<R> tabp, Phys ph) {
   constexpr int NC = Phys::NC;
   using S = Stage2DShape<P, NC, R>;
-  constexpr int NP = S::NP, NFP = S::NFP, K = S::K, BSTR = S::BSTR;
-  constexpr int EB = 2 * EC, G = NP / RI, QV = EB * NP * NC;
+  constexpr int NP = S::NP, K = S::K, BSTR = S::BSTR;
+  constexpr int EB = 2 * EC, QV = EB * NP * NC;
   constexpr bool BULK = (2 * NP * NC * sizeof(R)) % 16 == 0;
-  static_assert(NP % RI == 0, "row tile must divide NP");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
   KuhnTab2<R>* tab = reinterpret_cast<KuhnTab2<R>*>(smem_raw + 16);
@@ -64,7 +187,7 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(Stage2DArgs<R> args, KuhnTa
     mbar_arrive_expect_tx(&bar[buf], bytes);
     bulk_g2s(sQ + buf * QV, args.q_in + size_t(c0) * 2 * NP * NC, bytes, &bar[buf]);
   };
-  uint32_t parity[2] = {0u, 0u};
+  uint32_t par = 0u;  // bit b: phase parity of tile buffer b
   int buf = 0;
   if (BULK && tid == 0 && int(blockIdx.x) < ngroups) issue(blockIdx.x, 0);
 
@@ -73,114 +196,23 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(Stage2DArgs<R> args, KuhnTa
     const int ne_here = 2 * min(EC, args.ncell - cell0);
     R* q = sQ + buf * QV;
     if (BULK) {
-      const bool ok = mbar_wait_bounded(&bar[buf], parity[buf], kWaitLimitNs2);
-      parity[buf] ^= 1u;
-      if (!__syncthreads_and(ok)) {
-        if (tid == 0 && args.err) atomicOr(args.err, 1);
+      if (!block_wait_bounded(&bar[buf], (par >> buf) & 1u, kWaitLimitNs2)) {
+        // the copy into this tile is the only one in flight: give it one
+        // more bounded wait before the block (and its shared memory) ends
+        if (tid == 0) {
+          if (args.err) atomicOr(args.err, 1);
+          mbar_wait_bounded(&bar[buf], (par >> buf) & 1u, kWaitLimitNs2);
+        }
         return;
       }
+      par ^= 1u << buf;
       if (tid == 0 && grp + int(gridDim.x) < ngroups) issue(grp + gridDim.x, buf ^ 1);
     } else {
       const R* src = args.q_in + size_t(cell0) * 2 * NP * NC;
       for (int idx = tid; idx < ne_here * NP * NC; idx += NT) q[idx] = src[idx];
       __syncthreads();
     }
-    for (int idx = tid; idx < ne_here * NP; idx += NT) {
-      const int el = idx / NP, j = idx - el * NP, t = el & 1;
-      R Fx[NC], Fy[NC];
-      ph.flux(&q[(el * NP + j) * NC], Fx, Fy);
-      const R* iJ = tab->invJ[t];
-      R* b = &sB[el * BSTR + j * NC];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        b[c] = iJ[0] * Fx[c] + iJ[1] * Fy[c];
-        b[NP * NC + c] = iJ[2] * Fx[c] + iJ[3] * Fy[c];
-      }
-    }
-    for (int idx = tid; idx < ne_here * 3 * NFP; idx += NT) {
-      const int el = idx / (3 * NFP), fm = idx - el * 3 * NFP;
-      const int lf = fm / NFP, m = fm - lf * NFP, t = el & 1, cl = el >> 1;
-      const int cell = cell0 + cl;
-      const int cj = cell / args.nx, ci = cell - cj * args.nx;
-      const int ax = tab->axis[t][lf], dir = tab->dir[t][lf];
-      int code;
-      const int mode = face_mode(ax, dir, ax == 0 ? ci : cj, ax == 0 ? args.nx : args.ny, args.bc, code);
-      const R* qo = &q[(el * NP + tab->own_node[lf][m]) * NC];
-      R nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1];
-      R scale = tab->fscale[t][lf];
-      // one face-flux call per face node (the 2D face functions build the
-      // BC ghost state themselves from the left state and the BC code)
-      R qn[NC];
-      if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
-        const int nbt = tab->nb_t[t][lf], nbn = tab->nb_node[t][lf][m];
-        if (ax < 0) {
-#pragma unroll
-          for (int c = 0; c < NC; ++c) qn[c] = q[((cl * 2 + nbt) * NP + nbn) * NC + c];
-        } else {
-          const int ni = wrapi(ci + tab->off[t][lf][0], args.nx), nj = wrapi(cj + tab->off[t][lf][1], args.ny);
-          const R* gq = args.q_in + ((size_t(nj) * args.nx + ni) * 2 * NP + size_t(nbt) * NP + nbn) * NC;
-#pragma unroll
-          for (int c = 0; c < NC; ++c) qn[c] = __ldg(gq + c);
-        }
-      } else {
-#pragma unroll
-        for (int c = 0; c < NC; ++c) qn[c] = qo[c];
-      }
-      if (mode == FACE_BC_LO) {
-        nx = -nx;
-        ny = -ny;
-        scale = -scale;
-      }
-      const bool bcf = mode != FACE_INTERIOR;
-      const bool own_left = tab->side[t][lf] == 0;
-      const R* L = bcf ? qn : (own_left ? qo : qn);
-      const R* Rr = bcf ? qn : (own_left ? qn : qo);
-      R f[NC];
-      ph.face(L, Rr, bcf ? code : int(BC_INTERIOR), nx, ny, f);
-      R* b = &sB[el * BSTR + (2 * NP + fm) * NC];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) b[c] = scale * f[c];
-    }
-    __syncthreads();
-    const bool a_in = args.q_a == args.q_in, b_in = args.q_b == args.q_in;
-    for (int w = tid; w < ne_here * G; w += NT) {
-      const int el = w / G, g = w - el * G;
-      const int i0 = g * RI;
-      R acc[RI][NC];
-#pragma unroll
-      for (int r = 0; r < RI; ++r)
-#pragma unroll
-        for (int c = 0; c < NC; ++c) acc[r][c] = R(0);
-      const R* b = &sB[el * BSTR];
-#pragma unroll 4
-      for (int k = 0; k < K; ++k) {
-        R av[RI], bv[NC];
-#pragma unroll
-        for (int r = 0; r < RI; ++r) av[r] = sA[k * NP + i0 + r];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) bv[c] = b[k * NC + c];
-#pragma unroll
-        for (int r = 0; r < RI; ++r)
-#pragma unroll
-          for (int c = 0; c < NC; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
-      }
-      const size_t e = size_t(cell0) * 2 + el;
-#pragma unroll
-      for (int r = 0; r < RI; ++r) {
-        const int i = i0 + r;
-        const size_t base = (e * NP + i) * NC;
-        const R* ql = &q[(el * NP + i) * NC];
-        R src[NC];
-        if (Phys::kSource) ph.source(ql, src);
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          const R rhs = Phys::kSource ? acc[r][c] + src[c] : acc[r][c];
-          const R va = a_in ? ql[c] : args.q_a[base + c];
-          const R vb = b_in ? ql[c] : args.q_b[base + c];
-          args.q_out[base + c] = args.rhs_only ? rhs : args.a * va + args.b * vb + args.cdt * rhs;
-        }
-      }
-    }
+    stage2d_tile<R, Phys, P, NT>(args, tab, ph, q, sB, sA, cell0, ne_here);
   }
 }
 
@@ -188,10 +220,8 @@ template <class R, int P, int NC>
 struct Cfg2 {
   using S = Stage2DShape<P, NC, R>;
   static constexpr int NP = S::NP;
-  static constexpr int RI = P == 1 ? 3 : (P == 2 ? 2 : (P == 3 ? 5 : (P == 4 ? 5 : 3)));  // divisors of 3,6,10,15,21
   static constexpr size_t kFixed = 16 + (sizeof(KuhnTab2<R>) + 15) / 16 * 16 + sizeof(R) * S::K * S::NP;
-  static constexpr size_t kPerCell = 2 * sizeof(R) * (2 * size_t(S::NP) * NC + S::BSTR);
-  static constexpr int EC_RAW = int((100 * 1024 - kFixed) / kPerCell);
+  static constexpr int EC_RAW = int((100 * 1024 - kFixed) / S::kPerCell);
   static constexpr int EC = EC_RAW > 64 ? 64 : (EC_RAW < 1 ? 1 : EC_RAW);
   static constexpr int NT = 256;
   static constexpr size_t kSmem = kFixed + sizeof(R) * (2 * size_t(2 * EC) * S::NP * NC + size_t(2 * EC) * S::BSTR);
@@ -200,14 +230,11 @@ struct Cfg2 {
 template <class R, class Phys, int P>
 cudaError_t launch2_p(const Stage2DArgs<R>& a, const KuhnTab2<R>& tab, const Phys& ph, int nsm, cudaStream_t st) {
   using C = Cfg2<R, P, Phys::NC>;
-  auto kern = stage2d_kernel<R, Phys, P, C::EC, C::RI, C::NT>;
+  auto kern = stage2d_kernel<R, Phys, P, C::EC, C::NT>;
   static int bps = -1;
   if (bps < 0) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(C::kSmem));
+    cudaError_t e = persistent_blocks_per_sm((const void*)kern, C::NT, C::kSmem, &bps);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, C::NT, C::kSmem);
-    if (e != cudaSuccess) return e;
-    if (bps < 1) bps = 1;
   }
   const int ngroups = (a.ncell + C::EC - 1) / C::EC;
   int nblk = nsm * bps;

@@ -20,7 +20,10 @@
 //  * Connectivity is never read from memory: neighbour element and node
 //    follow from (cube, type) and a 1.7 KB topology table copied to shared
 //    memory.  Faces between tets of the same cube read both traces from the
-//    shared tile; only cube-boundary faces gather from global memory.
+//    shared tile and are solved once (by the side-0 tet, which writes both
+//    tets' rows); only cube-boundary faces gather from global memory, with
+//    the neighbour cube and BC treatment of each cube face resolved once per
+//    tile.
 //  * q_a / q_b equal to q_in (SSPRK3 stages 1-3) are read from the tile, so
 //    each stage moves the algorithmic minimum of state bytes.
 #pragma once
@@ -55,6 +58,8 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
   R* sQ = reinterpret_cast<R*>(smem_raw + 16 + kTabBytes);                     // [2][QV]
   R* sB = sQ + 2 * QV;                                                         // [EB][BSTR]
   R* sA = sB + EB * BSTR;                                                      // [K][NP] (ASMEM)
+  int* sNb = reinterpret_cast<int*>(sA + (ASMEM ? K * NP : 0));                // [EC][6] neighbour cubes
+  int* sMd = sNb + EC * 6;                                                     // [EC][6] face modes
   const R* Aop = ASMEM ? sA : args.A;
 
   const int tid = threadIdx.x;
@@ -80,29 +85,37 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
     mbar_arrive_expect_tx(&bar[buf], bytes);
     bulk_g2s(sQ + buf * QV, args.q_in + size_t(c0) * 6 * NP * NC, bytes, &bar[buf]);
   };
-  uint32_t parity[2] = {0u, 0u};
+  uint32_t par = 0u;  // bit b: phase parity of tile buffer b
   int buf = 0;
   if (BULK && tid == 0 && int(blockIdx.x) < ngroups) issue(blockIdx.x, 0);
 
-  const int nxy = args.nx * args.ny;
+  const int nwork = tab->n_face_work;
   for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x, buf ^= 1) {
     const int cell0 = grp * EC;
     const int nhere = min(EC, args.ncell - cell0);
     const int ne_here = 6 * nhere;
     R* q = sQ + buf * QV;
     if (BULK) {
-      const bool ok = mbar_wait_bounded(&bar[buf], parity[buf], kWaitLimitNs);
-      parity[buf] ^= 1u;
-      if (!__syncthreads_and(ok)) {
-        if (tid == 0 && args.err) atomicOr(args.err, 1);
+      if (!block_wait_bounded(&bar[buf], (par >> buf) & 1u, kWaitLimitNs)) {
+        // the copy into this tile is the only one in flight: give it one
+        // more bounded wait before the block (and its shared memory) ends
+        if (tid == 0) {
+          if (args.err) atomicOr(args.err, 1);
+          mbar_wait_bounded(&bar[buf], (par >> buf) & 1u, kWaitLimitNs);
+        }
         return;
       }
+      par ^= 1u << buf;
       if (tid == 0 && grp + int(gridDim.x) < ngroups) issue(grp + gridDim.x, buf ^ 1);
     } else {
       const R* src = args.q_in + size_t(cell0) * 6 * NP * NC;
       for (int idx = tid; idx < ne_here * NP * NC; idx += NT) q[idx] = src[idx];
-      __syncthreads();
     }
+    for (int w = tid; w < nhere * 6; w += NT) {
+      const int cl = w / 6, dd = w - cl * 6;
+      cube_dirs3(cell0 + cl, args.nx, args.ny, args.nz, args.bc, sNb + cl * 6, sMd + cl * 6, dd);
+    }
+    __syncthreads();
     // ---- volume fluxes in reference coordinates -> B rows k*NP + j
     for (int idx = tid; idx < ne_here * NP; idx += NT) {
       const int el = idx / NP, j = idx - el * NP, t = el % 6;
@@ -117,15 +130,19 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
           b[k * NP * NC + c] = iJ[k * 3 + 0] * F[c] + iJ[k * 3 + 1] * F[NC + c] + iJ[k * 3 + 2] * F[2 * NC + c];
     }
     // ---- face numerical fluxes, scaled by side*area/(6V) -> B rows 3NP + lf*NFP + m
-    for (int idx = tid; idx < ne_here * 4 * NFP; idx += NT) {
-      const int el = idx / (4 * NFP), fm = idx - el * 4 * NFP;
-      const int lf = fm / NFP, m = fm - lf * NFP, t = el % 6, cl = el / 6;
-      const int cell = cell0 + cl;
-      const int ck = cell / nxy, rem = cell - ck * nxy, cj = rem / args.nx, ci = rem - cj * args.nx;
-      const int ax = tab->axis[t][lf], dir = tab->dir[t][lf];
-      int code;
-      const int mode = face_mode(ax, dir, ax == 0 ? ci : (ax == 1 ? cj : ck),
-                                 ax == 0 ? args.nx : (ax == 1 ? args.ny : args.nz), args.bc, code);
+    for (int idx = tid; idx < EC * nwork * NFP; idx += NT) {
+      const int cl = idx % EC, rest = idx / EC, m = rest % NFP, wk = rest / NFP;
+      if (cl >= nhere) continue;
+      const int tl = tab->face_work[wk], t = tl >> 2, lf = tl & 3;
+      const int el = cl * 6 + t, ax = tab->axis[t][lf], nbt = tab->nb_t[t][lf];
+      int mode = FACE_INTERIOR, code = 0, nbcube = 0;
+      if (ax >= 0) {
+        const int dd = 2 * ax + (tab->dir[t][lf] > 0 ? 1 : 0);
+        const int md = sMd[cl * 6 + dd];
+        mode = md & 0xff;
+        code = md >> 8;
+        nbcube = sNb[cl * 6 + dd];
+      }
       const R* qo = &q[(el * NP + tab->own_node[lf][m]) * NC];
       R nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1], nz = tab->normal[t][lf][2];
       R scale = tab->fscale[t][lf];
@@ -134,15 +151,12 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
       // numerical_flux(q_int, ghost)), interior faces keep side-0 on the left.
       R qn[NC], qg[NC];
       if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
-        const int nbt = tab->nb_t[t][lf], nbn = tab->nb_node[t][lf][m];
+        const int nbn = tab->nb_node[t][lf][m];
         if (ax < 0) {  // face inside the cube: neighbour trace is in the tile
 #pragma unroll
           for (int c = 0; c < NC; ++c) qn[c] = q[((cl * 6 + nbt) * NP + nbn) * NC + c];
         } else {
-          const int ni = wrapi(ci + tab->off[t][lf][0], args.nx), nj = wrapi(cj + tab->off[t][lf][1], args.ny),
-                    nk = wrapi(ck + tab->off[t][lf][2], args.nz);
-          const size_t enb = (size_t(ni) + size_t(args.nx) * (nj + size_t(args.ny) * nk)) * 6 + nbt;
-          const R* gq = args.q_in + (enb * NP + nbn) * NC;
+          const R* gq = args.q_in + ((size_t(nbcube) * 6 + nbt) * NP + nbn) * NC;
 #pragma unroll
           for (int c = 0; c < NC; ++c) qn[c] = __ldg(gq + c);
         }
@@ -159,13 +173,27 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
       const bool bcf = mode != FACE_INTERIOR;
       if (bcf) ph.ghost(qn, code, nx, ny, nz, qg);  // BC_HI/BC_LO: qn = own trace; MIXED: neighbour's
       const bool own_left = bcf ? (mode != FACE_MIXED) : (tab->side[t][lf] == 0);
-      const R* L = bcf ? qn : (own_left ? qo : qn);
-      const R* Rr = bcf ? qg : (own_left ? qn : qo);
+      // left/right states by value (selecting between pointers would force
+      // the register arrays into local memory)
+      R L[NC], Rr[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const R o = qo[c];
+        L[c] = bcf ? qn[c] : (own_left ? o : qn[c]);
+        Rr[c] = bcf ? qg[c] : (own_left ? qn[c] : o);
+      }
       R f[NC];
       ph.num_flux(L, Rr, nx, ny, nz, f);
-      R* b = &sB[el * BSTR + (3 * NP + fm) * NC];
+      R* b = &sB[el * BSTR + (3 * NP + lf * NFP + m) * NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) b[c] = scale * f[c];
+      if (ax < 0) {  // the other tet of this inner face: same flux, its own scale
+        const int lf2 = tab->nb_lf[t][lf];
+        const R s2 = tab->fscale[nbt][lf2];
+        R* b2 = &sB[(cl * 6 + nbt) * BSTR + (3 * NP + lf2 * NFP + tab->nb_m[t][lf][m]) * NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) b2[c] = s2 * f[c];
+      }
     }
     __syncthreads();
     // ---- contraction rhs = A B, source, RK combine, floor, store
@@ -264,7 +292,8 @@ template <class R, int P, int NC, int EC, bool ASMEM>
 constexpr size_t stage3d_smem_bytes() {
   using S = Stage3DShape<P, NC, R>;
   return 16 + (sizeof(KuhnTab3<R>) + 15) / 16 * 16 +
-         sizeof(R) * (2 * size_t(6 * EC) * S::NP * NC + size_t(6 * EC) * S::BSTR + (ASMEM ? size_t(S::K) * S::NP : 0));
+         sizeof(R) * (2 * size_t(6 * EC) * S::NP * NC + size_t(6 * EC) * S::BSTR + (ASMEM ? size_t(S::K) * S::NP : 0)) +
+         size_t(EC) * 12 * sizeof(int);
 }
 
 }  // namespace mxm

@@ -28,11 +28,8 @@ cudaError_t launch3_p(const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phy
   auto kern = stage3d_kernel<R, Phys, P, C::EC, C::RI, C::NT, C::ASMEM>;
   static int bps = -1;
   if (bps < 0) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(C::kSmem));
+    cudaError_t e = persistent_blocks_per_sm((const void*)kern, C::NT, C::kSmem, &bps);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, C::NT, C::kSmem);
-    if (e != cudaSuccess) return e;
-    if (bps < 1) bps = 1;
   }
   const int ngroups = (a.ncell + C::EC - 1) / C::EC;
   int nblk = nsm * bps;

@@ -12,11 +12,8 @@ cudaError_t launch_tc_p(const Stage3DArgs<float>& a, const KuhnTab3<float>& tab,
   auto kern = stage3d_tc_kernel<Phys, P, NT>;
   static int bps = -1;
   if (bps < 0) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(S::SMEM));
+    cudaError_t e = persistent_blocks_per_sm((const void*)kern, NT, S::SMEM, &bps);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, NT, S::SMEM);
-    if (e != cudaSuccess) return e;
-    if (bps < 1) bps = 1;
   }
   const int ngroups = (a.ncell + S::EC - 1) / S::EC;
   int nblk = nsm * bps;

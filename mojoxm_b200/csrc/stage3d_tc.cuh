@@ -20,11 +20,16 @@
 // across the element.
 //
 // Layout: the (c,el) x K operand is MN-major (8 consecutive rows of one k in
-// 16 bytes), so threads that own consecutive nodes write disjoint banks.
-// Faces inside a cube are evaluated once, by their side-0 tet, which writes
-// both tets' rows.  One thread issues the MMAs; completion is tracked by
-// tcgen05.commit on an mbarrier with a bounded wait; warps 0-3 read the
-// accumulator with tcgen05.ld for the FP32 epilogue (source, RK, floor).
+// 16 bytes).  Work is mapped element-fastest: 8 consecutive threads take 8
+// consecutive elements at the same node, so a warp's operand stores land in
+// one or two 128-byte core matrices.  Faces are walked through a per-cube
+// work list (every cube-boundary face, and each face inside the cube once,
+// by its side-0 tet, which writes both tets' rows); the neighbour cube and
+// boundary treatment of the six cube faces are resolved once per tile.  One
+// thread issues the MMAs; completion is tracked by tcgen05.commit on an
+// mbarrier with a bounded wait; warps 0-3 read the accumulator with
+// tcgen05.ld into a padded [row][i] staging tile for the FP32 epilogue
+// (source, RK combine, positivity floor).
 #pragma once
 #include "dg_common.cuh"
 #include "physics.cuh"
@@ -51,19 +56,23 @@ struct TcShape {
   static constexpr int KP = rup16(K), NN = rup16(NP), M = 128;
   static constexpr int EBP = (M / NC) / 8 * 8;      // element slots per component (multiple of 8)
   static constexpr int EC = EBP / 6, EB = 6 * EC;   // whole cubes in a tile
+  static constexpr int NPO = NP | 1;                // odd row stride of the accumulator staging tile
   static constexpr int NCOLS = tmem_cols_for(NN);
   static constexpr size_t A_BYTES = size_t(NN) * KP * 2;  // one of hi / lo
   static constexpr size_t B_BYTES = size_t(M) * KP * 2;
   static constexpr size_t Q_BYTES = size_t(EB) * NP * NC * 4;
+  static constexpr size_t O_BYTES = size_t(M) * NPO * 4;
   static constexpr size_t FB_BYTES = size_t(EB) * 3 * NC * 4;
+  static constexpr size_t CD_BYTES = size_t(EC) * 12 * 4;  // per cube: 6 neighbour cubes + 6 face modes
   static constexpr size_t HDR = 128;
   static constexpr size_t TAB = (sizeof(KuhnTab3<float>) + 127) / 128 * 128;
   static constexpr size_t OFF_A = HDR + TAB;
   static constexpr size_t OFF_B = OFF_A + 2 * A_BYTES;
   static constexpr size_t OFF_Q = OFF_B + 2 * B_BYTES;
   static constexpr size_t OFF_O = OFF_Q + 2 * Q_BYTES;
-  static constexpr size_t OFF_F = OFF_O + Q_BYTES;
-  static constexpr size_t SMEM = OFF_F + FB_BYTES;
+  static constexpr size_t OFF_F = OFF_O + O_BYTES;
+  static constexpr size_t OFF_C = OFF_F + FB_BYTES;
+  static constexpr size_t SMEM = OFF_C + CD_BYTES;
   static constexpr bool BULK = (6 * NP * NC * 4) % 16 == 0;
 };
 
@@ -72,9 +81,10 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
                                                          const unsigned char* __restrict__ a_image) {
   constexpr int NC = Phys::NC;
   using S = TcShape<P, NC>;
-  constexpr int NP = S::NP, NFP = S::NFP, KP = S::KP, NN = S::NN, M = S::M;
+  constexpr int NP = S::NP, NFP = S::NFP, KP = S::KP, NN = S::NN, M = S::M, NPO = S::NPO;
   constexpr int EC = S::EC, EB = S::EB, EBP = S::EBP, QV = EB * NP * NC;
   constexpr uint32_t LBO_A = NN * 16, LBO_B = M * 16, SBO = 128;
+  constexpr uint32_t CSTRIDE = EBP * 16;  // byte step between the rows of consecutive components
   constexpr uint32_t IDESC = umma_idesc_bf16_f32_amn(M, NN);
   static_assert(NN % 16 == 0 && NN <= 256 && KP % 16 == 0 && EC >= 1 && EBP * NC <= M, "UMMA shape");
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -86,8 +96,10 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
   unsigned char* sBhi = smem + S::OFF_B;
   unsigned char* sBlo = sBhi + S::B_BYTES;
   float* sQ = reinterpret_cast<float*>(smem + S::OFF_Q);
-  float* sO = reinterpret_cast<float*>(smem + S::OFF_O);
-  float* sF = reinterpret_cast<float*>(smem + S::OFF_F);  // [EB][3][NC] element flux Fbar
+  float* sO = reinterpret_cast<float*>(smem + S::OFF_O);   // [M rows (c, el)][NPO]
+  float* sF = reinterpret_cast<float*>(smem + S::OFF_F);   // [EB][3][NC] element flux Fbar
+  int* sNb = reinterpret_cast<int*>(smem + S::OFF_C);      // [EC][6] neighbour cube per direction
+  int* sMd = sNb + EC * 6;                                 // [EC][6] face mode | code << 8
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ngroups = (args.ncell + EC - 1) / EC;
@@ -122,51 +134,62 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
     mbar_arrive_expect_tx(&bar[buf], bytes);
     bulk_g2s(sQ + buf * QV, args.q_in + size_t(c0) * 6 * NP * NC, bytes, &bar[buf]);
   };
-  // store one operand value (row (c, el), column k) as bf16 hi / lo
-  auto put = [&](int el, int c, int k, float v) {
-    __nv_bfloat16 h, l;
-    split_bf16(v, h, l);
-    const uint32_t off = umma_mn_offset(c * EBP + el, k, M);
-    *reinterpret_cast<__nv_bfloat16*>(sBhi + off) = h;
-    *reinterpret_cast<__nv_bfloat16*>(sBlo + off) = l;
+  // store the NC operand values v[c] of row (c, el), column k as bf16 hi / lo
+  auto put = [&](int el, int k, const float* v) {
+    const uint32_t off = umma_mn_offset(el, k, M);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      __nv_bfloat16 h, l;
+      split_bf16(v[c], h, l);
+      *reinterpret_cast<__nv_bfloat16*>(sBhi + off + c * CSTRIDE) = h;
+      *reinterpret_cast<__nv_bfloat16*>(sBlo + off + c * CSTRIDE) = l;
+    }
   };
-  uint32_t parity[2] = {0u, 0u}, mma_parity = 0u;
-  bool q_pending[2] = {false, false}, mma_pending = false;
+  // bit b: phase parity / copy in flight of tile buffer b (scalars, so they
+  // stay in registers)
+  uint32_t par = 0u, pend = 0u, mma_parity = 0u;
+  bool mma_pending = false;
   int buf = 0;
-  bool failed = !__syncthreads_and(mbar_wait_bounded(&bar[3], 0, kWaitLimitNs));
+  bool failed = !block_wait_bounded(&bar[3], 0, kWaitLimitNs);
   if (S::BULK && int(blockIdx.x) < ngroups && !failed) {
     if (tid == 0) issue(blockIdx.x, 0);
-    q_pending[0] = true;
+    pend |= 1u;
   }
-  const int nxy = args.nx * args.ny;
+  const int nwork = tab->n_face_work;
 
   for (int grp = blockIdx.x; grp < ngroups && !failed; grp += gridDim.x, buf ^= 1) {
     const int cell0 = grp * EC;
-    const int ne_here = 6 * min(EC, args.ncell - cell0);
+    const int nc_here = min(EC, args.ncell - cell0);
+    const int ne_here = 6 * nc_here;
     float* q = sQ + buf * QV;
     if (S::BULK) {
-      const bool ok = mbar_wait_bounded(&bar[buf], parity[buf], kWaitLimitNs);
-      if (!__syncthreads_and(ok)) {
+      if (!block_wait_bounded(&bar[buf], (par >> buf) & 1u, kWaitLimitNs)) {
         failed = true;
         break;
       }
-      parity[buf] ^= 1u;
-      q_pending[buf] = false;
+      par ^= 1u << buf;
+      pend &= ~(1u << buf);
       if (grp + int(gridDim.x) < ngroups) {
         if (tid == 0) issue(grp + gridDim.x, buf ^ 1);
-        q_pending[buf ^ 1] = true;
+        pend |= 1u << (buf ^ 1);
       }
     } else {
       const float* src = args.q_in + size_t(cell0) * 6 * NP * NC;
       for (int idx = tid; idx < ne_here * NP * NC; idx += NT) q[idx] = src[idx];
       __syncthreads();
     }
-    // ---- per-element constant flux Fbar = F(q at node 0)
+    // ---- per-element constant flux Fbar = F(q at node 0); cube-face treatment
     for (int el = tid; el < ne_here; el += NT) ph.flux(&q[el * NP * NC], &sF[el * 3 * NC]);
+    for (int w = tid; w < nc_here * 6; w += NT) {
+      const int cl = w / 6, dd = w - cl * 6;
+      cube_dirs3(cell0 + cl, args.nx, args.ny, args.nz, args.bc, sNb + cl * 6, sMd + cl * 6, dd);
+    }
     __syncthreads();
     // ---- volume fluxes (F - Fbar) in reference coordinates -> k = d*NP + j
-    for (int idx = tid; idx < ne_here * NP; idx += NT) {
-      const int el = idx / NP, j = idx - el * NP, t = el % 6;
+    for (int idx = tid; idx < EBP * NP; idx += NT) {
+      const int el8 = idx & 7, rest = idx >> 3, j = rest % NP, el = (rest / NP) * 8 + el8;
+      if (el >= ne_here) continue;
+      const int t = el % 6;
       float F[3 * NC];
       ph.flux(&q[(el * NP + j) * NC], F);
       const float* Fb = &sF[el * 3 * NC];
@@ -174,38 +197,40 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
       for (int k = 0; k < 3 * NC; ++k) F[k] -= Fb[k];
       const float* iJ = tab->invJ[t];
 #pragma unroll
-      for (int d = 0; d < 3; ++d)
+      for (int d = 0; d < 3; ++d) {
+        float v[NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c)
-          put(el, c, d * NP + j, iJ[d * 3 + 0] * F[c] + iJ[d * 3 + 1] * F[NC + c] + iJ[d * 3 + 2] * F[2 * NC + c]);
+        for (int c = 0; c < NC; ++c) v[c] = iJ[d * 3 + 0] * F[c] + iJ[d * 3 + 1] * F[NC + c] + iJ[d * 3 + 2] * F[2 * NC + c];
+        put(el, d * NP + j, v);
+      }
     }
     // ---- face fluxes: (f - Fbar.n) * side*area/(6V) -> k = 3NP + lf*NFP + m
-    for (int idx = tid; idx < ne_here * 4 * NFP; idx += NT) {
-      const int el = idx / (4 * NFP), fm = idx - el * 4 * NFP;
-      const int lf = fm / NFP, m = fm - lf * NFP, t = el % 6, cl = el / 6;
-      const int ax = tab->axis[t][lf];
+    for (int idx = tid; idx < EC * nwork * NFP; idx += NT) {
+      const int cl = idx % EC, rest = idx / EC, m = rest % NFP, wk = rest / NFP;
+      if (cl >= nc_here) continue;
+      const int tl = tab->face_work[wk], t = tl >> 2, lf = tl & 3;
+      const int el = cl * 6 + t, ax = tab->axis[t][lf];
       const bool own_left = tab->side[t][lf] == 0;
-      if (ax < 0 && !own_left) continue;  // inside the cube: the side-0 tet writes both rows
-      const int cell = cell0 + cl;
-      const int ck = cell / nxy, rem = cell - ck * nxy, cj = rem / args.nx, ci = rem - cj * args.nx;
-      int code;
-      const int mode = face_mode(ax, tab->dir[t][lf], ax == 0 ? ci : (ax == 1 ? cj : ck),
-                                 ax == 0 ? args.nx : (ax == 1 ? args.ny : args.nz), args.bc, code);
+      const int nbt = tab->nb_t[t][lf];
+      int mode = FACE_INTERIOR, code = 0, nbcube = 0;
+      if (ax >= 0) {
+        const int dd = 2 * ax + (tab->dir[t][lf] > 0 ? 1 : 0);
+        const int md = sMd[cl * 6 + dd];
+        mode = md & 0xff;
+        code = md >> 8;
+        nbcube = sNb[cl * 6 + dd];
+      }
       const float* qo = &q[(el * NP + tab->own_node[lf][m]) * NC];
       float nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1], nz = tab->normal[t][lf][2];
       float scale = tab->fscale[t][lf];
       float qn[NC], qg[NC];
-      const int nbt = tab->nb_t[t][lf];
       if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
         const int nbn = tab->nb_node[t][lf][m];
         if (ax < 0) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) qn[c] = q[((cl * 6 + nbt) * NP + nbn) * NC + c];
         } else {
-          const int ni = wrapi(ci + tab->off[t][lf][0], args.nx), nj = wrapi(cj + tab->off[t][lf][1], args.ny),
-                    nk = wrapi(ck + tab->off[t][lf][2], args.nz);
-          const size_t enb = (size_t(ni) + size_t(args.nx) * (nj + size_t(args.ny) * nk)) * 6 + nbt;
-          const float* gq = args.q_in + (enb * NP + nbn) * NC;
+          const float* gq = args.q_in + ((size_t(nbcube) * 6 + nbt) * NP + nbn) * NC;
 #pragma unroll
           for (int c = 0; c < NC; ++c) qn[c] = __ldg(gq + c);
         }
@@ -221,20 +246,28 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
       }
       const bool bcf = mode != FACE_INTERIOR;
       if (bcf) ph.ghost(qn, code, nx, ny, nz, qg);
-      const float* L = bcf ? qn : (own_left ? qo : qn);
-      const float* Rr = bcf ? qg : (own_left ? qn : qo);
-      float f[NC];
+      // left/right states by value (selecting between pointers would force
+      // the register arrays into local memory)
+      float L[NC], Rr[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float o = qo[c];
+        L[c] = bcf ? qn[c] : (own_left ? o : qn[c]);
+        Rr[c] = bcf ? qg[c] : (own_left ? qn[c] : o);
+      }
+      float f[NC], v[NC];
       ph.num_flux(L, Rr, nx, ny, nz, f);
       const float* Fb = &sF[el * 3 * NC];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) put(el, c, 3 * NP + fm, scale * (f[c] - (Fb[c] * nx + Fb[NC + c] * ny + Fb[2 * NC + c] * nz)));
-      if (ax < 0) {  // the other tet of this cube face: same flux, its own scale and Fbar
+      for (int c = 0; c < NC; ++c) v[c] = scale * (f[c] - (Fb[c] * nx + Fb[NC + c] * ny + Fb[2 * NC + c] * nz));
+      put(el, 3 * NP + lf * NFP + m, v);
+      if (ax < 0) {  // the other tet of this inner face: same flux, its own scale and Fbar
         const int el2 = cl * 6 + nbt, lf2 = tab->nb_lf[t][lf];
         const float s2 = tab->fscale[nbt][lf2];
         const float* Fb2 = &sF[el2 * 3 * NC];
-        const int k2 = 3 * NP + lf2 * NFP + tab->nb_m[t][lf][m];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) put(el2, c, k2, s2 * (f[c] - (Fb2[c] * nx + Fb2[NC + c] * ny + Fb2[2 * NC + c] * nz)));
+        for (int c = 0; c < NC; ++c) v[c] = s2 * (f[c] - (Fb2[c] * nx + Fb2[NC + c] * ny + Fb2[2 * NC + c] * nz));
+        put(el2, 3 * NP + lf2 * NFP + tab->nb_m[t][lf][m], v);
       }
     }
     // make the generic-proxy tile writes visible to the tensor-core (async) proxy
@@ -255,8 +288,7 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
       tc_commit(&bar[2]);
     }
     mma_pending = true;
-    const bool mok = mbar_wait_bounded(&bar[2], mma_parity, kWaitLimitNs);
-    if (!__syncthreads_and(mok)) {
+    if (!block_wait_bounded(&bar[2], mma_parity, kWaitLimitNs)) {
       failed = true;
       break;
     }
@@ -269,24 +301,23 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
 #pragma unroll
       for (int c0 = 0; c0 < NN; c0 += 16) tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + c0, v + c0);
       tmem_ld_wait();
-      const int c = row / EBP, el = row - c * EBP;
-      if (c < NC && el < ne_here) {
 #pragma unroll
-        for (int i = 0; i < NP; ++i) sO[(el * NP + i) * NC + c] = v[i];
-      }
+      for (int i = 0; i < NP; ++i) sO[row * NPO + i] = v[i];
     }
     tc_fence_before();
     __syncthreads();
     // ---- epilogue per node: source, RK combine, floor, store
     const bool a_in = args.q_a == args.q_in, b_in = args.q_b == args.q_in;
     for (int idx = tid; idx < ne_here * NP; idx += NT) {
+      const int el = idx / NP, i = idx - el * NP;
       const size_t base = (size_t(cell0) * 6 * NP + idx) * NC;
       const float* ql = &q[idx * NC];
       float src[NC], out[NC];
       if (Phys::kSource) ph.source(ql, src);
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        const float rhs = Phys::kSource ? sO[idx * NC + c] + src[c] : sO[idx * NC + c];
+        const float r = sO[(c * EBP + el) * NPO + i];
+        const float rhs = Phys::kSource ? r + src[c] : r;
         if (args.rhs_only) {
           out[c] = rhs;
         } else {
@@ -304,9 +335,11 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
     if (tid == 0 && args.err) atomicOr(args.err, 2);
     // let copies and the MMA batch still in flight land before the shared
     // tiles and the accumulator are released (each wait bounded)
-    for (int b = 0; b < 2; ++b)
-      if (q_pending[b]) mbar_wait_bounded(&bar[b], parity[b], kWaitLimitNs);
-    if (mma_pending) mbar_wait_bounded(&bar[2], mma_parity, kWaitLimitNs);
+    if (tid == 0) {
+      for (int b = 0; b < 2; ++b)
+        if ((pend >> b) & 1u) mbar_wait_bounded(&bar[b], (par >> b) & 1u, kWaitLimitNs);
+      if (mma_pending) mbar_wait_bounded(&bar[2], mma_parity, kWaitLimitNs);
+    }
   }
   tc_fence_before();
   __syncthreads();

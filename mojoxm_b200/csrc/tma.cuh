@@ -45,6 +45,20 @@ __device__ __forceinline__ bool mbar_test_parity(uint64_t* bar, uint32_t parity)
   return ok != 0;
 }
 
+// Potentially blocking test: the thread may be suspended for a short,
+// hardware-defined time while the phase is incomplete.
+__device__ __forceinline__ bool mbar_try_parity(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 __device__ __forceinline__ uint64_t global_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -57,10 +71,20 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   if (mbar_test_parity(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   while (true) {
-    for (int k = 0; k < 64; ++k)
-      if (mbar_test_parity(bar, parity)) return true;
+    for (int k = 0; k < 16; ++k)
+      if (mbar_try_parity(bar, parity)) return true;
     if (global_ns() - t0 > limit_ns) return false;
   }
+}
+
+// Block-wide wait: thread 0 polls the barrier (the other threads do not
+// spend issue slots on it), the result is agreed by a barrier, and the
+// barrier also orders the waited-for data (bulk-copy bytes, MMA results)
+// before every thread's later accesses.  Must be reached by all threads.
+__device__ __forceinline__ bool block_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+  bool ok = true;
+  if (threadIdx.x == 0) ok = mbar_wait_bounded(bar, parity, limit_ns);
+  return __syncthreads_and(ok) != 0;
 }
 
 }  // namespace mxm
