@@ -52,6 +52,13 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--l2-steps", type=int, default=100,
                     help="SSPRK3 steps of the accuracy check vs the FP64 path (0 = skip)")
+    ap.add_argument("--batch-solves", type=int, default=512, help="batched 2D leg: solves (0 = skip)")
+    ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--serve-requests", type=int, default=32, help="served leg: requests (0 = skip)")
+    ap.add_argument("--serve-lambda", type=float, default=200.0)
+    ap.add_argument("--serve-largest", action="store_true", help="add the 48^3x6 limited Sod P5 request")
+    ap.add_argument("--serve-slots", type=int, default=8, help="solves running at once in the served leg")
+    ap.add_argument("--cavity", type=int, default=1, help="run the 24^3x6 P=4 Maxwell cavity leg (1/0)")
     return ap.parse_args()
 
 
@@ -278,6 +285,168 @@ def run_reference(a, rank, world):
     print(json.dumps(line))
 
 
+def batched_2d(M, nsolves, steps, seed=2024):
+    """Batched 2D Euler on triangles: `nsolves` independent solves, n x n x 2
+    tris with n ~ U{16,32,64,128,256}, P ~ U{1..5}, ICs a seeded mix of
+    isentropic vortices (beta ~ U[2,6], periodic [0,10]^2) and tanh-smoothed
+    Sod tubes (left/right rho, p ~ U[0.1,1], width 8h, outflow x / periodic
+    y), HLLE flux, BJ limiter eps 0.1, FP32, dt = 0.3 h / ((2P+1) max|lambda|)
+    per solve from the device wave-speed reduction."""
+    rng = np.random.default_rng(seed)
+    batch = M.Batch()
+    solvers = []
+    for k in range(nsolves):
+        n = int(rng.choice([16, 32, 64, 128, 256]))
+        P = int(rng.integers(1, 6))
+        phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_HLLE, False)
+        if rng.random() < 0.5:
+            mesh = M.Mesh(n, n, 1, 10.0, 10.0, 1.0, dim=2)
+            s = M.Solver(mesh, phys, P=P, precision="f32")
+            s.fill_ic(M.IC_VORTEX, [rng.uniform(2, 6), 5.0, 5.0, 1.0, 1.0, 0.0, 1.0])
+            h = 10.0 / n
+        else:
+            mesh = M.Mesh(n, n, 1, 1.0, 1.0, 1.0, bcs=M.BoundaryConditions(2, 2, 0, 0), dim=2)
+            s = M.Solver(mesh, phys, P=P, precision="f32")
+            rl, pl, rr, pr = rng.uniform(0.1, 1.0, 4)
+            s.fill_ic(M.IC_SOD, [rl, pl, rr, pr, 0.5, 8.0 / n])
+            h = 1.0 / n
+        s.enable_cell_limiter(True, 0.1)
+        lam = s.max_wavespeed()
+        batch.add(s, 0.3 * h / ((2 * P + 1) * lam))
+        solvers.append(s)
+    dof = batch.dof_count()
+    t0 = time.perf_counter()
+    batch.step(3)  # autotune + graph capture on the first call, then 3 warm-up steps
+    batch.synchronize()
+    setup_s = time.perf_counter() - t0
+    ms = batch.time_steps(steps)
+    batch.synchronize()
+    tiles = {}
+    for i, s in enumerate(solvers):
+        tiles.setdefault(s.P, batch.tile_cells(i))
+    launches = batch.launches_per_step()
+    # the same solves advanced one at a time through their own handles
+    # (per-solve launches on per-solve streams), 2 steps, wall clock
+    for s in solvers:
+        s.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(2):
+        for i, s in enumerate(solvers):
+            s.step_n(batch.dts[i], 1)
+    for s in solvers:
+        s.synchronize()
+    loop_s = (time.perf_counter() - t0) / 2
+    value = 3 * dof * steps / (ms * 1e-3)
+    out = {"workload": f"{nsolves} independent 2D Euler solves (HLLE, BJ limiter, FP32), n in {{16..256}}, P in 1..5",
+           "solves": nsolves, "dof": dof, "value": value, "unit": UNIT, "ms_per_step": ms / steps,
+           "launches_per_step": launches, "tile_cells_per_P": {str(k): v for k, v in sorted(tiles.items())},
+           "setup_s": setup_s, "per_solve_loop_value": 3 * dof / loop_s,
+           "speedup_vs_per_solve_loop": value / (3 * dof / loop_s), "seed": seed}
+    batch.close()
+    for s in solvers:
+        s.close()
+    return out
+
+
+def maxwell_cavity(M, n=24, P=4, cfl=0.2, precision="mixed"):
+    """3D vacuum Maxwell PEC cavity standing wave: E_z = sin(pi x) sin(pi y)
+    cos(sqrt(2) pi t) on [0,1]^3 (PEC on x and y, periodic z), n^3 x 6 tets,
+    order P, Rusanov, one period T = sqrt(2); the field then equals its
+    initial value, so the analytic error is |q(T) - q(0)|."""
+    bcs = M.BoundaryConditions(1, 1, 1, 1, 0, 0)
+    phys = M.Maxwell(1.0, *([0.0] * 12))
+    T = np.sqrt(2.0)
+    dt = cfl * (1.0 / n) / (2 * P + 1)  # bench_maxwell_cavity_3d.mojo:128
+    nsteps = int(np.ceil(T / dt))
+    dt = T / nsteps
+    res = {}
+    for prec in (precision, "f64"):
+        s = M.Solver(M.Mesh(n, n, n, bcs=bcs), phys, P=P, precision=prec)
+        s.fill_ic(M.IC_CAVITY, [1.0, 1.0, 1.0])
+        q0 = s.download_state().astype(np.float64)
+        ms = s.time_steps(dt, nsteps)
+        res[prec] = (s.download_state().astype(np.float64), ms, s.dof_count())
+        s.close()
+    qa, ms, dof = res[precision]
+    q64, ms64, _ = res["f64"]
+
+    def rl2(a, b):
+        return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+    return {"workload": f"3D Maxwell PEC cavity, {n}^3x6 = {6 * n ** 3} tets, P={P}, Rusanov, one period "
+                        f"({nsteps} SSPRK3 steps)", "precision": precision,
+            "value": 3 * dof * nsteps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / nsteps,
+            "plain_f64_value": 3 * dof * nsteps / (ms64 * 1e-3),
+            "rel_l2_vs_f64": rl2(qa, q64), "rel_l2_vs_exact": rl2(qa, q0), "rel_l2_f64_vs_exact": rl2(q64, q0)}
+
+
+def served(M, nreq, lam, seed=7, largest=False, slots=8):
+    """Served stream: Poisson arrivals at `lam`/s of 2D/3D Euler, 2D
+    shallow-water dam breaks and 3D Maxwell plane waves, 2k-400k elements
+    (log-uniform), P in 2..5, 50-500 SSPRK3 steps, seeded ICs, admitted by a
+    150 GB HBM budget; `largest` adds the 3D limited Sod at P=5 on 48^3 x 6
+    tets (50 steps)."""
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for k in range(nreq):
+        kind = int(rng.integers(0, 4))
+        E = float(np.exp(rng.uniform(np.log(2e3), np.log(4e5))))
+        P = int(rng.integers(2, 6))
+        nsteps = int(rng.integers(50, 501))
+        if kind == 0:  # 2D Euler vortex
+            n = max(4, int(round(np.sqrt(E / 2))))
+            mesh = M.Mesh(n, n, 1, 10.0, 10.0, 1.0, dim=2)
+            phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_HLLE, False)
+            ic, prm, lam_est, h = M.IC_VORTEX, [rng.uniform(2, 6), 5, 5, 1, 1, 0, 1], 1.5 + 1.0 + np.sqrt(GAMMA), 10.0 / n
+            prec = "f32"
+        elif kind == 1:  # 3D Euler smooth wave
+            n = max(2, int(round((E / 6) ** (1 / 3))))
+            mesh = M.Mesh(n, n, n)
+            phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_RUSANOV, False)
+            ic, prm, lam_est, h = M.IC_SINE_WAVE, [1, 0.2, 1, 1, 1, 1, 1, 1, 1], np.sqrt(3) + 1.5, 1.0 / n
+            prec = "mixed" if P <= 4 else "f32"
+        elif kind == 2:  # dam break
+            n = max(4, int(round(np.sqrt(E / 2))))
+            mesh = M.Mesh(n, n, 1, 1.0, 1.0, 1.0, bcs=M.BoundaryConditions(1, 1, 1, 1), dim=2)
+            phys = M.ShallowWater(9.81, 1e-6, 1.0, 0.0, 0.0)
+            hl = rng.uniform(1, 3)
+            ic, prm, lam_est, h = M.IC_DAM_BREAK, [hl, 1.0, 0.5, 2.0 / n], 2 * np.sqrt(9.81 * hl), 1.0 / n
+            prec = "f32"
+        else:  # 3D Maxwell plane wave
+            n = max(2, int(round((E / 6) ** (1 / 3))))
+            mesh = M.Mesh(n, n, n)
+            phys = M.Maxwell(1.0, *([0.0] * 12))
+            ic, prm, lam_est, h = M.IC_PLANE_WAVE, [1.0, 1.0], 1.0, 1.0 / n
+            prec = "f32"
+        dt = 0.1 * h / (lam_est * (2 * P + 1))
+        reqs.append((mesh, phys, P, prec, ic, prm, dt, nsteps, None))
+    if largest:
+        mesh = M.Mesh(48, 48, 48, bcs=M.BoundaryConditions(2, 2, 1, 1, 1, 1))
+        phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_HLLEC, False)
+        reqs.append((mesh, phys, 5, "f32", M.IC_SOD, [1.0, 1.0, 0.125, 0.1, 0.5, 1.0 / 48], 0.1 / 48 / (2.5 * 11),
+                     50, 0.1))
+    gaps = rng.exponential(1.0 / lam, len(reqs))
+    srv = M.Server(hbm_budget_bytes=150e9, max_active=slots, steps_per_chunk=10)
+    t0 = time.perf_counter()
+    ids, t_next = [], 0.0
+    for r, g in zip(reqs, gaps):
+        t_next += g
+        delay = t_next - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(*r))
+    for i in ids:
+        srv.wait(i, timeout_s=900)
+    st = srv.stats()
+    srv.close()
+    return {"workload": f"{len(reqs)} requests, Poisson arrivals at {lam:g}/s: 2D/3D Euler, 2D dam break, 3D Maxwell "
+                        f"plane wave; 2k-400k elements, P 2..5, 50-500 steps" + ("; + 48^3x6 limited Sod P5" if largest else ""),
+            "requests": len(reqs), "lambda_per_s": lam, "solves_per_s": st["solves_per_s"], "p50_ms": st["p50_ms"],
+            "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "dof_stage_per_s": st["dof_stage_per_s"],
+            "completed": st["completed"], "failed": st["failed"], "peak_concurrent": st["peak_concurrent"],
+            "peak_admitted_bytes": st["peak_bytes"], "hbm_budget_bytes": 150e9, "slots": slots, "seed": seed}
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -296,6 +465,7 @@ def main():
         return
 
     import mojoxm_b200 as M
+    from mojoxm_b200 import replicas
 
     M.set_device(local)
     phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_RUSANOV, False)
@@ -316,14 +486,8 @@ def main():
     with clock_sampler(local) as clk:
         ms = s.time_steps(dt, a.steps)  # CUDA events on the solver's stream
     barrier()
-    ms_max = ms
-    if dist:
-        import torch
-
-        t = torch.tensor([ms], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = world * 3 * dof * a.steps / (ms_max * 1e-3)
+    ms_max = replicas.max_over_ranks(ms)  # job time = slowest replica
+    value = replicas.sum_over_ranks(3 * dof * a.steps) / (ms_max * 1e-3)
 
     # end to end through the host-buffer entry (pinned in/out, copies timed)
     pin_in = M.PinnedArray(s.shape, s.dtype)
@@ -337,13 +501,8 @@ def main():
         s.advance_host(pin_in.array, 1, dt, out=pin_out.array)
     el = time.perf_counter() - t0
     barrier()
-    if dist:
-        import torch
-
-        t = torch.tensor([el], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el = float(t.item())
-    e2e_value = world * 3 * dof * e2e_steps / el
+    el = replicas.max_over_ranks(el)
+    e2e_value = replicas.sum_over_ranks(3 * dof * e2e_steps) / el
     qbytes = int(np.prod(s.shape)) * np.dtype(s.dtype).itemsize
     pin_in.free()
     pin_out.free()
@@ -357,14 +516,9 @@ def main():
         barrier()
         ms64 = s64.time_steps(dt, a.steps)
         barrier()
-        if dist:
-            import torch
-
-            t = torch.tensor([ms64], dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms64 = float(t.item())
+        ms64 = replicas.max_over_ranks(ms64)
         s64.close()
-        v64 = world * 3 * dof * a.steps / (ms64 * 1e-3)
+        v64 = replicas.sum_over_ranks(3 * dof * a.steps) / (ms64 * 1e-3)
         plain = {"value": v64, "ms_per_step": ms64 / a.steps, "speedup": value / v64}
 
     if rank == 0:
@@ -376,6 +530,10 @@ def main():
         nsm_flops = 2 * (3 * s.NP + 4 * s.NFP) * dof  # contraction flops per stage
         cb = cpu_baseline(a, a.cpu_seconds)
         acc = accuracy_check(M, a, q0, dt) if a.l2_steps > 0 else None
+        bat = batched_2d(M, a.batch_solves, a.batch_steps) if a.batch_solves > 0 else None
+        cav = maxwell_cavity(M) if a.cavity else None
+        srv = served(M, a.serve_requests, a.serve_lambda, largest=a.serve_largest,
+                     slots=a.serve_slots) if a.serve_requests > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -393,6 +551,9 @@ def main():
                          "contraction_tflops": nsm_flops / avg_launch_s / 1e12},
             "cpu_baseline": cb,
             "plain_f64": plain,
+            "batched": bat,
+            "maxwell_cavity": cav,
+            "served": srv,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": qbytes,
                     "entry": "mxm_dg_advance_host (pinned host state in/out, 1 SSPRK3 step per call)"},
             "gpu_launches": launches * a.steps,

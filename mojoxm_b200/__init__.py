@@ -462,6 +462,7 @@ class Batch:
             raise DGError(rc, self._err(None))
         self.h = h
         self.members = []
+        self.dts = []
 
     @staticmethod
     def _err(h):
@@ -477,6 +478,7 @@ class Batch:
         i = ctypes.c_int32()
         self._c(lib().mxm_dg_batch_add(self.h, solver.h, dt, ctypes.byref(i)))
         self.members.append(solver)
+        self.dts.append(dt)
         return i.value
 
     def autotune(self):

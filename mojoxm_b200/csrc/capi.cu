@@ -42,19 +42,23 @@ static float bf16_value(uint16_t b) {
 }
 
 // Shared operator A (NP x K, row-major, FP64) as the tensor-core B operand:
-// N = NP rounded up to 16 rows, K rounded up to 16, K-major no-swizzle
-// core-matrix layout, split into a bfloat16 hi image followed by a lo image
+// N = NP rounded up to 16 rows; the volume columns [0, nvol) padded to
+// kvol = nvol rounded up to 16, then the face columns [nvol, K) from column
+// kvol on, padded to a multiple of 16; K-major no-swizzle core-matrix
+// layout, split into a bfloat16 hi image followed by a lo image
 // (a = hi + lo); padding entries are zero.
-static std::vector<unsigned char> tc_operator_image(const std::vector<double>& A, int NP, int K) {
-  const int NN = (NP + 15) / 16 * 16, KP = (K + 15) / 16 * 16;
-  const size_t half = size_t(NN) * KP * 2;
+static std::vector<unsigned char> tc_operator_image(const std::vector<double>& A, int NP, int K, int nvol) {
+  const int NN = (NP + 15) / 16 * 16, kvol = (nvol + 15) / 16 * 16;
+  const int KA = kvol + (K - nvol + 15) / 16 * 16;
+  const size_t half = size_t(NN) * KA * 2;
   std::vector<unsigned char> img(2 * half, 0);
-  for (int i = 0; i < NN; ++i)
-    for (int k = 0; k < KP; ++k) {
-      const double v = (i < NP && k < K) ? A[size_t(i) * K + k] : 0.0;
+  for (int i = 0; i < NP; ++i)
+    for (int k = 0; k < K; ++k) {
+      const double v = A[size_t(i) * K + k];
       const uint16_t hi = bf16_bits(float(v));
       const uint16_t lo = bf16_bits(float(v - double(bf16_value(hi))));
-      const size_t off = umma_tile_offset(i, k, NN);
+      const int col = k < nvol ? k : kvol + (k - nvol);
+      const size_t off = umma_tile_offset(i, col, NN);
       std::memcpy(&img[off], &hi, 2);
       std::memcpy(&img[half + off], &lo, 2);
     }
@@ -586,7 +590,7 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
     upload(&raw->A, At);
     upload(&raw->w, raw->ref.w);
     if (raw->use_tc) {
-      auto img = tc_operator_image(raw->Ahost, raw->NP, raw->K);
+      auto img = tc_operator_image(raw->Ahost, raw->NP, raw->K, 3 * raw->NP);
       CK(cudaMalloc(&raw->tcimg, img.size()));
       CK(cudaMemcpy(raw->tcimg, img.data(), img.size(), cudaMemcpyHostToDevice));
     }

@@ -50,30 +50,38 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16_f32_amn(int M, int N) {
   return umma_idesc_bf16_f32(M, N) | (1u << 15);  // A operand MN-major
 }
 
+// The K dimension is split into the volume columns (3 NP, padded to KV) and
+// the face columns (4 NFP, padded to KF); both halves reuse one operand
+// buffer of KB = max(KV, KF) columns, and the operator image stores the
+// face columns from KV on (tc_operator_image's `kvol`).
 template <int P, int NC>
 struct TcShape {
   static constexpr int NP = ntet(P), NFP = ntri(P), K = 3 * NP + 4 * NFP;
-  static constexpr int KP = rup16(K), NN = rup16(NP), M = 128;
+  static constexpr int KV = rup16(3 * NP), KF = rup16(4 * NFP), KA = KV + KF;
+  static constexpr int KB = KV > KF ? KV : KF;
+  static constexpr int NN = rup16(NP), M = 128;
   static constexpr int EBP = (M / NC) / 8 * 8;      // element slots per component (multiple of 8)
   static constexpr int EC = EBP / 6, EB = 6 * EC;   // whole cubes in a tile
   static constexpr int NPO = NP | 1;                // odd row stride of the accumulator staging tile
   static constexpr int NCOLS = tmem_cols_for(NN);
-  static constexpr size_t A_BYTES = size_t(NN) * KP * 2;  // one of hi / lo
-  static constexpr size_t B_BYTES = size_t(M) * KP * 2;
+  static constexpr size_t A_BYTES = size_t(NN) * KA * 2;  // one of hi / lo
+  static constexpr size_t B_BYTES = size_t(M) * KB * 2;
   static constexpr size_t Q_BYTES = size_t(EB) * NP * NC * 4;
-  static constexpr size_t O_BYTES = size_t(M) * NPO * 4;
+  static constexpr size_t O_BYTES = size_t(M) * NPO * 4;   // aliases the operand buffer (free by then)
   static constexpr size_t FB_BYTES = size_t(EB) * 3 * NC * 4;
+  static constexpr size_t FN_BYTES = size_t(EB) * 4 * NC * 4;  // Fbar . n per (element, face)
   static constexpr size_t CD_BYTES = size_t(EC) * 12 * 4;  // per cube: 6 neighbour cubes + 6 face modes
   static constexpr size_t HDR = 128;
   static constexpr size_t TAB = (sizeof(KuhnTab3<float>) + 127) / 128 * 128;
   static constexpr size_t OFF_A = HDR + TAB;
   static constexpr size_t OFF_B = OFF_A + 2 * A_BYTES;
   static constexpr size_t OFF_Q = OFF_B + 2 * B_BYTES;
-  static constexpr size_t OFF_O = OFF_Q + 2 * Q_BYTES;
-  static constexpr size_t OFF_F = OFF_O + O_BYTES;
-  static constexpr size_t OFF_C = OFF_F + FB_BYTES;
+  static constexpr size_t OFF_F = OFF_Q + 2 * Q_BYTES;
+  static constexpr size_t OFF_N = OFF_F + FB_BYTES;
+  static constexpr size_t OFF_C = OFF_N + FN_BYTES;
   static constexpr size_t SMEM = OFF_C + CD_BYTES;
   static constexpr bool BULK = (6 * NP * NC * 4) % 16 == 0;
+  static_assert(O_BYTES <= 2 * B_BYTES, "staging tile must fit the operand buffer");
 };
 
 template <class Phys, int P, int NT>
@@ -81,12 +89,13 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
                                                          const unsigned char* __restrict__ a_image) {
   constexpr int NC = Phys::NC;
   using S = TcShape<P, NC>;
-  constexpr int NP = S::NP, NFP = S::NFP, KP = S::KP, NN = S::NN, M = S::M, NPO = S::NPO;
+  constexpr int NP = S::NP, NFP = S::NFP, KV = S::KV, KF = S::KF, NN = S::NN, M = S::M, NPO = S::NPO;
   constexpr int EC = S::EC, EB = S::EB, EBP = S::EBP, QV = EB * NP * NC;
   constexpr uint32_t LBO_A = NN * 16, LBO_B = M * 16, SBO = 128;
   constexpr uint32_t CSTRIDE = EBP * 16;  // byte step between the rows of consecutive components
   constexpr uint32_t IDESC = umma_idesc_bf16_f32_amn(M, NN);
-  static_assert(NN % 16 == 0 && NN <= 256 && KP % 16 == 0 && EC >= 1 && EBP * NC <= M, "UMMA shape");
+  static_assert(NN % 16 == 0 && NN <= 256 && KV % 16 == 0 && KF % 16 == 0 && EC >= 1 && EBP * NC <= M,
+                "UMMA shape");
   extern __shared__ __align__(1024) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);  // [0..1] q tiles, [2] mma, [3] A image
   uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 32);
@@ -96,8 +105,9 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
   unsigned char* sBhi = smem + S::OFF_B;
   unsigned char* sBlo = sBhi + S::B_BYTES;
   float* sQ = reinterpret_cast<float*>(smem + S::OFF_Q);
-  float* sO = reinterpret_cast<float*>(smem + S::OFF_O);   // [M rows (c, el)][NPO]
+  float* sO = reinterpret_cast<float*>(sBhi);              // [M rows (c, el)][NPO], after the MMAs
   float* sF = reinterpret_cast<float*>(smem + S::OFF_F);   // [EB][3][NC] element flux Fbar
+  float* sFn = reinterpret_cast<float*>(smem + S::OFF_N);  // [EB][4][NC] Fbar . n of each face
   int* sNb = reinterpret_cast<int*>(smem + S::OFF_C);      // [EC][6] neighbour cube per direction
   int* sMd = sNb + EC * 6;                                 // [EC][6] face mode | code << 8
 
@@ -149,6 +159,35 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
   // stay in registers)
   uint32_t par = 0u, pend = 0u, mma_parity = 0u;
   bool mma_pending = false;
+  // One half of K: make the operand writes visible to the tensor-core
+  // (async) proxy, let one thread issue nks K-steps (hi*hi + hi*lo + lo*hi)
+  // against operator K-steps [ka0, ka0 + nks), and wait (bounded) until they
+  // completed; ka0 == 0 starts the accumulator.  All threads call it.
+  auto mma_half = [&](int ka0, int nks) -> bool {
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t ah = smem_u32(sAhi), al = smem_u32(sAlo), bh = smem_u32(sBhi), bl = smem_u32(sBlo);
+#pragma unroll 1
+      for (int ks = 0; ks < nks; ++ks) {
+        const uint32_t oa = uint32_t(ka0 + ks) * 2 * LBO_A, ob = uint32_t(ks) * 2 * LBO_B;
+        const uint64_t dAh = umma_desc(ah + oa, LBO_A, SBO), dAl = umma_desc(al + oa, LBO_A, SBO);
+        const uint64_t dBh = umma_desc(bh + ob, LBO_B, SBO), dBl = umma_desc(bl + ob, LBO_B, SBO);
+        tc_mma_bf16(tmem, dBh, dAh, IDESC, (ka0 + ks) > 0 ? 1u : 0u);
+        tc_mma_bf16(tmem, dBh, dAl, IDESC, 1u);
+        tc_mma_bf16(tmem, dBl, dAh, IDESC, 1u);
+      }
+      tc_commit(&bar[2]);
+    }
+    mma_pending = true;
+    if (!block_wait_bounded(&bar[2], mma_parity, kWaitLimitNs)) return false;
+    mma_parity ^= 1u;
+    mma_pending = false;
+    tc_fence_after();
+    return true;
+  };
   int buf = 0;
   bool failed = !block_wait_bounded(&bar[3], 0, kWaitLimitNs);
   if (S::BULK && int(blockIdx.x) < ngroups && !failed) {
@@ -179,7 +218,19 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
       __syncthreads();
     }
     // ---- per-element constant flux Fbar = F(q at node 0); cube-face treatment
-    for (int el = tid; el < ne_here; el += NT) ph.flux(&q[el * NP * NC], &sF[el * 3 * NC]);
+    for (int el = tid; el < ne_here; el += NT) {
+      float F[3 * NC];
+      ph.flux(&q[el * NP * NC], F);
+      const int t = el % 6;
+#pragma unroll
+      for (int k = 0; k < 3 * NC; ++k) sF[el * 3 * NC + k] = F[k];
+#pragma unroll
+      for (int lf = 0; lf < 4; ++lf) {
+        const float nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1], nz = tab->normal[t][lf][2];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) sFn[(el * 4 + lf) * NC + c] = F[c] * nx + F[NC + c] * ny + F[2 * NC + c] * nz;
+      }
+    }
     for (int w = tid; w < nc_here * 6; w += NT) {
       const int cl = w / 6, dd = w - cl * 6;
       cube_dirs3(cell0 + cl, args.nx, args.ny, args.nz, args.bc, sNb + cl * 6, sMd + cl * 6, dd);
@@ -204,7 +255,13 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
         put(el, d * NP + j, v);
       }
     }
-    // ---- face fluxes: (f - Fbar.n) * side*area/(6V) -> k = 3NP + lf*NFP + m
+    // volume half of K: operand columns [0, KV) against operator columns [0, KV)
+    if (!mma_half(0, KV / 16)) {
+      failed = true;
+      break;
+    }
+    // ---- face fluxes: (f - Fbar.n) * side*area/(6V) -> operand column lf*NFP + m
+    //      (operator column KV + lf*NFP + m), into the same operand buffer
     for (int idx = tid; idx < EC * nwork * NFP; idx += NT) {
       const int cl = idx % EC, rest = idx / EC, m = rest % NFP, wk = rest / NFP;
       if (cl >= nc_here) continue;
@@ -257,44 +314,26 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
       }
       float f[NC], v[NC];
       ph.num_flux(L, Rr, nx, ny, nz, f);
-      const float* Fb = &sF[el * 3 * NC];
+      // Fbar . n was taken with the table normal; a one-sided low face flips it
+      const float* Fn = &sFn[(el * 4 + lf) * NC];
+      const float sg = mode == FACE_BC_LO ? -1.f : 1.f;
 #pragma unroll
-      for (int c = 0; c < NC; ++c) v[c] = scale * (f[c] - (Fb[c] * nx + Fb[NC + c] * ny + Fb[2 * NC + c] * nz));
-      put(el, 3 * NP + lf * NFP + m, v);
-      if (ax < 0) {  // the other tet of this inner face: same flux, its own scale and Fbar
+      for (int c = 0; c < NC; ++c) v[c] = scale * (f[c] - sg * Fn[c]);
+      put(el, lf * NFP + m, v);
+      if (ax < 0) {  // the other tet of this inner face: same flux and normal, its own scale and Fbar
         const int el2 = cl * 6 + nbt, lf2 = tab->nb_lf[t][lf];
         const float s2 = tab->fscale[nbt][lf2];
-        const float* Fb2 = &sF[el2 * 3 * NC];
+        const float* Fn2 = &sFn[(el2 * 4 + lf2) * NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) v[c] = s2 * (f[c] - (Fb2[c] * nx + Fb2[NC + c] * ny + Fb2[2 * NC + c] * nz));
-        put(el2, 3 * NP + lf2 * NFP + tab->nb_m[t][lf][m], v);
+        for (int c = 0; c < NC; ++c) v[c] = s2 * (f[c] - Fn2[c]);
+        put(el2, lf2 * NFP + tab->nb_m[t][lf][m], v);
       }
     }
-    // make the generic-proxy tile writes visible to the tensor-core (async) proxy
-    fence_proxy_async();
-    tc_fence_before();
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      const uint32_t ah = smem_u32(sAhi), al = smem_u32(sAlo), bh = smem_u32(sBhi), bl = smem_u32(sBlo);
-#pragma unroll 1
-      for (int ks = 0; ks < KP / 16; ++ks) {
-        const uint64_t dAh = umma_desc(ah + ks * 2 * LBO_A, LBO_A, SBO), dAl = umma_desc(al + ks * 2 * LBO_A, LBO_A, SBO);
-        const uint64_t dBh = umma_desc(bh + ks * 2 * LBO_B, LBO_B, SBO), dBl = umma_desc(bl + ks * 2 * LBO_B, LBO_B, SBO);
-        tc_mma_bf16(tmem, dBh, dAh, IDESC, ks > 0 ? 1u : 0u);
-        tc_mma_bf16(tmem, dBh, dAl, IDESC, 1u);
-        tc_mma_bf16(tmem, dBl, dAh, IDESC, 1u);
-      }
-      tc_commit(&bar[2]);
-    }
-    mma_pending = true;
-    if (!block_wait_bounded(&bar[2], mma_parity, kWaitLimitNs)) {
+    // face half of K: operand columns [0, KF) against operator columns [KV, KV + KF)
+    if (!mma_half(KV / 16, KF / 16)) {
       failed = true;
       break;
     }
-    mma_parity ^= 1u;
-    mma_pending = false;
-    tc_fence_after();
     if (warp < 4) {  // warp w reads TMEM lanes [32w, 32w+32): rows (c, el)
       const int row = warp * 32 + lane;
       float v[NN];

@@ -1,0 +1,121 @@
+"""End-to-end runs of the benchmark configurations' physics at test sizes.
+
+* Isentropic vortex (3D Euler, [0,10]^3 periodic, 8^3 x 6 tets, P = 2,
+  HLLEC with and without the entropy fix, SSPRK3 at CFL 0.3 to T = 1): the
+  oracle and the product agree, and both stay within the reference's own
+  analytic gate (L2 <= 0.10 relative to the translated vortex,
+  benchmarks/bench_euler_vortex_3d.mojo:75).
+* Maxwell PEC cavity mode (E_z = sin(pi x) sin(pi y) at t = 0, PEC on x and
+  y, periodic z): after one period the field returns to its initial state;
+  FP64 and split-BF16 runs are checked against that and against each other."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import mojoxm_b200 as M
+from tests import dgcases as C
+
+GAMMA = 1.4
+HERE = os.path.dirname(os.path.abspath(__file__))
+with open(os.path.join(HERE, "golden", "known_answers.json")) as _f:
+    G = json.load(_f)["values"]
+
+BETA, X0, Y0, UBG, VBG = 5.0, 5.0, 5.0, 1.0, 1.0
+
+
+def vortex_state(xyz, t=0.0, L=10.0):
+    """Shu isentropic vortex advected by (UBG, VBG, 0), nearest periodic image."""
+    dx = xyz[..., 0] - (X0 + UBG * t)
+    dy = xyz[..., 1] - (Y0 + VBG * t)
+    dx -= L * np.floor(dx / L + 0.5)
+    dy -= L * np.floor(dy / L + 0.5)
+    r2 = dx * dx + dy * dy
+    f = BETA / (2 * np.pi)
+    ex = np.exp(0.5 * (1 - r2))
+    u, v = UBG - f * dy * ex, VBG + f * dx * ex
+    T = 1 - (GAMMA - 1) * f * f / (2 * GAMMA) * np.exp(1 - r2)
+    rho = T ** (1 / (GAMMA - 1))
+    p = rho ** GAMMA
+    q = np.zeros(xyz.shape[:-1] + (5,))
+    q[..., 0] = rho
+    q[..., 1] = rho * u
+    q[..., 2] = rho * v
+    q[..., 4] = p / (GAMMA - 1) + 0.5 * rho * (u * u + v * v)
+    return q
+
+
+def vortex_steps(P=2, n=8, L=10.0, T=1.0, cfl=0.3):
+    # examples/euler_vortex.mojo:137-144: dt = CFL h / (lambda (2P+1))
+    lam = np.hypot(UBG, VBG) + BETA / (2 * np.pi) + np.sqrt(GAMMA)
+    dt = cfl * (L / n) / (lam * (2 * P + 1))
+    nsteps = int(np.ceil(T / dt))
+    return T / nsteps, nsteps
+
+
+def rel_l2(a, b):
+    return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+
+@pytest.mark.parametrize("efix", [False, True])
+def test_vortex_oracle_within_reference_gate(oracle_mod, efix):
+    ph = C.euler(M.FLUX_HLLEC, efix=efix)
+    o = oracle_mod.Oracle3D(2, 8, 10.0, M.physics_dict(ph))
+    xyz = o.node_xyz()
+    o.set(vortex_state(xyz))
+    dt, n = vortex_steps()
+    o.step(dt, n)
+    err = rel_l2(o.get(), vortex_state(xyz, t=1.0))
+    assert err <= G["vortex_3d.l2_max_rel"], err
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("efix", [False, True])
+def test_vortex_product_vs_oracle(oracle_mod, prec, efix):
+    ph = C.euler(M.FLUX_HLLEC, efix=efix)
+    o = oracle_mod.Oracle3D(2, 8, 10.0, M.physics_dict(ph), real=prec)
+    s = M.Solver(M.Mesh(8, 8, 8, 10.0, 10.0, 10.0), ph, P=2, precision=prec)
+    xyz = o.node_xyz()
+    q0 = vortex_state(xyz)
+    o.set(q0)
+    s.upload_state(q0)
+    dt, n = vortex_steps()
+    o.step(dt, n)
+    s.step_n(dt, n)
+    qs = s.download_state().astype(np.float64)
+    assert rel_l2(qs, o.get()) <= (1e-11 if prec == "f64" else 2e-5)
+    assert rel_l2(qs, vortex_state(xyz, t=1.0)) <= G["vortex_3d.l2_max_rel"]
+    # the device IC fill gives the same field
+    s.fill_ic(M.IC_VORTEX, [BETA, X0, Y0, UBG, VBG, 0.0, 1.0])
+    assert rel_l2(s.download_state().astype(np.float64), q0) < (1e-7 if prec == "f64" else 1e-6)
+    s.close()
+
+
+def cavity_steps(P, n, cfl=0.2):
+    # bench_maxwell_cavity_3d.mojo:56,128-130: dt = CFL h / (c (2P+1)), T one period
+    T = np.sqrt(2.0)  # omega = sqrt(2) pi for the (1, 1) mode on the unit square
+    dt = cfl * (1.0 / n) / (2 * P + 1)
+    nsteps = int(np.ceil(T / dt))
+    return T / nsteps, nsteps
+
+
+@pytest.mark.gpu
+def test_maxwell_cavity_one_period():
+    n, P = 6, 3
+    bcs = M.BoundaryConditions(1, 1, 1, 1, 0, 0)  # PEC on x and y, periodic z
+    phys = M.Maxwell(1.0, *([0.0] * 12))
+    dt, nsteps = cavity_steps(P, n)
+    out = {}
+    for prec in ("f64", "mixed"):
+        s = M.Solver(M.Mesh(n, n, n, bcs=bcs), phys, P=P, precision=prec)
+        s.fill_ic(M.IC_CAVITY, [1.0, 1.0, 1.0])
+        q0 = s.download_state().astype(np.float64)
+        s.step_n(dt, nsteps)
+        out[prec] = s.download_state().astype(np.float64)
+        s.close()
+    # after one period E_z is back and B vanishes: error of the DG scheme
+    err64 = rel_l2(out["f64"], q0)
+    assert err64 < 5e-3, err64
+    assert rel_l2(out["mixed"], out["f64"]) < 1e-4

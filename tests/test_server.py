@@ -74,20 +74,21 @@ def test_result_alone_equals_in_mix_and_direct():
 
 @pytest.mark.gpu
 def test_admission_by_hbm_budget():
-    reqs = _requests()[:3]
-    # room for the largest single request only
-    sizes = []
-    for mesh, phys, P, prec, *_ in reqs:
-        ne, NP, NC = M.state_shape(mesh, phys, P)
-        sizes.append((3 * ne * NP * NC + ne * NC) * (8 if prec == "f64" else 4) + 2 ** 20)
-    srv = M.Server(hbm_budget_bytes=float(max(sizes)), max_active=8, steps_per_chunk=8)
-    ids = [srv.submit(*r) for r in reqs]
+    # three equal requests, budget for one and a half of them
+    req = _requests()[0]
+    mesh, phys, P, prec, *_ = req
+    ne, NP, NC = M.state_shape(mesh, phys, P)
+    one = (3 * ne * NP * NC + ne * NC) * (8 if prec == "f64" else 4)
+    srv = M.Server(hbm_budget_bytes=1.5 * one, max_active=8, steps_per_chunk=8)
+    ids = [srv.submit(*req) for _ in range(3)]
     for i in ids:
         srv.wait(i)
     st = srv.stats()
+    outs = [srv.result(i) for i in ids]
     srv.close()
     assert st["completed"] == 3 and st["peak_concurrent"] == 1
-    assert st["peak_bytes"] <= max(sizes)
+    assert one <= st["peak_bytes"] <= 1.5 * one
+    assert all(np.array_equal(o, outs[0]) for o in outs)
 
 
 @pytest.mark.gpu
