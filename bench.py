@@ -237,6 +237,39 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def fp_peaks(device):
+    """FP64 and FP32 (TF32 off) dense GEMM throughput of this GPU through
+    torch/cuBLAS (4096^3, best of 5, CUDA events): the denominators of the
+    FP64 kernels' contraction-flop fraction (MEASURED_PEAKS.json has only
+    the HBM and BF16 figures)."""
+    try:
+        import torch
+
+        torch.backends.cuda.matmul.allow_tf32 = False
+        dev = torch.device("cuda", device)
+        out = {}
+        for name, dt in (("fp64_tflops", torch.float64), ("fp32_tflops", torch.float32)):
+            n = 4096
+            x = torch.randn(n, n, device=dev, dtype=dt)
+            y = torch.randn(n, n, device=dev, dtype=dt)
+            torch.matmul(x, y)
+            best = 1e30
+            for _ in range(5):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                torch.matmul(x, y)
+                e1.record()
+                e1.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            out[name] = 2 * n ** 3 / (best * 1e-3) / 1e12
+            del x, y
+        torch.cuda.empty_cache()
+        out["how"] = "torch.matmul 4096^3 (cuBLAS), best of 5, CUDA events, TF32 off"
+        return out
+    except Exception as ex:  # torch without CUDA, etc.
+        return {"unavailable": str(ex)[:120]}
+
+
 def traffic_per_launch(a):
     """DRAM bytes per stage launch from the committed ncu summary, if any."""
     try:
@@ -519,7 +552,8 @@ def main():
         ms64 = replicas.max_over_ranks(ms64)
         s64.close()
         v64 = replicas.sum_over_ranks(3 * dof * a.steps) / (ms64 * 1e-3)
-        plain = {"value": v64, "ms_per_step": ms64 / a.steps, "speedup": value / v64}
+        plain = {"value": v64, "ms_per_step": ms64 / a.steps, "speedup": value / v64,
+                 "contraction_tflops": 2 * (3 * s.NP + 4 * s.NFP) * dof * 3 * a.steps / (ms64 * 1e-3) / 1e12}
 
     if rank == 0:
         peak, peak_kind = peaks()
@@ -530,6 +564,10 @@ def main():
         nsm_flops = 2 * (3 * s.NP + 4 * s.NFP) * dof  # contraction flops per stage
         cb = cpu_baseline(a, a.cpu_seconds)
         acc = accuracy_check(M, a, q0, dt) if a.l2_steps > 0 else None
+        fpp = fp_peaks(local)
+        if plain and "fp64_tflops" in fpp:
+            plain["fp64_peak_tflops"] = fpp["fp64_tflops"]
+            plain["contraction_frac_of_fp64_peak"] = plain["contraction_tflops"] / fpp["fp64_tflops"]
         bat = batched_2d(M, a.batch_solves, a.batch_steps) if a.batch_solves > 0 else None
         cav = maxwell_cavity(M) if a.cavity else None
         srv = served(M, a.serve_requests, a.serve_lambda, largest=a.serve_largest,
@@ -551,6 +589,7 @@ def main():
                          "contraction_tflops": nsm_flops / avg_launch_s / 1e12},
             "cpu_baseline": cb,
             "plain_f64": plain,
+            "measured_gemm_peaks": fpp,
             "batched": bat,
             "maxwell_cavity": cav,
             "served": srv,

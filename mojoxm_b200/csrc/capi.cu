@@ -805,6 +805,8 @@ int mxm_dg_rk_stage(void* handle, int s, double dt) {
 int mxm_dg_eval_rhs(void* handle, const void* q_dev, void* rhs_dev) {
   API_BEGIN
   if (!q_dev || !rhs_dev || q_dev == rhs_dev) throw mxm::ArgError("q and rhs must be distinct device buffers");
+  // the stage kernels bulk-copy state spans of q: its start must be 16-byte aligned
+  if (reinterpret_cast<uintptr_t>(q_dev) % 16 != 0) throw mxm::ArgError("q must be 16-byte aligned");
   mxm::stage(h, q_dev, q_dev, q_dev, rhs_dev, 0.0, 0.0, 0.0, 0.0, 1);
   CK(cudaStreamSynchronize(h->stream));
   API_END

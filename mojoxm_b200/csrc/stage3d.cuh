@@ -49,7 +49,6 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
   using S = Stage3DShape<P, NC, R>;
   constexpr int NP = S::NP, NFP = S::NFP, K = S::K, BSTR = S::BSTR;
   constexpr int EB = 6 * EC, G = NP / RI, QV = EB * NP * NC;
-  constexpr bool BULK = (6 * NP * NC * sizeof(R)) % 16 == 0;
   static_assert(NP % RI == 0, "row tile must divide NP");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);                       // [2]
@@ -85,9 +84,17 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
     mbar_arrive_expect_tx(&bar[buf], bytes);
     bulk_g2s(sQ + buf * QV, args.q_in + size_t(c0) * 6 * NP * NC, bytes, &bar[buf]);
   };
+  // bulk copy when the tile span starts and ends on 16-byte boundaries
+  // (whole tiles of the usual shapes; a partial last tile may take plain loads)
+  auto tile_bulk = [&](int g) -> bool {
+    const size_t per_cube = size_t(6) * NP * NC * sizeof(R);
+    const size_t start = reinterpret_cast<uintptr_t>(args.q_in) + size_t(g) * EC * per_cube;
+    const size_t bytes = size_t(min(EC, args.ncell - g * EC)) * per_cube;
+    return start % 16 == 0 && bytes % 16 == 0;
+  };
   uint32_t par = 0u;  // bit b: phase parity of tile buffer b
   int buf = 0;
-  if (BULK && tid == 0 && int(blockIdx.x) < ngroups) issue(blockIdx.x, 0);
+  if (tid == 0 && int(blockIdx.x) < ngroups && tile_bulk(blockIdx.x)) issue(blockIdx.x, 0);
 
   const int nwork = tab->n_face_work;
   for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x, buf ^= 1) {
@@ -95,7 +102,7 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
     const int nhere = min(EC, args.ncell - cell0);
     const int ne_here = 6 * nhere;
     R* q = sQ + buf * QV;
-    if (BULK) {
+    if (tile_bulk(grp)) {
       if (!block_wait_bounded(&bar[buf], (par >> buf) & 1u, kWaitLimitNs)) {
         // the copy into this tile is the only one in flight: give it one
         // more bounded wait before the block (and its shared memory) ends
@@ -106,7 +113,7 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
         return;
       }
       par ^= 1u << buf;
-      if (tid == 0 && grp + int(gridDim.x) < ngroups) issue(grp + gridDim.x, buf ^ 1);
+      if (tid == 0 && grp + int(gridDim.x) < ngroups && tile_bulk(grp + gridDim.x)) issue(grp + gridDim.x, buf ^ 1);
     } else {
       const R* src = args.q_in + size_t(cell0) * 6 * NP * NC;
       for (int idx = tid; idx < ne_here * NP * NC; idx += NT) q[idx] = src[idx];

@@ -73,10 +73,19 @@ struct TcShape {
   static constexpr size_t CD_BYTES = size_t(EC) * 12 * 4;  // per cube: 6 neighbour cubes + 6 face modes
   static constexpr size_t HDR = 128;
   static constexpr size_t TAB = (sizeof(KuhnTab3<float>) + 127) / 128 * 128;
+  static constexpr size_t FIXED = HDR + TAB + 2 * A_BYTES + 2 * B_BYTES + FB_BYTES + FN_BYTES + CD_BYTES;
+  // State tile buffers: two (prefetch the next tile during this one) unless
+  // a single buffer lets more blocks share an SM (228 KB of shared memory
+  // per SM, 1 KB reserved per block on sm_100a; at most 4 blocks of 256
+  // threads at the kernel's ~64 registers per thread).
+  static constexpr size_t blocks_for(size_t s) {
+    return size_t(228 * 1024) / (s + 1024) < 4 ? size_t(228 * 1024) / (s + 1024) : 4;
+  }
+  static constexpr int QB = blocks_for(FIXED + Q_BYTES) > blocks_for(FIXED + 2 * Q_BYTES) ? 1 : 2;
   static constexpr size_t OFF_A = HDR + TAB;
   static constexpr size_t OFF_B = OFF_A + 2 * A_BYTES;
   static constexpr size_t OFF_Q = OFF_B + 2 * B_BYTES;
-  static constexpr size_t OFF_F = OFF_Q + 2 * Q_BYTES;
+  static constexpr size_t OFF_F = OFF_Q + QB * Q_BYTES;
   static constexpr size_t OFF_N = OFF_F + FB_BYTES;
   static constexpr size_t OFF_C = OFF_N + FN_BYTES;
   static constexpr size_t SMEM = OFF_C + CD_BYTES;
@@ -188,31 +197,48 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
     tc_fence_after();
     return true;
   };
+  // A tile's state span goes by bulk copy when its start and length are
+  // multiples of 16 bytes (always for whole tiles of the usual shapes; the
+  // last, partial tile of an odd-sized span takes plain loads).
+  auto tile_bulk = [&](int g) -> bool {
+    const size_t per_cube = size_t(6) * NP * NC * 4;
+    const size_t start = reinterpret_cast<uintptr_t>(args.q_in) + size_t(g) * EC * per_cube;
+    const size_t bytes = size_t(min(EC, args.ncell - g * EC)) * per_cube;
+    return start % 16 == 0 && bytes % 16 == 0;
+  };
   int buf = 0;
   bool failed = !block_wait_bounded(&bar[3], 0, kWaitLimitNs);
-  if (S::BULK && int(blockIdx.x) < ngroups && !failed) {
+  if (int(blockIdx.x) < ngroups && !failed && tile_bulk(blockIdx.x)) {
     if (tid == 0) issue(blockIdx.x, 0);
     pend |= 1u;
   }
   const int nwork = tab->n_face_work;
 
-  for (int grp = blockIdx.x; grp < ngroups && !failed; grp += gridDim.x, buf ^= 1) {
+  for (int grp = blockIdx.x; grp < ngroups && !failed; grp += gridDim.x, buf ^= (S::QB - 1)) {
     const int cell0 = grp * EC;
     const int nc_here = min(EC, args.ncell - cell0);
     const int ne_here = 6 * nc_here;
     float* q = sQ + buf * QV;
-    if (S::BULK) {
+    if (tile_bulk(grp)) {
+      if (S::QB == 1 && grp != int(blockIdx.x)) {  // single buffer: load this tile now
+        __syncthreads();                            // every thread is done with the previous tile
+        if (tid == 0) issue(grp, 0);
+        pend |= 1u;
+      }
       if (!block_wait_bounded(&bar[buf], (par >> buf) & 1u, kWaitLimitNs)) {
         failed = true;
         break;
       }
       par ^= 1u << buf;
       pend &= ~(1u << buf);
-      if (grp + int(gridDim.x) < ngroups) {
+      if (S::QB == 2 && grp + int(gridDim.x) < ngroups && tile_bulk(grp + gridDim.x)) {
         if (tid == 0) issue(grp + gridDim.x, buf ^ 1);
         pend |= 1u << (buf ^ 1);
       }
     } else {
+      // plain loads; with one buffer, every thread must be done with the
+      // previous tile first
+      if (S::QB == 1) __syncthreads();
       const float* src = args.q_in + size_t(cell0) * 6 * NP * NC;
       for (int idx = tid; idx < ne_here * NP * NC; idx += NT) q[idx] = src[idx];
       __syncthreads();

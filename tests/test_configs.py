@@ -119,3 +119,30 @@ def test_maxwell_cavity_one_period():
     err64 = rel_l2(out["f64"], q0)
     assert err64 < 5e-3, err64
     assert rel_l2(out["mixed"], out["f64"]) < 1e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f32", "mixed"])
+@pytest.mark.parametrize("P", [2, 3, 4, 5])
+def test_reduced_precision_steps_track_f64(P, prec):
+    """Several SSPRK3 steps of the smooth density wave in FP32 / split-BF16
+    stay within FP32-state accuracy of the FP64 kernels.  5^3 cubes do not
+    fill whole tiles, so the last tile of every launch takes the partial-tile
+    path (plain loads where the bulk copy does not fit)."""
+    n = 5
+    phys = C.euler(M.FLUX_RUSANOV)
+    mesh = M.Mesh(n, n, n)
+    s64 = M.Solver(mesh, phys, P=P, precision="f64")
+    s64.fill_ic(M.IC_SINE_WAVE, [1.0, 0.2, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0])
+    q0 = s64.download_state()
+    h = 1.0 / n
+    dt = 0.1 * h / ((np.sqrt(3.0) + np.sqrt(GAMMA)) * (2 * P + 1))
+    s64.step_n(dt, 12)
+    q64 = s64.download_state()
+    s64.close()
+    s = M.Solver(mesh, phys, P=P, precision=prec)
+    s.upload_state(q0)
+    s.step_n(dt, 12)
+    q = s.download_state().astype(np.float64)
+    s.close()
+    assert rel_l2(q, q64) < 5e-6, rel_l2(q, q64)
