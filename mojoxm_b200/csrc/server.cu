@@ -46,6 +46,10 @@ struct Request {
   int enqueued = 0;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   int ev_head = 0, ev_count = 0;
+  // one full chunk of SSPRK3 steps as a CUDA graph (captured after the first
+  // chunk ran eagerly, replayed for every later full chunk)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
   int state = 0;  // 0 queued, 1 running, 2 done, 3 failed
   std::string err;
   Clock::time_point t_submit, t_admit, t_done;
@@ -111,6 +115,10 @@ void finish(Server* s, Request* r, bool ok) {
   }
   for (auto& ev : r->ev)
     if (ev) cudaEventDestroy(ev);
+  if (r->exec) cudaGraphExecDestroy(r->exec);
+  if (r->graph) cudaGraphDestroy(r->graph);
+  r->exec = nullptr;
+  r->graph = nullptr;
   if (r->h) destroy(r->h);
   r->h = nullptr;
   std::lock_guard<std::mutex> g(s->mu);
@@ -191,7 +199,26 @@ void worker_main(Server* s) {
       if (r->enqueued < r->nsteps && r->ev_count < 2) {
         const int n = std::min(s->chunk, r->nsteps - r->enqueued);
         try {
-          step_n(r->h, r->dt, n);
+          if (r->exec && n == s->chunk) {
+            CK(cudaGraphLaunch(r->exec, r->h->stream));
+          } else {
+            step_n(r->h, r->dt, n);
+            // after the first (eager) chunk, capture a full chunk once if
+            // more full chunks follow: one launch per chunk from then on
+            if (!r->exec && r->nsteps - r->enqueued - n >= 2 * s->chunk) {
+              CK(cudaStreamBeginCapture(r->h->stream, cudaStreamCaptureModeThreadLocal));
+              try {
+                step_n(r->h, r->dt, s->chunk);
+              } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(r->h->stream, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+              }
+              CK(cudaStreamEndCapture(r->h->stream, &r->graph));
+              CK(cudaGraphInstantiate(&r->exec, r->graph, 0));
+            }
+          }
           CK(cudaEventRecord(r->ev[r->ev_head], r->h->stream));
         } catch (std::exception& ex) {
           r->err = ex.what();
