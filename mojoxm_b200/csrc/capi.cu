@@ -547,7 +547,7 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   if (h->ne > (int64_t(1) << 31) / 64) throw ArgError("mesh too large for 32-bit cell indexing");
   h->rbytes = prec == MXM_DG_PREC_F64 ? 8 : 4;
   // split-BF16 tensor-core contraction for the 3D orders it is built for
-  h->use_tc = prec == MXM_DG_PREC_MIXED && m->dim == 3 && P >= 2 && P <= 4;
+  h->use_tc = prec == MXM_DG_PREC_MIXED && m->dim == 3 && P >= 2 && P <= 5;
   h->ref = build_refops(h->dim, P);
   h->NP = h->ref.NP;
   h->NFP = h->ref.NFP;

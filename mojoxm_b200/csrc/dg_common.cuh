@@ -178,7 +178,7 @@ cudaError_t launch_stage3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& ta
 template <class R, class Phys>
 cudaError_t launch_wavespeed3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phys& ph,
                                unsigned long long* out, cudaStream_t st);
-// Tensor-core (split-BF16 tcgen05) 3D stage for FP32 state, P = 2..4;
+// Tensor-core (split-BF16 tcgen05) 3D stage for FP32 state, P = 2..5;
 // `img` is the operator image built by tc_operator_image().
 template <class Phys>
 cudaError_t launch_stage3d_tc(int P, const Stage3DArgs<float>& a, const KuhnTab3<float>& tab, const Phys& ph,

@@ -1,5 +1,5 @@
 // Launch + explicit instantiation of the tensor-core (split-BF16) 3D stage
-// kernel for P = 2..4; other orders use the FP32 SIMT kernel.
+// kernel for P = 2..5; P = 1 uses the FP32 SIMT kernel.
 #include "stage3d_tc.cuh"
 
 namespace mxm {
@@ -30,6 +30,7 @@ cudaError_t launch_stage3d_tc(int P, const Stage3DArgs<float>& a, const KuhnTab3
     case 2: return launch_tc_p<Phys, 2>(a, tab, ph, img, nsm, st);
     case 3: return launch_tc_p<Phys, 3>(a, tab, ph, img, nsm, st);
     case 4: return launch_tc_p<Phys, 4>(a, tab, ph, img, nsm, st);
+    case 5: return launch_tc_p<Phys, 5>(a, tab, ph, img, nsm, st);
   }
   return cudaErrorInvalidValue;
 }

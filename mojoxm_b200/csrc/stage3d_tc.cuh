@@ -362,12 +362,15 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
     }
     if (warp < 4) {  // warp w reads TMEM lanes [32w, 32w+32): rows (c, el)
       const int row = warp * 32 + lane;
-      float v[NN];
 #pragma unroll
-      for (int c0 = 0; c0 < NN; c0 += 16) tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + c0, v + c0);
-      tmem_ld_wait();
+      for (int c0 = 0; c0 < NN; c0 += 16) {  // 16 columns at a time (bounded registers)
+        float v[16];
+        tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + c0, v);
+        tmem_ld_wait();
 #pragma unroll
-      for (int i = 0; i < NP; ++i) sO[row * NPO + i] = v[i];
+        for (int i = 0; i < 16; ++i)
+          if (c0 + i < NP) sO[row * NPO + c0 + i] = v[i];
+      }
     }
     tc_fence_before();
     __syncthreads();

@@ -198,8 +198,6 @@ def test_ssprk3_stage_plans_product(prec):
 @pytest.mark.parametrize("prec", ["f64", "f32", "mixed"])
 @pytest.mark.parametrize("P", [2, 3, 4, 5])
 def test_constant_state_product(P, prec):
-    if prec == "mixed" and P > 4:
-        pytest.skip("split-BF16 tensor-core stage covers P = 2..4")
     nx, ny, nz, L = G["euler3d_const.mesh"]
     s = M.Solver(M.Mesh(nx, ny, nz, L, L, L), C.euler(M.FLUX_HLLEC), P=P, precision=prec)
     q0 = np.broadcast_to(_const_state()[0], s.shape).copy()

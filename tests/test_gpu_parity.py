@@ -146,9 +146,12 @@ def test_reductions_and_wavespeed(oracle_mod):
 # carry ~16 significant bits; the bound leaves room for the cancellation in
 # the derivative/lift sums.
 TOL_MIXED = 5e-4
+# P = 5: the operator entries (and the cancellation in the sums) are larger;
+# the FP32 SIMT kernel shows the same growth on these random states
+TOL_MIXED_P = {2: TOL_MIXED, 3: TOL_MIXED, 4: TOL_MIXED, 5: 2e-3}
 
 
-@pytest.mark.parametrize("P", [2, 3, 4])
+@pytest.mark.parametrize("P", [2, 3, 4, 5])
 @pytest.mark.parametrize("name", ["euler_rusanov", "euler_hllec_fix", "maxwell", "advection", "shallow_water"])
 def test_rhs3d_mixed_vs_f64(oracle_mod, name, P):
     phys = C.PHYSICS_3D[name]()
@@ -158,7 +161,7 @@ def test_rhs3d_mixed_vs_f64(oracle_mod, name, P):
     o64 = oracle_mod.Oracle3D(P, N3, L3, M.physics_dict(phys), bcs=C.BCS_3D["outflow_x_wall_yz"], real="f64")
     err = C.rel_err(s.rhs(qf), o64.rhs(qf))
     print(f"mixed {name} P={P}: rel err vs FP64 oracle {err:.2e}")
-    assert err <= TOL_MIXED
+    assert err <= TOL_MIXED_P[P]
 
 
 def test_mixed_large_mesh_vs_f32(oracle_mod):
