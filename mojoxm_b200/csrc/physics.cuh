@@ -6,10 +6,11 @@
 //   Maxwell       src/maxwell.mojo:48-255
 //   ShallowWater  src/shallow_water.mojo:31-167
 // Each formula keeps the reference's operation order, except that the
-// pointwise Euler flux and the Rusanov flux divide by the density through one
-// reciprocal per state (a few ulp apart from the reference's quotients);
-// comparisons that the reference writes as `not (x > floor)` stay
-// NaN-catching.
+// pointwise Euler flux, the Rusanov flux and the positivity floor divide by
+// the density through one reciprocal per state, and in FP32 take the
+// hardware reciprocal / reciprocal square root (a few ulp apart from the
+// reference's quotients); comparisons that the reference writes as
+// `not (x > floor)` stay NaN-catching.
 #pragma once
 #include "dg_common.cuh"
 
@@ -21,6 +22,19 @@ template <class R>
 __device__ __forceinline__ R rmin(R a, R b) { return a < b ? a : b; }
 template <class R>
 __device__ __forceinline__ R rabs(R a) { return a >= R(0) ? a : -a; }
+
+// Reciprocal and square root of a positive, floored quantity (density,
+// pressure ratio).  FP64 keeps the correctly rounded operations; FP32 uses
+// the hardware approximations (within 2 ulp), which the FP32 state carries
+// anyway.  Arguments are > 0 and finite wherever these are used.
+template <class R>
+__device__ __forceinline__ R pos_rcp(R x) { return R(1) / x; }
+template <>
+__device__ __forceinline__ float pos_rcp<float>(float x) { return __fdividef(1.0f, x); }
+template <class R>
+__device__ __forceinline__ R pos_sqrt(R x) { return sqrt(x); }
+template <>
+__device__ __forceinline__ float pos_sqrt<float>(float x) { return x * rsqrtf(x); }
 
 // ------------------------------------------------------------------ advection
 template <class R>
@@ -71,7 +85,7 @@ struct EulerD {
     return p > p_min ? p : p_min;
   }
   __device__ void flux(const R* q, R* F) const {  // euler.mojo:597-621
-    const R ri = R(1) / rho_f(q);
+    const R ri = pos_rcp(rho_f(q));
     const R u = q[1] * ri, v = q[2] * ri, w = q[3] * ri;
     const R p = p_fi(q, u, v, w);
     F[0] = q[1]; F[1] = q[1] * u + p; F[2] = q[1] * v; F[3] = q[1] * w; F[4] = u * (q[4] + p);
@@ -225,12 +239,12 @@ struct EulerD {
       // frame (n, t, b), anti-rotating the face-frame Rusanov flux gives
       // 0.5 (m_L un_L + m_R un_R + (p_L + p_R) n + cmax (m_L - m_R)) for the
       // momentum, so the rotation pair and the tangent construction drop out.
-      const R rl = rho_f(q_l), rr = rho_f(q_r), il = R(1) / rl, ir = R(1) / rr;
+      const R rl = rho_f(q_l), rr = rho_f(q_r), il = pos_rcp(rl), ir = pos_rcp(rr);
       const R pl = p_fi(q_l, q_l[1] * il, q_l[2] * il, q_l[3] * il);
       const R pr = p_fi(q_r, q_r[1] * ir, q_r[2] * ir, q_r[3] * ir);
       const R mnl = nx * q_l[1] + ny * q_l[2] + nz * q_l[3], mnr = nx * q_r[1] + ny * q_r[2] + nz * q_r[3];
       const R ul = mnl * il, ur = mnr * ir;
-      const R cmax = rmax(rabs(ul) + sqrt(gamma * pl * il), rabs(ur) + sqrt(gamma * pr * ir));
+      const R cmax = rmax(rabs(ul) + pos_sqrt(gamma * pl * il), rabs(ur) + pos_sqrt(gamma * pr * ir));
       const R h = R(0.5), ps = pl + pr;
       flux[0] = h * (mnl + mnr + cmax * (rl - rr));
       flux[1] = h * (q_l[1] * ul + q_r[1] * ur + ps * nx + cmax * (q_l[1] - q_r[1]));
@@ -301,7 +315,7 @@ struct EulerD {
       q[4] = p_min / (gamma - R(1));
       return;
     }
-    R ke = R(0.5) * m2 / rho;
+    R ke = R(0.5) * m2 * pos_rcp(rho);
     R p = (gamma - R(1)) * (q[4] - ke);
     if (!(p > p_min)) q[4] = ke + p_min / (gamma - R(1));
   }

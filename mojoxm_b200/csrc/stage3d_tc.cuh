@@ -170,9 +170,10 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
   bool mma_pending = false;
   // One half of K: make the operand writes visible to the tensor-core
   // (async) proxy, let one thread issue nks K-steps (hi*hi + hi*lo + lo*hi)
-  // against operator K-steps [ka0, ka0 + nks), and wait (bounded) until they
-  // completed; ka0 == 0 starts the accumulator.  All threads call it.
-  auto mma_half = [&](int ka0, int nks) -> bool {
+  // against operator K-steps [ka0, ka0 + nks) (mma_issue), and wait
+  // (bounded) until they completed (mma_wait); ka0 == 0 starts the
+  // accumulator.  All threads call both.
+  auto mma_issue = [&](int ka0, int nks) {
     fence_proxy_async();
     tc_fence_before();
     __syncthreads();
@@ -191,6 +192,8 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
       tc_commit(&bar[2]);
     }
     mma_pending = true;
+  };
+  auto mma_wait = [&]() -> bool {
     if (!block_wait_bounded(&bar[2], mma_parity, kWaitLimitNs)) return false;
     mma_parity ^= 1u;
     mma_pending = false;
@@ -244,20 +247,23 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
       __syncthreads();
     }
     // ---- per-element constant flux Fbar = F(q at node 0); cube-face treatment
-    for (int el = tid; el < ne_here; el += NT) {
+    // one thread per (element, face): each evaluates the element's flux at
+    // node 0 (4x redundant, but the phase's latency is one flux, not four
+    // face products); the lf = 0 thread stores Fbar.  The cube-face
+    // treatment runs at the same time on threads from NT/2 on.
+    for (int w = tid; w < ne_here * 4; w += NT) {
+      const int el = w >> 2, lf = w & 3, t = el % 6;
       float F[3 * NC];
       ph.flux(&q[el * NP * NC], F);
-      const int t = el % 6;
+      if (lf == 0) {
 #pragma unroll
-      for (int k = 0; k < 3 * NC; ++k) sF[el * 3 * NC + k] = F[k];
-#pragma unroll
-      for (int lf = 0; lf < 4; ++lf) {
-        const float nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1], nz = tab->normal[t][lf][2];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) sFn[(el * 4 + lf) * NC + c] = F[c] * nx + F[NC + c] * ny + F[2 * NC + c] * nz;
+        for (int k = 0; k < 3 * NC; ++k) sF[el * 3 * NC + k] = F[k];
       }
+      const float nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1], nz = tab->normal[t][lf][2];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) sFn[w * NC + c] = F[c] * nx + F[NC + c] * ny + F[2 * NC + c] * nz;
     }
-    for (int w = tid; w < nc_here * 6; w += NT) {
+    for (int w = tid - NT / 2; w >= 0 && w < nc_here * 6; w += NT / 2) {
       const int cl = w / 6, dd = w - cl * 6;
       cube_dirs3(cell0 + cl, args.nx, args.ny, args.nz, args.bc, sNb + cl * 6, sMd + cl * 6, dd);
     }
@@ -281,16 +287,13 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
         put(el, d * NP + j, v);
       }
     }
-    // volume half of K: operand columns [0, KV) against operator columns [0, KV)
-    if (!mma_half(0, KV / 16)) {
-      failed = true;
-      break;
-    }
     // ---- face fluxes: (f - Fbar.n) * side*area/(6V) -> operand column lf*NFP + m
-    //      (operator column KV + lf*NFP + m), into the same operand buffer
-    for (int idx = tid; idx < EC * nwork * NFP; idx += NT) {
+    //      (operator column KV + lf*NFP + m), into the same operand buffer.
+    // face_item evaluates work item idx into up to two operand entries
+    // (element, column, NC values); it returns how many (0: nothing to do).
+    auto face_item = [&](int idx, int& e1, int& k1, float* v1, int& e2, int& k2, float* v2) -> int {
       const int cl = idx % EC, rest = idx / EC, m = rest % NFP, wk = rest / NFP;
-      if (cl >= nc_here) continue;
+      if (cl >= nc_here) return 0;
       const int tl = tab->face_work[wk], t = tl >> 2, lf = tl & 3;
       const int el = cl * 6 + t, ax = tab->axis[t][lf];
       const bool own_left = tab->side[t][lf] == 0;
@@ -338,25 +341,49 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
         L[c] = bcf ? qn[c] : (own_left ? o : qn[c]);
         Rr[c] = bcf ? qg[c] : (own_left ? qn[c] : o);
       }
-      float f[NC], v[NC];
+      float f[NC];
       ph.num_flux(L, Rr, nx, ny, nz, f);
       // Fbar . n was taken with the table normal; a one-sided low face flips it
       const float* Fn = &sFn[(el * 4 + lf) * NC];
       const float sg = mode == FACE_BC_LO ? -1.f : 1.f;
 #pragma unroll
-      for (int c = 0; c < NC; ++c) v[c] = scale * (f[c] - sg * Fn[c]);
-      put(el, lf * NFP + m, v);
-      if (ax < 0) {  // the other tet of this inner face: same flux and normal, its own scale and Fbar
-        const int el2 = cl * 6 + nbt, lf2 = tab->nb_lf[t][lf];
-        const float s2 = tab->fscale[nbt][lf2];
-        const float* Fn2 = &sFn[(el2 * 4 + lf2) * NC];
+      for (int c = 0; c < NC; ++c) v1[c] = scale * (f[c] - sg * Fn[c]);
+      e1 = el;
+      k1 = lf * NFP + m;
+      if (ax >= 0) return 1;
+      // the other tet of this inner face: same flux and normal, its own scale and Fbar
+      const int el2 = cl * 6 + nbt, lf2 = tab->nb_lf[t][lf];
+      const float s2 = tab->fscale[nbt][lf2];
+      const float* Fn2 = &sFn[(el2 * 4 + lf2) * NC];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) v[c] = s2 * (f[c] - Fn2[c]);
-        put(el2, lf2 * NFP + tab->nb_m[t][lf][m], v);
-      }
+      for (int c = 0; c < NC; ++c) v2[c] = s2 * (f[c] - Fn2[c]);
+      e2 = el2;
+      k2 = lf2 * NFP + tab->nb_m[t][lf][m];
+      return 2;
+    };
+    const int nface_items = EC * nwork * NFP;
+    // volume half of K: operand columns [0, KV) against operator columns
+    // [0, KV).  While those MMAs run, each thread evaluates its first face
+    // item into registers; the operand columns are overwritten only after
+    // the MMAs completed.
+    mma_issue(0, KV / 16);
+    int e1 = 0, k1 = 0, e2 = 0, k2 = 0;
+    float v1[NC], v2[NC];
+    const int nfirst = tid < nface_items ? face_item(tid, e1, k1, v1, e2, k2, v2) : 0;
+    if (!mma_wait()) {
+      failed = true;
+      break;
+    }
+    if (nfirst >= 1) put(e1, k1, v1);
+    if (nfirst == 2) put(e2, k2, v2);
+    for (int idx = tid + NT; idx < nface_items; idx += NT) {
+      const int n = face_item(idx, e1, k1, v1, e2, k2, v2);
+      if (n >= 1) put(e1, k1, v1);
+      if (n == 2) put(e2, k2, v2);
     }
     // face half of K: operand columns [0, KF) against operator columns [KV, KV + KF)
-    if (!mma_half(KV / 16, KF / 16)) {
+    mma_issue(KV / 16, KF / 16);
+    if (!mma_wait()) {
       failed = true;
       break;
     }
