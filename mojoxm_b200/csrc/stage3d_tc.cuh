@@ -383,6 +383,16 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
     }
     // face half of K: operand columns [0, KF) against operator columns [KV, KV + KF)
     mma_issue(KV / 16, KF / 16);
+    // while the face MMAs run: q_a of this thread's first epilogue node
+    // (global memory when q_a is not the tile's own state)
+    const bool a_in = args.q_a == args.q_in, b_in = args.q_b == args.q_in;
+    const bool pre_a = !args.rhs_only && !a_in && tid < ne_here * NP;
+    float pa[NC];
+    if (pre_a) {
+      const size_t base = (size_t(cell0) * 6 * NP + tid) * NC;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) pa[c] = args.q_a[base + c];
+    }
     if (!mma_wait()) {
       failed = true;
       break;
@@ -402,7 +412,6 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
     tc_fence_before();
     __syncthreads();
     // ---- epilogue per node: source, RK combine, floor, store
-    const bool a_in = args.q_a == args.q_in, b_in = args.q_b == args.q_in;
     for (int idx = tid; idx < ne_here * NP; idx += NT) {
       const int el = idx / NP, i = idx - el * NP;
       const size_t base = (size_t(cell0) * 6 * NP + idx) * NC;
@@ -416,7 +425,7 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
         if (args.rhs_only) {
           out[c] = rhs;
         } else {
-          const float va = a_in ? ql[c] : args.q_a[base + c];
+          const float va = a_in ? ql[c] : (pre_a && idx == tid ? pa[c] : args.q_a[base + c]);
           const float vb = b_in ? ql[c] : args.q_b[base + c];
           out[c] = args.a * va + args.b * vb + args.cdt * rhs;
         }
