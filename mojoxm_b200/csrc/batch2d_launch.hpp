@@ -20,7 +20,7 @@ constexpr int kBatchNT = 256;
 // B-tile row stride of the 2D stage (same padding rule as Stage2DShape)
 inline int bstr2d(int P, int NC, size_t rbytes) {
   const int NP = (P + 1) * (P + 2) / 2, K = 2 * NP + 3 * (P + 1);
-  const int raw = K * NC, mod = rbytes == 8 ? 16 : 32;
+  const int raw = K * (NC | 1), mod = rbytes == 8 ? 16 : 32;
   return raw + ((1 - raw % mod) + mod) % mod;
 }
 

@@ -25,7 +25,8 @@ namespace mxm {
 template <int P, int NC, class R>
 struct Stage2DShape {
   static constexpr int NP = ntri(P), NFP = P + 1, K = 2 * NP + 3 * NFP;
-  static constexpr int BSTR_RAW = K * NC;
+  static constexpr int NS = NC | 1;  // node stride of the B tile (odd: node-parallel accesses miss no bank)
+  static constexpr int BSTR_RAW = K * NS;
   static constexpr int BMOD = sizeof(R) == 8 ? 16 : 32;
   static constexpr int BSTR = BSTR_RAW + ((1 - BSTR_RAW % BMOD) + BMOD) % BMOD;
   // rows of the contraction per thread: a divisor of NP
@@ -34,6 +35,23 @@ struct Stage2DShape {
 };
 
 constexpr uint64_t kWaitLimitNs2 = 2000000000ull;
+
+// One node's NC state values from the shared tile; four-component nodes
+// (16- or 32-byte aligned in the tile) load as vectors, which keeps
+// node-parallel reads free of bank conflicts.
+template <int NC, class R>
+__device__ __forceinline__ void load_node(const R* p, R* v) {
+  if constexpr (NC == 4 && sizeof(R) == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+  } else if constexpr (NC == 4 && sizeof(R) == 8) {
+    const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  } else {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) v[c] = p[c];
+  }
+}
 
 // One tile of whole cells starting at cell0 (ne_here triangles), its state
 // already in shared memory at q: volume and edge fluxes into sB, then
@@ -44,19 +62,20 @@ __device__ __forceinline__ void stage2d_tile(const Stage2DArgs<R>& args, const K
                                              const R* q, R* sB, const R* sA, int cell0, int ne_here) {
   constexpr int NC = Phys::NC;
   using S = Stage2DShape<P, NC, R>;
-  constexpr int NP = S::NP, NFP = S::NFP, K = S::K, BSTR = S::BSTR, RI = S::RI, G = NP / RI;
+  constexpr int NP = S::NP, NFP = S::NFP, K = S::K, BSTR = S::BSTR, NS = S::NS, RI = S::RI, G = NP / RI;
   static_assert(NP % RI == 0, "row tile must divide NP");
   const int tid = threadIdx.x;
   for (int idx = tid; idx < ne_here * NP; idx += NT) {
     const int el = idx / NP, j = idx - el * NP, t = el & 1;
-    R Fx[NC], Fy[NC];
-    ph.flux(&q[(el * NP + j) * NC], Fx, Fy);
+    R Fx[NC], Fy[NC], qv[NC];
+    load_node<NC>(&q[(el * NP + j) * NC], qv);
+    ph.flux(qv, Fx, Fy);
     const R* iJ = tab->invJ[t];
-    R* b = &sB[el * BSTR + j * NC];
+    R* b = &sB[el * BSTR + j * NS];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
       b[c] = iJ[0] * Fx[c] + iJ[1] * Fy[c];
-      b[NP * NC + c] = iJ[2] * Fx[c] + iJ[3] * Fy[c];
+      b[NP * NS + c] = iJ[2] * Fx[c] + iJ[3] * Fy[c];
     }
   }
   for (int idx = tid; idx < ne_here * 3 * NFP; idx += NT) {
@@ -67,7 +86,8 @@ __device__ __forceinline__ void stage2d_tile(const Stage2DArgs<R>& args, const K
     const int ax = tab->axis[t][lf], dir = tab->dir[t][lf];
     int code;
     const int mode = face_mode(ax, dir, ax == 0 ? ci : cj, ax == 0 ? args.nx : args.ny, args.bc, code);
-    const R* qo = &q[(el * NP + tab->own_node[lf][m]) * NC];
+    R qo[NC];
+    load_node<NC>(&q[(el * NP + tab->own_node[lf][m]) * NC], qo);
     R nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1];
     R scale = tab->fscale[t][lf];
     // one face-flux call per face node (the 2D face functions build the
@@ -76,8 +96,7 @@ __device__ __forceinline__ void stage2d_tile(const Stage2DArgs<R>& args, const K
     if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
       const int nbt = tab->nb_t[t][lf], nbn = tab->nb_node[t][lf][m];
       if (ax < 0) {
-#pragma unroll
-        for (int c = 0; c < NC; ++c) qn[c] = q[((cl * 2 + nbt) * NP + nbn) * NC + c];
+        load_node<NC>(&q[((cl * 2 + nbt) * NP + nbn) * NC], qn);
       } else {
         const int ni = wrapi(ci + tab->off[t][lf][0], args.nx), nj = wrapi(cj + tab->off[t][lf][1], args.ny);
         const R* gq = args.q_in + ((size_t(nj) * args.nx + ni) * 2 * NP + size_t(nbt) * NP + nbn) * NC;
@@ -106,7 +125,7 @@ __device__ __forceinline__ void stage2d_tile(const Stage2DArgs<R>& args, const K
     }
     R f[NC];
     ph.face(L, Rr, bcf ? code : int(BC_INTERIOR), nx, ny, f);
-    R* b = &sB[el * BSTR + (2 * NP + fm) * NC];
+    R* b = &sB[el * BSTR + (2 * NP + fm) * NS];
 #pragma unroll
     for (int c = 0; c < NC; ++c) b[c] = scale * f[c];
   }
@@ -127,7 +146,7 @@ __device__ __forceinline__ void stage2d_tile(const Stage2DArgs<R>& args, const K
 #pragma unroll
       for (int r = 0; r < RI; ++r) av[r] = sA[k * NP + i0 + r];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) bv[c] = b[k * NC + c];
+      for (int c = 0; c < NC; ++c) bv[c] = b[k * NS + c];
 #pragma unroll
       for (int r = 0; r < RI; ++r)
 #pragma unroll
@@ -138,7 +157,8 @@ __device__ __forceinline__ void stage2d_tile(const Stage2DArgs<R>& args, const K
     for (int r = 0; r < RI; ++r) {
       const int i = i0 + r;
       const size_t base = (e * NP + i) * NC;
-      const R* ql = &q[(el * NP + i) * NC];
+      R ql[NC];
+      load_node<NC>(&q[(el * NP + i) * NC], ql);
       R src[NC];
       if (Phys::kSource) ph.source(ql, src);
 #pragma unroll
