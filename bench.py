@@ -437,7 +437,7 @@ def served(M, nreq, lam, seed=7, largest=False, slots=8):
             mesh = M.Mesh(n, n, n)
             phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_RUSANOV, False)
             ic, prm, lam_est, h = M.IC_SINE_WAVE, [1, 0.2, 1, 1, 1, 1, 1, 1, 1], np.sqrt(3) + 1.5, 1.0 / n
-            prec = "mixed" if P <= 4 else "f32"
+            prec = "mixed"  # split-BF16 tensor-core stage (P 2..5)
         elif kind == 2:  # dam break
             n = max(4, int(round(np.sqrt(E / 2))))
             mesh = M.Mesh(n, n, 1, 1.0, 1.0, 1.0, bcs=M.BoundaryConditions(1, 1, 1, 1), dim=2)
@@ -450,7 +450,7 @@ def served(M, nreq, lam, seed=7, largest=False, slots=8):
             mesh = M.Mesh(n, n, n)
             phys = M.Maxwell(1.0, *([0.0] * 12))
             ic, prm, lam_est, h = M.IC_PLANE_WAVE, [1.0, 1.0], 1.0, 1.0 / n
-            prec = "f32"
+            prec = "mixed"
         dt = 0.1 * h / (lam_est * (2 * P + 1))
         reqs.append((mesh, phys, P, prec, ic, prm, dt, nsteps, None))
     if largest:
