@@ -202,6 +202,13 @@ int mxm_dg_operator(void* handle, double* host, int64_t* count);
  * Lift [nfaces*NP*NFP] in the reference's face-local order, w [NP]. */
 int mxm_dg_reference_operators(int dim, int P, double* D, double* Lift, double* w);
 
+/* Self-test of the bounded device waits the stage kernels use (no
+ * reference counterpart): a kernel waits on a barrier that nothing
+ * completes, with a `limit_ms` limit (1..2000); it must give up by itself
+ * (*gave_up = 1) after about limit_ms (*waited_ms) and leave the context
+ * usable.  Runs on the calling thread's current device. */
+int mxm_dg_selftest_wait_timeout(double limit_ms, int32_t* gave_up, double* waited_ms);
+
 /* ---- initial conditions on the device ------------------------------------
  * Fill state buffer `which` from node coordinates computed on the device
  * (the role of the reference's IC kernels, e.g. examples/euler_vortex.mojo:

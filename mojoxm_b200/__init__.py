@@ -46,7 +46,7 @@ EXPORTED = [
     "mxm_dg_batch_create", "mxm_dg_batch_destroy", "mxm_dg_batch_add", "mxm_dg_batch_autotune",
     "mxm_dg_batch_tile_cells", "mxm_dg_batch_step", "mxm_dg_batch_time_steps", "mxm_dg_batch_synchronize",
     "mxm_dg_batch_dof_count", "mxm_dg_batch_launches_per_step", "mxm_dg_batch_last_error",
-    "mxm_dg_fill_ic",
+    "mxm_dg_fill_ic", "mxm_dg_selftest_wait_timeout",
     "mxm_dg_server_create", "mxm_dg_server_destroy", "mxm_dg_server_submit", "mxm_dg_server_poll",
     "mxm_dg_server_wait", "mxm_dg_server_stats", "mxm_dg_server_last_error",
 ]
@@ -127,6 +127,7 @@ def lib():
         L.mxm_dg_batch_launches_per_step.argtypes = [vp, i32p]
         L.mxm_dg_batch_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
         L.mxm_dg_fill_ic.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int]
+        L.mxm_dg_selftest_wait_timeout.argtypes = [ctypes.c_double, i32p, dp]
         L.mxm_dg_server_create.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
         L.mxm_dg_server_destroy.argtypes = [vp]
         L.mxm_dg_server_submit.argtypes = [vp, ctypes.POINTER(_MeshDesc), ctypes.POINTER(_PhysDesc), ctypes.c_int,
@@ -609,6 +610,13 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def selftest_wait_timeout(limit_ms=50.0):
+    """(gave_up, waited_ms) of a device wait on a barrier nothing completes."""
+    g, w = ctypes.c_int32(), ctypes.c_double()
+    _check(lib().mxm_dg_selftest_wait_timeout(limit_ms, ctypes.byref(g), ctypes.byref(w)))
+    return g.value, w.value
 
 
 def reference_operators(dim, P):
