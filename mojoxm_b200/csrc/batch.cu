@@ -268,6 +268,8 @@ void build(Batch* b) {
     CK(cudaMalloc(&g.d_counter, 3 * sizeof(int)));
     g.grid = grid_for<R>(b, g, g.smem, g.nitems);
   }
+  for (auto& g : b->groups)
+    if (g.nlitems > 0) CK(prepare_lim2d_batch<R>(g.NC));
   // one SSPRK3 step as a graph
   CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t cap = cudaSuccess;

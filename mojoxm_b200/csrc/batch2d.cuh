@@ -18,6 +18,7 @@
 // src/local_mesh_2d_gpu.mojo:180-198) run over the limited solves' element
 // chunks, one block per chunk.
 #pragma once
+#include "limiter.cuh"
 #include "stage2d.cuh"
 
 namespace mxm {
@@ -212,85 +213,22 @@ __global__ void avg_batch_kernel(LimBatch2DArgs<R> la) {
   }
 }
 
-// One warp per element (8 warps per block, striding over the chunk): theta
-// from component 0 against the face neighbours' means (BC faces do not
-// constrain), applied to every component when theta < 1.
-template <class R, int NP, int NC>
-__device__ __forceinline__ void theta_chunk(const SolveDesc2<R>* sd, int which, int e0, int ne, R* sq) {
-  constexpr int VALS = NP * NC;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  R* mine = sq + warp * VALS;
-  R* qb = sd->q[which];
-  for (int el = warp; el < ne; el += nw) {
-    const int64_t e = e0 + el;
-    for (int idx = lane; idx < VALS; idx += 32) mine[idx] = qb[e * VALS + idx];
-    __syncwarp();
-    const int t = int(e & 1);
-    const int cell = int(e >> 1);
-    const int cj = cell / sd->nx, ci = cell - cj * sd->nx;
-    int64_t nb = e;
-    if (lane < 3) {
-      const int lf = lane;
-      const int ax = sd->tab.axis[t][lf], dir = sd->tab.dir[t][lf];
-      int code;
-      const int mode = face_mode(ax, dir, ax == 0 ? ci : cj, ax == 0 ? sd->nx : sd->ny, sd->bc, code);
-      if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
-        const int ni = wrapi(ci + sd->tab.off[t][lf][0], sd->nx), nj = wrapi(cj + sd->tab.off[t][lf][1], sd->ny);
-        nb = (int64_t(nj) * sd->nx + ni) * 2 + sd->tab.nb_t[t][lf];
-      }
-    }
-    const R own = sd->avg[e * NC];
-    R lo = own, hi = own;
-#pragma unroll
-    for (int lf = 0; lf < 3; ++lf) {
-      const int64_t n = __shfl_sync(0xffffffffu, nb, lf);
-      if (n == e) continue;
-      const R v = sd->avg[n * NC];
-      if (v < lo) lo = v;
-      if (v > hi) hi = v;
-    }
-    R th = R(1);
-    const R tiny = R(1.0e-30);
-    for (int n = lane; n < NP; n += 32) {
-      const R dl = mine[n * NC] - own;
-      const R da = dl >= R(0) ? dl : -dl;
-      if (da <= tiny) continue;
-      R pD = hi - own;
-      if (pD < R(0)) pD = R(0);
-      R nD = own - lo;
-      if (nD < R(0)) nD = R(0);
-      const R D = dl > R(0) ? pD : nD;
-      const R D2 = D * D, d2 = da * da, Dd = D * da;
-      const R al = (D2 + R(2) * Dd + sd->eps2) / (D2 + R(2) * d2 + Dd + sd->eps2);
-      if (al < th) th = al;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const R v = __shfl_xor_sync(0xffffffffu, th, o);
-      th = v < th ? v : th;
-    }
-    if (th < R(1)) {
-      for (int idx = lane; idx < VALS; idx += 32) {
-        const int c = idx % NC;
-        const R bm = sd->avg[e * NC + c];
-        qb[e * VALS + idx] = bm + th * (mine[idx] - bm);
-      }
-    }
-    __syncwarp();
-  }
-}
-
+// Theta + apply of one chunk (blocks of kLim2dBlock threads, chunks of at
+// most kLim2dBlock elements): the single-solve limiter's staged block
+// function on this solve's buffers and table.  Dynamic shared memory sized
+// for P = 5.
 template <class R, int NC>
-__global__ void __launch_bounds__(256) theta_batch_kernel(LimBatch2DArgs<R> la) {
-  __shared__ R sq[8 * 21 * NC];
+__global__ void __launch_bounds__(kLim2dBlock) theta_batch_kernel(LimBatch2DArgs<R> la) {
+  extern __shared__ __align__(16) unsigned char lim_smem[];
   const int4 item = la.items[blockIdx.x];
   const SolveDesc2<R>* sd = &la.solves[item.x];
+  R* q = sd->q[la.which];
   switch (item.w) {
-    case 1: theta_chunk<R, ntri(1), NC>(sd, la.which, item.y, item.z, sq); break;
-    case 2: theta_chunk<R, ntri(2), NC>(sd, la.which, item.y, item.z, sq); break;
-    case 3: theta_chunk<R, ntri(3), NC>(sd, la.which, item.y, item.z, sq); break;
-    case 4: theta_chunk<R, ntri(4), NC>(sd, la.which, item.y, item.z, sq); break;
-    default: theta_chunk<R, ntri(5), NC>(sd, la.which, item.y, item.z, sq); break;
+    case 1: theta2d_block<R, ntri(1), NC>(q, sd->avg, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
+    case 2: theta2d_block<R, ntri(2), NC>(q, sd->avg, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
+    case 3: theta2d_block<R, ntri(3), NC>(q, sd->avg, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
+    case 4: theta2d_block<R, ntri(4), NC>(q, sd->avg, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
+    default: theta2d_block<R, ntri(5), NC>(q, sd->avg, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
   }
 }
 

@@ -69,36 +69,49 @@ cudaError_t launch_stage2d_batch(const mxm_dg_physics_desc& pd, const Batch2DArg
   });
 }
 
+template <class R, int NC>
+cudaError_t lim2d_batch_attr() {
+  return cudaFuncSetAttribute(theta_batch_kernel<R, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(lim2d_smem_bytes<R, ntri(5), NC>()));
+}
+
+// Kernel attributes of the batched limiter (call before any stream capture).
+template <class R>
+cudaError_t prepare_lim2d_batch(int NC) {
+  switch (NC) {
+    case 1: return lim2d_batch_attr<R, 1>();
+    case 3: return lim2d_batch_attr<R, 3>();
+    case 4: return lim2d_batch_attr<R, 4>();
+    case 6: return lim2d_batch_attr<R, 6>();
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class R, int NC>
+cudaError_t lim2d_batch_nc(const LimBatch2DArgs<R>& la, cudaStream_t st) {
+  constexpr size_t smem = lim2d_smem_bytes<R, ntri(5), NC>();
+  avg_batch_kernel<R, NC><<<la.nitems, 256, 0, st>>>(la);
+  theta_batch_kernel<R, NC><<<la.nitems, kLim2dBlock, smem, st>>>(la);
+  return cudaGetLastError();
+}
+
 template <class R>
 cudaError_t launch_lim2d_batch(int NC, const LimBatch2DArgs<R>& la, cudaStream_t st) {
   if (la.nitems <= 0) return cudaSuccess;
   switch (NC) {
-    case 1:
-      avg_batch_kernel<R, 1><<<la.nitems, 256, 0, st>>>(la);
-      theta_batch_kernel<R, 1><<<la.nitems, 256, 0, st>>>(la);
-      break;
-    case 3:
-      avg_batch_kernel<R, 3><<<la.nitems, 256, 0, st>>>(la);
-      theta_batch_kernel<R, 3><<<la.nitems, 256, 0, st>>>(la);
-      break;
-    case 4:
-      avg_batch_kernel<R, 4><<<la.nitems, 256, 0, st>>>(la);
-      theta_batch_kernel<R, 4><<<la.nitems, 256, 0, st>>>(la);
-      break;
-    case 6:
-      avg_batch_kernel<R, 6><<<la.nitems, 256, 0, st>>>(la);
-      theta_batch_kernel<R, 6><<<la.nitems, 256, 0, st>>>(la);
-      break;
-    default:
-      return cudaErrorInvalidValue;
+    case 1: return lim2d_batch_nc<R, 1>(la, st);
+    case 3: return lim2d_batch_nc<R, 3>(la, st);
+    case 4: return lim2d_batch_nc<R, 4>(la, st);
+    case 6: return lim2d_batch_nc<R, 6>(la, st);
   }
-  return cudaGetLastError();
+  return cudaErrorInvalidValue;
 }
 
 #define MXM_INSTANTIATE_BATCH2D(R)                                                                                  \
   template cudaError_t stage2d_batch_blocks_per_sm<R>(const mxm_dg_physics_desc&, size_t, int*);                   \
   template cudaError_t launch_stage2d_batch<R>(const mxm_dg_physics_desc&, const Batch2DArgs<R>&, int, size_t,     \
                                                cudaStream_t);                                                       \
-  template cudaError_t launch_lim2d_batch<R>(int, const LimBatch2DArgs<R>&, cudaStream_t);
+  template cudaError_t launch_lim2d_batch<R>(int, const LimBatch2DArgs<R>&, cudaStream_t);                       \
+  template cudaError_t prepare_lim2d_batch<R>(int);
 
 }  // namespace mxm

@@ -33,5 +33,8 @@ cudaError_t launch_stage2d_batch(const mxm_dg_physics_desc& pd, const Batch2DArg
                                  cudaStream_t st);
 template <class R>
 cudaError_t launch_lim2d_batch(int NC, const LimBatch2DArgs<R>& la, cudaStream_t st);
+// Set the batched limiter's kernel attributes (before any stream capture).
+template <class R>
+cudaError_t prepare_lim2d_batch(int NC);
 
 }  // namespace mxm

@@ -125,6 +125,101 @@ __global__ void __launch_bounds__(32 * EPB) theta_apply_kernel(LimArgs<R> a, Kuh
   }
 }
 
+// 2D theta + apply for one element (component 0 decides theta, faces whose
+// neighbour resolves to the element itself -- BC faces -- do not constrain,
+// theta scales every component's deviation from its cell mean), on the
+// element's values `row` (NP nodes x NC, node stride NC).  Same arithmetic
+// as the reference's 2D kernels; *changed = 1 when the row was rewritten.
+template <class R, int NP, int NC>
+__device__ __forceinline__ void theta2d_elem_row(R* row, const R* avg, int64_t e, const KuhnTab2<R>& tab, int nx,
+                                                 int ny, const int* bc, R eps2, int* changed) {
+  const int t = int(e & 1);
+  const int64_t cell = e >> 1;
+  const int cj = int(cell / nx), ci = int(cell - int64_t(cj) * nx);
+  const R own = avg[e * NC];
+  R lo = own, hi = own;
+#pragma unroll
+  for (int lf = 0; lf < 3; ++lf) {
+    const int ax = tab.axis[t][lf], dir = tab.dir[t][lf];
+    int code;
+    const int mode = face_mode(ax, dir, ax == 0 ? ci : cj, ax == 0 ? nx : ny, bc, code);
+    if (mode != FACE_INTERIOR && mode != FACE_MIXED) continue;
+    const int ni = wrapi(ci + tab.off[t][lf][0], nx), nj = wrapi(cj + tab.off[t][lf][1], ny);
+    const int64_t nb = (int64_t(nj) * nx + ni) * 2 + tab.nb_t[t][lf];
+    if (nb == e) continue;
+    const R v = avg[nb * NC];
+    if (v < lo) lo = v;
+    if (v > hi) hi = v;
+  }
+  R th = R(1);
+  const R tiny = R(1.0e-30);
+#pragma unroll 4
+  for (int n = 0; n < NP; ++n) {
+    const R dl = row[n * NC] - own;
+    const R da = dl >= R(0) ? dl : -dl;
+    if (da <= tiny) continue;
+    R pD = hi - own;
+    if (pD < R(0)) pD = R(0);
+    R nD = own - lo;
+    if (nD < R(0)) nD = R(0);
+    const R D = dl > R(0) ? pD : nD;
+    const R D2 = D * D, d2 = da * da, Dd = D * da;
+    const R al = (D2 + R(2) * Dd + eps2) / (D2 + R(2) * d2 + Dd + eps2);
+    if (al < th) th = al;
+  }
+  *changed = th < R(1) ? 1 : 0;
+  if (!(th < R(1))) return;
+  R bm[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) bm[c] = avg[e * NC + c];
+  for (int n = 0; n < NP; ++n)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) row[n * NC + c] = bm[c] + th * (row[n * NC + c] - bm[c]);
+}
+
+// A block of 128 threads limits 128 consecutive elements: their values are
+// staged into shared memory with coalesced loads (row stride VALS | 1, so
+// the per-element reads hit distinct banks), each thread runs
+// theta2d_elem_row on its element's row, and rows that changed go back with coalesced
+// stores.  kLim2dBlock elements per block; dynamic shared memory
+// lim2d_smem_bytes<R, NP, NC>().
+constexpr int kLim2dBlock = 128;
+template <class R, int NP, int NC>
+constexpr size_t lim2d_smem_bytes() {
+  return size_t(kLim2dBlock) * ((NP * NC) | 1) * sizeof(R) + kLim2dBlock * sizeof(int);
+}
+
+template <class R, int NP, int NC>
+__device__ __forceinline__ void theta2d_block(R* q, const R* avg, int64_t e0, int ne, const KuhnTab2<R>& tab, int nx,
+                                              int ny, const int* bc, R eps2, unsigned char* smem) {
+  constexpr int VALS = NP * NC, VS = VALS | 1;
+  R* sq = reinterpret_cast<R*>(smem);
+  int* changed = reinterpret_cast<int*>(smem + size_t(kLim2dBlock) * VS * sizeof(R));
+  const int tid = threadIdx.x;
+  R* base = q + e0 * VALS;
+  for (int idx = tid; idx < ne * VALS; idx += blockDim.x) {
+    const int el = idx / VALS;
+    sq[el * VS + (idx - el * VALS)] = base[idx];
+  }
+  __syncthreads();
+  if (tid < ne) {  // the element's cell means and its neighbours' from global memory
+    theta2d_elem_row<R, NP, NC>(sq + tid * VS, avg, e0 + tid, tab, nx, ny, bc, eps2, changed + tid);
+  }
+  __syncthreads();
+  for (int idx = tid; idx < ne * VALS; idx += blockDim.x) {
+    const int el = idx / VALS;
+    if (changed[el]) base[idx] = sq[el * VS + (idx - el * VALS)];
+  }
+}
+
+template <class R, int NP, int NC>
+__global__ void __launch_bounds__(kLim2dBlock) theta2d_kernel(LimArgs<R> a, KuhnTab2<R> t2) {
+  extern __shared__ __align__(16) unsigned char lim_smem[];
+  const int64_t e0 = int64_t(blockIdx.x) * kLim2dBlock;
+  const int ne = int(a.ne - e0 < kLim2dBlock ? a.ne - e0 : kLim2dBlock);
+  theta2d_block<R, NP, NC>(a.q, a.avg, e0, ne, t2, a.nx, a.ny, a.bc, a.eps2, lim_smem);
+}
+
 // ---- FP64 reductions: per-block partial sums, then a fixed-order final sum.
 template <class R, int NP, int NC>
 __global__ void reduce_partial_kernel(const R* q, const R* w, int64_t ne, int c, int kind, double* partial) {

@@ -21,8 +21,20 @@ template <class R, int DIM, int NP, int NC>
 cudaError_t lim_np(const LimArgs<R>& a, const KuhnTab3<R>& t3, const KuhnTab2<R>& t2, cudaStream_t st) {
   const int64_t n1 = a.ne * NC;
   cell_avg_kernel<R, NP, NC><<<int((n1 + 255) / 256), 256, 0, st>>>(a);
-  constexpr int EPB = 8;
-  theta_apply_kernel<R, DIM, NP, NC, EPB><<<int((a.ne + EPB - 1) / EPB), 32 * EPB, 0, st>>>(a, t3, t2);
+  if (DIM == 2) {
+    constexpr size_t smem = lim2d_smem_bytes<R, NP, NC>();
+    static bool attr = false;
+    if (!attr) {
+      cudaError_t e = cudaFuncSetAttribute(theta2d_kernel<R, NP, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           int(smem));
+      if (e != cudaSuccess) return e;
+      attr = true;
+    }
+    theta2d_kernel<R, NP, NC><<<int((a.ne + kLim2dBlock - 1) / kLim2dBlock), kLim2dBlock, smem, st>>>(a, t2);
+  } else {
+    constexpr int EPB = 8;
+    theta_apply_kernel<R, DIM, NP, NC, EPB><<<int((a.ne + EPB - 1) / EPB), 32 * EPB, 0, st>>>(a, t3, t2);
+  }
   return cudaGetLastError();
 }
 

@@ -30,7 +30,7 @@ struct Stage2DShape {
   static constexpr int BMOD = sizeof(R) == 8 ? 16 : 32;
   static constexpr int BSTR = BSTR_RAW + ((1 - BSTR_RAW % BMOD) + BMOD) % BMOD;
   // rows of the contraction per thread: a divisor of NP
-  static constexpr int RI = P == 1 ? 3 : (P == 2 ? 2 : (P == 3 ? 5 : (P == 4 ? 5 : 3)));
+  static constexpr int RI = P == 1 ? 1 : (P == 2 ? 2 : (P == 3 ? 2 : (P == 4 ? 3 : 3)));
   static constexpr size_t kPerCell = 2 * sizeof(R) * (2 * size_t(NP) * NC + BSTR);  // 2 q buffers + B rows
 };
 
