@@ -5,11 +5,11 @@
 //   Euler         src/euler.mojo:44-792 (Rusanov/Roe/HLLE/HLLEC, Harten-Hyman fix)
 //   Maxwell       src/maxwell.mojo:48-255
 //   ShallowWater  src/shallow_water.mojo:31-167
-// Each formula keeps the reference's operation order, except that the
-// pointwise Euler flux, the Rusanov flux and the positivity floor divide by
-// the density through one reciprocal per state, and in FP32 take the
-// hardware reciprocal / reciprocal square root (a few ulp apart from the
-// reference's quotients); comparisons that the reference writes as
+// Each formula keeps the reference's operation order, except that divisions
+// by positive quantities (floored densities, square roots of them, the HLLE
+// wave-speed span) are taken as one reciprocal and products, which in FP32
+// use the hardware reciprocal / reciprocal square root (a few ulp apart from
+// the reference's quotients); comparisons that the reference writes as
 // `not (x > floor)` stay NaN-catching.
 #pragma once
 #include "dg_common.cuh"
@@ -75,7 +75,7 @@ struct EulerD {
 
   __device__ __forceinline__ R rho_f(const R* q) const { return q[0] > rho_min ? q[0] : rho_min; }
   __device__ __forceinline__ R p_f(const R* q, R rho) const {
-    R ke = R(0.5) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) / rho;
+    R ke = R(0.5) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) * pos_rcp(rho);
     R p = (gamma - R(1)) * (q[4] - ke);
     return p > p_min ? p : p_min;
   }
@@ -94,15 +94,16 @@ struct EulerD {
   }
   __device__ void flux1d(const R* q, R* f) const {  // euler.mojo:64-72
     R rho = rho_f(q), p = p_f(q, rho);
-    R u = q[1] / rho;
+    R u = q[1] * pos_rcp(rho);
     f[0] = q[1]; f[1] = q[1] * u + p; f[2] = q[2] * u; f[3] = q[3] * u; f[4] = u * (q[4] + p);
   }
   __device__ void roe_avg(const R* ql, const R* qr, R pl, R pr, R& u, R& v, R& w, R& enth, R& a) const {
-    R sl = sqrt(rho_f(ql)), sr = sqrt(rho_f(qr)), s = sl + sr;  // euler.mojo:161-176
-    u = (ql[1] / sl + qr[1] / sr) / s;
-    v = (ql[2] / sl + qr[2] / sr) / s;
-    w = (ql[3] / sl + qr[3] / sr) / s;
-    enth = ((ql[4] + pl) / sl + (qr[4] + pr) / sr) / s;
+    R sl = pos_sqrt(rho_f(ql)), sr = pos_sqrt(rho_f(qr));  // euler.mojo:161-176
+    const R il = pos_rcp(sl), ir = pos_rcp(sr), is = pos_rcp(sl + sr);
+    u = (ql[1] * il + qr[1] * ir) * is;
+    v = (ql[2] * il + qr[2] * ir) * is;
+    w = (ql[3] * il + qr[3] * ir) * is;
+    enth = ((ql[4] + pl) * il + (qr[4] + pr) * ir) * is;
     R aa2 = rmax((gamma - R(1)) * (enth - R(0.5) * (u * u + v * v + w * w)), R(0));
     a = sqrt(aa2);
   }
@@ -190,8 +191,8 @@ struct EulerD {
         wv[2] = a5; wv[5] = a5 * (u + a); wv[8] = a5 * v; wv[11] = a5 * w; wv[14] = a5 * (enth + u * a);
         s[0] = u - a; s[1] = u; s[2] = u + a;
       } else {
-        R rl = rho_f(ql), al = sqrt(gamma * pl / rl), ul = ql[1] / rl;
-        R rr = rho_f(qr), ar = sqrt(gamma * pr / rr), ur = qr[1] / rr;
+        R rl = rho_f(ql), irl = pos_rcp(rl), al = pos_sqrt(gamma * pl * irl), ul = ql[1] * irl;
+        R rr = rho_f(qr), irr = pos_rcp(rr), ar = pos_sqrt(gamma * pr * irr), ur = qr[1] * irr;
         s[0] = rmin(ul - al, u - a);
         s[2] = rmax(ur + ar, u + a);
         if (FLUX == FLUX_HLLE) {  // euler.mojo:364-412
@@ -199,10 +200,10 @@ struct EulerD {
           R fl[5], fr[5];
           flux1d(ql, fl);
           flux1d(qr, fr);
-          R den = s[0] - s[2];
+          const R iden = -pos_rcp(s[2] - s[0]);  // s[2] > s[0]: 1 / (s[0] - s[2])
 #pragma unroll
           for (int m = 0; m < 5; ++m) {
-            R qh = (fr[m] - fl[m] - s[2] * qr[m] + s[0] * ql[m]) / den;
+            R qh = (fr[m] - fl[m] - s[2] * qr[m] + s[0] * ql[m]) * iden;
             wv[m * 3 + 0] = qh - ql[m];
             wv[m * 3 + 1] = R(0);
             wv[m * 3 + 2] = qr[m] - qh;
