@@ -93,7 +93,8 @@ void upload_solves(Batch* b) {
     for (int k = 0; k < 3; ++k) d.q[k] = (R*)h->q[k];
     d.avg = (R*)h->avg;
     d.w = (const R*)h->w;
-    d.dt = R(b->dt[i]);
+    const double cs[3] = {1.0, 0.25, 2.0 / 3.0};
+    for (int s = 0; s < 3; ++s) d.cdt[s] = R(cs[s] * b->dt[i]);
     if (sizeof(R) == 4) {
       const float ef = float(h->lim_eps);  // as the single-solve limiter: eps2 = eps*eps in FP32
       d.eps2 = R(ef * ef);

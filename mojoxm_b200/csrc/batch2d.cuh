@@ -29,7 +29,8 @@ struct SolveDesc2 {
   R* q[3];
   R* avg;
   const R* w;
-  R dt, eps2;
+  R cdt[3];  // c dt of the three SSPRK3 stages, rounded once from FP64
+  R eps2;
   int P, nx, ny, ncell;
   int bc[4];
   int limiter;
@@ -68,16 +69,16 @@ __device__ __forceinline__ bool bulk2d(int P) {
 
 template <class R>
 __device__ __forceinline__ void ssprk3_route(int stage, R* const* q, const R*& qi, const R*& qa, const R*& qb,
-                                             R*& qo, R& a, R& b, R& c) {
+                                             R*& qo, R& b) {
   if (stage == 0) {
     qi = q[0]; qa = q[0]; qb = q[0]; qo = q[1];
-    a = R(1); b = R(0); c = R(1);
+    b = R(0);
   } else if (stage == 1) {
     qi = q[1]; qa = q[0]; qb = q[1]; qo = q[2];
-    a = R(0.75); b = R(0.25); c = R(0.25);
+    b = R(0.25);
   } else {
     qi = q[2]; qa = q[0]; qb = q[2]; qo = q[0];
-    a = R(1.0 / 3.0); b = R(2.0 / 3.0); c = R(2.0 / 3.0);
+    b = R(2.0 / 3.0);
   }
 }
 
@@ -153,12 +154,11 @@ __global__ void __launch_bounds__(NT) stage2d_batch_kernel(Batch2DArgs<R> ba, Ph
       if (nx < ba.nitems && bulk2d<R, NC>(ba.items[nx].w)) issue(nx, buf ^ 1);
     }
     Stage2DArgs<R> args;
-    R a, b, c;
-    ssprk3_route(ba.stage, sd->q, args.q_in, args.q_a, args.q_b, args.q_out, a, b, c);
+    R b;
+    ssprk3_route(ba.stage, sd->q, args.q_in, args.q_a, args.q_b, args.q_out, b);
     args.A = nullptr;
-    args.a = a;
     args.b = b;
-    args.cdt = c * sd->dt;
+    args.cdt = sd->cdt[ba.stage];
     args.nx = sd->nx;
     args.ny = sd->ny;
     args.ncell = sd->ncell;

@@ -152,10 +152,10 @@ void fill_tab2(Handle* h, KuhnTab2<R>& t) {
 
 // ---------------------------------------------------------------- dispatch
 template <class R>
-cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double a, double b,
-                         double c, double dt, int rhs_only) {
+cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double b, double c,
+                         double dt, int rhs_only) {
   const double* p = h->phys.p;
-  const R cdt = R(c) * R(dt);
+  const R cdt = R(c * dt);
   if (h->dim == 3) {
     Stage3DArgs<R> ar;
     ar.q_in = (const R*)qi;
@@ -163,7 +163,6 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
     ar.q_b = (const R*)qb;
     ar.q_out = (R*)qo;
     ar.A = (const R*)h->A;
-    ar.a = R(a);
     ar.b = R(b);
     ar.cdt = cdt;
     ar.nx = h->nx;
@@ -225,7 +224,6 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
   ar.q_b = (const R*)qb;
   ar.q_out = (R*)qo;
   ar.A = (const R*)h->A;
-  ar.a = R(a);
   ar.b = R(b);
   ar.cdt = cdt;
   ar.nx = h->nx;
@@ -349,10 +347,11 @@ cudaError_t wavespeed_launch(Handle* h, const void* qi, unsigned long long* out)
   return cudaErrorInvalidValue;
 }
 
-void stage(Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double a, double b, double c, double dt,
+// One Shu-Osher stage q_out = (1 - b) q_a + b q_b + c dt L(q_in).
+void stage(Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double b, double c, double dt,
            int rhs_only) {
-  cudaError_t e = h->rbytes == 8 ? stage_launch<double>(h, qi, qa, qb, qo, a, b, c, dt, rhs_only)
-                                 : stage_launch<float>(h, qi, qa, qb, qo, a, b, c, dt, rhs_only);
+  cudaError_t e = h->rbytes == 8 ? stage_launch<double>(h, qi, qa, qb, qo, b, c, dt, rhs_only)
+                                 : stage_launch<float>(h, qi, qa, qb, qo, b, c, dt, rhs_only);
   if (e != cudaSuccess) throw CudaError(e, "stage kernel launch");
 }
 
@@ -386,9 +385,9 @@ void limit_buf(Handle* h, void* qv) {
 // Shu-Osher stage s of SSPRK3 (solver.mojo:1071-1092; ssprk3.mojo:56-78).
 void rk_stage(Handle* h, int s, double dt) {
   void *q0 = h->q[0], *q1 = h->q[1], *q2 = h->q[2];
-  if (s == 0) stage(h, q0, q0, q0, q1, 1.0, 0.0, 1.0, dt, 0);
-  else if (s == 1) stage(h, q1, q0, q1, q2, 0.75, 0.25, 0.25, dt, 0);
-  else stage(h, q2, q0, q2, q0, 1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0, dt, 0);
+  if (s == 0) stage(h, q0, q0, q0, q1, 0.0, 1.0, dt, 0);
+  else if (s == 1) stage(h, q1, q0, q1, q2, 0.25, 0.25, dt, 0);
+  else stage(h, q2, q0, q2, q0, 2.0 / 3.0, 2.0 / 3.0, dt, 0);
   if (h->lim_on) limit_buf(h, s == 0 ? q1 : (s == 1 ? q2 : q0));
 }
 
@@ -807,7 +806,7 @@ int mxm_dg_eval_rhs(void* handle, const void* q_dev, void* rhs_dev) {
   if (!q_dev || !rhs_dev || q_dev == rhs_dev) throw mxm::ArgError("q and rhs must be distinct device buffers");
   // the stage kernels bulk-copy state spans of q: its start must be 16-byte aligned
   if (reinterpret_cast<uintptr_t>(q_dev) % 16 != 0) throw mxm::ArgError("q must be 16-byte aligned");
-  mxm::stage(h, q_dev, q_dev, q_dev, rhs_dev, 0.0, 0.0, 0.0, 0.0, 1);
+  mxm::stage(h, q_dev, q_dev, q_dev, rhs_dev, 0.0, 0.0, 0.0, 1);
   CK(cudaStreamSynchronize(h->stream));
   API_END
 }

@@ -137,7 +137,11 @@ struct Stage3DArgs {
   const R* q_b;
   R* q_out;
   const R* A;  // [K][NP] shared operator [D_r|D_s|D_t|-Lift_0..3], k-major
-  R a, b, cdt;
+  // q_out = q_a + b (q_b - q_a) + cdt rhs: the weights of q_a and q_b sum to
+  // one exactly in any precision (in FP32, a = 1/3 and b = 2/3 rounded
+  // separately sum to 1 + 3e-8, which scales the state by that much every
+  // step); cdt = c dt is rounded once from FP64.
+  R b, cdt;
   int nx, ny, nz;
   int ncell;
   int bc[6];
@@ -152,7 +156,11 @@ struct Stage2DArgs {
   const R* q_b;
   R* q_out;
   const R* A;  // [K][NP] shared operator [D_r|D_s|-Lift_0..2], k-major
-  R a, b, cdt;
+  // q_out = q_a + b (q_b - q_a) + cdt rhs: the weights of q_a and q_b sum to
+  // one exactly in any precision (in FP32, a = 1/3 and b = 2/3 rounded
+  // separately sum to 1 + 3e-8, which scales the state by that much every
+  // step); cdt = c dt is rounded once from FP64.
+  R b, cdt;
   int nx, ny;
   int ncell;
   int bc[4];

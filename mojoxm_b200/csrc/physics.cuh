@@ -41,6 +41,7 @@ template <class R>
 struct AdvectionD {
   static constexpr int NC = 1;
   static constexpr bool kSource = false, kLimit = false;
+  static constexpr bool kLightFlux = true;
   R vx, vy, vz, inflow_q;
   __device__ void flux(const R* q, R* F) const {  // F[d*NC + c]
     F[0] = vx * q[0];
@@ -69,6 +70,9 @@ template <class R, int FLUX>
 struct EulerD {
   static constexpr int NC = 5;
   static constexpr bool kSource = true, kLimit = true;
+  // register-light numerical flux (the tensor-core stage kernel may then
+  // run as many blocks per SM as fit in shared memory, up to three)
+  static constexpr bool kLightFlux = FLUX == FLUX_RUSANOV;
   R gamma, rho_min, p_min, gx, gy, gz;
   R inflow[5];
   int entropy_fix;
@@ -327,6 +331,7 @@ template <class R>
 struct MaxwellD {
   static constexpr int NC = 6;
   static constexpr bool kSource = true, kLimit = false;
+  static constexpr bool kLightFlux = true;
   R c, J[3], M[3], inflow[6];
   __device__ void flux(const R* q, R* F) const {  // maxwell.mojo:127-156
     R c2 = c * c;
@@ -375,6 +380,7 @@ template <class R>
 struct ShallowWaterD {
   static constexpr int NC = 3;
   static constexpr bool kSource = false, kLimit = false;
+  static constexpr bool kLightFlux = true;
   R g, h_min, inflow[3];
   __device__ void flux(const R* q, R* F) const {  // shallow_water.mojo:63-86
     R h = q[0] > h_min ? q[0] : h_min;

@@ -166,7 +166,7 @@ __device__ __forceinline__ void stage2d_tile(const Stage2DArgs<R>& args, const K
         const R rhs = Phys::kSource ? acc[r][c] + src[c] : acc[r][c];
         const R va = a_in ? ql[c] : args.q_a[base + c];
         const R vb = b_in ? ql[c] : args.q_b[base + c];
-        args.q_out[base + c] = args.rhs_only ? rhs : args.a * va + args.b * vb + args.cdt * rhs;
+        args.q_out[base + c] = args.rhs_only ? rhs : va + args.b * (vb - va) + args.cdt * rhs;
       }
     }
   }

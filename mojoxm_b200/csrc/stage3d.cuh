@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
           } else {
             const R va = a_in ? ql[c] : args.q_a[base + c];
             const R vb = b_in ? ql[c] : args.q_b[base + c];
-            out[c] = args.a * va + args.b * vb + args.cdt * rhs;
+            out[c] = va + args.b * (vb - va) + args.cdt * rhs;
           }
         }
         if (Phys::kLimit && !args.rhs_only) ph.limit(out);

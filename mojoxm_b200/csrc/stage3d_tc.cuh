@@ -93,8 +93,18 @@ struct TcShape {
   static_assert(O_BYTES <= 2 * B_BYTES, "staging tile must fit the operand buffer");
 };
 
+// Blocks per SM the register allocation must allow: what fits in shared
+// memory, at most three for register-light fluxes and two for the Roe /
+// HLLE / HLLEC solvers (capping those at three blocks' registers spills).
+template <class Phys, int P>
+__host__ __device__ constexpr int tc_min_blocks() {
+  return int(TcShape<P, Phys::NC>::blocks_for(TcShape<P, Phys::NC>::SMEM)) < (Phys::kLightFlux ? 3 : 2)
+             ? int(TcShape<P, Phys::NC>::blocks_for(TcShape<P, Phys::NC>::SMEM))
+             : (Phys::kLightFlux ? 3 : 2);
+}
+
 template <class Phys, int P, int NT>
-__global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args, KuhnTab3<float> tabp, Phys ph,
+__global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kernel(Stage3DArgs<float> args, KuhnTab3<float> tabp, Phys ph,
                                                          const unsigned char* __restrict__ a_image) {
   constexpr int NC = Phys::NC;
   using S = TcShape<P, NC>;
@@ -216,13 +226,48 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
     pend |= 1u;
   }
   const int nwork = tab->n_face_work;
+  // ---- per-element constant flux Fbar = F(q at node 0) and the cube-face
+  // treatment of tile g (state tile qt): one thread per (element, face); each
+  // evaluates the element's flux at node 0 (4x redundant, but the phase's
+  // latency is one flux, not four face products); the lf = 0 thread stores
+  // Fbar.  The cube-face treatment runs at the same time on threads from
+  // NT/2 on.
+  auto fbar_phase = [&](int g, const float* qt) {
+    const int ncg = min(EC, args.ncell - g * EC);
+    for (int w = tid; w < ncg * 24; w += NT) {
+      const int el = w >> 2, lf = w & 3, t = el % 6;
+      float F[3 * NC];
+      ph.flux(&qt[el * NP * NC], F);
+      if (lf == 0) {
+#pragma unroll
+        for (int k = 0; k < 3 * NC; ++k) sF[el * 3 * NC + k] = F[k];
+      }
+      const float nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1], nz = tab->normal[t][lf][2];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) sFn[w * NC + c] = F[c] * nx + F[NC + c] * ny + F[2 * NC + c] * nz;
+    }
+    for (int w = tid - NT / 2; w >= 0 && w < ncg * 6; w += NT / 2) {
+      const int cl = w / 6, dd = w - cl * 6;
+      cube_dirs3(g * EC + cl, args.nx, args.ny, args.nz, args.bc, sNb + cl * 6, sMd + cl * 6, dd);
+    }
+  };
+  // With two state buffers the next tile's copy lands while this tile is
+  // computed; its Fbar phase then runs while this tile's face MMAs do
+  // (fb_ready: sF, sFn, sNb, sMd and the tile wait are done for grp).
+  bool fb_ready = false;
 
   for (int grp = blockIdx.x; grp < ngroups && !failed; grp += gridDim.x, buf ^= (S::QB - 1)) {
     const int cell0 = grp * EC;
     const int nc_here = min(EC, args.ncell - cell0);
     const int ne_here = 6 * nc_here;
     float* q = sQ + buf * QV;
-    if (tile_bulk(grp)) {
+    if (fb_ready) {
+      __syncthreads();  // every thread is done with the previous tile (its buffer, sO)
+      if (S::QB == 2 && grp + int(gridDim.x) < ngroups && tile_bulk(grp + gridDim.x)) {
+        if (tid == 0) issue(grp + gridDim.x, buf ^ 1);
+        pend |= 1u << (buf ^ 1);
+      }
+    } else if (tile_bulk(grp)) {
       if (S::QB == 1 && grp != int(blockIdx.x)) {  // single buffer: load this tile now
         __syncthreads();                            // every thread is done with the previous tile
         if (tid == 0) issue(grp, 0);
@@ -246,28 +291,10 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
       for (int idx = tid; idx < ne_here * NP * NC; idx += NT) q[idx] = src[idx];
       __syncthreads();
     }
-    // ---- per-element constant flux Fbar = F(q at node 0); cube-face treatment
-    // one thread per (element, face): each evaluates the element's flux at
-    // node 0 (4x redundant, but the phase's latency is one flux, not four
-    // face products); the lf = 0 thread stores Fbar.  The cube-face
-    // treatment runs at the same time on threads from NT/2 on.
-    for (int w = tid; w < ne_here * 4; w += NT) {
-      const int el = w >> 2, lf = w & 3, t = el % 6;
-      float F[3 * NC];
-      ph.flux(&q[el * NP * NC], F);
-      if (lf == 0) {
-#pragma unroll
-        for (int k = 0; k < 3 * NC; ++k) sF[el * 3 * NC + k] = F[k];
-      }
-      const float nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1], nz = tab->normal[t][lf][2];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) sFn[w * NC + c] = F[c] * nx + F[NC + c] * ny + F[2 * NC + c] * nz;
+    if (!fb_ready) {
+      fbar_phase(grp, q);
+      __syncthreads();
     }
-    for (int w = tid - NT / 2; w >= 0 && w < nc_here * 6; w += NT / 2) {
-      const int cl = w / 6, dd = w - cl * 6;
-      cube_dirs3(cell0 + cl, args.nx, args.ny, args.nz, args.bc, sNb + cl * 6, sMd + cl * 6, dd);
-    }
-    __syncthreads();
     // ---- volume fluxes (F - Fbar) in reference coordinates -> k = d*NP + j
     for (int idx = tid; idx < EBP * NP; idx += NT) {
       const int el8 = idx & 7, rest = idx >> 3, j = rest % NP, el = (rest / NP) * 8 + el8;
@@ -383,8 +410,24 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
     }
     // face half of K: operand columns [0, KF) against operator columns [KV, KV + KF)
     mma_issue(KV / 16, KF / 16);
-    // while the face MMAs run: q_a of this thread's first epilogue node
-    // (global memory when q_a is not the tile's own state)
+    // while the face MMAs run: the next tile's wait and Fbar phase (its
+    // copy was issued a whole tile earlier) ...
+    fb_ready = false;
+    if (S::QB == 2) {
+      const int nxt = grp + int(gridDim.x);
+      if (nxt < ngroups && tile_bulk(nxt)) {
+        if (!block_wait_bounded(&bar[buf ^ 1], (par >> (buf ^ 1)) & 1u, kWaitLimitNs)) {
+          failed = true;
+          break;
+        }
+        par ^= 1u << (buf ^ 1);
+        pend &= ~(1u << (buf ^ 1));
+        fbar_phase(nxt, sQ + (buf ^ 1) * QV);
+        fb_ready = true;
+      }
+    }
+    // ... and q_a of this thread's first epilogue node (global memory when
+    // q_a is not the tile's own state)
     const bool a_in = args.q_a == args.q_in, b_in = args.q_b == args.q_in;
     const bool pre_a = !args.rhs_only && !a_in && tid < ne_here * NP;
     float pa[NC];
@@ -397,12 +440,13 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
       failed = true;
       break;
     }
-    if (warp < 4) {  // warp w reads TMEM lanes [32w, 32w+32): rows (c, el)
-      const int row = warp * 32 + lane;
+    {  // warp w reads TMEM lanes [32 (w % 4), +32) (rows (c, el)), columns
+       // [16 (w / 4), +16) of every 32 (16 at a time: bounded registers)
+      const int row = (warp & 3) * 32 + lane;
 #pragma unroll
-      for (int c0 = 0; c0 < NN; c0 += 16) {  // 16 columns at a time (bounded registers)
+      for (int c0 = (warp >> 2) * 16; c0 < NN; c0 += 32) {
         float v[16];
-        tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + c0, v);
+        tmem_ld16(tmem + (uint32_t((warp & 3) * 32) << 16) + c0, v);
         tmem_ld_wait();
 #pragma unroll
         for (int i = 0; i < 16; ++i)
@@ -427,7 +471,7 @@ __global__ void __launch_bounds__(NT) stage3d_tc_kernel(Stage3DArgs<float> args,
         } else {
           const float va = a_in ? ql[c] : (pre_a && idx == tid ? pa[c] : args.q_a[base + c]);
           const float vb = b_in ? ql[c] : args.q_b[base + c];
-          out[c] = args.a * va + args.b * vb + args.cdt * rhs;
+          out[c] = va + args.b * (vb - va) + args.cdt * rhs;
         }
       }
       if (Phys::kLimit && !args.rhs_only) ph.limit(out);
