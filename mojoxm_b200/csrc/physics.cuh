@@ -307,22 +307,27 @@ struct EulerD {
     s[3] = q[0] * gz;
     s[4] = q[1] * gx + q[2] * gy + q[3] * gz;
   }
+  // Positivity floor after the RK write.  The pressure recovery
+  // p = (gamma - 1)(E - |m|^2 / 2 rho) runs in FP64 for every state type:
+  // near vacuum E and the kinetic energy cancel, and an FP32 difference
+  // would decide the floor on rounding noise.
   __device__ void limit(R* q) const {  // euler.mojo:758-792
-    R rho = q[0];
-    if (!(rho > rho_min)) {
+    const double rho = double(q[0]), g1 = double(gamma) - 1.0, pm = double(p_min);
+    if (!(rho > double(rho_min))) {
       q[0] = rho_min; q[1] = R(0); q[2] = R(0); q[3] = R(0);
-      q[4] = p_min / (gamma - R(1));
+      q[4] = R(pm / g1);
       return;
     }
-    R m2 = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
-    if (!(m2 >= R(0))) {
+    const double m1 = double(q[1]), m2_ = double(q[2]), m3 = double(q[3]);
+    const double m2 = m1 * m1 + m2_ * m2_ + m3 * m3;
+    if (!(m2 >= 0.0)) {
       q[1] = R(0); q[2] = R(0); q[3] = R(0);
-      q[4] = p_min / (gamma - R(1));
+      q[4] = R(pm / g1);
       return;
     }
-    R ke = R(0.5) * m2 * pos_rcp(rho);
-    R p = (gamma - R(1)) * (q[4] - ke);
-    if (!(p > p_min)) q[4] = ke + p_min / (gamma - R(1));
+    const double ke = 0.5 * m2 * (1.0 / rho);
+    const double p = g1 * (double(q[4]) - ke);
+    if (!(p > pm)) q[4] = R(ke + pm / g1);
   }
 };
 

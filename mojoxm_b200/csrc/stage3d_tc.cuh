@@ -296,22 +296,59 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
       __syncthreads();
     }
     // ---- volume fluxes (F - Fbar) in reference coordinates -> k = d*NP + j
-    for (int idx = tid; idx < EBP * NP; idx += NT) {
-      const int el8 = idx & 7, rest = idx >> 3, j = rest % NP, el = (rest / NP) * 8 + el8;
-      if (el >= ne_here) continue;
-      const int t = el % 6;
-      float F[3 * NC];
-      ph.flux(&q[(el * NP + j) * NC], F);
-      const float* Fb = &sF[el * 3 * NC];
+    // Up to five components, each thread takes two neighbouring elements
+    // (rows el, el + 1) at one node: their operand values share a 4-byte
+    // word of the MN-major tile, so each hi / lo pair is one packed
+    // conversion and one 32-bit store.  Six components (36 flux values per
+    // pair) take one element per thread.
+    if constexpr (NC > 5) {
+      for (int idx = tid; idx < EBP * NP; idx += NT) {
+        const int el8 = idx & 7, rest = idx >> 3, j = rest % NP, el = (rest / NP) * 8 + el8;
+        if (el >= ne_here) continue;
+        const int t = el % 6;
+        float F[3 * NC];
+        ph.flux(&q[(el * NP + j) * NC], F);
+        const float* Fb = &sF[el * 3 * NC];
 #pragma unroll
-      for (int k = 0; k < 3 * NC; ++k) F[k] -= Fb[k];
-      const float* iJ = tab->invJ[t];
+        for (int k = 0; k < 3 * NC; ++k) F[k] -= Fb[k];
+        const float* iJ = tab->invJ[t];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          float v[NC];
+#pragma unroll
+          for (int c = 0; c < NC; ++c)
+            v[c] = iJ[d * 3 + 0] * F[c] + iJ[d * 3 + 1] * F[NC + c] + iJ[d * 3 + 2] * F[2 * NC + c];
+          put(el, d * NP + j, v);
+        }
+      }
+    } else
+    for (int idx = tid; idx < (EBP / 2) * NP; idx += NT) {
+      const int e4 = idx & 3, rest = idx >> 2, j = rest % NP, el = (rest / NP) * 8 + 2 * e4;
+      if (el >= ne_here) continue;  // ne_here is even: el + 1 is in the tile too
+      const int t0 = el % 6, t1 = t0 + 1;  // el even: t0 in {0, 2, 4}
+      float Fa[3 * NC], Fb[3 * NC];
+      ph.flux(&q[(el * NP + j) * NC], Fa);
+      ph.flux(&q[((el + 1) * NP + j) * NC], Fb);
+      const float* Fba = &sF[el * 3 * NC];
+#pragma unroll
+      for (int k = 0; k < 3 * NC; ++k) {
+        Fa[k] -= Fba[k];
+        Fb[k] -= Fba[3 * NC + k];
+      }
+      const float* iJa = tab->invJ[t0];
+      const float* iJb = tab->invJ[t1];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        float v[NC];
+        const uint32_t off = umma_mn_offset(el, d * NP + j, M);
 #pragma unroll
-        for (int c = 0; c < NC; ++c) v[c] = iJ[d * 3 + 0] * F[c] + iJ[d * 3 + 1] * F[NC + c] + iJ[d * 3 + 2] * F[2 * NC + c];
-        put(el, d * NP + j, v);
+        for (int c = 0; c < NC; ++c) {
+          const float va = iJa[d * 3 + 0] * Fa[c] + iJa[d * 3 + 1] * Fa[NC + c] + iJa[d * 3 + 2] * Fa[2 * NC + c];
+          const float vb = iJb[d * 3 + 0] * Fb[c] + iJb[d * 3 + 1] * Fb[NC + c] + iJb[d * 3 + 2] * Fb[2 * NC + c];
+          uint32_t h, l;
+          split_bf16x2(va, vb, h, l);
+          *reinterpret_cast<uint32_t*>(sBhi + off + c * CSTRIDE) = h;
+          *reinterpret_cast<uint32_t*>(sBlo + off + c * CSTRIDE) = l;
+        }
       }
     }
     // ---- face fluxes: (f - Fbar.n) * side*area/(6V) -> operand column lf*NFP + m
