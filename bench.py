@@ -318,34 +318,40 @@ def run_reference(a, rank, world):
     print(json.dumps(line))
 
 
-def batched_2d(M, nsolves, steps, seed=2024):
+def batched_2d(M, nsolves, steps, seed=2024, precision="f32", loop=True, ref=None, keep=False):
     """Batched 2D Euler on triangles: `nsolves` independent solves, n x n x 2
     tris with n ~ U{16,32,64,128,256}, P ~ U{1..5}, ICs a seeded mix of
     isentropic vortices (beta ~ U[2,6], periodic [0,10]^2) and tanh-smoothed
     Sod tubes (left/right rho, p ~ U[0.1,1], width 8h, outflow x / periodic
-    y), HLLE flux, BJ limiter eps 0.1, FP32, dt = 0.3 h / ((2P+1) max|lambda|)
-    per solve from the device wave-speed reduction."""
+    y), HLLE flux, BJ limiter eps 0.1, FP32 (or FP64: the plain comparison),
+    dt = 0.3 h / ((2P+1) max|lambda|) per solve from the device wave-speed
+    reduction.  `ref`: a kept FP64 run of the same seed; its time steps are
+    used and the states are compared after the timed steps (relative L2 per
+    IC kind).  `keep`: return the solvers open, for use as `ref`."""
     rng = np.random.default_rng(seed)
     batch = M.Batch()
-    solvers = []
+    solvers, kinds, dts = [], [], []
     for k in range(nsolves):
         n = int(rng.choice([16, 32, 64, 128, 256]))
         P = int(rng.integers(1, 6))
         phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_HLLE, False)
         if rng.random() < 0.5:
             mesh = M.Mesh(n, n, 1, 10.0, 10.0, 1.0, dim=2)
-            s = M.Solver(mesh, phys, P=P, precision="f32")
+            s = M.Solver(mesh, phys, P=P, precision=precision)
             s.fill_ic(M.IC_VORTEX, [rng.uniform(2, 6), 5.0, 5.0, 1.0, 1.0, 0.0, 1.0])
             h = 10.0 / n
+            kinds.append("vortex")
         else:
             mesh = M.Mesh(n, n, 1, 1.0, 1.0, 1.0, bcs=M.BoundaryConditions(2, 2, 0, 0), dim=2)
-            s = M.Solver(mesh, phys, P=P, precision="f32")
+            s = M.Solver(mesh, phys, P=P, precision=precision)
             rl, pl, rr, pr = rng.uniform(0.1, 1.0, 4)
             s.fill_ic(M.IC_SOD, [rl, pl, rr, pr, 0.5, 8.0 / n])
             h = 1.0 / n
+            kinds.append("sod")
         s.enable_cell_limiter(True, 0.1)
-        lam = s.max_wavespeed()
-        batch.add(s, 0.3 * h / ((2 * P + 1) * lam))
+        dt = ref["dts"][k] if ref else 0.3 * h / ((2 * P + 1) * s.max_wavespeed())
+        batch.add(s, dt)
+        dts.append(dt)
         solvers.append(s)
     dof = batch.dof_count()
     t0 = time.perf_counter()
@@ -358,26 +364,41 @@ def batched_2d(M, nsolves, steps, seed=2024):
     for i, s in enumerate(solvers):
         tiles.setdefault(s.P, batch.tile_cells(i))
     launches = batch.launches_per_step()
-    # the same solves advanced one at a time through their own handles
-    # (per-solve launches on per-solve streams), 2 steps, wall clock
-    for s in solvers:
-        s.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(2):
-        for i, s in enumerate(solvers):
-            s.step_n(batch.dts[i], 1)
-    for s in solvers:
-        s.synchronize()
-    loop_s = (time.perf_counter() - t0) / 2
     value = 3 * dof * steps / (ms * 1e-3)
-    out = {"workload": f"{nsolves} independent 2D Euler solves (HLLE, BJ limiter, FP32), n in {{16..256}}, P in 1..5",
+    out = {"workload": f"{nsolves} independent 2D Euler solves (HLLE, BJ limiter, {precision.upper()}), "
+                       "n in {16..256}, P in 1..5",
            "solves": nsolves, "dof": dof, "value": value, "unit": UNIT, "ms_per_step": ms / steps,
            "launches_per_step": launches, "tile_cells_per_P": {str(k): v for k, v in sorted(tiles.items())},
-           "setup_s": setup_s, "per_solve_loop_value": 3 * dof / loop_s,
-           "speedup_vs_per_solve_loop": value / (3 * dof / loop_s), "seed": seed}
+           "setup_s": setup_s, "seed": seed}
+    if ref:
+        num, den = {}, {}
+        for i, s in enumerate(solvers):
+            a = s.download_state().astype(np.float64)
+            b = ref["solvers"][i].download_state()
+            num[kinds[i]] = num.get(kinds[i], 0.0) + float(((a - b) ** 2).sum())
+            den[kinds[i]] = den.get(kinds[i], 0.0) + float((b ** 2).sum())
+        out["rel_l2_vs_f64"] = {k: float(np.sqrt(num[k] / den[k])) for k in sorted(num)}
+        out["rel_l2_vs_f64_steps"] = 3 + steps
+    if loop:
+        # the same solves advanced one at a time through their own handles
+        # (per-solve launches on per-solve streams), 2 steps, wall clock
+        for s in solvers:
+            s.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(2):
+            for i, s in enumerate(solvers):
+                s.step_n(batch.dts[i], 1)
+        for s in solvers:
+            s.synchronize()
+        loop_s = (time.perf_counter() - t0) / 2
+        out["per_solve_loop_value"] = 3 * dof / loop_s
+        out["speedup_vs_per_solve_loop"] = value / (3 * dof / loop_s)
     batch.close()
-    for s in solvers:
-        s.close()
+    if keep:
+        out["_keep"] = {"solvers": solvers, "dts": dts}
+    else:
+        for s in solvers:
+            s.close()
     return out
 
 
@@ -413,12 +434,13 @@ def maxwell_cavity(M, n=24, P=4, cfl=0.2, precision="mixed"):
             "rel_l2_vs_f64": rl2(qa, q64), "rel_l2_vs_exact": rl2(qa, q0), "rel_l2_f64_vs_exact": rl2(q64, q0)}
 
 
-def served(M, nreq, lam, seed=7, largest=False, slots=8):
+def served(M, nreq, lam, seed=7, largest=False, slots=8, precision=None):
     """Served stream: Poisson arrivals at `lam`/s of 2D/3D Euler, 2D
     shallow-water dam breaks and 3D Maxwell plane waves, 2k-400k elements
     (log-uniform), P in 2..5, 50-500 SSPRK3 steps, seeded ICs, admitted by a
     150 GB HBM budget; `largest` adds the 3D limited Sod at P=5 on 48^3 x 6
-    tets (50 steps)."""
+    tets (50 steps).  `precision` replaces every request's precision (the
+    plain FP64 comparison replays the same stream in "f64")."""
     rng = np.random.default_rng(seed)
     reqs = []
     for k in range(nreq):
@@ -452,11 +474,11 @@ def served(M, nreq, lam, seed=7, largest=False, slots=8):
             ic, prm, lam_est, h = M.IC_PLANE_WAVE, [1.0, 1.0], 1.0, 1.0 / n
             prec = "mixed"
         dt = 0.1 * h / (lam_est * (2 * P + 1))
-        reqs.append((mesh, phys, P, prec, ic, prm, dt, nsteps, None))
+        reqs.append((mesh, phys, P, precision or prec, ic, prm, dt, nsteps, None))
     if largest:
         mesh = M.Mesh(48, 48, 48, bcs=M.BoundaryConditions(2, 2, 1, 1, 1, 1))
         phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_HLLEC, False)
-        reqs.append((mesh, phys, 5, "f32", M.IC_SOD, [1.0, 1.0, 0.125, 0.1, 0.5, 1.0 / 48], 0.1 / 48 / (2.5 * 11),
+        reqs.append((mesh, phys, 5, precision or "f32", M.IC_SOD, [1.0, 1.0, 0.125, 0.1, 0.5, 1.0 / 48], 0.1 / 48 / (2.5 * 11),
                      50, 0.1))
     gaps = rng.exponential(1.0 / lam, len(reqs))
     # warm-up (untimed): one tiny request of every (physics, order, precision)
@@ -583,10 +605,24 @@ def main():
         if plain and "fp64_tflops" in fpp:
             plain["fp64_peak_tflops"] = fpp["fp64_tflops"]
             plain["contraction_frac_of_fp64_peak"] = plain["contraction_tflops"] / fpp["fp64_tflops"]
-        bat = batched_2d(M, a.batch_solves, a.batch_steps) if a.batch_solves > 0 else None
+        bat = None
+        if a.batch_solves > 0:  # the same batch in FP64 first: the plain comparison and the accuracy reference
+            b64 = batched_2d(M, a.batch_solves, a.batch_steps, precision="f64", loop=False, keep=True)
+            keep = b64.pop("_keep")
+            bat = batched_2d(M, a.batch_solves, a.batch_steps, ref=keep)
+            for s64 in keep["solvers"]:
+                s64.close()
+            bat["plain_f64_value"] = b64["value"]
+            bat["plain_f64_ms_per_step"] = b64["ms_per_step"]
+            bat["speedup_vs_f64"] = bat["value"] / b64["value"]
         cav = maxwell_cavity(M) if a.cavity else None
         srv = served(M, a.serve_requests, a.serve_lambda, largest=a.serve_largest,
                      slots=a.serve_slots) if a.serve_requests > 0 else None
+        if srv is not None:  # the same stream with every request in FP64
+            s64 = served(M, a.serve_requests, a.serve_lambda, largest=a.serve_largest, slots=a.serve_slots,
+                         precision="f64")
+            srv["plain_f64"] = {k: s64[k] for k in ("solves_per_s", "dof_stage_per_s", "p50_ms", "p99_ms")}
+            srv["speedup_vs_f64"] = srv["dof_stage_per_s"] / s64["dof_stage_per_s"]
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
