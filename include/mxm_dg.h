@@ -44,11 +44,12 @@ extern "C" {
 #define MXM_DG_ENOTREADY (-6)  /* request not finished yet (serving poll)    */
 
 /* Physics kinds: src/advection.mojo, src/euler.mojo, src/maxwell.mojo,
- * src/shallow_water.mojo. */
+ * src/shallow_water.mojo, src/mhd.mojo (IdealMHD, 3D only). */
 #define MXM_DG_PHYS_ADVECTION 0
 #define MXM_DG_PHYS_EULER 1
 #define MXM_DG_PHYS_MAXWELL 2
 #define MXM_DG_PHYS_SHALLOW_WATER 3
+#define MXM_DG_PHYS_MHD 4
 
 /* Numerical fluxes.  3D Euler: FLUX_RUSANOV..FLUX_HLLEC (euler.mojo:33-36).
  * 2D Euler: RUSANOV (|v|+c speed, local_mesh_2d_gpu_euler.mojo:220-337),
@@ -83,7 +84,11 @@ extern "C" {
  *  MAXWELL (maxwell.mojo:55-74): p = {c, Jx, Jy, Jz, Mx, My, Mz, inflow_Ex,
  *        inflow_Ey, inflow_Ez, inflow_Bx, inflow_By, inflow_Bz}
  *  SHALLOW_WATER (shallow_water.mojo:34-40): p = {g, h_min, inflow_h,
- *        inflow_hu, inflow_hv} */
+ *        inflow_hu, inflow_hv}
+ *  MHD (mhd.mojo:202-254): p = {gamma, min_density, min_pressure, c_h,
+ *        alpha_d, inflow_rho, inflow_rhou, inflow_rhov, inflow_rhow,
+ *        inflow_E, inflow_Bx, inflow_By, inflow_Bz, inflow_psi}; 9 components
+ *        [rho, rho u, rho v, rho w, E, Bx, By, Bz, psi] */
 typedef struct mxm_dg_physics_desc {
   int32_t kind;
   int32_t flux_type;

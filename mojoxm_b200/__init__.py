@@ -29,7 +29,7 @@ LIB_PATH = os.path.join(_HERE, "libmxm_dg.so")
 
 # include/mxm_dg.h constants
 OK, EINVAL, ENOMEM, ECUDA, ENONFINITE, ETIMEDOUT, ENOTREADY = 0, -1, -2, -3, -4, -5, -6
-PHYS_ADVECTION, PHYS_EULER, PHYS_MAXWELL, PHYS_SHALLOW_WATER = 0, 1, 2, 3
+PHYS_ADVECTION, PHYS_EULER, PHYS_MAXWELL, PHYS_SHALLOW_WATER, PHYS_MHD = 0, 1, 2, 3, 4
 FLUX_RUSANOV, FLUX_ROE, FLUX_HLLE, FLUX_HLLEC, FLUX_HLLC, FLUX_HLL = 0, 1, 2, 3, 4, 5
 BC_INTERIOR, BC_WALL, BC_OUTFLOW, BC_INFLOW = 0, 1, 2, 3
 PREC = {"f64": 0, "f32": 1, "mixed": 2}
@@ -248,6 +248,32 @@ class ShallowWater:  # src/shallow_water.mojo:31-47
 
     def params(self):
         return [self.g, self.h_min, self.inflow_h, self.inflow_hu, self.inflow_hv]
+
+
+@dataclass
+class IdealMHD:  # src/mhd.mojo:199-254 (3D; q = [rho, rho u, rho v, rho w, E, Bx, By, Bz, psi])
+    gamma: float = 5.0 / 3.0
+    min_density: float = 1e-6
+    min_pressure: float = 1e-6
+    c_h: float = 0.0
+    alpha_d: float = 0.0
+    inflow_rho: float = 0.0
+    inflow_rhou: float = 0.0
+    inflow_rhov: float = 0.0
+    inflow_rhow: float = 0.0
+    inflow_E: float = 0.0
+    inflow_Bx: float = 0.0
+    inflow_By: float = 0.0
+    inflow_Bz: float = 0.0
+    inflow_psi: float = 0.0
+    kind: int = field(default=PHYS_MHD, init=False)
+    flux_type: int = field(default=0, init=False)
+    entropy_fix: bool = field(default=False, init=False)
+
+    def params(self):
+        return [self.gamma, self.min_density, self.min_pressure, self.c_h, self.alpha_d, self.inflow_rho,
+                self.inflow_rhou, self.inflow_rhov, self.inflow_rhow, self.inflow_E, self.inflow_Bx, self.inflow_By,
+                self.inflow_Bz, self.inflow_psi]
 
 
 def physics_dict(ph):

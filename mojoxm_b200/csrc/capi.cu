@@ -152,6 +152,14 @@ void fill_tab2(Handle* h, KuhnTab2<R>& t) {
 
 // ---------------------------------------------------------------- dispatch
 template <class R>
+MhdD<R> make_mhd(const double* p) {  // mxm_dg_physics_desc field order (mhd.mojo:202-254)
+  MhdD<R> ph;
+  ph.gamma = R(p[0]); ph.rho_min = R(p[1]); ph.p_min = R(p[2]); ph.c_h = R(p[3]); ph.alpha_d = R(p[4]);
+  for (int k = 0; k < 9; ++k) ph.inflow[k] = R(p[5 + k]);
+  return ph;
+}
+
+template <class R>
 cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double b, double c,
                          double dt, int rhs_only) {
   const double* p = h->phys.p;
@@ -215,6 +223,7 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
         for (int k = 0; k < 3; ++k) ph.inflow[k] = R(p[2 + k]);
         return go(ph);
       }
+      case MXM_DG_PHYS_MHD: return go(make_mhd<R>(p));
     }
     return cudaErrorInvalidValue;
   }
@@ -319,6 +328,7 @@ cudaError_t wavespeed_launch(Handle* h, const void* qi, unsigned long long* out)
         for (int k = 0; k < 3; ++k) ph.inflow[k] = R(p[2 + k]);
         return launch_wavespeed3d<R>(h->P, ar, t, ph, out, h->stream);
       }
+      case MXM_DG_PHYS_MHD: return launch_wavespeed3d<R>(h->P, ar, t, make_mhd<R>(p), out, h->stream);
     }
     return cudaErrorInvalidValue;
   }
@@ -512,7 +522,8 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   if (P < 1 || P > 5) throw ArgError("order P must be in 1..5");
   if (prec != MXM_DG_PREC_F64 && prec != MXM_DG_PREC_F32 && prec != MXM_DG_PREC_MIXED)
     throw ArgError("precision must be MXM_DG_PREC_F64, MXM_DG_PREC_F32 or MXM_DG_PREC_MIXED");
-  if (ph->kind < 0 || ph->kind > 3) throw ArgError("unknown physics kind");
+  if (ph->kind < 0 || ph->kind > MXM_DG_PHYS_MHD) throw ArgError("unknown physics kind");
+  if (ph->kind == MXM_DG_PHYS_MHD && m->dim != 3) throw ArgError("MHD physics is 3D only");
   if (m->nx < 1 || m->ny < 1 || (m->dim == 3 && m->nz < 1)) throw ArgError("cell counts must be >= 1");
   for (int k = 0; k < 2 * m->dim; ++k)
     if (m->bc[k] < 0 || m->bc[k] > 3) throw ArgError("bc codes must be 0..3");
@@ -539,6 +550,7 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   h->NC = ph->kind == MXM_DG_PHYS_ADVECTION ? 1
         : ph->kind == MXM_DG_PHYS_EULER     ? (m->dim == 3 ? 5 : 4)
         : ph->kind == MXM_DG_PHYS_MAXWELL   ? 6
+        : ph->kind == MXM_DG_PHYS_MHD       ? 9
                                             : 3;
   h->ntypes = m->dim == 3 ? 6 : 2;
   h->ncell = int64_t(h->nx) * h->ny * h->nz;

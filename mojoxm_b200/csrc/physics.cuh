@@ -5,6 +5,7 @@
 //   Euler         src/euler.mojo:44-792 (Rusanov/Roe/HLLE/HLLEC, Harten-Hyman fix)
 //   Maxwell       src/maxwell.mojo:48-255
 //   ShallowWater  src/shallow_water.mojo:31-167
+//   IdealMHD      src/mhd.mojo:1-367 (GLM divergence cleaning)
 // Each formula keeps the reference's operation order, except that divisions
 // by positive quantities (floored densities, square roots of them, the HLLE
 // wave-speed span) are taken as one reciprocal and products, which in FP32
@@ -422,6 +423,103 @@ struct ShallowWaterD {
     }
   }
   __device__ void source(const R*, R* s) const { s[0] = s[1] = s[2] = R(0); }
+  __device__ void limit(R*) const {}
+};
+
+// ------------------------------------------------------------------ ideal MHD
+// q = [rho, rho u, rho v, rho w, E, Bx, By, Bz, psi]; Dedner GLM cleaning
+// (psi carries div B at speed c_h and decays at rate alpha_d).
+template <class R>
+struct MhdD {
+  static constexpr int NC = 9;
+  static constexpr bool kSource = true, kLimit = false;
+  static constexpr bool kLightFlux = true;
+  R gamma, rho_min, p_min, c_h, alpha_d, inflow[9];
+
+  __device__ __forceinline__ R rho_f(const R* q) const { return q[0] > rho_min ? q[0] : rho_min; }  // mhd.mojo:46-48
+  // floored gas pressure from ri = 1 / rho (mhd.mojo:51-62)
+  __device__ __forceinline__ R p_gas(const R* q, R ri) const {
+    const R ke = R(0.5) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) * ri;
+    const R me = R(0.5) * (q[5] * q[5] + q[6] * q[6] + q[7] * q[7]);
+    const R p = (gamma - R(1)) * (q[4] - ke - me);
+    return p > p_min ? p : p_min;
+  }
+  // fast magnetosonic speed along n (mhd.mojo:71-85)
+  __device__ __forceinline__ R fast_speed(const R* q, R ri, R p, R nx, R ny, R nz) const {
+    const R bx = q[5], by = q[6], bz = q[7], bn = bx * nx + by * ny + bz * nz;
+    const R cs2 = gamma * p * ri, ca2 = (bx * bx + by * by + bz * bz) * ri, can2 = (bn * bn) * ri;
+    R disc = (cs2 + ca2) * (cs2 + ca2) - R(4) * cs2 * can2;
+    if (disc < R(0)) disc = R(0);
+    return sqrt(R(0.5) * (cs2 + ca2 + sqrt(disc)));
+  }
+  __device__ void flux(const R* q, R* F) const {  // mhd.mojo:92-146
+    const R ri = pos_rcp(rho_f(q));
+    const R mx = q[1], my = q[2], mz = q[3], u = mx * ri, v = my * ri, w = mz * ri;
+    const R E = q[4], bx = q[5], by = q[6], bz = q[7], psi = q[8];
+    const R pt = p_gas(q, ri) + R(0.5) * (bx * bx + by * by + bz * bz);
+    const R ub = u * bx + v * by + w * bz, ch2 = c_h * c_h;
+    F[0] = mx; F[1] = mx * u + pt - bx * bx; F[2] = mx * v - bx * by; F[3] = mx * w - bx * bz;
+    F[4] = u * (E + pt) - bx * ub; F[5] = psi; F[6] = u * by - v * bx; F[7] = u * bz - w * bx; F[8] = ch2 * bx;
+    F[9] = my; F[10] = my * u - by * bx; F[11] = my * v + pt - by * by; F[12] = my * w - by * bz;
+    F[13] = v * (E + pt) - by * ub; F[14] = v * bx - u * by; F[15] = psi; F[16] = v * bz - w * by; F[17] = ch2 * by;
+    F[18] = mz; F[19] = mz * u - bz * bx; F[20] = mz * v - bz * by; F[21] = mz * w + pt - bz * bz;
+    F[22] = w * (E + pt) - bz * ub; F[23] = w * bx - u * bz; F[24] = w * by - v * bz; F[25] = psi; F[26] = ch2 * bz;
+  }
+  // F . n of one state (mhd.mojo:151-194)
+  __device__ __forceinline__ void normal_flux(const R* q, R ri, R p, R nx, R ny, R nz, R* F) const {
+    const R rho = rho_f(q), u = q[1] * ri, v = q[2] * ri, w = q[3] * ri;
+    const R E = q[4], bx = q[5], by = q[6], bz = q[7], psi = q[8];
+    const R pt = p + R(0.5) * (bx * bx + by * by + bz * bz);
+    const R ub = u * bx + v * by + w * bz, un = u * nx + v * ny + w * nz, bn = bx * nx + by * ny + bz * nz;
+    F[0] = rho * un;
+    F[1] = rho * u * un + pt * nx - bn * bx;
+    F[2] = rho * v * un + pt * ny - bn * by;
+    F[3] = rho * w * un + pt * nz - bn * bz;
+    F[4] = un * (E + pt) - bn * ub;
+    F[5] = un * bx - u * bn + psi * nx;
+    F[6] = un * by - v * bn + psi * ny;
+    F[7] = un * bz - w * bn + psi * nz;
+    F[8] = c_h * c_h * bn;
+  }
+  // Rusanov with alpha = max(|u_n| + c_f, c_h) (mhd.mojo:280-307)
+  __device__ R num_flux(const R* l, const R* r, R nx, R ny, R nz, R* f) const {
+    const R il = pos_rcp(rho_f(l)), ir = pos_rcp(rho_f(r));
+    const R pl = p_gas(l, il), pr = p_gas(r, ir);
+    R Fl[9], Fr[9];
+    normal_flux(l, il, pl, nx, ny, nz, Fl);
+    normal_flux(r, ir, pr, nx, ny, nz, Fr);
+    const R cfl = fast_speed(l, il, pl, nx, ny, nz), cfr = fast_speed(r, ir, pr, nx, ny, nz);
+    const R unl = (l[1] * nx + l[2] * ny + l[3] * nz) * il, unr = (r[1] * nx + r[2] * ny + r[3] * nz) * ir;
+    const R al = rmax(rmax(rabs(unl) + cfl, rabs(unr) + cfr), c_h), h = R(0.5);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) f[c] = h * (Fl[c] + Fr[c]) - h * al * (r[c] - l[c]);
+    return al;
+  }
+  // ghost state: conducting wall reflects u_n and B_n; inflow; outflow copies (mhd.mojo:312-353)
+  __device__ void ghost(const R* q, int bc, R nx, R ny, R nz, R* g) const {
+    if (bc == BC_WALL) {
+      const R mn = q[1] * nx + q[2] * ny + q[3] * nz, bn = q[5] * nx + q[6] * ny + q[7] * nz;
+      g[0] = q[0]; g[4] = q[4]; g[8] = q[8];
+      g[1] = q[1] - R(2) * mn * nx; g[2] = q[2] - R(2) * mn * ny; g[3] = q[3] - R(2) * mn * nz;
+      g[5] = q[5] - R(2) * bn * nx; g[6] = q[6] - R(2) * bn * ny; g[7] = q[7] - R(2) * bn * nz;
+    } else if (bc == BC_INFLOW) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) g[k] = inflow[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) g[k] = q[k];
+    }
+  }
+  __device__ R bnd_flux(const R* q, int bc, R nx, R ny, R nz, R* f) const {
+    R g[9];
+    ghost(q, bc, nx, ny, nz, g);
+    return num_flux(q, g, nx, ny, nz, f);
+  }
+  __device__ void source(const R* q, R* s) const {  // mhd.mojo:357-361: GLM damping of psi
+#pragma unroll
+    for (int c = 0; c < 8; ++c) s[c] = R(0);
+    s[8] = -alpha_d * q[8];
+  }
   __device__ void limit(R*) const {}
 };
 

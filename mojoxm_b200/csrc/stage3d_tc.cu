@@ -42,6 +42,7 @@ using TEE = EulerD<float, FLUX_HLLE>;
 using TEC = EulerD<float, FLUX_HLLEC>;
 using TM = MaxwellD<float>;
 using TS = ShallowWaterD<float>;
+using TH = MhdD<float>;
 #define MXM_INST_TC(PH)                                                                                           \
   template cudaError_t launch_stage3d_tc<PH>(int, const Stage3DArgs<float>&, const KuhnTab3<float>&, const PH&, \
                                              const unsigned char*, int, cudaStream_t);
@@ -52,5 +53,6 @@ MXM_INST_TC(TEE)
 MXM_INST_TC(TEC)
 MXM_INST_TC(TM)
 MXM_INST_TC(TS)
+MXM_INST_TC(TH)
 
 }  // namespace mxm

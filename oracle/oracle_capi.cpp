@@ -45,6 +45,12 @@ static SolverBase* make3(int P, int nx, int ny, int nz, double Lx, double Ly, do
     for (int k = 0; k < 3; ++k) ph.inflow[k] = R(p[2 + k]);
     return new Solver3D<R, ShallowWater<R>>(P, nx, ny, nz, Lx, Ly, Lz, bcs, ph);
   }
+  if (kind == PHYS_MHD) {
+    IdealMHD<R> ph;
+    ph.gamma = R(p[0]); ph.min_density = R(p[1]); ph.min_pressure = R(p[2]); ph.c_h = R(p[3]); ph.alpha_d = R(p[4]);
+    for (int k = 0; k < 9; ++k) ph.inflow[k] = R(p[5 + k]);
+    return new Solver3D<R, IdealMHD<R>>(P, nx, ny, nz, Lx, Ly, Lz, bcs, ph);
+  }
   throw std::runtime_error("unknown physics kind");
 }
 

@@ -2,7 +2,8 @@
 // CPU restatement of mojoxm's `Physics` implementations used by the 3D
 // solver: Advection (src/advection.mojo), Euler with Rusanov / Roe / HLLE /
 // HLLEC and the Harten-Hyman entropy fix (src/euler.mojo), vacuum Maxwell
-// (src/maxwell.mojo) and shallow water embedded in 3D (src/shallow_water.mojo).
+// (src/maxwell.mojo), shallow water embedded in 3D (src/shallow_water.mojo)
+// and ideal MHD with GLM divergence cleaning (src/mhd.mojo).
 // Templated on the arithmetic type so the same code runs in FP64 (the oracle
 // proper) and in FP32 (mimicking the reference's all-Float32 GPU path).
 #pragma once
@@ -13,7 +14,7 @@
 
 namespace orc {
 
-enum { PHYS_ADVECTION = 0, PHYS_EULER = 1, PHYS_MAXWELL = 2, PHYS_SW = 3 };
+enum { PHYS_ADVECTION = 0, PHYS_EULER = 1, PHYS_MAXWELL = 2, PHYS_SW = 3, PHYS_MHD = 4 };
 enum { FLUX_RUSANOV = 0, FLUX_ROE = 1, FLUX_HLLE = 2, FLUX_HLLEC = 3, FLUX_HLLC = 4, FLUX_HLL = 5 };
 
 template <typename R>
@@ -399,6 +400,88 @@ struct ShallowWater {  // shallow_water.mojo:31-167
     return numerical_flux(q, gs, nx, ny, nz, f);
   }
   void source_term(const R*, R* s) const { s[0] = R(0); s[1] = R(0); s[2] = R(0); }
+  void limit_state(R*) const {}
+};
+
+// ------------------------------------------------------------------ IdealMHD
+// q = [rho, rho u, rho v, rho w, E, Bx, By, Bz, psi]
+template <typename R>
+struct IdealMHD {  // mhd.mojo:199-367
+  static constexpr int NC = 9;
+  R gamma, min_density, min_pressure, c_h, alpha_d, inflow[9];
+  R rho_f(const R* q) const { return q[0] > min_density ? q[0] : min_density; }  // :46-48
+  R gas_pressure(const R* q) const {  // :51-62
+    R rho = rho_f(q);
+    R ke = R(0.5) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) / rho;
+    R me = R(0.5) * (q[5] * q[5] + q[6] * q[6] + q[7] * q[7]);
+    R p = (gamma - R(1)) * (q[4] - ke - me);
+    return p > min_pressure ? p : min_pressure;
+  }
+  R fast_speed(const R* q, R nx, R ny, R nz) const {  // :71-85
+    R rho = rho_f(q), p = gas_pressure(q);
+    R bx = q[5], by = q[6], bz = q[7], bn = bx * nx + by * ny + bz * nz;
+    R cs2 = gamma * p / rho, ca2 = (bx * bx + by * by + bz * bz) / rho, can2 = (bn * bn) / rho;
+    R disc = (cs2 + ca2) * (cs2 + ca2) - R(4) * cs2 * can2;
+    if (disc < R(0)) disc = R(0);
+    return std::sqrt(R(0.5) * (cs2 + ca2 + std::sqrt(disc)));
+  }
+  void internal_flux(const R* q, R* f) const {  // :92-146
+    R rho = rho_f(q), mx = q[1], my = q[2], mz = q[3], u = mx / rho, v = my / rho, w = mz / rho;
+    R E = q[4], bx = q[5], by = q[6], bz = q[7], psi = q[8];
+    R pt = gas_pressure(q) + R(0.5) * (bx * bx + by * by + bz * bz);
+    R ub = u * bx + v * by + w * bz, ch2 = c_h * c_h;
+    f[0] = mx; f[1] = mx * u + pt - bx * bx; f[2] = mx * v - bx * by; f[3] = mx * w - bx * bz;
+    f[4] = u * (E + pt) - bx * ub; f[5] = psi; f[6] = u * by - v * bx; f[7] = u * bz - w * bx; f[8] = ch2 * bx;
+    f[9] = my; f[10] = my * u - by * bx; f[11] = my * v + pt - by * by; f[12] = my * w - by * bz;
+    f[13] = v * (E + pt) - by * ub; f[14] = v * bx - u * by; f[15] = psi; f[16] = v * bz - w * by; f[17] = ch2 * by;
+    f[18] = mz; f[19] = mz * u - bz * bx; f[20] = mz * v - bz * by; f[21] = mz * w + pt - bz * bz;
+    f[22] = w * (E + pt) - bz * ub; f[23] = w * bx - u * bz; f[24] = w * by - v * bz; f[25] = psi; f[26] = ch2 * bz;
+  }
+  void normal_flux(const R* q, R nx, R ny, R nz, R* F) const {  // :151-194
+    R rho = rho_f(q), u = q[1] / rho, v = q[2] / rho, w = q[3] / rho;
+    R E = q[4], bx = q[5], by = q[6], bz = q[7], psi = q[8];
+    R pt = gas_pressure(q) + R(0.5) * (bx * bx + by * by + bz * bz);
+    R ub = u * bx + v * by + w * bz, un = u * nx + v * ny + w * nz, bn = bx * nx + by * ny + bz * nz;
+    F[0] = rho * un;
+    F[1] = rho * u * un + pt * nx - bn * bx;
+    F[2] = rho * v * un + pt * ny - bn * by;
+    F[3] = rho * w * un + pt * nz - bn * bz;
+    F[4] = un * (E + pt) - bn * ub;
+    F[5] = un * bx - u * bn + psi * nx;
+    F[6] = un * by - v * bn + psi * ny;
+    F[7] = un * bz - w * bn + psi * nz;
+    F[8] = c_h * c_h * bn;
+  }
+  R numerical_flux(const R* l, const R* r, R nx, R ny, R nz, R* f) const {  // :280-307
+    R Fl[9], Fr[9];
+    normal_flux(l, nx, ny, nz, Fl);
+    normal_flux(r, nx, ny, nz, Fr);
+    R cfl = fast_speed(l, nx, ny, nz), cfr = fast_speed(r, nx, ny, nz);
+    R unl = (l[1] * nx + l[2] * ny + l[3] * nz) / rho_f(l), unr = (r[1] * nx + r[2] * ny + r[3] * nz) / rho_f(r);
+    R al = rmax(rmax(rabs(unl) + cfl, rabs(unr) + cfr), c_h);
+    R h = R(0.5);
+    for (int c = 0; c < 9; ++c) f[c] = h * (Fl[c] + Fr[c]) - h * al * (r[c] - l[c]);
+    return al;
+  }
+  R boundary_flux(const R* q, int bc, R nx, R ny, R nz, R* f) const {  // :312-353
+    R g[9];
+    if (bc == BC_WALL) {  // conducting wall: reflect u_n and B_n
+      g[0] = q[0]; g[4] = q[4]; g[8] = q[8];
+      R mn = q[1] * nx + q[2] * ny + q[3] * nz;
+      g[1] = q[1] - R(2) * mn * nx; g[2] = q[2] - R(2) * mn * ny; g[3] = q[3] - R(2) * mn * nz;
+      R bn = q[5] * nx + q[6] * ny + q[7] * nz;
+      g[5] = q[5] - R(2) * bn * nx; g[6] = q[6] - R(2) * bn * ny; g[7] = q[7] - R(2) * bn * nz;
+    } else if (bc == BC_INFLOW) {
+      for (int k = 0; k < 9; ++k) g[k] = inflow[k];
+    } else {
+      for (int k = 0; k < 9; ++k) g[k] = q[k];
+    }
+    return numerical_flux(q, g, nx, ny, nz, f);
+  }
+  void source_term(const R* q, R* s) const {  // :357-361 (GLM damping)
+    for (int c = 0; c < 8; ++c) s[c] = R(0);
+    s[8] = -alpha_d * q[8];
+  }
   void limit_state(R*) const {}
 };
 

@@ -107,7 +107,7 @@ struct Solver3D : SolverBase {
     const R inv6V = mesh.elem_inv_6V[e];
     for (int i = 0; i < NP; ++i) {
       const int64_t ob = (e * NP + i) * NC;
-      R src[8];
+      R src[NCc];
       phys.source_term(q_in + ob, src);
       for (int c = 0; c < NC; ++c) {
         R vc = R(0);
@@ -152,7 +152,7 @@ struct Solver3D : SolverBase {
   double max_face_speed() override {
     double best = 0.0;
     const R* qi = q[0].data();
-    R fs[8];
+    R fs[NCc];
     for (int64_t e = 0; e < Ne; ++e)
       for (int lf = 0; lf < 4; ++lf)
         for (int m = 0; m < NFP; ++m) {
@@ -188,7 +188,7 @@ struct Solver3D : SolverBase {
       }
 #pragma omp parallel for schedule(static)
     for (int64_t e = 0; e < n; ++e) {
-      R own[8], mn[8], mx[8], pD[8], nD[8];
+      R own[NCc], mn[NCc], mx[NCc], pD[NCc], nD[NCc];
       for (int c = 0; c < NC; ++c) own[c] = mn[c] = mx[c] = cell_avg[e * NC + c];
       for (int lf = 0; lf < 4; ++lf) {
         int64_t fid = mesh.elem_faces[e * 4 + lf];

@@ -25,6 +25,7 @@ PHYSICS_3D = {
     "euler_hllec_fix": lambda: euler(M.FLUX_HLLEC, efix=True),
     "maxwell": lambda: M.Maxwell(1.0, 0.1, -0.2, 0.05, 0.02, 0.0, -0.03, 0.1, 0.2, -0.1, 0.05, 0.0, 0.1),
     "shallow_water": lambda: M.ShallowWater(9.81, 1e-6, 1.5, 0.2, -0.1),
+    "mhd": lambda: M.IdealMHD(5.0 / 3.0, 1e-6, 1e-6, 1.3, 0.4, 1.1, 0.2, -0.1, 0.05, 3.0, 0.3, -0.2, 0.1, 0.02),
 }
 
 PHYSICS_2D = {
@@ -70,6 +71,16 @@ def random_state(shape, physics, seed, xyz=None):
             q[..., 0] = rho
             q[..., 1:3] = rho[..., None] * vel[..., :2]
             q[..., 3] = p / (GAMMA - 1) + 0.5 * rho * (vel[..., :2] ** 2).sum(-1)
+    elif k == M.PHYS_MHD:
+        rho = 1.0 + 0.2 * rng.uniform(-1, 1, (ne, npn))
+        vel = 0.5 * rng.uniform(-1, 1, (ne, npn, 3))
+        B = 0.5 * rng.uniform(-1, 1, (ne, npn, 3))
+        p = 1.0 + 0.2 * rng.uniform(-1, 1, (ne, npn))
+        q[..., 0] = rho
+        q[..., 1:4] = rho[..., None] * vel
+        q[..., 4] = p / (5.0 / 3.0 - 1) + 0.5 * rho * (vel ** 2).sum(-1) + 0.5 * (B ** 2).sum(-1)
+        q[..., 5:8] = B
+        q[..., 8] = 0.1 * rng.uniform(-1, 1, (ne, npn))
     elif k == M.PHYS_SHALLOW_WATER:
         h = 1.0 + 0.3 * rng.uniform(-1, 1, (ne, npn))
         q[..., 0] = h

@@ -225,3 +225,21 @@ def test_limiter_conservation_product(prec):
     assert np.abs(_cell_means(out, w) - _cell_means(q, w)).max() <= G["limiter3d.mean_tol"]
     assert np.abs(out - q).max() > G["limiter3d.fired_min"]
     s.close()
+
+
+def test_oracle_mhd_constant_state_and_conducting_wall(oracle_mod):
+    """Ideal MHD (src/mhd.mojo): a uniform magnetised state is steady on a
+    periodic mesh, and at a conducting wall a state at rest with B tangent to
+    the wall gives no mass or normal-B flux (the ghost reflects u_n and B_n)."""
+    ph = M.IdealMHD(5.0 / 3.0, 1e-6, 1e-6, 1.0, 0.2)
+    o = oracle_mod.Oracle3D(2, 2, 1.0, M.physics_dict(ph))
+    q = np.zeros((o.Ne, o.NP, o.NC))
+    q[..., 0], q[..., 1:4], q[..., 5:8] = 1.2, [0.3, -0.2, 0.1], [0.4, 0.1, -0.3]
+    q[..., 4] = 1.5 + 0.5 * 0.14 / 1.2 + 0.13
+    assert np.abs(o.rhs(q)).max() < 1e-12
+    ow = oracle_mod.Oracle3D(2, 2, 1.0, M.physics_dict(ph), bcs=(1, 1, 1, 1, 1, 1))
+    qw = np.zeros((ow.Ne, ow.NP, ow.NC))
+    qw[..., 0], qw[..., 4] = 1.0, 2.0
+    qw[..., 7] = 0.5  # B along z: tangent to the x and y walls, normal to the z walls
+    r = ow.rhs(qw)
+    assert np.abs(r[..., 0]).max() < 1e-12  # no mass flux anywhere

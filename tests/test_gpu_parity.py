@@ -41,7 +41,7 @@ def test_rhs3d_f64_periodic(oracle_mod, name, P):
 
 
 @pytest.mark.parametrize("bcname", [b for b in C.BCS_3D if b != "periodic"])
-@pytest.mark.parametrize("name", ["advection", "euler_hllec_fix", "euler_rusanov", "maxwell", "shallow_water"])
+@pytest.mark.parametrize("name", ["advection", "euler_hllec_fix", "euler_rusanov", "maxwell", "shallow_water", "mhd"])
 @pytest.mark.parametrize("P", [2, 3])
 def test_rhs3d_f64_boundaries(oracle_mod, name, bcname, P):
     phys = C.PHYSICS_3D[name]()
@@ -50,7 +50,7 @@ def test_rhs3d_f64_boundaries(oracle_mod, name, bcname, P):
     assert C.rel_err(s.rhs(q), o.rhs(q)) <= C.TOL_F64_3D[P]
 
 
-@pytest.mark.parametrize("name", ["euler_hllec", "euler_roe_fix", "maxwell", "advection", "shallow_water"])
+@pytest.mark.parametrize("name", ["euler_hllec", "euler_roe_fix", "maxwell", "advection", "shallow_water", "mhd"])
 @pytest.mark.parametrize("P", [1, 3, 5])
 def test_rhs3d_f32(oracle_mod, name, P):
     phys = C.PHYSICS_3D[name]()
@@ -152,7 +152,7 @@ TOL_MIXED_P = {2: TOL_MIXED, 3: TOL_MIXED, 4: TOL_MIXED, 5: 2e-3}
 
 
 @pytest.mark.parametrize("P", [2, 3, 4, 5])
-@pytest.mark.parametrize("name", ["euler_rusanov", "euler_hllec_fix", "maxwell", "advection", "shallow_water"])
+@pytest.mark.parametrize("name", ["euler_rusanov", "euler_hllec_fix", "maxwell", "advection", "shallow_water", "mhd"])
 def test_rhs3d_mixed_vs_f64(oracle_mod, name, P):
     phys = C.PHYSICS_3D[name]()
     s, o = make_pair(oracle_mod, phys, P, N3, L3, C.BCS_3D["outflow_x_wall_yz"], prec="mixed")
@@ -174,3 +174,35 @@ def test_mixed_large_mesh_vs_f32(oracle_mod):
     err = C.rel_err(sm.rhs(q), sf.rhs(q))
     print(f"mixed vs f32 on {n}: {err:.2e}")
     assert err <= TOL_MIXED
+
+
+@pytest.mark.parametrize("limiter", [False, True])
+@pytest.mark.parametrize("P", [2, 3])
+def test_mhd_ssprk3_steps_f64(oracle_mod, P, limiter):
+    """Ideal MHD with GLM cleaning: three SSPRK3 steps (conducting walls in x,
+    outflow in y, periodic z), with and without the cell limiter."""
+    phys = C.PHYSICS_3D["mhd"]()
+    bcs = (1, 1, 2, 2, 0, 0)
+    s, o = make_pair(oracle_mod, phys, P, N3, L3, bcs)
+    q = C.random_state(s.shape, phys, seed=41)
+    s.upload_state(q)
+    o.set(q)
+    if limiter:
+        s.enable_cell_limiter(True, 0.1)
+        o.enable_limiter(True, 0.1)
+    dt = 0.02 / (2 * P + 1)
+    s.step_n(dt, 3)
+    o.step(dt, 3)
+    assert C.rel_err(s.download_state(0), o.get(0)) <= 50 * C.TOL_F64_3D[P]
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32", "mixed"])
+def test_mhd_constant_state_preserved(prec):
+    """A uniform magnetised state on a periodic mesh is a steady solution."""
+    s = M.Solver(M.Mesh(3, 2, 2), C.PHYSICS_3D["mhd"](), P=3, precision=prec)
+    q = np.zeros(s.shape)
+    q[..., 0], q[..., 1:4], q[..., 5:8] = 1.2, [0.3, -0.2, 0.1], [0.4, 0.1, -0.3]
+    q[..., 4] = 1.0 / (5.0 / 3.0 - 1) + 0.5 * (0.3 ** 2 + 0.2 ** 2 + 0.1 ** 2) / 1.2 + 0.5 * 0.26
+    r = s.rhs(q)
+    s.close()
+    assert np.abs(r).max() <= (1e-11 if prec == "f64" else 2e-4)
