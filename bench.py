@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--serve-largest", action="store_true", help="add the 48^3x6 limited Sod P5 request")
     ap.add_argument("--serve-slots", type=int, default=8, help="solves running at once in the served leg")
     ap.add_argument("--cavity", type=int, default=1, help="run the 24^3x6 P=4 Maxwell cavity leg (1/0)")
+    ap.add_argument("--mhd", type=int, default=1, help="run the 3D ideal-MHD Alfven-wave leg (1/0)")
     return ap.parse_args()
 
 
@@ -434,6 +435,34 @@ def maxwell_cavity(M, n=24, P=4, cfl=0.2, precision="mixed"):
             "rel_l2_vs_f64": rl2(qa, q64), "rel_l2_vs_exact": rl2(qa, q0), "rel_l2_f64_vs_exact": rl2(q64, q0)}
 
 
+def mhd_alfven(M, nx=64, P=3, steps=30, precision="mixed"):
+    """3D ideal MHD with GLM cleaning: the right-going Alfven wave of
+    benchmarks/bench_mhd_alfven_3d_p3.mojo (gamma 5/3, rho0 = B0 = 1, p0 = 0.1,
+    amplitude 0.1, c_h = 1.5, alpha_d = 0.5) on an nx x nx/4 x nx/4 periodic
+    slab of [0,1] x [0,1/4]^2, `steps` SSPRK3 steps at CFL 0.1, in
+    `precision` and in FP64."""
+    ph = M.IdealMHD(5.0 / 3.0, 1e-6, 1e-6, 1.5, 0.5)
+    ny = nx // 4
+    cf = np.sqrt(5.0 / 3.0 * 0.1 + 1.01)
+    dt = 0.1 * (1.0 / nx) / (max(cf, 1.5) * (2 * P + 1))
+    res = {}
+    for prec in (precision, "f64"):
+        s = M.Solver(M.Mesh(nx, ny, ny, 1.0, 0.25, 0.25), ph, P=P, precision=prec)
+        s.fill_ic(M.IC_ALFVEN, [1.0, 1.0, 0.1, 0.1, 1.0])
+        s.step_n(dt, 3)
+        ms = s.time_steps(dt, steps)
+        res[prec] = (s.download_state().astype(np.float64), ms, s.dof_count())
+        s.close()
+    qa, ms, dof = res[precision]
+    q64, ms64, _ = res["f64"]
+    value = 3 * dof * steps / (ms * 1e-3)
+    return {"workload": f"3D ideal MHD + GLM Alfven wave, {nx}x{ny}x{ny}x6 = {6 * nx * ny * ny} tets, P={P}, "
+                        f"9 components, Rusanov", "precision": precision, "value": value, "unit": UNIT,
+            "ms_per_step": ms / steps, "plain_f64_value": 3 * dof * steps / (ms64 * 1e-3),
+            "speedup_vs_f64": value / (3 * dof * steps / (ms64 * 1e-3)),
+            "rel_l2_vs_f64": float(np.sqrt(((qa - q64) ** 2).sum() / (q64 ** 2).sum())), "steps": 3 + steps}
+
+
 def served(M, nreq, lam, seed=7, largest=False, slots=8, precision=None):
     """Served stream: Poisson arrivals at `lam`/s of 2D/3D Euler, 2D
     shallow-water dam breaks and 3D Maxwell plane waves, 2k-400k elements
@@ -616,6 +645,7 @@ def main():
             bat["plain_f64_ms_per_step"] = b64["ms_per_step"]
             bat["speedup_vs_f64"] = bat["value"] / b64["value"]
         cav = maxwell_cavity(M) if a.cavity else None
+        mhd = mhd_alfven(M) if a.mhd else None
         srv = served(M, a.serve_requests, a.serve_lambda, largest=a.serve_largest,
                      slots=a.serve_slots) if a.serve_requests > 0 else None
         if srv is not None:  # the same stream with every request in FP64
@@ -642,7 +672,7 @@ def main():
             "plain_f64": plain,
             "measured_gemm_peaks": fpp,
             "batched": bat,
-            "maxwell_cavity": cav,
+            "maxwell_cavity": cav, "mhd_alfven": mhd,
             "served": srv,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": qbytes,
                     "entry": "mxm_dg_advance_host (pinned host state in/out, 1 SSPRK3 step per call)"},

@@ -226,7 +226,10 @@ int mxm_dg_selftest_wait_timeout(double limit_ms, int32_t* gave_up, double* wait
  *   SOD         Euler tanh-smoothed tube along x: rhoL, pL, rhoR, pR, x0, width
  *   DAM_BREAK   shallow water at rest: hL, hR, x0, width
  *   CAVITY      Maxwell: mx, my, amp: E_z = amp sin(mx pi x/Lx) sin(my pi y/Ly)
- *   PLANE_WAVE  Maxwell: amp, k: E_z = amp sin(2 pi k x/Lx), B_y = -E_z/c */
+ *   PLANE_WAVE  Maxwell: amp, k: E_z = amp sin(2 pi k x/Lx), B_y = -E_z/c
+ *   ALFVEN      MHD: rho0, B0, p0, amp, k: right-going Alfven wave along x,
+ *               v = amp sin(2 pi k x/Lx), B = (B0, -amp sqrt(rho0) sin(.), 0),
+ *               psi = 0 (benchmarks/bench_mhd_alfven_3d_p3.mojo:68-102) */
 #define MXM_DG_IC_CONSTANT 0
 #define MXM_DG_IC_SINE_WAVE 1
 #define MXM_DG_IC_VORTEX 2
@@ -234,6 +237,7 @@ int mxm_dg_selftest_wait_timeout(double limit_ms, int32_t* gave_up, double* wait
 #define MXM_DG_IC_DAM_BREAK 4
 #define MXM_DG_IC_CAVITY 5
 #define MXM_DG_IC_PLANE_WAVE 6
+#define MXM_DG_IC_ALFVEN 7
 int mxm_dg_fill_ic(void* handle, int which, int kind, const double* params, int nparams);
 
 /* ---- batched engine (no reference counterpart: the reference runs each

@@ -51,7 +51,7 @@ EXPORTED = [
     "mxm_dg_server_wait", "mxm_dg_server_stats", "mxm_dg_server_last_error",
 ]
 
-IC_CONSTANT, IC_SINE_WAVE, IC_VORTEX, IC_SOD, IC_DAM_BREAK, IC_CAVITY, IC_PLANE_WAVE = range(7)
+IC_CONSTANT, IC_SINE_WAVE, IC_VORTEX, IC_SOD, IC_DAM_BREAK, IC_CAVITY, IC_PLANE_WAVE, IC_ALFVEN = range(8)
 
 
 class DGError(RuntimeError):

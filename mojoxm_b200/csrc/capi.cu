@@ -459,14 +459,15 @@ void build_xyz(Handle* h) {
 // Device IC fill of state buffer `which` (asynchronous on the handle's stream).
 void fill_ic(Handle* h, int which, int kind, const double* params, int nparams) {
   if (which < 0 || which > 2) throw ArgError("which must be 0..2");
-  if (kind < MXM_DG_IC_CONSTANT || kind > MXM_DG_IC_PLANE_WAVE) throw ArgError("unknown initial-condition kind");
+  if (kind < MXM_DG_IC_CONSTANT || kind > MXM_DG_IC_ALFVEN) throw ArgError("unknown initial-condition kind");
   if (nparams < 0 || nparams > 16 || (nparams > 0 && !params)) throw ArgError("nparams must be 0..16");
   const int k = h->phys.kind;
   const bool ok = kind == MXM_DG_IC_CONSTANT ||
                   ((kind == MXM_DG_IC_SINE_WAVE || kind == MXM_DG_IC_VORTEX || kind == MXM_DG_IC_SOD) &&
                    k == MXM_DG_PHYS_EULER) ||
                   (kind == MXM_DG_IC_DAM_BREAK && k == MXM_DG_PHYS_SHALLOW_WATER) ||
-                  ((kind == MXM_DG_IC_CAVITY || kind == MXM_DG_IC_PLANE_WAVE) && k == MXM_DG_PHYS_MAXWELL);
+                  ((kind == MXM_DG_IC_CAVITY || kind == MXM_DG_IC_PLANE_WAVE) && k == MXM_DG_PHYS_MAXWELL) ||
+                  (kind == MXM_DG_IC_ALFVEN && k == MXM_DG_PHYS_MHD);
   if (!ok) throw ArgError("initial-condition kind does not match the physics");
   IcArgs a;
   std::memset(&a, 0, sizeof(a));

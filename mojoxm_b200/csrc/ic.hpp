@@ -5,6 +5,8 @@
 
 namespace mxm {
 
+constexpr int kMaxIcNC = 9;  // components of the widest physics (MHD)
+
 struct IcArgs {
   int64_t ne;
   int dim, P, NP, NC, nx, ny, nz, kind;

@@ -48,7 +48,7 @@ __global__ void ic_kernel(IcArgs a, R* q) {
   x[2] = a.dim == 3 ? (ck + x[2]) * a.h[2] : 0.0;
   const double* p = a.prm;
   const double g = a.gamma, g1 = g - 1.0;
-  double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double s[kMaxIcNC] = {};
   const bool e3 = a.dim == 3;  // Euler: 3D (rho, m, E) or 2D (rho, mx, my, E)
   auto euler = [&](double rho, double u, double v, double w, double pr) {
     if (e3) {
@@ -99,6 +99,14 @@ __global__ void ic_kernel(IcArgs a, R* q) {
       const double ez = p[0] * sin(2.0 * kPi * p[1] * x[0] / a.L[0]);
       s[2] = ez;
       s[4] = -ez / a.c;
+      break;
+    }
+    case MXM_DG_IC_ALFVEN: {  // MHD: right-going Alfven wave along x (bench_mhd_alfven_3d_p3.mojo:68-102)
+      const double sn = sin(2.0 * kPi * p[4] * x[0] / a.L[0]);
+      const double rho = p[0], bx = p[1], v = p[3] * sn, by = -p[3] * sqrt(rho) * sn;
+      s[0] = rho; s[2] = rho * v;
+      s[4] = p[2] / g1 + 0.5 * rho * v * v + 0.5 * (bx * bx + by * by);
+      s[5] = bx; s[6] = by;
       break;
     }
   }

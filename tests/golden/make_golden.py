@@ -93,6 +93,16 @@ ENTRIES = [
     ("smooth_wave_p3.cfl", 0.1, "benchmarks/bench_euler_smooth_wave_3d_p3.mojo", "57", "CFL = Float32(0.1)"),
     ("vortex_3d.l2_max_rel", 0.10, "benchmarks/bench_euler_vortex_3d.mojo", "75",
      "L2_MAX_REL: Float64 = 0.10"),
+    # 3D ideal MHD (benchmarks/bench_mhd_alfven_3d_p3.mojo)
+    ("mhd_alfven_3d_p3.mesh", [16, 4, 4, 1.0, 0.25, 0.25], "benchmarks/bench_mhd_alfven_3d_p3.mojo", "47-52",
+     "comptime LY = Float64(4.0 / 16.0)"),
+    ("mhd_alfven_3d_p3.gamma_rho0_b0_p0_amp", [5.0 / 3.0, 1.0, 1.0, 0.1, 0.1], "benchmarks/bench_mhd_alfven_3d_p3.mojo",
+     "54-58", "comptime AMPLITUDE = Float32(0.1)"),
+    ("mhd_alfven_3d_p3.c_h_alpha_d", [1.5, 0.5], "benchmarks/bench_mhd_alfven_3d_p3.mojo", "59-60",
+     "comptime ALPHA_D = Float32(0.5)"),
+    ("mhd_alfven_3d_p3.cfl", 0.10, "benchmarks/bench_mhd_alfven_3d_p3.mojo", "65", "comptime CFL = Float32(0.10)"),
+    ("mhd_alfven_3d_p3.l2_max_rel", 5.0e-3, "benchmarks/bench_mhd_alfven_3d_p3.mojo", "71",
+     "comptime L2_MAX_REL: Float64 = 5.0e-3"),
 ]
 
 

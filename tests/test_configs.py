@@ -176,3 +176,71 @@ def test_reduced_precision_l2_after_100_steps(P, prec):
     s.close()
     print(f"P{P} {prec}: rel L2 vs FP64 after 100 steps {err:.2e}")
     assert err <= (1e-6 if P == 3 else 2e-6), err
+
+
+def alfven_case():
+    """benchmarks/bench_mhd_alfven_3d_p3.mojo: 16 x 4 x 4 periodic slab, P=3,
+    one Alfven period with dt = CFL h / (max(c_f, c_h) (2P+1))."""
+    nx, ny, nz, lx, ly, lz = G["mhd_alfven_3d_p3.mesh"]
+    gamma, rho0, b0, p0, amp = G["mhd_alfven_3d_p3.gamma_rho0_b0_p0_amp"]
+    c_h, alpha_d = G["mhd_alfven_3d_p3.c_h_alpha_d"]
+    ph = M.IdealMHD(gamma, 1e-6, 1e-6, c_h, alpha_d)
+    cf = np.sqrt(gamma * p0 / rho0 + (b0 * b0 + amp * amp) / rho0)
+    P = 3
+    dt_est = G["mhd_alfven_3d_p3.cfl"] * (lx / nx) / (max(cf, c_h) * (2 * P + 1))
+    nsteps = int(1.0 / dt_est) + 1
+    mesh = (int(nx), int(ny), int(nz)), (lx, ly, lz)
+    return ph, P, mesh, 1.0 / nsteps, nsteps, (rho0, b0, p0, amp, 1.0)
+
+
+def alfven_state(xyz, gamma, rho0, b0, p0, amp, k, lx=1.0):
+    s = np.sin(2 * np.pi * k * xyz[..., 0] / lx)
+    q = np.zeros(xyz.shape[:-1] + (9,))
+    v, by = amp * s, -amp * np.sqrt(rho0) * s
+    q[..., 0], q[..., 2] = rho0, rho0 * v
+    q[..., 4] = p0 / (gamma - 1) + 0.5 * rho0 * v * v + 0.5 * (b0 * b0 + by * by)
+    q[..., 5], q[..., 6] = b0, by
+    return q
+
+
+_ALFVEN_ORACLE = {}
+
+
+def alfven_oracle(oracle_mod):
+    """(initial state, state after one period) of the FP64 oracle, computed once."""
+    if "q" not in _ALFVEN_ORACLE:
+        ph, P, (n, L), dt, nsteps, prm = alfven_case()
+        o = oracle_mod.Oracle3D(P, n, L, M.physics_dict(ph))
+        q0 = alfven_state(o.node_xyz(), ph.gamma, *prm)
+        o.set(q0)
+        o.step(dt, nsteps)
+        _ALFVEN_ORACLE["q0"], _ALFVEN_ORACLE["q"] = q0, o.get()
+    return _ALFVEN_ORACLE["q0"], _ALFVEN_ORACLE["q"]
+
+
+def test_mhd_alfven_gate_oracle(oracle_mod):
+    """The oracle's ideal MHD passes the reference bench's one-period gate."""
+    q0, q = alfven_oracle(oracle_mod)
+    assert np.isfinite(q).all()
+    assert rel_l2(q, q0) < G["mhd_alfven_3d_p3.l2_max_rel"], rel_l2(q, q0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f64", "f32", "mixed"])
+def test_mhd_alfven_gate_product(oracle_mod, prec):
+    ph, P, (n, L), dt, nsteps, prm = alfven_case()
+    s = M.Solver(M.Mesh(*n, *L), ph, P=P, precision=prec)
+    s.fill_ic(M.IC_ALFVEN, list(prm))
+    q0 = s.download_state().astype(np.float64)
+    assert rel_l2(q0, alfven_state(s.node_xyz(), ph.gamma, *prm)) < (1e-14 if prec == "f64" else 1e-7)
+    s.step_n(dt, nsteps)
+    q = s.download_state().astype(np.float64)
+    s.close()
+    assert np.isfinite(q).all()
+    err = rel_l2(q, q0)
+    assert err < G["mhd_alfven_3d_p3.l2_max_rel"], err
+    q0o, qo = alfven_oracle(oracle_mod)
+    assert rel_l2(q0, q0o) < (1e-14 if prec == "f64" else 1e-7)
+    d = rel_l2(q, qo)
+    print(f"alfven {prec}: rel L2 vs IC {err:.3e}, vs oracle FP64 {d:.2e}")
+    assert d < (1e-10 if prec == "f64" else 2e-4)
