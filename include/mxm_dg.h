@@ -44,12 +44,17 @@ extern "C" {
 #define MXM_DG_ENOTREADY (-6)  /* request not finished yet (serving poll)    */
 
 /* Physics kinds: src/advection.mojo, src/euler.mojo, src/maxwell.mojo,
- * src/shallow_water.mojo, src/mhd.mojo (IdealMHD, 3D only). */
+ * src/shallow_water.mojo, src/mhd.mojo.  MHD in 3D is IdealMHD (9
+ * components); in 2D it is the GLM stack of src/local_mesh_2d_gpu_mhd_glm.mojo
+ * (7 components: rho, mx, my, Bx, By, E, psi; psi *= exp(-alpha_d dt) after
+ * every SSPRK3 step).  MHD_PLAIN is the 2D stack without cleaning,
+ * src/local_mesh_2d_gpu_mhd.mojo (6 components, 2D only). */
 #define MXM_DG_PHYS_ADVECTION 0
 #define MXM_DG_PHYS_EULER 1
 #define MXM_DG_PHYS_MAXWELL 2
 #define MXM_DG_PHYS_SHALLOW_WATER 3
 #define MXM_DG_PHYS_MHD 4
+#define MXM_DG_PHYS_MHD_PLAIN 5
 
 /* Numerical fluxes.  3D Euler: FLUX_RUSANOV..FLUX_HLLEC (euler.mojo:33-36).
  * 2D Euler: RUSANOV (|v|+c speed, local_mesh_2d_gpu_euler.mojo:220-337),
@@ -88,7 +93,9 @@ extern "C" {
  *  MHD (mhd.mojo:202-254): p = {gamma, min_density, min_pressure, c_h,
  *        alpha_d, inflow_rho, inflow_rhou, inflow_rhov, inflow_rhow,
  *        inflow_E, inflow_Bx, inflow_By, inflow_Bz, inflow_psi}; 9 components
- *        [rho, rho u, rho v, rho w, E, Bx, By, Bz, psi] */
+ *        [rho, rho u, rho v, rho w, E, Bx, By, Bz, psi].  2D MHD and
+ *        MHD_PLAIN use the same layout (rhow and Bz unused; c_h, alpha_d and
+ *        psi only with GLM). */
 typedef struct mxm_dg_physics_desc {
   int32_t kind;
   int32_t flux_type;
@@ -227,9 +234,9 @@ int mxm_dg_selftest_wait_timeout(double limit_ms, int32_t* gave_up, double* wait
  *   DAM_BREAK   shallow water at rest: hL, hR, x0, width
  *   CAVITY      Maxwell: mx, my, amp: E_z = amp sin(mx pi x/Lx) sin(my pi y/Ly)
  *   PLANE_WAVE  Maxwell: amp, k: E_z = amp sin(2 pi k x/Lx), B_y = -E_z/c
- *   ALFVEN      MHD: rho0, B0, p0, amp, k: right-going Alfven wave along x,
- *               v = amp sin(2 pi k x/Lx), B = (B0, -amp sqrt(rho0) sin(.), 0),
- *               psi = 0 (benchmarks/bench_mhd_alfven_3d_p3.mojo:68-102) */
+ *   ALFVEN      MHD (3D and 2D): rho0, B0, p0, amp, k: right-going Alfven
+ *               wave along x, v = amp sin(2 pi k x/Lx), B = (B0, -amp sqrt(rho0)
+ *               sin(.), 0), psi = 0 (benchmarks/bench_mhd_alfven_3d_p3.mojo:68-102) */
 #define MXM_DG_IC_CONSTANT 0
 #define MXM_DG_IC_SINE_WAVE 1
 #define MXM_DG_IC_VORTEX 2

@@ -29,7 +29,7 @@ LIB_PATH = os.path.join(_HERE, "libmxm_dg.so")
 
 # include/mxm_dg.h constants
 OK, EINVAL, ENOMEM, ECUDA, ENONFINITE, ETIMEDOUT, ENOTREADY = 0, -1, -2, -3, -4, -5, -6
-PHYS_ADVECTION, PHYS_EULER, PHYS_MAXWELL, PHYS_SHALLOW_WATER, PHYS_MHD = 0, 1, 2, 3, 4
+PHYS_ADVECTION, PHYS_EULER, PHYS_MAXWELL, PHYS_SHALLOW_WATER, PHYS_MHD, PHYS_MHD_PLAIN = 0, 1, 2, 3, 4, 5
 FLUX_RUSANOV, FLUX_ROE, FLUX_HLLE, FLUX_HLLEC, FLUX_HLLC, FLUX_HLL = 0, 1, 2, 3, 4, 5
 BC_INTERIOR, BC_WALL, BC_OUTFLOW, BC_INFLOW = 0, 1, 2, 3
 PREC = {"f64": 0, "f32": 1, "mixed": 2}
@@ -274,6 +274,15 @@ class IdealMHD:  # src/mhd.mojo:199-254 (3D; q = [rho, rho u, rho v, rho w, E, B
         return [self.gamma, self.min_density, self.min_pressure, self.c_h, self.alpha_d, self.inflow_rho,
                 self.inflow_rhou, self.inflow_rhov, self.inflow_rhow, self.inflow_E, self.inflow_Bx, self.inflow_By,
                 self.inflow_Bz, self.inflow_psi]
+
+
+@dataclass
+class IdealMHDPlain(IdealMHD):
+    """2D ideal MHD without divergence cleaning (src/local_mesh_2d_gpu_mhd.mojo):
+    state (rho, mx, my, Bx, By, E); c_h, alpha_d and psi are unused.  An
+    IdealMHD on a 2D mesh is the GLM stack (src/local_mesh_2d_gpu_mhd_glm.mojo)
+    with state (rho, mx, my, Bx, By, E, psi)."""
+    kind: int = field(default=PHYS_MHD_PLAIN, init=False)
 
 
 def physics_dict(ph):

@@ -382,6 +382,8 @@ int mxm_dg_batch_add(void* batch, void* solver, double dt, int32_t* index) {
   mxm::Handle* h = (mxm::Handle*)solver;
   if (!h) throw mxm::ArgError("null solver handle");
   if (h->dim != 2) throw mxm::ArgError("batched solves are 2D (triangle meshes)");
+  if (h->phys.kind == MXM_DG_PHYS_MHD || h->phys.kind == MXM_DG_PHYS_MHD_PLAIN)
+    throw mxm::ArgError("2D MHD solves are not batched (run them through their own handles)");
   if (h->device != b->device) throw mxm::ArgError("solver lives on another device than the batch");
   if (!(dt > 0.0)) throw mxm::ArgError("dt must be positive");
   if (b->rbytes && h->rbytes != b->rbytes) throw mxm::ArgError("all solves of a batch share one precision");

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -159,6 +160,16 @@ MhdD<R> make_mhd(const double* p) {  // mxm_dg_physics_desc field order (mhd.moj
   return ph;
 }
 
+// 2D MHD from the same layout: state (rho, mx, my, Bx, By, E[, psi])
+template <class R, bool GLM>
+Mhd2D<R, GLM> make_mhd2d(const double* p) {
+  Mhd2D<R, GLM> ph;
+  ph.gamma = R(p[0]); ph.rho_min = R(p[1]); ph.p_min = R(p[2]); ph.c_h = R(p[3]);
+  const int map[7] = {5, 6, 7, 10, 11, 9, 13};
+  for (int k = 0; k < 7; ++k) ph.inflow[k] = R(p[map[k]]);
+  return ph;
+}
+
 template <class R>
 cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double b, double c,
                          double dt, int rhs_only) {
@@ -278,6 +289,8 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
       for (int k = 0; k < 6; ++k) ph.inflow[k] = R(p[7 + k]);
       return launch_stage2d<R>(h->P, ar, t, ph, h->nsm, h->stream);
     }
+    case MXM_DG_PHYS_MHD: return launch_stage2d<R>(h->P, ar, t, make_mhd2d<R, true>(p), h->nsm, h->stream);
+    case MXM_DG_PHYS_MHD_PLAIN: return launch_stage2d<R>(h->P, ar, t, make_mhd2d<R, false>(p), h->nsm, h->stream);
   }
   return cudaErrorInvalidValue;
 }
@@ -353,6 +366,9 @@ cudaError_t wavespeed_launch(Handle* h, const void* qi, unsigned long long* out)
       ph.c = R(p[0]);
       return launch_wavespeed2d<R>((const R*)qi, nn, ph, out, h->stream);
     }
+    case MXM_DG_PHYS_MHD: return launch_wavespeed2d<R>((const R*)qi, nn, make_mhd2d<R, true>(p), out, h->stream);
+    case MXM_DG_PHYS_MHD_PLAIN:
+      return launch_wavespeed2d<R>((const R*)qi, nn, make_mhd2d<R, false>(p), out, h->stream);
   }
   return cudaErrorInvalidValue;
 }
@@ -402,8 +418,23 @@ void rk_stage(Handle* h, int s, double dt) {
 }
 
 void step_n(Handle* h, double dt, int n) {
-  for (int k = 0; k < n; ++k)
+  // 2D GLM-MHD: psi *= exp(-alpha_d dt) once per SSPRK3 step, operator-split
+  // after the step (local_mesh_2d_gpu_mhd_glm.mojo:464-485); the factor as
+  // the reference forms it: FP64 exp of the (FP32 in the FP32 paths) inputs
+  const bool damp = h->dim == 2 && h->phys.kind == MXM_DG_PHYS_MHD && h->phys.p[4] > 0.0;
+  double decay = 1.0;
+  if (damp) {
+    const double ad = h->rbytes == 8 ? h->phys.p[4] : double(float(h->phys.p[4]));
+    const double dd = h->rbytes == 8 ? dt : double(float(dt));
+    decay = std::exp(-ad * dd);
+  }
+  for (int k = 0; k < n; ++k) {
     for (int s = 0; s < 3; ++s) rk_stage(h, s, dt);
+    if (damp) {
+      cudaError_t e = launch_scale_component(h->q[0], h->rbytes, h->ne * h->NP, h->NC, h->NC - 1, decay, h->stream);
+      if (e != cudaSuccess) throw CudaError(e, "psi damping launch");
+    }
+  }
 }
 
 // Float32 node coordinates exactly as the reference builds elem_node_xyz.
@@ -467,7 +498,7 @@ void fill_ic(Handle* h, int which, int kind, const double* params, int nparams) 
                    k == MXM_DG_PHYS_EULER) ||
                   (kind == MXM_DG_IC_DAM_BREAK && k == MXM_DG_PHYS_SHALLOW_WATER) ||
                   ((kind == MXM_DG_IC_CAVITY || kind == MXM_DG_IC_PLANE_WAVE) && k == MXM_DG_PHYS_MAXWELL) ||
-                  (kind == MXM_DG_IC_ALFVEN && k == MXM_DG_PHYS_MHD);
+                  (kind == MXM_DG_IC_ALFVEN && (k == MXM_DG_PHYS_MHD || k == MXM_DG_PHYS_MHD_PLAIN));
   if (!ok) throw ArgError("initial-condition kind does not match the physics");
   IcArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -523,8 +554,8 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   if (P < 1 || P > 5) throw ArgError("order P must be in 1..5");
   if (prec != MXM_DG_PREC_F64 && prec != MXM_DG_PREC_F32 && prec != MXM_DG_PREC_MIXED)
     throw ArgError("precision must be MXM_DG_PREC_F64, MXM_DG_PREC_F32 or MXM_DG_PREC_MIXED");
-  if (ph->kind < 0 || ph->kind > MXM_DG_PHYS_MHD) throw ArgError("unknown physics kind");
-  if (ph->kind == MXM_DG_PHYS_MHD && m->dim != 3) throw ArgError("MHD physics is 3D only");
+  if (ph->kind < 0 || ph->kind > MXM_DG_PHYS_MHD_PLAIN) throw ArgError("unknown physics kind");
+  if (ph->kind == MXM_DG_PHYS_MHD_PLAIN && m->dim != 2) throw ArgError("MHD_PLAIN physics is 2D only");
   if (m->nx < 1 || m->ny < 1 || (m->dim == 3 && m->nz < 1)) throw ArgError("cell counts must be >= 1");
   for (int k = 0; k < 2 * m->dim; ++k)
     if (m->bc[k] < 0 || m->bc[k] > 3) throw ArgError("bc codes must be 0..3");
@@ -551,7 +582,8 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   h->NC = ph->kind == MXM_DG_PHYS_ADVECTION ? 1
         : ph->kind == MXM_DG_PHYS_EULER     ? (m->dim == 3 ? 5 : 4)
         : ph->kind == MXM_DG_PHYS_MAXWELL   ? 6
-        : ph->kind == MXM_DG_PHYS_MHD       ? 9
+        : ph->kind == MXM_DG_PHYS_MHD       ? (m->dim == 3 ? 9 : 7)
+        : ph->kind == MXM_DG_PHYS_MHD_PLAIN ? 6
                                             : 3;
   h->ntypes = m->dim == 3 ? 6 : 2;
   h->ncell = int64_t(h->nx) * h->ny * h->nz;

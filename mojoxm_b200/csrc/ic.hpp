@@ -18,5 +18,8 @@ struct IcArgs {
 };
 
 cudaError_t launch_ic(const IcArgs& a, void* q, size_t rbytes, cudaStream_t st);
+// q[node * NC + c] *= f for every node (FP32 states multiply by float(f))
+cudaError_t launch_scale_component(void* q, size_t rbytes, int64_t nnodes, int NC, int c, double f,
+                                   cudaStream_t st);
 
 }  // namespace mxm

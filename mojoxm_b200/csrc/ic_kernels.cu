@@ -104,9 +104,13 @@ __global__ void ic_kernel(IcArgs a, R* q) {
     case MXM_DG_IC_ALFVEN: {  // MHD: right-going Alfven wave along x (bench_mhd_alfven_3d_p3.mojo:68-102)
       const double sn = sin(2.0 * kPi * p[4] * x[0] / a.L[0]);
       const double rho = p[0], bx = p[1], v = p[3] * sn, by = -p[3] * sqrt(rho) * sn;
+      const double E = p[2] / g1 + 0.5 * rho * v * v + 0.5 * (bx * bx + by * by);
       s[0] = rho; s[2] = rho * v;
-      s[4] = p[2] / g1 + 0.5 * rho * v * v + 0.5 * (bx * bx + by * by);
-      s[5] = bx; s[6] = by;
+      if (e3) {  // (rho, m, E, B, psi)
+        s[4] = E; s[5] = bx; s[6] = by;
+      } else {   // (rho, mx, my, Bx, By, E[, psi])
+        s[3] = bx; s[4] = by; s[5] = E;
+      }
       break;
     }
   }
@@ -115,6 +119,21 @@ __global__ void ic_kernel(IcArgs a, R* q) {
 }
 
 }  // namespace
+
+template <class R>
+__global__ void scale_component_kernel(R* q, int64_t nnodes, int NC, int c, R f) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < nnodes) q[i * NC + c] = q[i * NC + c] * f;
+}
+
+cudaError_t launch_scale_component(void* q, size_t rbytes, int64_t nnodes, int NC, int c, double f,
+                                   cudaStream_t st) {
+  const int nb = int((nnodes + 255) / 256);
+  if (nb == 0) return cudaSuccess;
+  if (rbytes == 8) scale_component_kernel<double><<<nb, 256, 0, st>>>((double*)q, nnodes, NC, c, f);
+  else scale_component_kernel<float><<<nb, 256, 0, st>>>((float*)q, nnodes, NC, c, float(f));
+  return cudaGetLastError();
+}
 
 cudaError_t launch_ic(const IcArgs& a, void* q, size_t rbytes, cudaStream_t st) {
   const int64_t n = a.ne * a.NP;

@@ -67,6 +67,7 @@ cudaError_t launch_limiter(int dim, int P, int NC, const LimArgs<R>& a, const Ku
       case 3: return lim_nc<R, 2, 3>(P, a, t3, t2, st);
       case 4: return lim_nc<R, 2, 4>(P, a, t3, t2, st);
       case 6: return lim_nc<R, 2, 6>(P, a, t3, t2, st);
+      case 7: return lim_nc<R, 2, 7>(P, a, t3, t2, st);
     }
   }
   return cudaErrorInvalidValue;
@@ -92,6 +93,7 @@ cudaError_t red_nc(int NC, const R* q, const R* w, int64_t ne, int c, int kind, 
     case 4: return red_np<R, NP, 4>(q, w, ne, c, kind, scale, partial, npartial, out, st);
     case 5: return red_np<R, NP, 5>(q, w, ne, c, kind, scale, partial, npartial, out, st);
     case 6: return red_np<R, NP, 6>(q, w, ne, c, kind, scale, partial, npartial, out, st);
+    case 7: return red_np<R, NP, 7>(q, w, ne, c, kind, scale, partial, npartial, out, st);
     case 9: return red_np<R, NP, 9>(q, w, ne, c, kind, scale, partial, npartial, out, st);
   }
   return cudaErrorInvalidValue;

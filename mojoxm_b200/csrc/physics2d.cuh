@@ -7,6 +7,9 @@
 //   SW      src/local_mesh_2d_gpu_sw.mojo:27-176 (vol), :178-306 (Rusanov), :308-450 (HLL)
 //   Maxwell src/local_mesh_2d_gpu_maxwell.mojo:31-218 (vol), :219-377 (Rusanov + PEC)
 //   Advect. src/local_mesh_2d_gpu_advection.mojo:117-182 (vol), :249-300 (upwind)
+//   MHD     src/local_mesh_2d_gpu_mhd.mojo (6 components, no cleaning) and
+//           src/local_mesh_2d_gpu_mhd_glm.mojo (7, GLM psi; psi damping is
+//           operator-split per SSPRK3 step, outside the stage)
 #pragma once
 #include "physics.cuh"
 
@@ -250,6 +253,76 @@ struct Maxwell2D {
     s[3] = -M[0]; s[4] = -M[1]; s[5] = -M[2];
   }
   __device__ R speed(const R*) const { return c; }
+};
+
+// 2D ideal MHD, state (rho, mx, my, Bx, By, E[, psi]).  Rusanov against
+// |v| + c_f (c_f from Bx^2, as the reference writes it) and, with GLM, c_h.
+template <class R, bool GLM>
+struct Mhd2D {
+  static constexpr int NC = GLM ? 7 : 6;
+  static constexpr bool kSource = false;
+  R gamma, rho_min, p_min, c_h, inflow[7];
+  // physical fluxes and the Rusanov speed of one state
+  // (local_mesh_2d_gpu_mhd.mojo:73-102 / _glm.mojo:89-124; speeds :321-331 / :355-363)
+  __device__ R flux_speed(const R* q, R* Fx, R* Fy) const {
+    R rho = q[0];
+    if (rho < rho_min) rho = rho_min;
+    const R ri = pos_rcp(rho);
+    const R mx = q[1], my = q[2], Bx = q[3], By = q[4], E = q[5];
+    const R u = mx * ri, v = my * ri, BB = Bx * Bx + By * By;
+    const R ke = R(0.5) * (mx * mx + my * my) * ri;
+    R p = (gamma - R(1)) * (E - ke - R(0.5) * BB);
+    if (p < p_min) p = p_min;
+    const R ps = p + R(0.5) * BB, ub = u * Bx + v * By;
+    const R psi = GLM ? q[NC - 1] : R(0);
+    Fx[0] = mx; Fx[1] = mx * u + ps - Bx * Bx; Fx[2] = mx * v - Bx * By; Fx[3] = psi;
+    Fx[4] = u * By - v * Bx; Fx[5] = (E + ps) * u - Bx * ub;
+    Fy[0] = my; Fy[1] = my * u - By * Bx; Fy[2] = my * v + ps - By * By; Fy[3] = v * Bx - u * By;
+    Fy[4] = psi; Fy[5] = (E + ps) * v - By * ub;
+    if (GLM) {
+      const R ch2 = c_h * c_h;
+      Fx[NC - 1] = ch2 * Bx;
+      Fy[NC - 1] = ch2 * By;
+    }
+    const R cs2 = gamma * p * ri, ca2 = BB * ri, sm = cs2 + ca2;
+    R disc = sm * sm - R(4) * cs2 * (Bx * Bx) * ri;
+    if (disc < R(0)) disc = R(0);
+    R sp = sqrt(u * u + v * v) + sqrt(R(0.5) * (sm + sqrt(disc)));
+    if (GLM && c_h > sp) sp = c_h;
+    return sp;
+  }
+  __device__ void flux(const R* q, R* Fx, R* Fy) const { (void)flux_speed(q, Fx, Fy); }
+  __device__ void face(const R* qL, const R* qRin, int bc, R nx, R ny, R* f) const {
+    R qR[NC];
+    if (bc == BC_INTERIOR) {
+#pragma unroll
+      for (int k = 0; k < NC; ++k) qR[k] = qRin[k];
+    } else if (bc == BC_WALL) {  // conducting slip wall: reflect m_n and B_n (GLM: psi too)
+      const R mn = qL[1] * nx + qL[2] * ny, bn = qL[3] * nx + qL[4] * ny;
+      qR[0] = qL[0]; qR[1] = qL[1] - R(2) * mn * nx; qR[2] = qL[2] - R(2) * mn * ny;
+      qR[3] = qL[3] - R(2) * bn * nx; qR[4] = qL[4] - R(2) * bn * ny; qR[5] = qL[5];
+      if (GLM) qR[NC - 1] = -qL[NC - 1];
+    } else if (bc == BC_INFLOW) {
+#pragma unroll
+      for (int k = 0; k < NC; ++k) qR[k] = inflow[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < NC; ++k) qR[k] = qL[k];
+    }
+    R FxL[NC], FyL[NC], FxR[NC], FyR[NC];
+    const R sL = flux_speed(qL, FxL, FyL), sR = flux_speed(qR, FxR, FyR);
+    const R al = sL > sR ? sL : sR, h = R(0.5);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) f[k] = h * ((FxL[k] + FxR[k]) * nx + (FyL[k] + FyR[k]) * ny) - h * al * (qR[k] - qL[k]);
+  }
+  __device__ void source(const R*, R* s) const {
+#pragma unroll
+    for (int k = 0; k < NC; ++k) s[k] = R(0);
+  }
+  __device__ R speed(const R* q) const {
+    R Fx[NC], Fy[NC];
+    return flux_speed(q, Fx, Fy);
+  }
 };
 
 }  // namespace mxm

@@ -83,7 +83,8 @@ int nc_of(const mxm_dg_physics_desc& p, int dim) {
   return p.kind == MXM_DG_PHYS_ADVECTION ? 1
        : p.kind == MXM_DG_PHYS_EULER     ? (dim == 3 ? 5 : 4)
        : p.kind == MXM_DG_PHYS_MAXWELL   ? 6
-       : p.kind == MXM_DG_PHYS_MHD       ? 9
+       : p.kind == MXM_DG_PHYS_MHD       ? (dim == 3 ? 9 : 7)
+       : p.kind == MXM_DG_PHYS_MHD_PLAIN ? 6
                                          : 3;
 }
 
@@ -314,8 +315,8 @@ int mxm_dg_server_submit(void* server, const mxm_dg_mesh_desc* mesh, const mxm_d
   if (nparams < 0 || nparams > 16 || (nparams > 0 && !ic_params)) throw mxm::ArgError("nparams must be 0..16");
   if (!(dt > 0.0) || nsteps < 0) throw mxm::ArgError("dt > 0 and nsteps >= 0");
   if (P < 1 || P > 5 || (mesh->dim != 2 && mesh->dim != 3) || precision < 0 || precision > 2 || phys->kind < 0 ||
-      phys->kind > MXM_DG_PHYS_MHD || mesh->nx < 1 || mesh->ny < 1 || (mesh->dim == 3 && mesh->nz < 1))
-    throw mxm::ArgError("order 1..5, dim 2 or 3, precision 0..2, physics kind 0..4, cell counts >= 1");
+      phys->kind > MXM_DG_PHYS_MHD_PLAIN || mesh->nx < 1 || mesh->ny < 1 || (mesh->dim == 3 && mesh->nz < 1))
+    throw mxm::ArgError("order 1..5, dim 2 or 3, precision 0..2, physics kind 0..5, cell counts >= 1");
   std::unique_ptr<mxm::Request> r(new mxm::Request);
   r->mesh = *mesh;
   r->phys = *phys;

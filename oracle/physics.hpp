@@ -14,7 +14,9 @@
 
 namespace orc {
 
-enum { PHYS_ADVECTION = 0, PHYS_EULER = 1, PHYS_MAXWELL = 2, PHYS_SW = 3, PHYS_MHD = 4 };
+// PHYS_MHD: 3D IdealMHD (9 components); in 2D the GLM stack (7 components).
+// PHYS_MHD_PLAIN: the 2D stack without divergence cleaning (6 components).
+enum { PHYS_ADVECTION = 0, PHYS_EULER = 1, PHYS_MAXWELL = 2, PHYS_SW = 3, PHYS_MHD = 4, PHYS_MHD_PLAIN = 5 };
 enum { FLUX_RUSANOV = 0, FLUX_ROE = 1, FLUX_HLLE = 2, FLUX_HLLEC = 3, FLUX_HLLC = 4, FLUX_HLL = 5 };
 
 template <typename R>

@@ -133,12 +133,16 @@ template <typename R>
 struct Phys2D {
   int kind, flux;
   R gamma = R(1.4), min_density = R(0), min_pressure = R(0), gx = R(0), gy = R(0);
-  R inflow[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+  R inflow[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
+  R c_h = R(0), alpha_d = R(0);              // 2D MHD (GLM)
   R vx = R(0), vy = R(0), inflow_q = R(0);  // advection
   R g = R(9.81), h_min = R(0);              // shallow water
   R c = R(1), J[3] = {R(0), R(0), R(0)}, M[3] = {R(0), R(0), R(0)};
   bool entropy_fix = false;
-  int nc() const { return kind == PHYS_ADVECTION ? 1 : kind == PHYS_EULER ? 4 : kind == PHYS_MAXWELL ? 6 : 3; }
+  int nc() const {
+    return kind == PHYS_ADVECTION ? 1 : kind == PHYS_EULER ? 4 : kind == PHYS_MAXWELL ? 6
+         : kind == PHYS_MHD ? 7 : kind == PHYS_MHD_PLAIN ? 6 : 3;
+  }
 
   // Ghost state for BC faces; identical plumbing in every 2D face kernel.
   void ghost(const R* qL, int bc, R nx, R ny, R* qR) const {
@@ -154,6 +158,12 @@ struct Phys2D {
         R En = qL[0] * nx + qL[1] * ny, Bn = qL[3] * nx + qL[4] * ny;
         qR[0] = R(2) * En * nx - qL[0]; qR[1] = R(2) * En * ny - qL[1]; qR[2] = -qL[2];
         qR[3] = qL[3] - R(2) * Bn * nx; qR[4] = qL[4] - R(2) * Bn * ny; qR[5] = qL[5];
+      } else if (kind == PHYS_MHD || kind == PHYS_MHD_PLAIN) {
+        // local_mesh_2d_gpu_mhd.mojo:276-284, _mhd_glm.mojo:296-305 (psi reflects)
+        R mn = qL[1] * nx + qL[2] * ny, bn = qL[3] * nx + qL[4] * ny;
+        qR[0] = qL[0]; qR[1] = qL[1] - R(2) * mn * nx; qR[2] = qL[2] - R(2) * mn * ny;
+        qR[3] = qL[3] - R(2) * bn * nx; qR[4] = qL[4] - R(2) * bn * ny; qR[5] = qL[5];
+        if (kind == PHYS_MHD) qR[6] = -qL[6];
       }
     } else if (bc == BC_INFLOW) {
       for (int k = 0; k < n; ++k) qR[k] = inflow[k];
@@ -164,7 +174,7 @@ struct Phys2D {
 
   void face_flux(const R* qL, const R* qRin, int bc, R nx, R ny, R* f) const {
     const int n = nc();
-    R qR[6];
+    R qR[8];
     if (kind == PHYS_ADVECTION) {  // local_mesh_2d_gpu_advection.mojo:249-300
       R vn = vx * nx + vy * ny;
       if (bc == BC_INTERIOR) f[0] = vn >= R(0) ? vn * qL[0] : vn * qRin[0];
@@ -243,6 +253,33 @@ struct Phys2D {
       f[0] = f3[0]; f[1] = f3[1]; f[2] = f3[2]; f[3] = f3[4];
       return;
     }
+    if (kind == PHYS_MHD || kind == PHYS_MHD_PLAIN) {
+      // Rusanov against |v| + c_f (c_f with Bx^2), and c_h for GLM:
+      // local_mesh_2d_gpu_mhd.mojo:301-378, local_mesh_2d_gpu_mhd_glm.mojo:325-413
+      const bool glm = kind == PHYS_MHD;
+      R FxL[7], FyL[7], FxR[7], FyR[7];
+      vol_flux(qL, FxL, FyL);
+      vol_flux(qR, FxR, FyR);
+      auto speed = [&](const R* q) {
+        R rho = q[0];
+        if (rho < min_density) rho = min_density;
+        R u = q[1] / rho, v = q[2] / rho, BB = q[3] * q[3] + q[4] * q[4];
+        R ke = R(0.5) * (q[1] * q[1] + q[2] * q[2]) / rho;
+        R pr = (gamma - R(1)) * (q[5] - ke - R(0.5) * BB);
+        if (pr < min_pressure) pr = min_pressure;
+        R cs2 = gamma * pr / rho, ca2 = BB / rho, sm = cs2 + ca2;
+        R disc = sm * sm - R(4) * cs2 * (q[3] * q[3]) / rho;
+        if (disc < R(0)) disc = R(0);
+        R cf = std::sqrt(R(0.5) * (sm + std::sqrt(disc)));
+        R sp = std::sqrt(u * u + v * v) + cf;
+        if (glm && c_h > sp) sp = c_h;
+        return sp;
+      };
+      R sL = speed(qL), sR = speed(qR);
+      R al = sL > sR ? sL : sR;
+      for (int k = 0; k < n; ++k) f[k] = h * ((FxL[k] + FxR[k]) * nx + (FyL[k] + FyR[k]) * ny) - h * al * (qR[k] - qL[k]);
+      return;
+    }
     if (kind == PHYS_SW) {
       R hL = qL[0] < h_min ? h_min : qL[0], hR = qR[0] < h_min ? h_min : qR[0];
       R uL = qL[1] / hL, vL = qL[2] / hL, uR = qR[1] / hR, vR = qR[2] / hR;
@@ -306,12 +343,31 @@ struct Phys2D {
       Fy[0] = q[2]; Fy[1] = q[2] * u; Fy[2] = q[2] * v + p;
       return;
     }
+    if (kind == PHYS_MHD || kind == PHYS_MHD_PLAIN) {
+      // (rho, mx, my, Bx, By, E[, psi]): local_mesh_2d_gpu_mhd.mojo:73-102, _mhd_glm.mojo:89-124
+      R rho = q[0];
+      if (rho < min_density) rho = min_density;
+      R mx = q[1], my = q[2], Bx = q[3], By = q[4], E = q[5];
+      R u = mx / rho, v = my / rho, BB = Bx * Bx + By * By;
+      R ke = R(0.5) * (mx * mx + my * my) / rho, mp = R(0.5) * BB;
+      R pr = (gamma - R(1)) * (E - ke - mp);
+      if (pr < min_pressure) pr = min_pressure;
+      R ps = pr + R(0.5) * BB;
+      const bool glm = kind == PHYS_MHD;
+      R psi = glm ? q[6] : R(0), ch2 = c_h * c_h;
+      Fx[0] = mx; Fx[1] = mx * u + ps - Bx * Bx; Fx[2] = mx * v - Bx * By; Fx[3] = glm ? psi : R(0);
+      Fx[4] = u * By - v * Bx; Fx[5] = (E + ps) * u - Bx * (u * Bx + v * By);
+      Fy[0] = my; Fy[1] = my * u - By * Bx; Fy[2] = my * v + ps - By * By; Fy[3] = v * Bx - u * By;
+      Fy[4] = glm ? psi : R(0); Fy[5] = (E + ps) * v - By * (u * Bx + v * By);
+      if (glm) { Fx[6] = ch2 * Bx; Fy[6] = ch2 * By; }
+      return;
+    }
     R c2 = c * c;  // maxwell 2D vol  local_mesh_2d_gpu_maxwell.mojo:31-218
     Fx[0] = R(0); Fx[1] = c2 * q[5]; Fx[2] = -c2 * q[4]; Fx[3] = R(0); Fx[4] = -q[2]; Fx[5] = q[1];
     Fy[0] = -c2 * q[5]; Fy[1] = R(0); Fy[2] = c2 * q[3]; Fy[3] = q[2]; Fy[4] = R(0); Fy[5] = -q[0];
   }
   void source(const R* q, R* s) const {
-    for (int k = 0; k < 6; ++k) s[k] = R(0);
+    for (int k = 0; k < 8; ++k) s[k] = R(0);
     if (kind == PHYS_EULER) {
       R rho = q[0] < min_density ? min_density : q[0];
       s[1] = rho * gx;
@@ -390,9 +446,10 @@ struct Solver2D : Solver2DBase {
       int64_t e = t / NP;
       int i = int(t % NP);
       const R* iJ = &mesh.elem_invJ[e * 4];
-      R acc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)}, fc[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+      R acc[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
+      R fc[8] = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
       for (int j = 0; j < NP; ++j) {
-        R Fx[6], Fy[6];
+        R Fx[8], Fy[8];
         ph.vol_flux(qi + (e * NP + j) * NC, Fx, Fy);
         R dr = Dr[i * NP + j], ds = Ds[i * NP + j];
         for (int c = 0; c < NC; ++c)
@@ -408,7 +465,7 @@ struct Solver2D : Solver2DBase {
           for (int c = 0; c < NC; ++c) fc[c] += sLf * fstar[(fid * NFP + m) * NC + c];
         }
       }
-      R src[6];
+      R src[8];
       ph.source(qi + (e * NP + i) * NC, src);
       R i2A = mesh.elem_inv_2A[e];
       for (int c = 0; c < NC; ++c) {
@@ -490,6 +547,13 @@ struct Solver2D : Solver2DBase {
   }
   void step(double dt) override {
     for (int s = 0; s < 3; ++s) stage(s, dt);
+    // GLM psi damping, operator-split once per step: psi *= exp(-alpha_d dt)
+    // (local_mesh_2d_gpu_mhd_glm.mojo:464-485, examples/mhd_alfven_glm_2d_gpu.mojo:240-241)
+    if (ph.kind == PHYS_MHD && ph.alpha_d > R(0)) {
+      const R decay = R(std::exp(-double(ph.alpha_d) * double(R(dt))));
+      R* q0 = q[0].data();
+      for (int64_t t = 0; t < Ne * NP; ++t) q0[t * 7 + 6] = q0[t * 7 + 6] * decay;
+    }
   }
 };
 
@@ -514,6 +578,14 @@ Solver2DBase* make2(int P, int nx, int ny, double Lx, double Ly, const int* bcs,
   } else if (kind == PHYS_SW) {
     ph.g = R(p[0]); ph.h_min = R(p[1]);
     for (int k = 0; k < 3; ++k) ph.inflow[k] = R(p[2 + k]);
+  } else if (kind == PHYS_MHD || kind == PHYS_MHD_PLAIN) {
+    // the 3D IdealMHD parameter layout {gamma, rho_min, p_min, c_h, alpha_d,
+    // inflow rho, rhou, rhov, rhow, E, Bx, By, Bz, psi}; 2D state order
+    // (rho, mx, my, Bx, By, E[, psi])
+    ph.gamma = R(p[0]); ph.min_density = R(p[1]); ph.min_pressure = R(p[2]);
+    ph.c_h = R(p[3]); ph.alpha_d = R(p[4]);
+    ph.inflow[0] = R(p[5]); ph.inflow[1] = R(p[6]); ph.inflow[2] = R(p[7]); ph.inflow[3] = R(p[10]);
+    ph.inflow[4] = R(p[11]); ph.inflow[5] = R(p[9]); ph.inflow[6] = R(p[13]);
   } else {
     throw std::runtime_error("unknown physics kind");
   }

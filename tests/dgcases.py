@@ -36,6 +36,8 @@ PHYSICS_2D = {
     "maxwell": lambda: M.Maxwell(1.0, 0.1, -0.2, 0.05, 0.02, 0.0, -0.03, 0.1, 0.2, -0.1, 0.05, 0.0, 0.1),
     "shallow_water": lambda: M.ShallowWater(9.81, 1e-6, 1.5, 0.2, -0.1),
     "shallow_water_hll": lambda: M.ShallowWater(9.81, 1e-6, 1.5, 0.2, -0.1, flux_type=M.FLUX_HLL),
+    "mhd_glm": lambda: M.IdealMHD(5.0 / 3.0, 1e-6, 1e-6, 1.3, 0.4, 1.1, 0.2, -0.1, 0.0, 3.0, 0.3, -0.2, 0.0, 0.02),
+    "mhd_plain": lambda: M.IdealMHDPlain(5.0 / 3.0, 1e-6, 1e-6, 0.0, 0.0, 1.1, 0.2, -0.1, 0.0, 3.0, 0.3, -0.2),
 }
 
 BCS_3D = {
@@ -71,6 +73,17 @@ def random_state(shape, physics, seed, xyz=None):
             q[..., 0] = rho
             q[..., 1:3] = rho[..., None] * vel[..., :2]
             q[..., 3] = p / (GAMMA - 1) + 0.5 * rho * (vel[..., :2] ** 2).sum(-1)
+    elif k in (M.PHYS_MHD, M.PHYS_MHD_PLAIN) and nc in (6, 7):  # 2D (rho, mx, my, Bx, By, E[, psi])
+        rho = 1.0 + 0.2 * rng.uniform(-1, 1, (ne, npn))
+        vel = 0.5 * rng.uniform(-1, 1, (ne, npn, 2))
+        B = 0.5 * rng.uniform(-1, 1, (ne, npn, 2))
+        p = 1.0 + 0.2 * rng.uniform(-1, 1, (ne, npn))
+        q[..., 0] = rho
+        q[..., 1:3] = rho[..., None] * vel
+        q[..., 3:5] = B
+        q[..., 5] = p / (5.0 / 3.0 - 1) + 0.5 * rho * (vel ** 2).sum(-1) + 0.5 * (B ** 2).sum(-1)
+        if nc == 7:
+            q[..., 6] = 0.1 * rng.uniform(-1, 1, (ne, npn))
     elif k == M.PHYS_MHD:
         rho = 1.0 + 0.2 * rng.uniform(-1, 1, (ne, npn))
         vel = 0.5 * rng.uniform(-1, 1, (ne, npn, 3))

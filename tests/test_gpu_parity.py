@@ -206,3 +206,49 @@ def test_mhd_constant_state_preserved(prec):
     r = s.rhs(q)
     s.close()
     assert np.abs(r).max() <= (1e-11 if prec == "f64" else 2e-4)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("bcname", list(C.BCS_2D))
+@pytest.mark.parametrize("name", ["mhd_glm", "mhd_plain"])
+def test_mhd2d_steps(oracle_mod, name, bcname, prec):
+    """2D MHD (plain and GLM): every BC arm, three SSPRK3 steps with the
+    limiter; with GLM the psi damping exp(-alpha_d dt) after every step."""
+    P = 3
+    phys = C.PHYSICS_2D[name]()
+    s, o = make_pair(oracle_mod, phys, P, N2, L2, C.BCS_2D[bcname], prec=prec, dim=2)
+    q = C.random_state(s.shape, phys, seed=61)
+    if prec == "f32":
+        q = q.astype(np.float32).astype(np.float64)
+    s.upload_state(q)
+    o.set(q)
+    s.enable_cell_limiter(True, 0.05)
+    o.enable_limiter(True, 0.05)
+    s.step_n(2e-3, 3)
+    o.step(2e-3, 3)
+    assert C.rel_err(s.download_state(0), o.get(0)) <= (50 * C.TOL_F64_2D[P] if prec == "f64" else 1e-4)
+
+
+def test_mhd2d_batch_rejected():
+    s = M.Solver(M.Mesh(4, 4, dim=2), C.PHYSICS_2D["mhd_glm"](), P=2, precision="f32")
+    b = M.Batch()
+    with pytest.raises(M.DGError):
+        b.add(s, 1e-3)
+    b.close()
+    s.close()
+
+
+def test_mhd_wavespeed_and_integrals(oracle_mod):
+    """3D MHD: the CFL reduction (max Rusanov alpha over face nodes) and the
+    FP64 integrals of all nine components."""
+    phys = C.PHYSICS_3D["mhd"]()
+    s, o = make_pair(oracle_mod, phys, 3, N3, L3, C.BCS_3D["inflow_outflow"])
+    q = C.random_state(s.shape, phys, seed=17)
+    s.upload_state(q)
+    o.set(q)
+    w = oracle_mod.refelem3d(3)["w"]
+    vol = (L3[0] / N3[0]) * (L3[1] / N3[1]) * (L3[2] / N3[2]) / 6.0
+    for c in range(9):
+        want = vol * float((q[..., c] * w[None, :]).sum())
+        assert abs(s.integral(c) - want) <= 1e-13 * max(abs(want), 1e-3)
+    assert abs(s.max_wavespeed() - o.max_face_speed()) <= 1e-13 * o.max_face_speed()
