@@ -55,6 +55,7 @@ extern "C" {
 #define MXM_DG_PHYS_SHALLOW_WATER 3
 #define MXM_DG_PHYS_MHD 4
 #define MXM_DG_PHYS_MHD_PLAIN 5
+#define MXM_DG_PHYS_TWO_FLUID 6 /* src/two_fluid.mojo, 3D, 17 components */
 
 /* Numerical fluxes.  3D Euler: FLUX_RUSANOV..FLUX_HLLEC (euler.mojo:33-36).
  * 2D Euler: RUSANOV (|v|+c speed, local_mesh_2d_gpu_euler.mojo:220-337),
@@ -95,13 +96,20 @@ extern "C" {
  *        inflow_E, inflow_Bx, inflow_By, inflow_Bz, inflow_psi}; 9 components
  *        [rho, rho u, rho v, rho w, E, Bx, By, Bz, psi].  2D MHD and
  *        MHD_PLAIN use the same layout (rhow and Bz unused; c_h, alpha_d and
- *        psi only with GLM). */
+ *        psi only with GLM).
+ *  TWO_FLUID (two_fluid.mojo:141-206): p = {gamma_e, gamma_i, q_e, m_e, q_i,
+ *        m_i, eps0, c_light, c_h, alpha_d, min_density, min_pressure,
+ *        inflow[17]}; 17 components [electrons rho, m, E | ions rho, m, E |
+ *        Ex, Ey, Ez, Bx, By, Bz | psi].  MIXED runs it on the FP32 kernel (a
+ *        128-row tensor-core tile holds fewer than 8 elements of 17
+ *        components); FP64 at P5 exceeds the stage tile's shared memory
+ *        (mxm_dg_create returns MXM_DG_EINVAL). */
 typedef struct mxm_dg_physics_desc {
   int32_t kind;
   int32_t flux_type;
   int32_t entropy_fix;
   int32_t reserved;
-  double p[16];
+  double p[32];
 } mxm_dg_physics_desc;
 
 /* Mesh: dim 3 -> Nx*Ny*Nz cubes x 6 Kuhn tets on [0,Lx]x[0,Ly]x[0,Lz]
@@ -224,7 +232,7 @@ int mxm_dg_selftest_wait_timeout(double limit_ms, int32_t* gave_up, double* wait
 /* ---- initial conditions on the device ------------------------------------
  * Fill state buffer `which` from node coordinates computed on the device
  * (the role of the reference's IC kernels, e.g. examples/euler_vortex.mojo:
- * 87-129).  params (nparams <= 16):
+ * 87-129).  params (nparams <= 32):
  *   CONSTANT    NC state values
  *   SINE_WAVE   Euler: rho0, amp, u, v, w, p, kx, ky, kz:
  *               rho = rho0 + amp sin(2 pi (kx x + ky y + kz z)), uniform u, p

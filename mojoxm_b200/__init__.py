@@ -29,7 +29,7 @@ LIB_PATH = os.path.join(_HERE, "libmxm_dg.so")
 
 # include/mxm_dg.h constants
 OK, EINVAL, ENOMEM, ECUDA, ENONFINITE, ETIMEDOUT, ENOTREADY = 0, -1, -2, -3, -4, -5, -6
-PHYS_ADVECTION, PHYS_EULER, PHYS_MAXWELL, PHYS_SHALLOW_WATER, PHYS_MHD, PHYS_MHD_PLAIN = 0, 1, 2, 3, 4, 5
+PHYS_ADVECTION, PHYS_EULER, PHYS_MAXWELL, PHYS_SHALLOW_WATER, PHYS_MHD, PHYS_MHD_PLAIN, PHYS_TWO_FLUID = range(7)
 FLUX_RUSANOV, FLUX_ROE, FLUX_HLLE, FLUX_HLLEC, FLUX_HLLC, FLUX_HLL = 0, 1, 2, 3, 4, 5
 BC_INTERIOR, BC_WALL, BC_OUTFLOW, BC_INFLOW = 0, 1, 2, 3
 PREC = {"f64": 0, "f32": 1, "mixed": 2}
@@ -62,7 +62,7 @@ class DGError(RuntimeError):
 
 class _PhysDesc(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("flux_type", ctypes.c_int32), ("entropy_fix", ctypes.c_int32),
-                ("reserved", ctypes.c_int32), ("p", ctypes.c_double * 16)]
+                ("reserved", ctypes.c_int32), ("p", ctypes.c_double * 32)]
 
 
 class _MeshDesc(ctypes.Structure):
@@ -283,6 +283,30 @@ class IdealMHDPlain(IdealMHD):
     IdealMHD on a 2D mesh is the GLM stack (src/local_mesh_2d_gpu_mhd_glm.mojo)
     with state (rho, mx, my, Bx, By, E, psi)."""
     kind: int = field(default=PHYS_MHD_PLAIN, init=False)
+
+
+@dataclass
+class FiveMomentTwoFluid:  # src/two_fluid.mojo:139-206 (3D, 17 components)
+    gamma_e: float = 5.0 / 3.0
+    gamma_i: float = 5.0 / 3.0
+    q_e: float = -1.0
+    m_e: float = 1.0
+    q_i: float = 1.0
+    m_i: float = 25.0
+    eps0: float = 1.0
+    c_light: float = 10.0
+    c_h: float = 0.0
+    alpha_d: float = 0.0
+    min_density: float = 1e-6
+    min_pressure: float = 1e-8
+    inflow: tuple = (0.0,) * 17
+    kind: int = field(default=PHYS_TWO_FLUID, init=False)
+    flux_type: int = field(default=0, init=False)
+    entropy_fix: bool = field(default=False, init=False)
+
+    def params(self):
+        return [self.gamma_e, self.gamma_i, self.q_e, self.m_e, self.q_i, self.m_i, self.eps0, self.c_light,
+                self.c_h, self.alpha_d, self.min_density, self.min_pressure] + list(self.inflow)
 
 
 def physics_dict(ph):

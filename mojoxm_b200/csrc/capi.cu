@@ -160,6 +160,16 @@ MhdD<R> make_mhd(const double* p) {  // mxm_dg_physics_desc field order (mhd.moj
   return ph;
 }
 
+template <class R>
+TwoFluidD<R> make_two_fluid(const double* p) {  // two_fluid.mojo:141-206 field order
+  TwoFluidD<R> ph;
+  ph.gamma_e = R(p[0]); ph.gamma_i = R(p[1]); ph.q_e = R(p[2]); ph.m_e = R(p[3]); ph.q_i = R(p[4]);
+  ph.m_i = R(p[5]); ph.eps0 = R(p[6]); ph.c_light = R(p[7]); ph.c_h = R(p[8]); ph.alpha_d = R(p[9]);
+  ph.rho_min = R(p[10]); ph.p_min = R(p[11]);
+  for (int k = 0; k < 17; ++k) ph.inflow[k] = R(p[12 + k]);
+  return ph;
+}
+
 // 2D MHD from the same layout: state (rho, mx, my, Bx, By, E[, psi])
 template <class R, bool GLM>
 Mhd2D<R, GLM> make_mhd2d(const double* p) {
@@ -194,7 +204,8 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
     const KuhnTab3<R>& t = tab3<R>(h);
     // MIXED precision routes the 3D stage through the tensor-core kernel
     auto go = [&](const auto& ph) -> cudaError_t {
-      if constexpr (std::is_same<R, float>::value) {
+      if constexpr (std::is_same<R, float>::value &&
+                    std::decay<decltype(ph)>::type::NC <= 16) {
         if (h->use_tc)
           return launch_stage3d_tc(h->P, ar, t, ph, (const unsigned char*)h->tcimg, h->nsm, h->stream);
       }
@@ -235,6 +246,7 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
         return go(ph);
       }
       case MXM_DG_PHYS_MHD: return go(make_mhd<R>(p));
+      case MXM_DG_PHYS_TWO_FLUID: return go(make_two_fluid<R>(p));
     }
     return cudaErrorInvalidValue;
   }
@@ -342,6 +354,7 @@ cudaError_t wavespeed_launch(Handle* h, const void* qi, unsigned long long* out)
         return launch_wavespeed3d<R>(h->P, ar, t, ph, out, h->stream);
       }
       case MXM_DG_PHYS_MHD: return launch_wavespeed3d<R>(h->P, ar, t, make_mhd<R>(p), out, h->stream);
+      case MXM_DG_PHYS_TWO_FLUID: return launch_wavespeed3d<R>(h->P, ar, t, make_two_fluid<R>(p), out, h->stream);
     }
     return cudaErrorInvalidValue;
   }
@@ -491,7 +504,7 @@ void build_xyz(Handle* h) {
 void fill_ic(Handle* h, int which, int kind, const double* params, int nparams) {
   if (which < 0 || which > 2) throw ArgError("which must be 0..2");
   if (kind < MXM_DG_IC_CONSTANT || kind > MXM_DG_IC_ALFVEN) throw ArgError("unknown initial-condition kind");
-  if (nparams < 0 || nparams > 16 || (nparams > 0 && !params)) throw ArgError("nparams must be 0..16");
+  if (nparams < 0 || nparams > 32 || (nparams > 0 && !params)) throw ArgError("nparams must be 0..32");
   const int k = h->phys.kind;
   const bool ok = kind == MXM_DG_IC_CONSTANT ||
                   ((kind == MXM_DG_IC_SINE_WAVE || kind == MXM_DG_IC_VORTEX || kind == MXM_DG_IC_SOD) &&
@@ -554,7 +567,8 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   if (P < 1 || P > 5) throw ArgError("order P must be in 1..5");
   if (prec != MXM_DG_PREC_F64 && prec != MXM_DG_PREC_F32 && prec != MXM_DG_PREC_MIXED)
     throw ArgError("precision must be MXM_DG_PREC_F64, MXM_DG_PREC_F32 or MXM_DG_PREC_MIXED");
-  if (ph->kind < 0 || ph->kind > MXM_DG_PHYS_MHD_PLAIN) throw ArgError("unknown physics kind");
+  if (ph->kind < 0 || ph->kind > MXM_DG_PHYS_TWO_FLUID) throw ArgError("unknown physics kind");
+  if (ph->kind == MXM_DG_PHYS_TWO_FLUID && m->dim != 3) throw ArgError("two-fluid physics is 3D only");
   if (ph->kind == MXM_DG_PHYS_MHD_PLAIN && m->dim != 2) throw ArgError("MHD_PLAIN physics is 2D only");
   if (m->nx < 1 || m->ny < 1 || (m->dim == 3 && m->nz < 1)) throw ArgError("cell counts must be >= 1");
   for (int k = 0; k < 2 * m->dim; ++k)
@@ -584,6 +598,7 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
         : ph->kind == MXM_DG_PHYS_MAXWELL   ? 6
         : ph->kind == MXM_DG_PHYS_MHD       ? (m->dim == 3 ? 9 : 7)
         : ph->kind == MXM_DG_PHYS_MHD_PLAIN ? 6
+        : ph->kind == MXM_DG_PHYS_TWO_FLUID ? 17
                                             : 3;
   h->ntypes = m->dim == 3 ? 6 : 2;
   h->ncell = int64_t(h->nx) * h->ny * h->nz;
@@ -591,7 +606,10 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   if (h->ne > (int64_t(1) << 31) / 64) throw ArgError("mesh too large for 32-bit cell indexing");
   h->rbytes = prec == MXM_DG_PREC_F64 ? 8 : 4;
   // split-BF16 tensor-core contraction for the 3D orders it is built for
-  h->use_tc = prec == MXM_DG_PREC_MIXED && m->dim == 3 && P >= 2 && P <= 5;
+  // (a 128-row tile needs at least 8 element slots: NC <= 16)
+  h->use_tc = prec == MXM_DG_PREC_MIXED && m->dim == 3 && P >= 2 && P <= 5 && h->NC <= 16;
+  if (m->dim == 3 && !h->use_tc && stage3d_smem_need(P, h->NC, h->rbytes) > kMaxSmemPerBlock)
+    throw ArgError("this order, component count and precision exceed the stage tile's shared memory");
   h->ref = build_refops(h->dim, P);
   h->NP = h->ref.NP;
   h->NFP = h->ref.NFP;

@@ -49,6 +49,29 @@ struct KuhnTab2 {
   uint8_t nb_node[2][3][kMaxNFP2];
 };
 
+// Dynamic shared memory one block may use on sm_100a.
+constexpr size_t kMaxSmemPerBlock = 227 * 1024;
+
+// Element stride of the 3D SIMT stage's B tile (K columns x NC values,
+// padded so that elements read by one warp fall in distinct banks).
+__host__ __device__ constexpr int stage3d_bstr(int P, int NC, int rb) {
+  const int K = 3 * ntet(P) + 4 * ntri(P), raw = K * NC, mod = rb == 8 ? 16 : 32;
+  return raw + ((1 - raw % mod) + mod) % mod;
+}
+// Shared memory of the 3D SIMT stage with EC cubes per tile: barriers, the
+// Kuhn table, two state tiles, the B tile, the operator (asmem) and the
+// per-cube neighbour table.
+__host__ __device__ constexpr size_t stage3d_smem(int P, int NC, int rb, int EC, bool asmem) {
+  const size_t tab = rb == 8 ? (sizeof(KuhnTab3<double>) + 15) / 16 * 16 : (sizeof(KuhnTab3<float>) + 15) / 16 * 16;
+  const size_t NP = size_t(ntet(P)), K = size_t(3 * ntet(P) + 4 * ntri(P));
+  return 16 + tab + size_t(rb) * (2 * size_t(6 * EC) * NP * NC + size_t(6 * EC) * stage3d_bstr(P, NC, rb) +
+                                  (asmem ? K * NP : 0)) +
+         size_t(EC) * 12 * sizeof(int);
+}
+// Least shared memory the 3D SIMT stage needs (one cube per tile, operator
+// read from global memory).
+inline size_t stage3d_smem_need(int P, int NC, size_t rb) { return stage3d_smem(P, NC, int(rb), 1, false); }
+
 // Face treatment for an element's face, resolved from the cell position and
 // the six BC codes exactly as mojoxm's BC overlay resolves it
 // (src/local_mesh.mojo:946-1187): the +axis cube face of the last cell

@@ -5,13 +5,13 @@
 
 namespace mxm {
 
-constexpr int kMaxIcNC = 9;  // components of the widest physics (MHD)
+constexpr int kMaxIcNC = 17;  // components of the widest physics (two-fluid)
 
 struct IcArgs {
   int64_t ne;
   int dim, P, NP, NC, nx, ny, nz, kind;
   double h[3], L[3];
-  double prm[16];
+  double prm[32];
   double gamma, c;          // Euler gamma, Maxwell wave speed (from the physics)
   int8_t vert[6][4][3];     // cube-/cell-corner coordinates of each element type's vertices
   uint8_t bary[56][4];      // barycentric exponents of each node (sum P)

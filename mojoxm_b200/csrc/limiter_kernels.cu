@@ -32,7 +32,9 @@ cudaError_t lim_np(const LimArgs<R>& a, const KuhnTab3<R>& t3, const KuhnTab2<R>
     }
     theta2d_kernel<R, NP, NC><<<int((a.ne + kLim2dBlock - 1) / kLim2dBlock), kLim2dBlock, smem, st>>>(a, t2);
   } else {
-    constexpr int EPB = 8;
+    // elements per block: their staged states stay within 40 KB of static shared memory
+    constexpr size_t kElem = sizeof(R) * NP * NC;
+    constexpr int EPB = kElem * 8 <= 40960 ? 8 : (kElem * 4 <= 40960 ? 4 : 2);
     theta_apply_kernel<R, DIM, NP, NC, EPB><<<int((a.ne + EPB - 1) / EPB), 32 * EPB, 0, st>>>(a, t3, t2);
   }
   return cudaGetLastError();
@@ -60,6 +62,7 @@ cudaError_t launch_limiter(int dim, int P, int NC, const LimArgs<R>& a, const Ku
       case 5: return lim_nc<R, 3, 5>(P, a, t3, t2, st);
       case 6: return lim_nc<R, 3, 6>(P, a, t3, t2, st);
       case 9: return lim_nc<R, 3, 9>(P, a, t3, t2, st);
+      case 17: return lim_nc<R, 3, 17>(P, a, t3, t2, st);
     }
   } else {
     switch (NC) {
@@ -95,6 +98,7 @@ cudaError_t red_nc(int NC, const R* q, const R* w, int64_t ne, int c, int kind, 
     case 6: return red_np<R, NP, 6>(q, w, ne, c, kind, scale, partial, npartial, out, st);
     case 7: return red_np<R, NP, 7>(q, w, ne, c, kind, scale, partial, npartial, out, st);
     case 9: return red_np<R, NP, 9>(q, w, ne, c, kind, scale, partial, npartial, out, st);
+    case 17: return red_np<R, NP, 17>(q, w, ne, c, kind, scale, partial, npartial, out, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -6,6 +6,7 @@
 //   Maxwell       src/maxwell.mojo:48-255
 //   ShallowWater  src/shallow_water.mojo:31-167
 //   IdealMHD      src/mhd.mojo:1-367 (GLM divergence cleaning)
+//   TwoFluid      src/two_fluid.mojo:1-513 (five-moment electrons + ions + Maxwell + GLM)
 // Each formula keeps the reference's operation order, except that divisions
 // by positive quantities (floored densities, square roots of them, the HLLE
 // wave-speed span) are taken as one reciprocal and products, which in FP32
@@ -519,6 +520,118 @@ struct MhdD {
 #pragma unroll
     for (int c = 0; c < 8; ++c) s[c] = R(0);
     s[8] = -alpha_d * q[8];
+  }
+  __device__ void limit(R*) const {}
+};
+
+// ----------------------------------------------------------- five-moment two-fluid
+// q[0..4] electrons (rho, m, E), q[5..9] ions, q[10..15] (E, B), q[16] psi;
+// fluids couple to the field only through the source (Lorentz force, work,
+// Ampere current), the GLM psi cleans div B.
+template <class R>
+struct TwoFluidD {
+  static constexpr int NC = 17;
+  static constexpr bool kSource = true, kLimit = false;
+  static constexpr bool kLightFlux = true;
+  R gamma_e, gamma_i, q_e, m_e, q_i, m_i, eps0, c_light, c_h, alpha_d, rho_min, p_min, inflow[17];
+
+  __device__ __forceinline__ R rho_f(const R* s) const { return s[0] > rho_min ? s[0] : rho_min; }  // two_fluid.mojo:52-54
+  // floored species pressure from ri = 1 / rho (two_fluid.mojo:57-65)
+  __device__ __forceinline__ R p_s(const R* s, R g, R ri) const {
+    const R p = (g - R(1)) * (s[4] - R(0.5) * (s[1] * s[1] + s[2] * s[2] + s[3] * s[3]) * ri);
+    return p > p_min ? p : p_min;
+  }
+  __device__ __forceinline__ void species_flux(const R* s, R g, R* F) const {  // two_fluid.mojo:76-101 (F[d*NC + c])
+    const R ri = pos_rcp(rho_f(s)), u = s[1] * ri, v = s[2] * ri, w = s[3] * ri, p = p_s(s, g, ri);
+    F[0] = s[1]; F[1] = s[1] * u + p; F[2] = s[1] * v; F[3] = s[1] * w; F[4] = u * (s[4] + p);
+    F[NC + 0] = s[2]; F[NC + 1] = s[2] * u; F[NC + 2] = s[2] * v + p; F[NC + 3] = s[2] * w; F[NC + 4] = v * (s[4] + p);
+    F[2 * NC + 0] = s[3]; F[2 * NC + 1] = s[3] * u; F[2 * NC + 2] = s[3] * v; F[2 * NC + 3] = s[3] * w + p;
+    F[2 * NC + 4] = w * (s[4] + p);
+  }
+  __device__ void flux(const R* q, R* F) const {  // two_fluid.mojo:258-305
+    species_flux(q, gamma_e, F);
+    species_flux(q + 5, gamma_i, F + 5);
+    const R c2 = c_light * c_light, ch2 = c_h * c_h;
+    const R Ex = q[10], Ey = q[11], Ez = q[12], Bx = q[13], By = q[14], Bz = q[15], psi = q[16];
+    F[10] = R(0); F[11] = c2 * Bz; F[12] = -c2 * By; F[13] = psi; F[14] = -Ez; F[15] = Ey; F[16] = ch2 * Bx;
+    F[NC + 10] = -c2 * Bz; F[NC + 11] = R(0); F[NC + 12] = c2 * Bx; F[NC + 13] = Ez; F[NC + 14] = psi;
+    F[NC + 15] = -Ex; F[NC + 16] = ch2 * By;
+    F[2 * NC + 10] = c2 * By; F[2 * NC + 11] = -c2 * Bx; F[2 * NC + 12] = R(0); F[2 * NC + 13] = -Ey;
+    F[2 * NC + 14] = Ex; F[2 * NC + 15] = psi; F[2 * NC + 16] = ch2 * Bz;
+  }
+  // species F.n and Rusanov speed |u.n| + c_s (two_fluid.mojo:107-132, :349-366)
+  __device__ __forceinline__ R species_normal(const R* s, R g, R nx, R ny, R nz, R* F) const {
+    const R rho = rho_f(s), ri = pos_rcp(rho), u = s[1] * ri, v = s[2] * ri, w = s[3] * ri, p = p_s(s, g, ri);
+    const R un = u * nx + v * ny + w * nz;
+    F[0] = rho * un; F[1] = rho * u * un + p * nx; F[2] = rho * v * un + p * ny; F[3] = rho * w * un + p * nz;
+    F[4] = un * (s[4] + p);
+    const R unm = (s[1] * nx + s[2] * ny + s[3] * nz) * ri;
+    return rabs(unm) + sqrt(g * p * ri);
+  }
+  __device__ __forceinline__ void field_normal(const R* q, R nx, R ny, R nz, R* F) const {  // :329-347
+    const R c2 = c_light * c_light, ch2 = c_h * c_h;
+    const R Ex = q[10], Ey = q[11], Ez = q[12], Bx = q[13], By = q[14], Bz = q[15], psi = q[16];
+    F[10] = c2 * (By * nz - Bz * ny); F[11] = c2 * (Bz * nx - Bx * nz); F[12] = c2 * (Bx * ny - By * nx);
+    F[13] = (ny * Ez - nz * Ey) + psi * nx; F[14] = (nz * Ex - nx * Ez) + psi * ny;
+    F[15] = (nx * Ey - ny * Ex) + psi * nz; F[16] = ch2 * (Bx * nx + By * ny + Bz * nz);
+  }
+  // Rusanov: alpha = max(fluid speeds of both sides, c, c_h) (two_fluid.mojo:307-374)
+  __device__ R num_flux(const R* l, const R* r, R nx, R ny, R nz, R* f) const {
+    R Fl[17], Fr[17];
+    const R ael = species_normal(l, gamma_e, nx, ny, nz, Fl), aer = species_normal(r, gamma_e, nx, ny, nz, Fr);
+    const R ail = species_normal(l + 5, gamma_i, nx, ny, nz, Fl + 5), air = species_normal(r + 5, gamma_i, nx, ny, nz, Fr + 5);
+    field_normal(l, nx, ny, nz, Fl);
+    field_normal(r, nx, ny, nz, Fr);
+    const R al = rmax(rmax(rmax(ael, aer), rmax(ail, air)), rmax(c_light, c_h)), h = R(0.5);
+#pragma unroll
+    for (int c = 0; c < 17; ++c) f[c] = h * (Fl[c] + Fr[c]) - h * al * (r[c] - l[c]);
+    return al;
+  }
+  // wall: slip for both fluids, PEC for the field (two_fluid.mojo:376-428)
+  __device__ void ghost(const R* q, int bc, R nx, R ny, R nz, R* g) const {
+    if (bc == BC_INFLOW) {
+#pragma unroll
+      for (int k = 0; k < 17; ++k) g[k] = inflow[k];
+      return;
+    }
+#pragma unroll
+    for (int k = 0; k < 17; ++k) g[k] = q[k];
+    if (bc == BC_WALL) {
+      const R me = q[1] * nx + q[2] * ny + q[3] * nz, mi = q[6] * nx + q[7] * ny + q[8] * nz;
+      g[1] = q[1] - R(2) * me * nx; g[2] = q[2] - R(2) * me * ny; g[3] = q[3] - R(2) * me * nz;
+      g[6] = q[6] - R(2) * mi * nx; g[7] = q[7] - R(2) * mi * ny; g[8] = q[8] - R(2) * mi * nz;
+      const R En = q[10] * nx + q[11] * ny + q[12] * nz, Bn = q[13] * nx + q[14] * ny + q[15] * nz;
+      g[10] = R(2) * En * nx - q[10]; g[11] = R(2) * En * ny - q[11]; g[12] = R(2) * En * nz - q[12];
+      g[13] = q[13] - R(2) * Bn * nx; g[14] = q[14] - R(2) * Bn * ny; g[15] = q[15] - R(2) * Bn * nz;
+    }
+  }
+  __device__ R bnd_flux(const R* q, int bc, R nx, R ny, R nz, R* f) const {
+    R g[17];
+    ghost(q, bc, nx, ny, nz, g);
+    return num_flux(q, g, nx, ny, nz, f);
+  }
+  __device__ void source(const R* q, R* s) const {  // two_fluid.mojo:430-510
+    const R ie = pos_rcp(rho_f(q)), ii = pos_rcp(rho_f(q + 5));
+    const R rho_e = rho_f(q), rho_i = rho_f(q + 5);
+    const R ue = q[1] * ie, ve = q[2] * ie, we = q[3] * ie, ui = q[6] * ii, vi = q[7] * ii, wi = q[8] * ii;
+    const R Ex = q[10], Ey = q[11], Ez = q[12], Bx = q[13], By = q[14], Bz = q[15];
+    const R qme = q_e / m_e, qmi = q_i / m_i;
+    s[0] = R(0);
+    s[1] = qme * rho_e * (Ex + (ve * Bz - we * By));
+    s[2] = qme * rho_e * (Ey + (we * Bx - ue * Bz));
+    s[3] = qme * rho_e * (Ez + (ue * By - ve * Bx));
+    s[4] = qme * rho_e * (ue * Ex + ve * Ey + we * Ez);
+    s[5] = R(0);
+    s[6] = qmi * rho_i * (Ex + (vi * Bz - wi * By));
+    s[7] = qmi * rho_i * (Ey + (wi * Bx - ui * Bz));
+    s[8] = qmi * rho_i * (Ez + (ui * By - vi * Bx));
+    s[9] = qmi * rho_i * (ui * Ex + vi * Ey + wi * Ez);
+    const R ie0 = R(1) / eps0;
+    s[10] = -(qme * rho_e * ue + qmi * rho_i * ui) * ie0;
+    s[11] = -(qme * rho_e * ve + qmi * rho_i * vi) * ie0;
+    s[12] = -(qme * rho_e * we + qmi * rho_i * wi) * ie0;
+    s[13] = R(0); s[14] = R(0); s[15] = R(0);
+    s[16] = -alpha_d * q[16];
   }
   __device__ void limit(R*) const {}
 };

@@ -36,7 +36,7 @@ struct Request {
   mxm_dg_mesh_desc mesh{};
   mxm_dg_physics_desc phys{};
   int P = 1, prec = 0, ic_kind = 0, nparams = 0, limiter = 0;
-  double params[16] = {};
+  double params[32] = {};
   double eps = 0.1, dt = 0.0;
   int nsteps = 0;
   void* out = nullptr;  // caller-owned host buffer (state bytes), may be null
@@ -85,6 +85,7 @@ int nc_of(const mxm_dg_physics_desc& p, int dim) {
        : p.kind == MXM_DG_PHYS_MAXWELL   ? 6
        : p.kind == MXM_DG_PHYS_MHD       ? (dim == 3 ? 9 : 7)
        : p.kind == MXM_DG_PHYS_MHD_PLAIN ? 6
+       : p.kind == MXM_DG_PHYS_TWO_FLUID ? 17
                                          : 3;
 }
 
@@ -312,11 +313,11 @@ int mxm_dg_server_submit(void* server, const mxm_dg_mesh_desc* mesh, const mxm_d
                          double venkat_eps, double dt, int nsteps, void* out_host, int64_t* request_id) {
   SERVER_BEGIN
   if (!mesh || !phys || !request_id) throw mxm::ArgError("mesh, phys and request_id must be non-null");
-  if (nparams < 0 || nparams > 16 || (nparams > 0 && !ic_params)) throw mxm::ArgError("nparams must be 0..16");
+  if (nparams < 0 || nparams > 32 || (nparams > 0 && !ic_params)) throw mxm::ArgError("nparams must be 0..32");
   if (!(dt > 0.0) || nsteps < 0) throw mxm::ArgError("dt > 0 and nsteps >= 0");
   if (P < 1 || P > 5 || (mesh->dim != 2 && mesh->dim != 3) || precision < 0 || precision > 2 || phys->kind < 0 ||
-      phys->kind > MXM_DG_PHYS_MHD_PLAIN || mesh->nx < 1 || mesh->ny < 1 || (mesh->dim == 3 && mesh->nz < 1))
-    throw mxm::ArgError("order 1..5, dim 2 or 3, precision 0..2, physics kind 0..5, cell counts >= 1");
+      phys->kind > MXM_DG_PHYS_TWO_FLUID || mesh->nx < 1 || mesh->ny < 1 || (mesh->dim == 3 && mesh->nz < 1))
+    throw mxm::ArgError("order 1..5, dim 2 or 3, precision 0..2, physics kind 0..6, cell counts >= 1");
   std::unique_ptr<mxm::Request> r(new mxm::Request);
   r->mesh = *mesh;
   r->phys = *phys;

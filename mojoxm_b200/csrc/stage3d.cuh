@@ -38,9 +38,7 @@ struct Stage3DShape {
   static constexpr int NP = ntet(P), NFP = ntri(P), K = 3 * NP + 4 * NFP;
   // element stride of the B tile, padded so that elements read in the same
   // warp land in distinct banks
-  static constexpr int BSTR_RAW = K * NC;
-  static constexpr int BMOD = sizeof(R) == 8 ? 16 : 32;
-  static constexpr int BSTR = BSTR_RAW + ((1 - BSTR_RAW % BMOD) + BMOD) % BMOD;
+  static constexpr int BSTR = stage3d_bstr(P, NC, int(sizeof(R)));
 };
 
 template <class R, class Phys, int P, int EC, int RI, int NT, bool ASMEM>
@@ -297,10 +295,7 @@ __global__ void wavespeed3d_kernel(Stage3DArgs<R> args, KuhnTab3<R> tab, Phys ph
 
 template <class R, int P, int NC, int EC, bool ASMEM>
 constexpr size_t stage3d_smem_bytes() {
-  using S = Stage3DShape<P, NC, R>;
-  return 16 + (sizeof(KuhnTab3<R>) + 15) / 16 * 16 +
-         sizeof(R) * (2 * size_t(6 * EC) * S::NP * NC + size_t(6 * EC) * S::BSTR + (ASMEM ? size_t(S::K) * S::NP : 0)) +
-         size_t(EC) * 12 * sizeof(int);
+  return stage3d_smem(P, NC, int(sizeof(R)), EC, ASMEM);
 }
 
 }  // namespace mxm

@@ -4,15 +4,26 @@
 
 namespace mxm {
 
+// Largest divisor of NP not above `base` whose RI x NC accumulator tile
+// stays within `cap` registers' worth of values (at least 1).
+constexpr int ri_capped(int base, int NP, int NC, int cap) {
+  for (int r = base; r > 1; --r)
+    if (NP % r == 0 && r * NC <= cap) return r;
+  return 1;
+}
+
 template <class R, int P, int NC>
 struct Cfg3 {
   using S = Stage3DShape<P, NC, R>;
   static constexpr int NP = S::NP;
-  // rows per thread: a divisor of NP
-  static constexpr int RI = sizeof(R) == 8 ? (P <= 3 ? 2 : (P == 4 ? 5 : 4))
-                                           : (P == 1 ? 4 : (P == 2 ? 5 : (P == 3 ? 4 : (P == 4 ? 5 : 8))));
-  // keep the shared operator in shared memory when it takes <= 64 KB
-  static constexpr bool ASMEM = sizeof(R) * S::K * S::NP <= 64 * 1024;
+  // rows per thread: a divisor of NP (fewer for wide states)
+  static constexpr int RI0 = sizeof(R) == 8 ? (P <= 3 ? 2 : (P == 4 ? 5 : 4))
+                                            : (P == 1 ? 4 : (P == 2 ? 5 : (P == 3 ? 4 : (P == 4 ? 5 : 8))));
+  static constexpr int RI = NC > 6 ? ri_capped(RI0, NP, NC, sizeof(R) == 8 ? 48 : 64) : RI0;
+  // keep the shared operator in shared memory when it takes <= 64 KB and a
+  // one-cube tile still fits beside it
+  static constexpr bool ASMEM = sizeof(R) * S::K * S::NP <= 64 * 1024 &&
+                                stage3d_smem(P, NC, int(sizeof(R)), 1, true) <= kMaxSmemPerBlock;
   static constexpr size_t kBudget = 110 * 1024;  // two blocks per SM
   static constexpr size_t kFixed = 16 + (sizeof(KuhnTab3<R>) + 15) / 16 * 16 + (ASMEM ? sizeof(R) * S::K * S::NP : 0);
   static constexpr size_t kPerCube = 6 * sizeof(R) * (2 * size_t(S::NP) * NC + S::BSTR);
@@ -20,11 +31,15 @@ struct Cfg3 {
   static constexpr int EC = EC_RAW > 16 ? 16 : (EC_RAW < 1 ? 1 : EC_RAW);
   static constexpr int NT = 256;
   static constexpr size_t kSmem = stage3d_smem_bytes<R, P, NC, EC, ASMEM>();
+  static constexpr bool FITS = kSmem <= kMaxSmemPerBlock;
 };
 
 template <class R, class Phys, int P>
 cudaError_t launch3_p(const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phys& ph, int nsm, cudaStream_t st) {
   using C = Cfg3<R, P, Phys::NC>;
+  if constexpr (!C::FITS) {
+    return cudaErrorInvalidConfiguration;  // refused at mxm_dg_create already
+  } else {
   auto kern = stage3d_kernel<R, Phys, P, C::EC, C::RI, C::NT, C::ASMEM>;
   static int bps = -1;
   if (bps < 0) {
@@ -37,6 +52,7 @@ cudaError_t launch3_p(const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phy
   if (nblk < 1) nblk = 1;
   kern<<<nblk, C::NT, C::kSmem, st>>>(a, tab, ph);
   return cudaGetLastError();
+  }
 }
 
 template <class R, class Phys>

@@ -121,7 +121,7 @@ class Oracle3D:
     def __init__(self, P, n, L, physics, bcs=(0,) * 6, real="f64"):
         nx, ny, nz = (n, n, n) if np.isscalar(n) else n
         Lx, Ly, Lz = (L, L, L) if np.isscalar(L) else L
-        p = np.zeros(16)
+        p = np.zeros(32)
         p[: len(physics["p"])] = physics["p"]
         b = np.array(bcs, np.int32)
         h = ctypes.c_void_p()
@@ -198,7 +198,7 @@ class Oracle2D:
     def __init__(self, P, n, L, physics, bcs=(0,) * 4, real="f64"):
         nx, ny = (n, n) if np.isscalar(n) else n
         Lx, Ly = (L, L) if np.isscalar(L) else L
-        p = np.zeros(16)
+        p = np.zeros(32)
         p[: len(physics["p"])] = physics["p"]
         b = np.array(bcs, np.int32)
         h = ctypes.c_void_p()

@@ -51,6 +51,14 @@ static SolverBase* make3(int P, int nx, int ny, int nz, double Lx, double Ly, do
     for (int k = 0; k < 9; ++k) ph.inflow[k] = R(p[5 + k]);
     return new Solver3D<R, IdealMHD<R>>(P, nx, ny, nz, Lx, Ly, Lz, bcs, ph);
   }
+  if (kind == PHYS_TWO_FLUID) {
+    TwoFluid<R> ph;
+    ph.gamma_e = R(p[0]); ph.gamma_i = R(p[1]); ph.q_e = R(p[2]); ph.m_e = R(p[3]); ph.q_i = R(p[4]);
+    ph.m_i = R(p[5]); ph.eps0 = R(p[6]); ph.c_light = R(p[7]); ph.c_h = R(p[8]); ph.alpha_d = R(p[9]);
+    ph.min_density = R(p[10]); ph.min_pressure = R(p[11]);
+    for (int k = 0; k < 17; ++k) ph.inflow[k] = R(p[12 + k]);
+    return new Solver3D<R, TwoFluid<R>>(P, nx, ny, nz, Lx, Ly, Lz, bcs, ph);
+  }
   throw std::runtime_error("unknown physics kind");
 }
 

@@ -3,7 +3,8 @@
 // solver: Advection (src/advection.mojo), Euler with Rusanov / Roe / HLLE /
 // HLLEC and the Harten-Hyman entropy fix (src/euler.mojo), vacuum Maxwell
 // (src/maxwell.mojo), shallow water embedded in 3D (src/shallow_water.mojo)
-// and ideal MHD with GLM divergence cleaning (src/mhd.mojo).
+// ideal MHD with GLM divergence cleaning (src/mhd.mojo) and the five-moment
+// two-fluid plasma model (src/two_fluid.mojo).
 // Templated on the arithmetic type so the same code runs in FP64 (the oracle
 // proper) and in FP32 (mimicking the reference's all-Float32 GPU path).
 #pragma once
@@ -16,7 +17,8 @@ namespace orc {
 
 // PHYS_MHD: 3D IdealMHD (9 components); in 2D the GLM stack (7 components).
 // PHYS_MHD_PLAIN: the 2D stack without divergence cleaning (6 components).
-enum { PHYS_ADVECTION = 0, PHYS_EULER = 1, PHYS_MAXWELL = 2, PHYS_SW = 3, PHYS_MHD = 4, PHYS_MHD_PLAIN = 5 };
+enum { PHYS_ADVECTION = 0, PHYS_EULER = 1, PHYS_MAXWELL = 2, PHYS_SW = 3, PHYS_MHD = 4, PHYS_MHD_PLAIN = 5,
+       PHYS_TWO_FLUID = 6 };
 enum { FLUX_RUSANOV = 0, FLUX_ROE = 1, FLUX_HLLE = 2, FLUX_HLLEC = 3, FLUX_HLLC = 4, FLUX_HLL = 5 };
 
 template <typename R>
@@ -483,6 +485,108 @@ struct IdealMHD {  // mhd.mojo:199-367
   void source_term(const R* q, R* s) const {  // :357-361 (GLM damping)
     for (int c = 0; c < 8; ++c) s[c] = R(0);
     s[8] = -alpha_d * q[8];
+  }
+  void limit_state(R*) const {}
+};
+
+// --------------------------------------------------------- FiveMomentTwoFluid
+// q[0..4] electrons, q[5..9] ions, q[10..15] (E, B), q[16] psi
+template <typename R>
+struct TwoFluid {  // two_fluid.mojo:139-513
+  static constexpr int NC = 17;
+  R gamma_e, gamma_i, q_e, m_e, q_i, m_i, eps0, c_light, c_h, alpha_d, min_density, min_pressure, inflow[17];
+  R rho_f(const R* s) const { return s[0] > min_density ? s[0] : min_density; }  // :52-54
+  R pressure(const R* s, R g) const {  // :57-65
+    R rho = rho_f(s);
+    R ke = R(0.5) * (s[1] * s[1] + s[2] * s[2] + s[3] * s[3]) / rho;
+    R p = (g - R(1)) * (s[4] - ke);
+    return p > min_pressure ? p : min_pressure;
+  }
+  R sound(const R* s, R g) const { return std::sqrt(g * pressure(s, g) / rho_f(s)); }  // :68-71
+  void species_flux_dir(const R* s, R g, int d, R* f) const {  // :76-101
+    R rho = rho_f(s), mx = s[1], my = s[2], mz = s[3], u = mx / rho, v = my / rho, w = mz / rho, E = s[4];
+    R p = pressure(s, g);
+    if (d == 0) { f[0] = mx; f[1] = mx * u + p; f[2] = mx * v; f[3] = mx * w; f[4] = u * (E + p); }
+    else if (d == 1) { f[0] = my; f[1] = my * u; f[2] = my * v + p; f[3] = my * w; f[4] = v * (E + p); }
+    else { f[0] = mz; f[1] = mz * u; f[2] = mz * v; f[3] = mz * w + p; f[4] = w * (E + p); }
+  }
+  void species_normal(const R* s, R g, R nx, R ny, R nz, R* f) const {  // :107-132
+    R rho = rho_f(s), u = s[1] / rho, v = s[2] / rho, w = s[3] / rho, E = s[4], p = pressure(s, g);
+    R un = u * nx + v * ny + w * nz;
+    f[0] = rho * un; f[1] = rho * u * un + p * nx; f[2] = rho * v * un + p * ny; f[3] = rho * w * un + p * nz;
+    f[4] = un * (E + p);
+  }
+  void internal_flux(const R* q, R* f) const {  // :258-305
+    R c2 = c_light * c_light, ch2 = c_h * c_h;
+    R Ex = q[10], Ey = q[11], Ez = q[12], Bx = q[13], By = q[14], Bz = q[15], psi = q[16];
+    for (int d = 0; d < 3; ++d) {
+      species_flux_dir(q, gamma_e, d, f + d * 17);
+      species_flux_dir(q + 5, gamma_i, d, f + d * 17 + 5);
+      R* F = f + d * 17;
+      if (d == 0) { F[10] = R(0); F[11] = c2 * Bz; F[12] = -c2 * By; F[13] = psi; F[14] = -Ez; F[15] = Ey; F[16] = ch2 * Bx; }
+      else if (d == 1) { F[10] = -c2 * Bz; F[11] = R(0); F[12] = c2 * Bx; F[13] = Ez; F[14] = psi; F[15] = -Ex; F[16] = ch2 * By; }
+      else { F[10] = c2 * By; F[11] = -c2 * Bx; F[12] = R(0); F[13] = -Ey; F[14] = Ex; F[15] = psi; F[16] = ch2 * Bz; }
+    }
+  }
+  R numerical_flux(const R* l, const R* r, R nx, R ny, R nz, R* f) const {  // :307-374
+    R Fl[17], Fr[17];
+    species_normal(l, gamma_e, nx, ny, nz, Fl);
+    species_normal(r, gamma_e, nx, ny, nz, Fr);
+    species_normal(l + 5, gamma_i, nx, ny, nz, Fl + 5);
+    species_normal(r + 5, gamma_i, nx, ny, nz, Fr + 5);
+    R c2 = c_light * c_light, ch2 = c_h * c_h;
+    for (int side = 0; side < 2; ++side) {
+      const R* q = side == 0 ? l : r;
+      R* F = side == 0 ? Fl : Fr;
+      R Ex = q[10], Ey = q[11], Ez = q[12], Bx = q[13], By = q[14], Bz = q[15], psi = q[16];
+      R bn = Bx * nx + By * ny + Bz * nz;
+      F[10] = c2 * (By * nz - Bz * ny); F[11] = c2 * (Bz * nx - Bx * nz); F[12] = c2 * (Bx * ny - By * nx);
+      F[13] = (ny * Ez - nz * Ey) + psi * nx; F[14] = (nz * Ex - nx * Ez) + psi * ny;
+      F[15] = (nx * Ey - ny * Ex) + psi * nz; F[16] = ch2 * bn;
+    }
+    R un_el = (l[1] * nx + l[2] * ny + l[3] * nz) / rho_f(l), un_er = (r[1] * nx + r[2] * ny + r[3] * nz) / rho_f(r);
+    R un_il = (l[6] * nx + l[7] * ny + l[8] * nz) / rho_f(l + 5), un_ir = (r[6] * nx + r[7] * ny + r[8] * nz) / rho_f(r + 5);
+    R ae = rmax(rabs(un_el) + sound(l, gamma_e), rabs(un_er) + sound(r, gamma_e));
+    R ai = rmax(rabs(un_il) + sound(l + 5, gamma_i), rabs(un_ir) + sound(r + 5, gamma_i));
+    R al = rmax(rmax(ae, ai), rmax(c_light, c_h)), h = R(0.5);
+    for (int c = 0; c < 17; ++c) f[c] = h * (Fl[c] + Fr[c]) - h * al * (r[c] - l[c]);
+    return al;
+  }
+  R boundary_flux(const R* q, int bc, R nx, R ny, R nz, R* f) const {  // :376-446
+    R g[17];
+    for (int k = 0; k < 17; ++k) g[k] = q[k];
+    if (bc == BC_WALL) {
+      R me = q[1] * nx + q[2] * ny + q[3] * nz, mi = q[6] * nx + q[7] * ny + q[8] * nz;
+      g[1] = q[1] - R(2) * me * nx; g[2] = q[2] - R(2) * me * ny; g[3] = q[3] - R(2) * me * nz;
+      g[6] = q[6] - R(2) * mi * nx; g[7] = q[7] - R(2) * mi * ny; g[8] = q[8] - R(2) * mi * nz;
+      R En = q[10] * nx + q[11] * ny + q[12] * nz, Bn = q[13] * nx + q[14] * ny + q[15] * nz;
+      g[10] = R(2) * En * nx - q[10]; g[11] = R(2) * En * ny - q[11]; g[12] = R(2) * En * nz - q[12];
+      g[13] = q[13] - R(2) * Bn * nx; g[14] = q[14] - R(2) * Bn * ny; g[15] = q[15] - R(2) * Bn * nz;
+    } else if (bc == BC_INFLOW) {
+      for (int k = 0; k < 17; ++k) g[k] = inflow[k];
+    }
+    return numerical_flux(q, g, nx, ny, nz, f);
+  }
+  void source_term(const R* q, R* s) const {  // :448-510
+    R rho_e = rho_f(q), ue = q[1] / rho_e, ve = q[2] / rho_e, we = q[3] / rho_e;
+    R rho_i = rho_f(q + 5), ui = q[6] / rho_i, vi = q[7] / rho_i, wi = q[8] / rho_i;
+    R Ex = q[10], Ey = q[11], Ez = q[12], Bx = q[13], By = q[14], Bz = q[15], psi = q[16];
+    R qme = q_e / m_e, qmi = q_i / m_i;
+    s[0] = R(0);
+    s[1] = qme * rho_e * (Ex + (ve * Bz - we * By));
+    s[2] = qme * rho_e * (Ey + (we * Bx - ue * Bz));
+    s[3] = qme * rho_e * (Ez + (ue * By - ve * Bx));
+    s[4] = qme * rho_e * (ue * Ex + ve * Ey + we * Ez);
+    s[5] = R(0);
+    s[6] = qmi * rho_i * (Ex + (vi * Bz - wi * By));
+    s[7] = qmi * rho_i * (Ey + (wi * Bx - ui * Bz));
+    s[8] = qmi * rho_i * (Ez + (ui * By - vi * Bx));
+    s[9] = qmi * rho_i * (ui * Ex + vi * Ey + wi * Ez);
+    R Jx = qme * rho_e * ue + qmi * rho_i * ui, Jy = qme * rho_e * ve + qmi * rho_i * vi;
+    R Jz = qme * rho_e * we + qmi * rho_i * wi, inv_eps0 = R(1) / eps0;
+    s[10] = -Jx * inv_eps0; s[11] = -Jy * inv_eps0; s[12] = -Jz * inv_eps0;
+    s[13] = R(0); s[14] = R(0); s[15] = R(0);
+    s[16] = -alpha_d * psi;
   }
   void limit_state(R*) const {}
 };

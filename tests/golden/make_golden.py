@@ -103,6 +103,20 @@ ENTRIES = [
     ("mhd_alfven_3d_p3.cfl", 0.10, "benchmarks/bench_mhd_alfven_3d_p3.mojo", "65", "comptime CFL = Float32(0.10)"),
     ("mhd_alfven_3d_p3.l2_max_rel", 5.0e-3, "benchmarks/bench_mhd_alfven_3d_p3.mojo", "71",
      "comptime L2_MAX_REL: Float64 = 5.0e-3"),
+    # five-moment two-fluid plasma oscillation (benchmarks/bench_two_fluid_langmuir_3d_p3.mojo)
+    ("langmuir_3d_p3.mesh", [8, 2, 2, 1.0, 0.25, 0.25], "benchmarks/bench_two_fluid_langmuir_3d_p3.mojo", "60-65",
+     "comptime LZ = Float64(2.0 / 8.0)"),
+    ("langmuir_3d_p3.species", [5.0 / 3.0, 5.0 / 3.0, -1.0, 1.0, 1.0, 25.0, 1.0, 10.0],
+     "benchmarks/bench_two_fluid_langmuir_3d_p3.mojo", "67-74", "comptime M_I: Float32 = 25.0"),
+    ("langmuir_3d_p3.n0_pe_pi_upert", [1.0, 0.01, 0.01, 0.01], "benchmarks/bench_two_fluid_langmuir_3d_p3.mojo",
+     "75-78", "comptime U_PERTURB: Float32 = 0.01"),
+    ("langmuir_3d_p3.c_h_alpha_d_rhomin_pmin", [12.0, 0.5, 1.0e-6, 1.0e-8],
+     "benchmarks/bench_two_fluid_langmuir_3d_p3.mojo", "79-82", "comptime MIN_PRESSURE: Float32 = 1.0e-8"),
+    ("langmuir_3d_p3.cfl", 0.2, "benchmarks/bench_two_fluid_langmuir_3d_p3.mojo", "84", "comptime CFL = Float32(0.2)"),
+    ("langmuir_3d_p3.t_final", 6.1612348, "benchmarks/bench_two_fluid_langmuir_3d_p3.mojo", "90",
+     "comptime T_FINAL: Float32 = Float32(6.1612348)"),
+    ("langmuir_3d_p3.drift_tol_rel", 0.02, "benchmarks/bench_two_fluid_langmuir_3d_p3.mojo", "92",
+     "comptime DRIFT_TOL_REL: Float64 = 0.02"),
 ]
 
 

@@ -244,3 +244,36 @@ def test_mhd_alfven_gate_product(oracle_mod, prec):
     d = rel_l2(q, qo)
     print(f"alfven {prec}: rel L2 vs IC {err:.3e}, vs oracle FP64 {d:.2e}")
     assert d < (1e-10 if prec == "f64" else 2e-4)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_two_fluid_langmuir_gate(prec):
+    """benchmarks/bench_two_fluid_langmuir_3d_p3.mojo: a uniform electron
+    velocity perturbation oscillates at the plasma frequency; after one
+    period the mean electron momentum is back within 2 % and the mean E_x
+    within 2 % of A m_e n0 omega_p."""
+    nx, ny, nz, lx, ly, lz = G["langmuir_3d_p3.mesh"]
+    ge, gi, qe, me, qi, mi, eps0, c = G["langmuir_3d_p3.species"]
+    n0, pe, pi, a = G["langmuir_3d_p3.n0_pe_pi_upert"]
+    c_h, alpha_d, rho_min, p_min = G["langmuir_3d_p3.c_h_alpha_d_rhomin_pmin"]
+    ph = M.FiveMomentTwoFluid(ge, gi, qe, me, qi, mi, eps0, c, c_h, alpha_d, rho_min, p_min)
+    P = 3
+    s = M.Solver(M.Mesh(int(nx), int(ny), int(nz), lx, ly, lz), ph, P=P, precision=prec)
+    rho_e, rho_i = me * n0, mi * n0
+    state = [rho_e, rho_e * a, 0.0, 0.0, pe / (ge - 1) + 0.5 * rho_e * a * a,
+             rho_i, 0.0, 0.0, 0.0, pi / (gi - 1)] + [0.0] * 7
+    s.fill_ic(M.IC_CONSTANT, state)
+    T = G["langmuir_3d_p3.t_final"]
+    dt_est = G["langmuir_3d_p3.cfl"] * (lx / nx) / (max(c, c_h) * (2 * P + 1))
+    nsteps = int(T / dt_est) + 1
+    s.step_n(T / nsteps, nsteps)
+    q = s.download_state().astype(np.float64)
+    s.close()
+    assert np.isfinite(q).all()
+    wp = np.sqrt(n0 * (qe * qe / me + qi * qi / mi) / eps0)
+    mom_err = abs(q[..., 1].mean() - a * me * n0) / (a * me * n0)
+    ex_rel = abs(q[..., 10].mean()) / (a * me * n0 * wp)
+    print(f"langmuir {prec}: {nsteps} steps, momentum drift {mom_err:.2e}, E_x {ex_rel:.2e}")
+    assert mom_err < G["langmuir_3d_p3.drift_tol_rel"], mom_err
+    assert ex_rel < G["langmuir_3d_p3.drift_tol_rel"], ex_rel

@@ -252,3 +252,44 @@ def test_mhd_wavespeed_and_integrals(oracle_mod):
         want = vol * float((q[..., c] * w[None, :]).sum())
         assert abs(s.integral(c) - want) <= 1e-13 * max(abs(want), 1e-3)
     assert abs(s.max_wavespeed() - o.max_face_speed()) <= 1e-13 * o.max_face_speed()
+
+
+@pytest.mark.parametrize("bcname", list(C.BCS_3D))
+@pytest.mark.parametrize("P", [1, 2, 3, 4])
+def test_two_fluid_rhs_f64(oracle_mod, bcname, P):
+    phys = C.two_fluid()
+    s, o = make_pair(oracle_mod, phys, P, N3, L3, C.BCS_3D[bcname])
+    q = C.random_state(s.shape, phys, seed=71 + P)
+    assert C.rel_err(s.rhs(q), o.rhs(q)) <= C.TOL_F64_3D[P]
+
+
+@pytest.mark.parametrize("prec", ["f32", "mixed"])
+@pytest.mark.parametrize("P", [2, 3, 5])
+def test_two_fluid_rhs_reduced(oracle_mod, prec, P):
+    """17 components: MIXED runs the FP32 kernel (no tensor-core tile)."""
+    phys = C.two_fluid()
+    s, o = make_pair(oracle_mod, phys, P, N3, L3, C.BCS_3D["walls"], prec=prec)
+    q = C.random_state(s.shape, phys, seed=81)
+    qf = q.astype(np.float32).astype(np.float64)
+    assert C.rel_err(s.rhs(qf), o.rhs(qf)) <= C.TOL_F32
+
+
+@pytest.mark.parametrize("limiter", [False, True])
+def test_two_fluid_steps_f64(oracle_mod, limiter):
+    phys = C.two_fluid()
+    s, o = make_pair(oracle_mod, phys, 2, N3, L3, C.BCS_3D["inflow_outflow"])
+    q = C.random_state(s.shape, phys, seed=91)
+    s.upload_state(q)
+    o.set(q)
+    if limiter:
+        s.enable_cell_limiter(True, 0.1)
+        o.enable_limiter(True, 0.1)
+    s.step_n(1e-3, 3)
+    o.step(1e-3, 3)
+    assert C.rel_err(s.download_state(0), o.get(0)) <= 50 * C.TOL_F64_3D[2]
+    assert abs(s.max_wavespeed() - o.max_face_speed()) <= 1e-13 * o.max_face_speed()
+
+
+def test_two_fluid_f64_p5_refused():
+    with pytest.raises(M.DGError):
+        M.Solver(M.Mesh(2, 2, 2), C.two_fluid(), P=5, precision="f64")
