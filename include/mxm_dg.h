@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define MXM_DG_VERSION 10000 /* 1.0.0 */
+#define MXM_DG_VERSION 20000 /* 2.0.0: physics descriptor p[32] (was p[16]) */
 
 /* Return codes (mpi_shim.c returns the MPI error code; we use negatives). */
 #define MXM_DG_OK 0
