@@ -183,8 +183,12 @@ int mxm_dg_advance_host(void* handle, const void* q_host, void* q_out_host, int 
  * return (discarded by the reference, solver.mojo:266-268), on d_q. */
 int mxm_dg_max_wavespeed(void* handle, double* out);
 /* kind 0: integral of q_c over the domain (sum_e V_e sum_i w_i q);
- * kind 1: integral of q_c^2 (nodal quadrature); kind 2: max |q_c|.
- * Reductions accumulate in FP64 on the device in a fixed order. */
+ * kind 1: integral of q_c^2 (nodal quadrature); kind 2: max |q_c|;
+ * kinds 3 and 4: the reference's DiagnosticsWriter "linear" and "squared"
+ * rows (src/diagnostics.mojo:162-229), sum over all nodes of q_c (q_c^2)
+ * times domain volume / (elements x nodes per element), without the
+ * per-component download.  Reductions accumulate in FP64 on the device in a
+ * fixed order. */
 int mxm_dg_reduce_conserved(void* handle, int which, int c, int kind, double* out);
 /* The same reduction without any device allocation; it has no counterpart
  * in the reference.  Its scratch is a static device array of the library

@@ -510,6 +510,50 @@ class Solver:
         return out
 
 
+class DiagComponents:  # src/diagnostics.mojo:73-94
+    """Named components for DiagnosticsWriter: linear (sum q), squared (sum q^2), max |q|."""
+
+    def __init__(self):
+        self.linear_, self.squared_, self.maxabs_ = [], [], []
+
+    def linear(self, name, c):
+        self.linear_.append((name, c))
+        return self
+
+    def squared(self, name, c):
+        self.squared_.append((name, c))
+        return self
+
+    def maxabs(self, name, c):
+        self.maxabs_.append((name, c))
+        return self
+
+
+class DiagnosticsWriter:  # src/diagnostics.mojo:96-229
+    """CSV diagnostics of a Solver with the reference's columns and
+    definitions (linear / squared rows: node sums times domain volume /
+    (elements x nodes); max |q|), computed by FP64 device reductions
+    (reduction kinds 3, 4, 2) instead of downloading each component."""
+
+    def __init__(self, solver, components, csv_path=None):
+        self.solver, self.comp, self.csv_path = solver, components, csv_path
+        self.last_row = []
+        if csv_path:
+            cols = ["t"] + [n for n, _ in components.linear_ + components.squared_ + components.maxabs_]
+            with open(csv_path, "w") as f:
+                f.write(",".join(cols) + "\n")
+
+    def record(self, t, which=0):
+        s = self.solver
+        self.last_row = ([s.integral(c, which, kind=3) for _, c in self.comp.linear_] +
+                         [s.integral(c, which, kind=4) for _, c in self.comp.squared_] +
+                         [s.integral(c, which, kind=2) for _, c in self.comp.maxabs_])
+        if self.csv_path:
+            with open(self.csv_path, "a") as f:
+                f.write(",".join(repr(float(v)) for v in [t] + self.last_row) + "\n")
+        return self.last_row
+
+
 class Batch:
     """Many independent 2D solves advanced together (mxm_dg_batch_*): one
     persistent stage launch per physics group and stage, the SSPRK3 step

@@ -450,6 +450,19 @@ void step_n(Handle* h, double dt, int n) {
   }
 }
 
+// Factor applied to a reduction's FP64 sum: the element volume (quadrature
+// integrals, kinds 0-1), 1 (max, kind 2), or the reference diagnostics'
+// domain volume / (elements x nodes) for its plain node sums (kinds 3-4,
+// src/diagnostics.mojo:135-140,169-192).
+double reduce_scale(const Handle* h, int kind) {
+  if (kind == 2) return 1.0;
+  if (kind >= 3) {
+    const double dom = h->dim == 3 ? h->lx * h->ly * h->lz : h->lx * h->ly;
+    return dom / (double(h->ne) * h->NP);
+  }
+  return h->dim == 3 ? (h->lx / h->nx) * (h->ly / h->ny) * (h->lz / h->nz) / 6.0 : (h->lx / h->nx) * (h->ly / h->ny) / 2.0;
+}
+
 // Float32 node coordinates exactly as the reference builds elem_node_xyz.
 void build_xyz(Handle* h) {
   std::vector<float> x(size_t(h->ne) * h->NP * h->dim);
@@ -910,11 +923,9 @@ int mxm_dg_max_wavespeed(void* handle, double* out) {
 
 int mxm_dg_reduce_conserved(void* handle, int which, int c, int kind, double* out) {
   API_BEGIN
-  if (which < 0 || which > 2 || c < 0 || c >= h->NC || kind < 0 || kind > 2)
-    throw mxm::ArgError("which 0..2, component in range, kind 0..2");
-  const double vol = h->dim == 3 ? (h->lx / h->nx) * (h->ly / h->ny) * (h->lz / h->nz) / 6.0
-                                 : (h->lx / h->nx) * (h->ly / h->ny) / 2.0;
-  const double scale = kind == 2 ? 1.0 : vol;
+  if (which < 0 || which > 2 || c < 0 || c >= h->NC || kind < 0 || kind > 4)
+    throw mxm::ArgError("which 0..2, component in range, kind 0..4");
+  const double scale = mxm::reduce_scale(h, kind);
   cudaError_t e = h->rbytes == 8
                       ? mxm::launch_reduce<double>(h->P, h->dim, h->NC, (const double*)h->q[which], (const double*)h->w,
                                                    h->ne, c, kind, scale, h->partial, h->npartial, h->dscalar, h->stream)
@@ -946,8 +957,8 @@ double* g_static_scratch[64] = {};
 
 int mxm_dg_reduce_conserved_noalloc(void* handle, int which, int c, int kind, int nblocks, double* out) {
   API_BEGIN
-  if (which < 0 || which > 2 || c < 0 || c >= h->NC || kind < 0 || kind > 2 || !out)
-    throw mxm::ArgError("which 0..2, component in range, kind 0..2, out non-null");
+  if (which < 0 || which > 2 || c < 0 || c >= h->NC || kind < 0 || kind > 4 || !out)
+    throw mxm::ArgError("which 0..2, component in range, kind 0..4, out non-null");
   if (nblocks < 0 || nblocks > mxm::kStaticPartials)
     throw mxm::ArgError("nblocks " + std::to_string(nblocks) + " is outside 0.." +
                         std::to_string(mxm::kStaticPartials) + ", the size of the static reduction scratch");
@@ -962,9 +973,7 @@ int mxm_dg_reduce_conserved_noalloc(void* handle, int which, int c, int kind, in
   }
   const int64_t want = (h->ne + 255) / 256;
   const int nb = nblocks > 0 ? nblocks : int(want < h->npartial ? want : h->npartial);
-  const double vol = h->dim == 3 ? (h->lx / h->nx) * (h->ly / h->ny) * (h->lz / h->nz) / 6.0
-                                 : (h->lx / h->nx) * (h->ly / h->ny) / 2.0;
-  const double scale = kind == 2 ? 1.0 : vol;
+  const double scale = mxm::reduce_scale(h, kind);
   double* result = scratch + mxm::kStaticPartials;
   cudaError_t e = h->rbytes == 8
                       ? mxm::launch_reduce<double>(h->P, h->dim, h->NC, (const double*)h->q[which], (const double*)h->w,

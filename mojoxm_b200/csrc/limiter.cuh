@@ -233,6 +233,8 @@ __global__ void reduce_partial_kernel(const R* q, const R* w, int64_t ne, int c,
       const double v = double(qe[n * NC]);
       if (kind == 0) s += double(__ldg(&w[n])) * v;
       else if (kind == 1) s += double(__ldg(&w[n])) * v * v;
+      else if (kind == 3) s += v;
+      else if (kind == 4) s += v * v;
       else s = fmax(s, fabs(v));
     }
     if (kind == 2) acc = fmax(acc, s);

@@ -293,3 +293,23 @@ def test_two_fluid_steps_f64(oracle_mod, limiter):
 def test_two_fluid_f64_p5_refused():
     with pytest.raises(M.DGError):
         M.Solver(M.Mesh(2, 2, 2), C.two_fluid(), P=5, precision="f64")
+
+
+def test_reference_diagnostics_rows(tmp_path):
+    """DiagnosticsWriter rows (src/diagnostics.mojo:162-229) from device
+    reductions: sum q and sum q^2 over all nodes times domain volume /
+    (elements x nodes), and max |q|, against the same sums in numpy."""
+    phys = C.PHYSICS_3D["euler_rusanov"]()
+    s = M.Solver(M.Mesh(*N3, *L3), phys, P=3, precision="f32")
+    q = C.random_state(s.shape, phys, seed=23).astype(np.float32).astype(np.float64)
+    s.upload_state(q)
+    dw = M.DiagnosticsWriter(s, M.DiagComponents().linear("mass", 0).squared("rho2", 0).maxabs("maxE", 4),
+                             csv_path=str(tmp_path / "diag.csv"))
+    row = dw.record(0.5)
+    scale = L3[0] * L3[1] * L3[2] / (q.shape[0] * q.shape[1])
+    assert abs(row[0] - q[..., 0].sum() * scale) <= 1e-13 * abs(row[0])
+    assert abs(row[1] - (q[..., 0] ** 2).sum() * scale) <= 1e-13 * abs(row[1])
+    assert row[2] == np.abs(q[..., 4]).max()
+    lines = open(tmp_path / "diag.csv").read().splitlines()
+    assert lines[0] == "t,mass,rho2,maxE" and lines[1].startswith("0.5,")
+    s.close()
