@@ -20,6 +20,7 @@
 #include "batch2d.cuh"
 #include "batch2d_launch.hpp"
 #include "handle.hpp"
+#include "ic.hpp"
 
 namespace mxm {
 
@@ -291,6 +292,13 @@ void build(Batch* b) {
       cap = launch_lim2d_batch<R>(g.NC, la, b->stream);
     }
   }
+  // 2D GLM-MHD members: psi *= exp(-alpha_d dt) after the step, each with its own dt
+  for (size_t i = 0; i < b->members.size() && cap == cudaSuccess; ++i) {
+    const Handle* h = b->members[i];
+    if (!glm_damped(h)) continue;
+    cap = launch_scale_component(h->q[0], h->rbytes, h->ne * h->NP, h->NC, h->NC - 1, psi_decay(h, b->dt[i]),
+                                 b->stream);
+  }
   cudaGraph_t graph = nullptr;
   const cudaError_t end = cudaStreamEndCapture(b->stream, &graph);
   if (cap != cudaSuccess) {
@@ -382,8 +390,6 @@ int mxm_dg_batch_add(void* batch, void* solver, double dt, int32_t* index) {
   mxm::Handle* h = (mxm::Handle*)solver;
   if (!h) throw mxm::ArgError("null solver handle");
   if (h->dim != 2) throw mxm::ArgError("batched solves are 2D (triangle meshes)");
-  if (h->phys.kind == MXM_DG_PHYS_MHD || h->phys.kind == MXM_DG_PHYS_MHD_PLAIN)
-    throw mxm::ArgError("2D MHD solves are not batched (run them through their own handles)");
   if (h->device != b->device) throw mxm::ArgError("solver lives on another device than the batch");
   if (!(dt > 0.0)) throw mxm::ArgError("dt must be positive");
   if (b->rbytes && h->rbytes != b->rbytes) throw mxm::ArgError("all solves of a batch share one precision");
@@ -491,6 +497,7 @@ int mxm_dg_batch_launches_per_step(void* batch, int32_t* n) {
     for (int m : g.members) lim = lim || b->members[m]->lim_on;
     k += 3 * (lim ? 3 : 1);
   }
+  for (const mxm::Handle* h : b->members) k += mxm::glm_damped(h) ? 1 : 0;  // psi damping
   *n = k;
   BATCH_END
 }

@@ -47,6 +47,17 @@ cudaError_t with_phys2d(const mxm_dg_physics_desc& pd, F&& f) {
       for (int k = 0; k < 6; ++k) ph.inflow[k] = R(p[7 + k]);
       return f(ph);
     }
+    case MXM_DG_PHYS_MHD:
+    case MXM_DG_PHYS_MHD_PLAIN: {  // state (rho, mx, my, Bx, By, E[, psi]) from the 3D layout
+      auto mk = [&](auto ph) {
+        ph.gamma = R(p[0]); ph.rho_min = R(p[1]); ph.p_min = R(p[2]); ph.c_h = R(p[3]);
+        const int map[7] = {5, 6, 7, 10, 11, 9, 13};
+        for (int k = 0; k < 7; ++k) ph.inflow[k] = R(p[map[k]]);
+        return f(ph);
+      };
+      if (pd.kind == MXM_DG_PHYS_MHD) return mk(Mhd2D<R, true>{});
+      return mk(Mhd2D<R, false>{});
+    }
   }
   return cudaErrorInvalidValue;
 }
@@ -83,6 +94,7 @@ cudaError_t prepare_lim2d_batch(int NC) {
     case 3: return lim2d_batch_attr<R, 3>();
     case 4: return lim2d_batch_attr<R, 4>();
     case 6: return lim2d_batch_attr<R, 6>();
+    case 7: return lim2d_batch_attr<R, 7>();
   }
   return cudaErrorInvalidValue;
 }
@@ -103,6 +115,7 @@ cudaError_t launch_lim2d_batch(int NC, const LimBatch2DArgs<R>& la, cudaStream_t
     case 3: return lim2d_batch_nc<R, 3>(la, st);
     case 4: return lim2d_batch_nc<R, 4>(la, st);
     case 6: return lim2d_batch_nc<R, 6>(la, st);
+    case 7: return lim2d_batch_nc<R, 7>(la, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -430,17 +430,19 @@ void rk_stage(Handle* h, int s, double dt) {
   if (h->lim_on) limit_buf(h, s == 0 ? q1 : (s == 1 ? q2 : q0));
 }
 
+// 2D GLM-MHD: psi *= exp(-alpha_d dt) once per SSPRK3 step, operator-split
+// after the step (local_mesh_2d_gpu_mhd_glm.mojo:464-485); the factor as the
+// reference forms it: FP64 exp of the (FP32 in the FP32 paths) inputs.
+bool glm_damped(const Handle* h) { return h->dim == 2 && h->phys.kind == MXM_DG_PHYS_MHD && h->phys.p[4] > 0.0; }
+double psi_decay(const Handle* h, double dt) {
+  const double ad = h->rbytes == 8 ? h->phys.p[4] : double(float(h->phys.p[4]));
+  const double dd = h->rbytes == 8 ? dt : double(float(dt));
+  return std::exp(-ad * dd);
+}
+
 void step_n(Handle* h, double dt, int n) {
-  // 2D GLM-MHD: psi *= exp(-alpha_d dt) once per SSPRK3 step, operator-split
-  // after the step (local_mesh_2d_gpu_mhd_glm.mojo:464-485); the factor as
-  // the reference forms it: FP64 exp of the (FP32 in the FP32 paths) inputs
-  const bool damp = h->dim == 2 && h->phys.kind == MXM_DG_PHYS_MHD && h->phys.p[4] > 0.0;
-  double decay = 1.0;
-  if (damp) {
-    const double ad = h->rbytes == 8 ? h->phys.p[4] : double(float(h->phys.p[4]));
-    const double dd = h->rbytes == 8 ? dt : double(float(dt));
-    decay = std::exp(-ad * dd);
-  }
+  const bool damp = glm_damped(h);
+  const double decay = damp ? psi_decay(h, dt) : 1.0;
   for (int k = 0; k < n; ++k) {
     for (int s = 0; s < 3; ++s) rk_stage(h, s, dt);
     if (damp) {

@@ -78,5 +78,8 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
 void destroy(Handle* h);
 void step_n(Handle* h, double dt, int n);
 void fill_ic(Handle* h, int which, int kind, const double* params, int nparams);
+// 2D GLM-MHD psi damping after each step: whether h has it, and its factor
+bool glm_damped(const Handle* h);
+double psi_decay(const Handle* h, double dt);
 
 }  // namespace mxm

@@ -73,3 +73,30 @@ def test_batch_rejects_3d_and_mixed_precision():
     with pytest.raises(M.DGError):
         batch.add(a, 1e-3)  # already a member
     batch.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_batch_mhd2d_members_match_alone(prec):
+    """2D MHD in a batch (plain and GLM, limited and not, uneven dt): each
+    member equals the same solve stepped alone, psi damping included."""
+    cases = [(6, 3, "mhd_glm", True, "walls", 1e-3), (5, 2, "mhd_plain", False, "periodic", 2e-3),
+             (4, 4, "mhd_glm", False, "inflow_outflow", 5e-4), (7, 1, "euler_hlle", True, "periodic", 1e-3)]
+    solo, mem, b = [], [], M.Batch()
+    for k, (n, P, name, lim, bcn, dt) in enumerate(cases):
+        for lst in (solo, mem):
+            s, phys = _make(prec, n, P, name, lim, bcn)
+            q = C.random_state(s.shape, phys, seed=200 + k)
+            s.upload_state(q)
+            lst.append((s, dt))
+        b.add(mem[-1][0], dt)
+    b.step(4)
+    b.synchronize()
+    for (s1, dt), (s2, _) in zip(solo, mem):
+        s1.step_n(dt, 4)
+        a, c = s1.download_state(), s2.download_state()
+        assert np.array_equal(a, c)
+        s1.close()
+    b.close()
+    for s2, _ in mem:
+        s2.close()

@@ -229,15 +229,6 @@ def test_mhd2d_steps(oracle_mod, name, bcname, prec):
     assert C.rel_err(s.download_state(0), o.get(0)) <= (50 * C.TOL_F64_2D[P] if prec == "f64" else 1e-4)
 
 
-def test_mhd2d_batch_rejected():
-    s = M.Solver(M.Mesh(4, 4, dim=2), C.PHYSICS_2D["mhd_glm"](), P=2, precision="f32")
-    b = M.Batch()
-    with pytest.raises(M.DGError):
-        b.add(s, 1e-3)
-    b.close()
-    s.close()
-
-
 def test_mhd_wavespeed_and_integrals(oracle_mod):
     """3D MHD: the CFL reduction (max Rusanov alpha over face nodes) and the
     FP64 integrals of all nine components."""
