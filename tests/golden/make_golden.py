@@ -117,6 +117,20 @@ ENTRIES = [
      "comptime T_FINAL: Float32 = Float32(6.1612348)"),
     ("langmuir_3d_p3.drift_tol_rel", 0.02, "benchmarks/bench_two_fluid_langmuir_3d_p3.mojo", "92",
      "comptime DRIFT_TOL_REL: Float64 = 0.02"),
+    # outputs of the reference itself, as its README reports them for three
+    # periodic 2D drivers (relative L2 against the IC after one period)
+    ("reported.adv2d_gauss.rel_l2", 0.0007, "README.md", "187-188", "0.07 % rel L2 over one period"),
+    ("reported.euler2d_vortex.rel_l2", 0.068, "README.md", "189", "6.8 % rel L2 at P=2 / 32x32"),
+    ("reported.mhd2d_alfven.rel_l2", 0.0036, "README.md", "191-192", "0.36 % rel L2 on a one-period"),
+    # P, NX, NY, LX, LY, VX, VY, T, frames, CFL, sigma, cx, cy
+    ("adv2d_gauss.config", [2, 32, 32, 1.0, 1.0, 1.0, 1.0, 1.0, 20, 0.3, 0.12, 0.5, 0.5],
+     "examples/advection_gaussian_2d_gpu.mojo", "29-41", "comptime SIGMA: Float32 = 0.12"),
+    # P, NX, NY, LX, LY, T, frames, CFL, gamma, T_inf, u0, v0, beta, cx, cy
+    ("euler2d_vortex.config", [2, 32, 32, 10.0, 10.0, 10.0, 20, 0.15, 1.4, 1.0, 1.0, 1.0, 5.0, 5.0, 5.0],
+     "examples/euler_vortex_2d_gpu.mojo", "36-51", "comptime BETA = 5.0"),
+    # P, NX, NY, LX, LY, gamma, rho0, B0, p0, amplitude, T, frames, CFL
+    ("mhd2d_alfven.config", [2, 64, 4, 1.0, 4.0 / 64.0, 5.0 / 3.0, 1.0, 1.0, 0.1, 0.1, 1.0, 20, 0.15],
+     "examples/mhd_alfven_2d_gpu.mojo", "39-54", "comptime LY = Float64(4.0 / 64.0)"),
 ]
 
 
