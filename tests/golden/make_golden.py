@@ -131,6 +131,10 @@ ENTRIES = [
     # P, NX, NY, LX, LY, gamma, rho0, B0, p0, amplitude, T, frames, CFL
     ("mhd2d_alfven.config", [2, 64, 4, 1.0, 4.0 / 64.0, 5.0 / 3.0, 1.0, 1.0, 0.1, 0.1, 1.0, 20, 0.15],
      "examples/mhd_alfven_2d_gpu.mojo", "39-54", "comptime LY = Float64(4.0 / 64.0)"),
+    ("reported.euler3d_vortex.rel_l2", 0.068, "README.md", "369-371", "rel L2 ~6.8 %%"),
+    # NX, NY, NZ, LX, LY, T, CFL, gamma, T_inf, u0, v0, beta, cx, cy (LZ = NZ / NX * LX; HLLEC, no fix)
+    ("euler3d_vortex.config", [32, 32, 4, 10.0, 10.0, 10.0, 0.15, 1.4, 1.0, 1.0, 1.0, 5.0, 5.0, 5.0],
+     "benchmarks/bench_euler_vortex_3d.mojo", "49-64", "comptime LZ = Float64(NZ) / Float64(NX) * LX"),
 ]
 
 

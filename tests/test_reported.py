@@ -142,3 +142,54 @@ def test_product_reproduces_reported_output(name):
     print(f"product {name}: {steps} steps, rel L2 {100 * err:.4f} % (reported {100 * want:g} %)")
     lo, hi = INTERVAL[name]
     assert lo <= err < hi, err
+
+
+def vortex3d_case(P):
+    """benchmarks/bench_euler_vortex_3d.mojo(+_p3): the 2D vortex extruded in z
+    on 32 x 32 x 4 cubes, HLLEC without the entropy fix, T = 10; IC and dt in
+    Float32 (:78-117, :162-167)."""
+    nx, ny, nz, lx, ly, T, cfl, gamma, tinf, u0, v0, beta, cx, cy = G["euler3d_vortex.config"]
+    lz = nz / nx * lx
+    two_pi = f32(2.0) * f32(np.pi)
+    wave = np.sqrt(f32(u0) * f32(u0) + f32(v0) * f32(v0)) + np.sqrt(f32(gamma) * f32(tinf)) + f32(beta) / two_pi
+    dt_est = f32(cfl) * (f32(lx) / f32(nx)) / (wave * f32(5.0))
+    steps = int(f32(T) / dt_est) + 1
+    dt = float(f32(T) / f32(steps))
+
+    def ic(xyz):
+        x, y = xyz[..., 0].astype(f32), xyz[..., 1].astype(f32)
+        dx, dy = x - f32(cx), y - f32(cy)
+        dx = np.where(dx > f32(lx * 0.5), dx - f32(lx), dx)
+        dx = np.where(dx < -f32(lx * 0.5), dx + f32(lx), dx)
+        dy = np.where(dy > f32(ly * 0.5), dy - f32(ly), dy)
+        dy = np.where(dy < -f32(ly * 0.5), dy + f32(ly), dy)
+        r2 = dx * dx + dy * dy
+        g = f32(gamma)
+        factor = (g - f32(1.0)) * f32(beta) * f32(beta) / (f32(8.0) * g * two_pi * two_pi)
+        Tv = f32(tinf) - factor * np.exp(f32(1.0) - r2)
+        e_half = np.exp(f32(0.5) * (f32(1.0) - r2))
+        u = f32(u0) - (f32(beta) / two_pi) * dy * e_half
+        v = f32(v0) + (f32(beta) / two_pi) * dx * e_half
+        rho = Tv ** (f32(1.0) / (g - f32(1.0)))
+        p = rho * Tv
+        E = p / (g - f32(1.0)) + f32(0.5) * rho * (u * u + v * v)
+        z = np.zeros_like(rho)
+        return np.stack([rho, rho * u, rho * v, z, E], -1).astype(f32)
+
+    ph = M.Euler(gamma, 1e-6, 1e-6, M.FLUX_HLLEC, False)
+    return ph, (int(nx), int(ny), int(nz)), (lx, ly, lz), dt, steps, ic
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("P", [2, 3])
+def test_product_reproduces_reported_3d_vortex(P):
+    """README.md:369-373: rel L2 ~6.8 % over one period at P=2 and P=3."""
+    ph, n, L, dt, steps, ic = vortex3d_case(P)
+    s = M.Solver(M.Mesh(*n, *L), ph, P=P, precision="f32")
+    q0 = ic(s.node_xyz())
+    s.upload_state(q0.astype(np.float64))
+    s.step_n(dt, steps)
+    err = rel_l2(s.download_state(), q0)
+    s.close()
+    print(f"product 3D vortex P{P}: {steps} steps, rel L2 {100 * err:.3f} % (reported ~6.8 %)")
+    assert 0.0675 <= err < 0.0685, err
