@@ -135,6 +135,23 @@ ENTRIES = [
     # NX, NY, NZ, LX, LY, T, CFL, gamma, T_inf, u0, v0, beta, cx, cy (LZ = NZ / NX * LX; HLLEC, no fix)
     ("euler3d_vortex.config", [32, 32, 4, 10.0, 10.0, 10.0, 0.15, 1.4, 1.0, 1.0, 1.0, 5.0, 5.0, 5.0],
      "benchmarks/bench_euler_vortex_3d.mojo", "49-64", "comptime LZ = Float64(NZ) / Float64(NX) * LX"),
+    ("reported.maxwell_cavity_2d.rel_l2", 2.8e-4, "benchmarks/bench_maxwell_cavity_2d.mojo", "53",
+     "Measured 2.8e-4 on current code (NX=NY=16, P=2, 566 SSPRK3 steps)"),
+    ("reported.maxwell_cavity_2d.steps", 566, "benchmarks/bench_maxwell_cavity_2d.mojo", "53", "566 SSPRK3 steps"),
+    # P, NX, NY, LX, LY, c, CFL, T (PEC walls; Ez = sin(pi x) sin(pi y))
+    ("maxwell_cavity_2d.config", [2, 16, 16, 1.0, 1.0, 1.0, 0.2, 1.41421356237],
+     "benchmarks/bench_maxwell_cavity_2d.mojo", "42-51", "comptime T_FINAL: Float64 = 1.41421356237"),
+    ("reported.maxwell_plane_wave_2d.rel_l2", 5.8e-4, "benchmarks/bench_maxwell_plane_wave_2d.mojo", "64",
+     "Empirical: ~5.8e-4 at P=2, NX=NY=16"),
+    ("reported.maxwell_plane_wave_2d.leakage", 2.7e-4, "benchmarks/bench_maxwell_plane_wave_2d.mojo", "68",
+     "Empirical zero-component leakage ~2.7e-4"),
+    # P, NX, NY, LX, LY, c, CFL, T (periodic; Ez = cos(2 pi x), By = -Ez / c)
+    ("maxwell_plane_wave_2d.config", [2, 16, 16, 1.0, 1.0, 1.0, 0.2, 1.0],
+     "benchmarks/bench_maxwell_plane_wave_2d.mojo", "54-62", "comptime T_FINAL: Float64 = 1.0  # exactly one period"),
+    ("reported.mhd_alfven_3d.rel_l2", 3.6e-3, "benchmarks/bench_mhd_alfven_3d.mojo", "59", "Measured ~3.6e-3"),
+    # P, NX, NY, NZ, LX, LY, LZ, CFL (physics and IC as mhd_alfven_3d_p3)
+    ("mhd_alfven_3d.config", [2, 32, 4, 4, 1.0, 0.125, 0.125, 0.2], "benchmarks/bench_mhd_alfven_3d.mojo", "36-55",
+     "comptime LY = Float64(4.0 / 32.0)"),
 ]
 
 

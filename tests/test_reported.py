@@ -193,3 +193,93 @@ def test_product_reproduces_reported_3d_vortex(P):
     s.close()
     print(f"product 3D vortex P{P}: {steps} steps, rel L2 {100 * err:.3f} % (reported ~6.8 %)")
     assert 0.0675 <= err < 0.0685, err
+
+
+def maxwell2d_case(name):
+    """benchmarks/bench_maxwell_cavity_2d.mojo / bench_maxwell_plane_wave_2d.mojo
+    (P2, 16 x 16, c = 1, dt = CFL h / (c (2P+1)) in Float64, rounded to Float32)."""
+    P, nx, ny, lx, ly, c, cfl, T = G[f"{name}.config"]
+    dt_est = cfl * (lx / nx) / (c * (2 * P + 1))
+    steps = int(T / dt_est) + 1
+    dt = float(f32(T / steps))
+    cavity = name == "maxwell_cavity_2d"
+    bcs = (1, 1, 1, 1) if cavity else (0, 0, 0, 0)
+
+    def ic(xy):
+        x, y = xy[..., 0].astype(np.float64), xy[..., 1].astype(np.float64)
+        q = np.zeros(xy.shape[:-1] + (6,))
+        if cavity:
+            q[..., 2] = np.sin(np.pi * x) * np.sin(np.pi * y)
+        else:
+            q[..., 2] = np.cos(2.0 * np.pi * x)
+            q[..., 4] = -(1.0 / c) * np.cos(2.0 * np.pi * x)
+        return q.astype(f32)
+
+    return M.Maxwell(c), int(P), (int(nx), int(ny)), (lx, ly), bcs, dt, steps, ic
+
+
+MAXWELL = {"maxwell_cavity_2d": (2.75e-4, 2.85e-4), "maxwell_plane_wave_2d": (5.75e-4, 5.85e-4)}
+
+
+def leakage(q):
+    return float(np.abs(q[..., [0, 1, 3, 5]]).max())
+
+
+@pytest.mark.parametrize("name", list(MAXWELL))
+def test_oracle_reproduces_reported_maxwell_2d(oracle_mod, name):
+    ph, P, n, L, bcs, dt, steps, ic = maxwell2d_case(name)
+    if name == "maxwell_cavity_2d":
+        assert steps == G["reported.maxwell_cavity_2d.steps"]
+    o = oracle_mod.Oracle2D(P, n, L, M.physics_dict(ph), bcs=bcs, real="f32")
+    q0 = ic(o.node_xy())
+    o.set(q0.astype(np.float64))
+    o.step(dt, steps)
+    q = o.get()
+    err = rel_l2(q, q0)
+    print(f"oracle {name}: {steps} steps, rel L2 {err:.3e} (reported {G['reported.' + name + '.rel_l2']:g})")
+    lo, hi = MAXWELL[name]
+    assert lo <= err < hi, err
+    if name == "maxwell_plane_wave_2d":
+        assert 2.65e-4 <= leakage(q) < 2.75e-4, leakage(q)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(MAXWELL))
+def test_product_reproduces_reported_maxwell_2d(name):
+    ph, P, n, L, bcs, dt, steps, ic = maxwell2d_case(name)
+    mesh = M.Mesh(n[0], n[1], 1, L[0], L[1], 1.0, bcs=M.BoundaryConditions(*bcs, 0, 0), dim=2)
+    s = M.Solver(mesh, ph, P=P, precision="f32")
+    q0 = ic(s.node_xyz())
+    s.upload_state(q0.astype(np.float64))
+    s.step_n(dt, steps)
+    q = s.download_state()
+    s.close()
+    err = rel_l2(q, q0)
+    print(f"product {name}: {steps} steps, rel L2 {err:.3e}, leakage {leakage(q):.2e}")
+    lo, hi = MAXWELL[name]
+    assert lo <= err < hi, err
+    if name == "maxwell_plane_wave_2d":
+        assert 2.65e-4 <= leakage(q) < 2.75e-4, leakage(q)
+
+
+@pytest.mark.gpu
+def test_product_reproduces_reported_mhd_alfven_3d():
+    """benchmarks/bench_mhd_alfven_3d.mojo: 'Measured ~3.6e-3' at P2, 32 x 4 x 4,
+    CFL 0.2, dt = CFL h / (max(c_f, c_h) 5) in Float32 (:141-148)."""
+    P, nx, ny, nz, lx, ly, lz, cfl = G["mhd_alfven_3d.config"]
+    gamma, rho0, b0, p0, amp = G["mhd_alfven_3d_p3.gamma_rho0_b0_p0_amp"]
+    c_h, alpha_d = G["mhd_alfven_3d_p3.c_h_alpha_d"]
+    cf = np.sqrt(f32(gamma) * f32(p0) / f32(rho0) + (f32(b0) * f32(b0) + f32(amp) * f32(amp)) / f32(rho0))
+    wave = max(cf, f32(c_h))
+    dt_est = f32(cfl) * (f32(lx) / f32(nx)) / (wave * f32(5.0))
+    steps = int(f32(1.0) / dt_est) + 1
+    dt = float(f32(1.0) / f32(steps))
+    ph = M.IdealMHD(gamma, 1e-6, 1e-6, c_h, alpha_d)
+    s = M.Solver(M.Mesh(int(nx), int(ny), int(nz), lx, ly, lz), ph, P=int(P), precision="f32")
+    s.fill_ic(M.IC_ALFVEN, [rho0, b0, p0, amp, 1.0])
+    q0 = s.download_state()
+    s.step_n(dt, steps)
+    err = rel_l2(s.download_state(), q0)
+    s.close()
+    print(f"product 3D MHD Alfven P2: {steps} steps, rel L2 {err:.3e} (reported ~3.6e-3)")
+    assert 3.55e-3 <= err < 3.65e-3, err
