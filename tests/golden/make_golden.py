@@ -152,6 +152,24 @@ ENTRIES = [
     # P, NX, NY, NZ, LX, LY, LZ, CFL (physics and IC as mhd_alfven_3d_p3)
     ("mhd_alfven_3d.config", [2, 32, 4, 4, 1.0, 0.125, 0.125, 0.2], "benchmarks/bench_mhd_alfven_3d.mojo", "36-55",
      "comptime LY = Float64(4.0 / 32.0)"),
+    # further "Measured" / "Empirical" values in the benches' own comments
+    ("reported.adv3d_p2_n16.rel_l2", 9.5e-3, "benchmarks/bench_advection_3d.mojo", "49",
+     "Measured rel L2 at N=16 is ~9.5e-3"),
+    ("reported.adv3d_p3_n12.rel_l2", 2.4e-3, "benchmarks/bench_advection_3d_p3.mojo", "55", "Measured ~2.4e-3 at N=12"),
+    ("reported.adv2d_translation_n32.rel_l2", 7.2e-4, "benchmarks/bench_advection_translation_2d.mojo", "49",
+     "Measured ~7.2e-4 at N=32"),
+    ("reported.euler2d_vortex_p3_hllc.rel_l2", 0.0681, "benchmarks/bench_euler_vortex_2d_p3.mojo", "61",
+     "Empirical 6.81%% at P=3 / HLLC"),
+    ("reported.maxwell_plane_wave_3d.rel_l2", 6.5e-4, "benchmarks/bench_maxwell_plane_wave_3d.mojo", "59",
+     "Empirical: ~6.5e-4 at NX=16 NY=NZ=4 P=2"),
+    ("reported.maxwell_plane_wave_3d.leakage", 4.5e-4, "benchmarks/bench_maxwell_plane_wave_3d.mojo", "61",
+     "Empirical leakage ~4.5e-4"),
+    ("reported.sw_wave_2d_hll.rel_l2", 1.7e-4, "benchmarks/bench_shallow_water_wave_2d.mojo", "54",
+     "Measured ~1.7e-4 across N = 32, 48, 64"),
+    ("reported.langmuir_3d_p2.drift_and_ex", [3.5e-4, 6e-5], "benchmarks/bench_two_fluid_langmuir_3d.mojo", "25",
+     "Measured values: rho_e u_e drift = 0.035%%, Ex / E_scale = 6e-5"),
+    ("langmuir_3d_p2.mesh", [8, 2, 2, 1.0, 0.25, 0.25], "benchmarks/bench_two_fluid_langmuir_3d.mojo", "53-58",
+     "comptime LZ = Float64(2.0 / 8.0)"),
 ]
 
 

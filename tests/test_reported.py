@@ -283,3 +283,172 @@ def test_product_reproduces_reported_mhd_alfven_3d():
     s.close()
     print(f"product 3D MHD Alfven P2: {steps} steps, rel L2 {err:.3e} (reported ~3.6e-3)")
     assert 3.55e-3 <= err < 3.65e-3, err
+
+
+# ---- further values the benches' comments record for their own runs -----------
+def _gauss_ic(L, c, sigma):
+    """Periodic Gaussian (the advection benches' IC kernels, Float32)."""
+    def ic(x):
+        r2 = np.zeros(x.shape[:-1], f32)
+        for d in range(x.shape[-1]):
+            dd = x[..., d].astype(f32) - f32(c[d])
+            dd = np.where(dd > f32(L[d] * 0.5), dd - f32(L[d]), dd)
+            dd = np.where(dd < -f32(L[d] * 0.5), dd + f32(L[d]), dd)
+            r2 = r2 + dd * dd
+        return np.exp(-r2 * (f32(1.0) / (f32(2.0) * f32(sigma) * f32(sigma))))[..., None].astype(f32)
+    return ic
+
+
+def bench_case(name):
+    """(physics, P, mesh dims, lengths, BCs, dt, steps, IC, band) of one bench run."""
+    if name in ("adv3d_p2_n16", "adv3d_p3_n12"):  # bench_advection_3d(.mojo:37-143), _p3 (:41-148)
+        P, N, cfl = (2, 16, 0.2) if name == "adv3d_p2_n16" else (3, 12, 0.1)
+        v = np.sqrt(f32(3.0))
+        dt_est = f32(cfl) * (f32(1.0) / f32(N)) / (v * f32(2 * P + 1))
+        steps = int(f32(1.0) / dt_est) + 1
+        band = (9.45e-3, 9.55e-3) if P == 2 else (2.35e-3, 2.45e-3)
+        return (M.Advection(1.0, 1.0, 1.0), P, (N, N, N), (1.0, 1.0, 1.0), (0,) * 6, float(f32(1.0) / f32(steps)),
+                steps, _gauss_ic((1.0, 1.0, 1.0), (0.5, 0.5, 0.5), 0.12), band)
+    if name == "adv2d_translation_n32":  # bench_advection_translation_2d.mojo:38-108
+        P, N = 2, 32
+        dt_est = f32(0.3) * (f32(1.0) / f32(N)) / (np.sqrt(f32(2.0)) * f32(2 * P + 1))
+        steps = int(f32(1.0) / dt_est) + 1
+        return (M.Advection(1.0, 1.0, 0.0), P, (N, N), (1.0, 1.0), (0,) * 4, float(f32(1.0) / f32(steps)), steps,
+                _gauss_ic((1.0, 1.0), (0.5, 0.5), 0.12), (7.15e-4, 7.25e-4))
+    if name == "euler2d_vortex_p3_hllc":  # bench_euler_vortex_2d_p3.mojo:47-133 (HLLC, N=32)
+        ph, _, n, L, dt, steps, ic = vortex_case()
+        P = 3
+        two_pi = 2.0 * np.pi
+        wave = np.sqrt(2.0) + np.sqrt(1.4) + 5.0 / two_pi
+        dt_est = 0.15 * (10.0 / 32) / (wave * (2 * P + 1))
+        steps = int(10.0 / dt_est) + 1
+        ph = M.Euler(1.4, 1e-6, 1e-6, M.FLUX_HLLC, False)
+        return ph, P, n, L, (0,) * 4, float(f32(10.0 / steps)), steps, ic, (0.06805, 0.06815)
+    if name == "maxwell_plane_wave_3d":  # bench_maxwell_plane_wave_3d.mojo:46-140 (P2, 16 x 4 x 4 over [0,1]^3)
+        dt_est = f32(0.2) * (f32(1.0) / f32(16)) / (f32(1.0) * f32(5.0))
+        steps = int(f32(1.0) / dt_est) + 1
+        two_pi = f32(6.28318530717958647692)
+
+        def ic(x):
+            q = np.zeros(x.shape[:-1] + (6,), f32)
+            q[..., 2] = np.cos(two_pi * x[..., 0].astype(f32))
+            q[..., 4] = -np.cos(two_pi * x[..., 0].astype(f32))
+            return q
+        return (M.Maxwell(1.0), 2, (16, 4, 4), (1.0, 1.0, 1.0), (0,) * 6, float(f32(1.0) / f32(steps)), steps, ic,
+                (6.45e-4, 6.55e-4))
+    if name == "sw_wave_2d_hll":  # bench_shallow_water_wave_2d.mojo:40-109 (HLL, N=32, square cells)
+        P, N, NY = 2, 32, 4
+        c = 1.0
+        dt_est = 0.15 * (1.0 / N) / (c * (2 * P + 1))
+        steps = int(1.0 / dt_est) + 1
+
+        def ic(x):
+            q = np.zeros(x.shape[:-1] + (3,))
+            q[..., 0] = 1.0 + 0.01 * np.sin(2.0 * np.pi * x[..., 0].astype(np.float64))
+            return q.astype(f32)
+        return (M.ShallowWater(1.0, 1e-6, flux_type=M.FLUX_HLL), P, (N, NY), (1.0, NY / N), (0,) * 4,
+                float(f32(1.0 / steps)), steps, ic, (1.65e-4, 1.75e-4))
+    raise KeyError(name)
+
+
+BENCH = ["adv3d_p2_n16", "adv3d_p3_n12", "adv2d_translation_n32", "euler2d_vortex_p3_hllc", "maxwell_plane_wave_3d",
+         "sw_wave_2d_hll"]
+ORACLE_CHEAP = ["adv3d_p2_n16", "adv2d_translation_n32", "maxwell_plane_wave_3d", "sw_wave_2d_hll"]
+
+
+def _check(name, q, q0):
+    err = rel_l2(q, q0)
+    lo, hi = bench_case(name)[-1]
+    print(f"{name}: rel L2 {err:.4e} (reported {G['reported.' + name + '.rel_l2']:g})", end="")
+    if name == "maxwell_plane_wave_3d":
+        leak = float(np.abs(q[..., [0, 1, 3, 5]]).max())
+        print(f", leakage {leak:.2e} (reported ~4.5e-4)", end="")
+        assert 4.45e-4 <= leak < 4.55e-4, leak
+    print()
+    assert lo <= err < hi, err
+
+
+@pytest.mark.parametrize("name", ORACLE_CHEAP)
+def test_oracle_reproduces_bench_values(oracle_mod, name):
+    ph, P, n, L, bcs, dt, steps, ic, band = bench_case(name)
+    if len(n) == 3:
+        o = oracle_mod.Oracle3D(P, n, L, M.physics_dict(ph), bcs=bcs, real="f32")
+        q0 = ic(o.node_xyz())
+    else:
+        o = oracle_mod.Oracle2D(P, n, L, M.physics_dict(ph), bcs=bcs, real="f32")
+        q0 = ic(o.node_xy())
+    o.set(q0.astype(np.float64))
+    o.step(dt, steps)
+    _check(name, o.get(), q0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", BENCH)
+def test_product_reproduces_bench_values(name):
+    ph, P, n, L, bcs, dt, steps, ic, band = bench_case(name)
+    if len(n) == 3:
+        mesh = M.Mesh(*n, *L, bcs=M.BoundaryConditions(*bcs))
+    else:
+        mesh = M.Mesh(n[0], n[1], 1, L[0], L[1], 1.0, bcs=M.BoundaryConditions(*bcs, 0, 0), dim=2)
+    s = M.Solver(mesh, ph, P=P, precision="f32")
+    q0 = ic(s.node_xyz())
+    s.upload_state(q0.astype(np.float64))
+    s.step_n(dt, steps)
+    q = s.download_state()
+    s.close()
+    _check(name, q, q0)
+
+
+def langmuir_p2():
+    """benchmarks/bench_two_fluid_langmuir_3d.mojo (P2, 8 x 2 x 2, CFL 0.2, dt in Float32)."""
+    nx, ny, nz, lx, ly, lz = G["langmuir_3d_p2.mesh"]
+    ge, gi, qe, me, qi, mi, eps0, c = G["langmuir_3d_p3.species"]
+    n0, pe, pi, a = G["langmuir_3d_p3.n0_pe_pi_upert"]
+    c_h, alpha_d, rho_min, p_min = G["langmuir_3d_p3.c_h_alpha_d_rhomin_pmin"]
+    ph = M.FiveMomentTwoFluid(ge, gi, qe, me, qi, mi, eps0, c, c_h, alpha_d, rho_min, p_min)
+    rho_e, rho_i = me * n0, mi * n0
+    state = [rho_e, rho_e * a, 0.0, 0.0, pe / (ge - 1) + 0.5 * rho_e * a * a,
+             rho_i, 0.0, 0.0, 0.0, pi / (gi - 1)] + [0.0] * 7
+    T = f32(G["langmuir_3d_p3.t_final"])
+    dt_est = f32(0.2) * (f32(lx) / f32(nx)) / (max(f32(c), f32(c_h)) * f32(5.0))
+    steps = int(T / dt_est) + 1
+    wp = np.sqrt(n0 * (qe * qe / me + qi * qi / mi) / eps0)
+
+    def metrics(q):
+        drift = abs(q[..., 1].mean() - a * me * n0) / (a * me * n0)
+        return drift, abs(q[..., 10].mean()) / (a * me * n0 * wp)
+
+    return ph, (int(nx), int(ny), int(nz)), (lx, ly, lz), np.array(state), float(T / f32(steps)), steps, metrics
+
+
+def test_oracle_reproduces_langmuir_p2(oracle_mod):
+    """The reference records 'rho_e u_e drift = 0.035 %, Ex / E_scale = 6e-5'
+    (bench_two_fluid_langmuir_3d.mojo:25).  The oracle keeps the reference's
+    FP32 stage combine a q_a + b q_b, whose third-stage weights sum to
+    1 + 3e-8: over 14787 steps that bias alone is a 0.04 % momentum drift.
+    The oracle lands at 0.043 % (E_x 6.8e-5); the last digit depends on how
+    the FP32 products are fused, so the drift is checked for its size, not
+    its digits.  (The product, with exact weights, drifts 7e-7.)"""
+    ph, n, L, state, dt, steps, metrics = langmuir_p2()
+    o = oracle_mod.Oracle3D(2, n, L, M.physics_dict(ph), real="f32")
+    o.set(np.broadcast_to(state, (o.Ne, o.NP, 17)).copy())
+    o.step(dt, steps)
+    drift, ex = metrics(o.get())
+    print(f"oracle langmuir P2: {steps} steps, drift {100 * drift:.4f} %, Ex {ex:.2e} (reported 0.035 %, 6e-5)")
+    assert 2.5e-4 <= drift < 5e-4, drift
+    assert 5e-5 <= ex < 8e-5, ex
+
+
+@pytest.mark.gpu
+def test_product_reproduces_langmuir_p2():
+    """E_x as reported (6e-5); the momentum drift is gone (the product's stage
+    weights sum to one exactly), so it is bounded instead of matched."""
+    ph, n, L, state, dt, steps, metrics = langmuir_p2()
+    s = M.Solver(M.Mesh(*n, *L), ph, P=2, precision="f32")
+    s.fill_ic(M.IC_CONSTANT, list(state))
+    s.step_n(dt, steps)
+    drift, ex = metrics(s.download_state().astype(np.float64))
+    s.close()
+    print(f"product langmuir P2: {steps} steps, drift {100 * drift:.5f} %, Ex {ex:.2e} (reported 0.035 %, 6e-5)")
+    assert drift < 1e-5, drift
+    assert 5.5e-5 <= ex < 6.5e-5, ex
