@@ -170,6 +170,11 @@ ENTRIES = [
      "Measured values: rho_e u_e drift = 0.035%%, Ex / E_scale = 6e-5"),
     ("langmuir_3d_p2.mesh", [8, 2, 2, 1.0, 0.25, 0.25], "benchmarks/bench_two_fluid_langmuir_3d.mojo", "53-58",
      "comptime LZ = Float64(2.0 / 8.0)"),
+    ("reported.smooth_wave_3d_p3_n12.rel_l2", 5.5e-5, "benchmarks/bench_euler_smooth_wave_3d_p3.mojo", "61",
+     "Measured ~5.5e-5 at N=12 (Float32 floor)"),
+    # gamma, rho0, u, v, w, p0, amplitude, T, CFL (HLLEC, periodic unit cube)
+    ("smooth_wave_3d_p3.config", [1.4, 1.0, 1.0, 1.0, 1.0, 1.0, 0.1, 1.0, 0.1],
+     "benchmarks/bench_euler_smooth_wave_3d_p3.mojo", "49-57", "comptime AMPLITUDE: Float32 = 0.1"),
 ]
 
 

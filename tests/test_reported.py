@@ -452,3 +452,31 @@ def test_product_reproduces_langmuir_p2():
     print(f"product langmuir P2: {steps} steps, drift {100 * drift:.5f} %, Ex {ex:.2e} (reported 0.035 %, 6e-5)")
     assert drift < 1e-5, drift
     assert 5.5e-5 <= ex < 6.5e-5, ex
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f64", "f32", "mixed"])
+def test_smooth_wave_3d_p3_at_or_below_recorded_floor(prec):
+    """benchmarks/bench_euler_smooth_wave_3d_p3.mojo (HLLEC, N=12, one period,
+    IC and dt in Float32) records '~5.5e-5 at N=12 (Float32 floor)'.  That
+    floor is mostly the reference's FP32 stage-weight bias (3e-8 per step
+    over 2453 steps, ~4e-5): the product, whose weights sum to one exactly,
+    sits at the scheme's own error (~1.8e-5) in every precision, a third of
+    the recorded value."""
+    gamma, rho0, u0, v0, w0, p0, amp, T, cfl = G["smooth_wave_3d_p3.config"]
+    P, N = 3, 12
+    wave = np.sqrt(f32(u0) * f32(u0) + f32(v0) * f32(v0) + f32(w0) * f32(w0)) + np.sqrt(f32(gamma) * f32(p0) / f32(rho0))
+    dt_est = f32(cfl) * (f32(1.0) / f32(N)) / (wave * f32(2 * P + 1))
+    steps = int(f32(T) / dt_est) + 1
+    s = M.Solver(M.Mesh(N, N, N), M.Euler(gamma, 1e-6, 1e-6, M.FLUX_HLLEC, False), P=P, precision=prec)
+    x = s.node_xyz().astype(f32)
+    k = f32(2.0) * f32(np.pi)
+    rho = f32(rho0) + f32(amp) * np.sin(k * x[..., 0]) * np.sin(k * x[..., 1]) * np.sin(k * x[..., 2])
+    E = f32(p0) / (f32(gamma) - f32(1.0)) + f32(0.5) * rho * f32(u0 * u0 + v0 * v0 + w0 * w0)
+    q0 = np.stack([rho, rho * f32(u0), rho * f32(v0), rho * f32(w0), E], -1).astype(f32)
+    s.upload_state(q0.astype(np.float64))
+    s.step_n(float(f32(T) / f32(steps)), steps)
+    err = rel_l2(s.download_state(), q0)
+    s.close()
+    print(f"smooth wave P3 N=12 {prec}: {steps} steps, rel L2 {err:.3e} (recorded ~5.5e-5, FP32)")
+    assert err < G["reported.smooth_wave_3d_p3_n12.rel_l2"] / 2, err
