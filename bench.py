@@ -302,7 +302,8 @@ def cpu_baseline(a, seconds):
             break
     dof = o.Ne * o.NP * o.NC
     return dict(value=3 * dof * steps / el, unit=UNIT, cores=os.cpu_count(), kind="port",
-                sample=f"oracle FP64 restatement, {n}^3x6 = {6 * n ** 3} tets P={a.P} Rusanov, {steps} SSPRK3 steps "
+                sample=f"oracle {'FP64' if a.precision == 'f64' else 'FP32'} restatement, {n}^3x6 = {6 * n ** 3} tets "
+                       f"P={a.P} Rusanov, {steps} SSPRK3 steps "
                        f"in {el:.1f} s, OpenMP {os.cpu_count()} threads")
 
 
