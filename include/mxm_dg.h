@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define MXM_DG_VERSION 20000 /* 2.0.0: physics descriptor p[32] (was p[16]) */
+#define MXM_DG_VERSION 20100 /* 2.1.0: z-slab decomposition; 2.0.0: physics descriptor p[32] */
 
 /* Return codes (mpi_shim.c returns the MPI error code; we use negatives). */
 #define MXM_DG_OK 0
@@ -258,6 +258,57 @@ int mxm_dg_selftest_wait_timeout(double limit_ms, int32_t* gave_up, double* wait
 #define MXM_DG_IC_PLANE_WAVE 6
 #define MXM_DG_IC_ALFVEN 7
 int mxm_dg_fill_ic(void* handle, int which, int kind, const double* params, int nparams);
+
+/* ---- z-slab domain decomposition (np > 1) ---------------------------------
+ * Replaces Partition/build_partition (src/partition.mojo:26-228) and
+ * HaloExchange (src/halo_exchange.mojo:187-395): one 3D mesh split into
+ * `nparts` slabs of whole z layers of cubes, part r owning global layers
+ * [r*Nz/nparts, (r+1)*Nz/nparts).  A part's state buffers hold its owned
+ * layers between one ghost layer below and one above (where a neighbouring
+ * part exists: z periodic, or not the first/last part); the ghost layers are
+ * refilled from the neighbours before every stage, and before the limiter.
+ * Owned results are bit-identical to the undecomposed solve.  The z
+ * boundaries must be both periodic or both bounded.  Reductions,
+ * max_wavespeed and download_component cover the owned elements only (sum
+ * or max them over the parts for the global value); node coordinates and
+ * fill_ic use global positions. */
+/* Host-only plan of part `part`: out8 = {cz0, cz1 (owned global z layers),
+ * ghost_lo, ghost_hi (0/1), local bc_z_lo, local bc_z_hi, lo neighbour part,
+ * hi neighbour part (-1 = none)}.  Needs no GPU. */
+int mxm_dg_slab_plan(int nz, int bc_z_lo, int bc_z_hi, int nparts, int part, int32_t* out8);
+/* As mxm_dg_create, for part `part` of an nparts-slab decomposition of the
+ * global mesh `mesh` (nparts = 1: a plain handle). */
+int mxm_dg_create_slab(const mxm_dg_mesh_desc* mesh, const mxm_dg_physics_desc* phys, int P, int precision,
+                       int nparts, int part, void** handle);
+/* out8 = {nparts, part, cz0, cz1, ghost_lo, ghost_hi, first owned element,
+ * owned element count}. */
+int mxm_dg_slab_info(void* handle, int64_t* out8);
+/* For a caller-driven exchange: out5 = {values per z layer, offset of the
+ * bottom owned layer, of the top owned layer, of the ghost layer below, of
+ * the ghost layer above (-1 = none)}, offsets in values from the start of a
+ * state buffer.  Ghost below <- the lo neighbour's top owned layer; ghost
+ * above <- the hi neighbour's bottom owned layer. */
+int mxm_dg_slab_layout(void* handle, int64_t* out5);
+/* Stage kernel of Shu-Osher stage s over the owned cells only (no exchange,
+ * no limiter; the caller refills the ghost layers of the stage's input
+ * first and runs mxm_dg_limit on its output after refilling those). */
+int mxm_dg_slab_stage(void* handle, int s, double dt);
+/* Multi-process transport: rank 0 makes a 128-byte NCCL id and sends it to
+ * every part (MPI_Bcast or any other channel); each part then connects
+ * (collective: all parts call it) and afterwards steps by itself
+ * (mxm_dg_step_ssprk3 / step_n / rk_stage exchange over NCCL point-to-point
+ * on the handle's stream).  NCCL is loaded at run time (libnccl.so.2). */
+int mxm_dg_nccl_unique_id(unsigned char* id128);
+int mxm_dg_slab_connect_nccl(void* handle, const unsigned char* id128);
+/* In-process transport: the parts 0..n-1 (on one or several devices of this
+ * process) stepped in lock-step by one host thread; ghost layers are copied
+ * with cudaMemcpyPeerAsync, ordered by events.  The group does not own the
+ * handles; destroy it before them. */
+int mxm_dg_group_create(void* const* handles, int n, void** group);
+int mxm_dg_group_step_n(void* group, double dt, int nsteps);
+int mxm_dg_group_synchronize(void* group);
+int mxm_dg_group_last_error(void* group, char* buf, int len);
+int mxm_dg_group_destroy(void* group);
 
 /* ---- batched engine (no reference counterpart: the reference runs each
  * 2D solve through its own driver loop, examples/euler_sod_2d_gpu.mojo +

@@ -35,6 +35,9 @@ BC_INTERIOR, BC_WALL, BC_OUTFLOW, BC_INFLOW = 0, 1, 2, 3
 PREC = {"f64": 0, "f32": 1, "mixed": 2}
 
 EXPORTED = [
+    "mxm_dg_slab_plan", "mxm_dg_create_slab", "mxm_dg_slab_info", "mxm_dg_slab_layout", "mxm_dg_slab_stage",
+    "mxm_dg_nccl_unique_id", "mxm_dg_slab_connect_nccl", "mxm_dg_group_create", "mxm_dg_group_step_n",
+    "mxm_dg_group_synchronize", "mxm_dg_group_last_error", "mxm_dg_group_destroy",
     "mxm_dg_version", "mxm_dg_create", "mxm_dg_destroy", "mxm_dg_sizes", "mxm_dg_dof_count",
     "mxm_dg_state_bytes_per_step", "mxm_dg_state_ptr", "mxm_dg_node_xyz_ptr", "mxm_dg_node_xyz",
     "mxm_dg_upload_state", "mxm_dg_download_state", "mxm_dg_download_component", "mxm_dg_download_component_f64",
@@ -137,6 +140,19 @@ def lib():
         L.mxm_dg_server_wait.argtypes = [vp, ctypes.c_int64, ctypes.c_double, dp]
         L.mxm_dg_server_stats.argtypes = [vp, dp, ctypes.c_int]
         L.mxm_dg_server_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+        L.mxm_dg_slab_plan.argtypes = [ctypes.c_int] * 5 + [i32p]
+        L.mxm_dg_create_slab.argtypes = [ctypes.POINTER(_MeshDesc), ctypes.POINTER(_PhysDesc), ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.mxm_dg_slab_info.argtypes = [vp, i64p]
+        L.mxm_dg_slab_layout.argtypes = [vp, i64p]
+        L.mxm_dg_slab_stage.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+        L.mxm_dg_nccl_unique_id.argtypes = [ctypes.c_char_p]
+        L.mxm_dg_slab_connect_nccl.argtypes = [vp, ctypes.c_char_p]
+        L.mxm_dg_group_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.mxm_dg_group_step_n.argtypes = [vp, ctypes.c_double, ctypes.c_int]
+        L.mxm_dg_group_synchronize.argtypes = [vp]
+        L.mxm_dg_group_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+        L.mxm_dg_group_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -358,7 +374,9 @@ class Mesh:
 class Solver:
     """Solver[PhysT, P] over the C ABI: device state q/q1/q2, SSPRK3, limiter."""
 
-    def __init__(self, mesh: Mesh, physics, P: int = 2, precision: str = "f64"):
+    def __init__(self, mesh: Mesh, physics, P: int = 2, precision: str = "f64", nparts: int = 1, part: int = 0):
+        """`nparts` > 1: part `part` of a z-slab decomposition of `mesh` (3D), the
+        reference's per-rank Solver over build_partition (src/partition.mojo:162)."""
         L = lib()
         pd = _PhysDesc()
         pd.kind, pd.flux_type, pd.entropy_fix = physics.kind, physics.flux_type, int(physics.entropy_fix)
@@ -366,7 +384,11 @@ class Solver:
             pd.p[k] = v
         md = mesh.desc()
         h = ctypes.c_void_p()
-        _check(L.mxm_dg_create(ctypes.byref(md), ctypes.byref(pd), P, PREC[precision], ctypes.byref(h)))
+        if nparts == 1:
+            _check(L.mxm_dg_create(ctypes.byref(md), ctypes.byref(pd), P, PREC[precision], ctypes.byref(h)))
+        else:
+            _check(L.mxm_dg_create_slab(ctypes.byref(md), ctypes.byref(pd), P, PREC[precision], nparts, part,
+                                        ctypes.byref(h)))
         self.h = h
         self.mesh, self.physics, self.P, self.precision = mesh, physics, P, precision
         ne, np_, nfp, nc, rb = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
@@ -375,6 +397,10 @@ class Solver:
         self.num_elements, self.NP, self.NFP, self.NC = ne.value, np_.value, nfp.value, nc.value
         self.dtype = np.float64 if rb.value == 8 else np.float32
         self.shape = (self.num_elements, self.NP, self.NC)
+        info = (ctypes.c_int64 * 8)()
+        _check(L.mxm_dg_slab_info(h, info), h)
+        self.nparts, self.part, cz0, cz1, glo, ghi, self.owned_e0, self.owned_ne = list(info)
+        self.owned_layers, self.ghosts = (cz0, cz1), (glo, ghi)
 
     def close(self):
         if getattr(self, "h", None):
@@ -426,7 +452,7 @@ class Solver:
         return out
 
     def download_owned_component(self, c):  # solver.mojo:711-729 (Float32 as the reference)
-        out = np.empty(self.num_elements * self.NP, dtype=np.float32)
+        out = np.empty(self.owned_ne * self.NP, dtype=np.float32)
         self._c(lib().mxm_dg_download_component(self.h, c, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return out
 
@@ -460,6 +486,22 @@ class Solver:
 
     def synchronize(self):
         self._c(lib().mxm_dg_synchronize(self.h))
+
+    # -- z-slab decomposition
+    def slab_layout(self):
+        """{values per z layer, offsets of the bottom/top owned and lower/upper
+        ghost layers in a state buffer (-1 = none)}."""
+        out = (ctypes.c_int64 * 5)()
+        self._c(lib().mxm_dg_slab_layout(self.h, out))
+        return dict(zip(("layer", "owned_lo", "owned_hi", "ghost_lo", "ghost_hi"), list(out)))
+
+    def slab_stage(self, stage, dt):
+        """Stage kernel over the owned cells, without exchange or limiter."""
+        self._c(lib().mxm_dg_slab_stage(self.h, stage, dt))
+
+    def connect_nccl(self, unique_id: bytes):
+        """Join the parts' NCCL communicator (collective over all parts)."""
+        self._c(lib().mxm_dg_slab_connect_nccl(self.h, unique_id))
 
     # -- diagnostics
     def max_wavespeed(self):
@@ -508,6 +550,48 @@ class Solver:
         out = np.zeros(n.value)
         self._c(lib().mxm_dg_operator(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(n)))
         return out
+
+
+def nccl_unique_id() -> bytes:
+    """128-byte NCCL id for mxm_dg_slab_connect_nccl (made on one part, sent to all)."""
+    buf = ctypes.create_string_buffer(128)
+    _check(lib().mxm_dg_nccl_unique_id(buf))
+    return buf.raw
+
+
+class SlabGroup:
+    """Parts 0..n-1 of one slab decomposition stepped in lock-step from this
+    process (mxm_dg_group_*): ghost layers by cudaMemcpyPeerAsync."""
+
+    def __init__(self, parts):
+        self.parts = list(parts)
+        arr = (ctypes.c_void_p * len(self.parts))(*[p.h.value for p in self.parts])
+        g = ctypes.c_void_p()
+        _check(lib().mxm_dg_group_create(arr, len(self.parts), ctypes.byref(g)))
+        self.g = g
+
+    def _c(self, rc):
+        if rc != 0:
+            buf = ctypes.create_string_buffer(512)
+            lib().mxm_dg_group_last_error(self.g, buf, 512)
+            raise DGError(rc, buf.value.decode())
+
+    def step_n(self, dt, nsteps):
+        self._c(lib().mxm_dg_group_step_n(self.g, dt, nsteps))
+
+    def synchronize(self):
+        self._c(lib().mxm_dg_group_synchronize(self.g))
+
+    def close(self):
+        if getattr(self, "g", None):
+            lib().mxm_dg_group_destroy(self.g)
+            self.g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class DiagComponents:  # src/diagnostics.mojo:73-94

@@ -197,7 +197,8 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
     ar.nx = h->nx;
     ar.ny = h->ny;
     ar.nz = h->nz;
-    ar.ncell = int(h->ncell);
+    ar.cbeg = int(h->cbeg);
+    ar.ncell = int(h->cend);
     for (int k = 0; k < 6; ++k) ar.bc[k] = h->bc[k];
     ar.rhs_only = rhs_only;
     ar.err = h->derr;
@@ -316,7 +317,8 @@ cudaError_t wavespeed_launch(Handle* h, const void* qi, unsigned long long* out)
     ar.nx = h->nx;
     ar.ny = h->ny;
     ar.nz = h->nz;
-    ar.ncell = int(h->ncell);
+    ar.cbeg = int(h->cbeg);
+    ar.ncell = int(h->cend);
     for (int k = 0; k < 6; ++k) ar.bc[k] = h->bc[k];
     const KuhnTab3<R>& t = tab3<R>(h);
     switch (h->phys.kind) {
@@ -402,6 +404,8 @@ void limit_buf(Handle* h, void* qv) {
     a.avg = (double*)h->avg;
     a.w = (const double*)h->w;
     a.ne = h->ne;
+    a.e0 = h->own_e0();
+    a.e1 = h->own_e0() + h->own_ne();
     a.nx = h->nx; a.ny = h->ny; a.nz = h->dim == 3 ? h->nz : 1;
     for (int k = 0; k < 6; ++k) a.bc[k] = h->bc[k];
     a.eps2 = h->lim_eps * h->lim_eps;
@@ -412,6 +416,8 @@ void limit_buf(Handle* h, void* qv) {
     a.avg = (float*)h->avg;
     a.w = (const float*)h->w;
     a.ne = h->ne;
+    a.e0 = h->own_e0();
+    a.e1 = h->own_e0() + h->own_ne();
     a.nx = h->nx; a.ny = h->ny; a.nz = h->dim == 3 ? h->nz : 1;
     for (int k = 0; k < 6; ++k) a.bc[k] = h->bc[k];
     const float ef = float(h->lim_eps);  // reference: venkat_eps Float32, eps2 = eps*eps in Float32
@@ -421,13 +427,34 @@ void limit_buf(Handle* h, void* qv) {
   if (e != cudaSuccess) throw CudaError(e, "limiter launch");
 }
 
-// Shu-Osher stage s of SSPRK3 (solver.mojo:1071-1092; ssprk3.mojo:56-78).
-void rk_stage(Handle* h, int s, double dt) {
+// Shu-Osher stage s of SSPRK3 (solver.mojo:1071-1092; ssprk3.mojo:56-78):
+// reads q, q1, q2 and writes q1, q2, q.
+int stage_in(int s) { return s; }
+int stage_out(int s) { return s == 0 ? 1 : (s == 1 ? 2 : 0); }
+void stage_only(Handle* h, int s, double dt) {
   void *q0 = h->q[0], *q1 = h->q[1], *q2 = h->q[2];
   if (s == 0) stage(h, q0, q0, q0, q1, 0.0, 1.0, dt, 0);
   else if (s == 1) stage(h, q1, q0, q1, q2, 0.25, 0.25, dt, 0);
   else stage(h, q2, q0, q2, q0, 2.0 / 3.0, 2.0 / 3.0, dt, 0);
-  if (h->lim_on) limit_buf(h, s == 0 ? q1 : (s == 1 ? q2 : q0));
+}
+
+// A slab part exchanges the ghost layers of the stage's input first and,
+// with the limiter on, those of its output before the limiter (its cell
+// means reach into the ghost layers), as the reference exchanges once per
+// stage before its kernel (src/solver.mojo:1038-1068).
+void rk_stage(Handle* h, int s, double dt) {
+  const bool halo = h->glo || h->ghi;
+  if (halo) {
+    if (!h->nccl)
+      throw ArgError("a slab part with ghost layers steps through mxm_dg_group_step_n, or by itself after "
+                     "mxm_dg_slab_connect_nccl");
+    nccl_exchange(h, stage_in(s));
+  }
+  stage_only(h, s, dt);
+  if (h->lim_on) {
+    if (halo) nccl_exchange(h, stage_out(s));
+    limit_buf(h, h->q[stage_out(s)]);
+  }
 }
 
 // 2D GLM-MHD: psi *= exp(-alpha_d dt) once per SSPRK3 step, operator-split
@@ -459,10 +486,12 @@ void step_n(Handle* h, double dt, int n) {
 double reduce_scale(const Handle* h, int kind) {
   if (kind == 2) return 1.0;
   if (kind >= 3) {
+    // global domain and element count: a slab part's sum is its share
     const double dom = h->dim == 3 ? h->lx * h->ly * h->lz : h->lx * h->ly;
-    return dom / (double(h->ne) * h->NP);
+    const double ne_glob = double(h->nx) * h->ny * (h->dim == 3 ? h->nzg : 1) * h->ntypes;
+    return dom / (ne_glob * h->NP);
   }
-  return h->dim == 3 ? (h->lx / h->nx) * (h->ly / h->ny) * (h->lz / h->nz) / 6.0 : (h->lx / h->nx) * (h->ly / h->ny) / 2.0;
+  return h->dim == 3 ? (h->lx / h->nx) * (h->ly / h->ny) * h->hz() / 6.0 : (h->lx / h->nx) * (h->ly / h->ny) / 2.0;
 }
 
 // Float32 node coordinates exactly as the reference builds elem_node_xyz.
@@ -470,7 +499,7 @@ void build_xyz(Handle* h) {
   std::vector<float> x(size_t(h->ne) * h->NP * h->dim);
   if (h->dim == 3) {
     // local_mesh.mojo:568-580 (rel coords in Float32) and :814-827
-    const float dx = float(h->lx / h->nx), dy = float(h->ly / h->ny), dz = float(h->lz / h->nz);
+    const float dx = float(h->lx / h->nx), dy = float(h->ly / h->ny), dz = float(h->hz());
     const float Pf = float(h->P);
     std::vector<float> rel(6 * h->NP * 3);
     for (int t = 0; t < 6; ++t)
@@ -483,8 +512,8 @@ void build_xyz(Handle* h) {
     for (int64_t e = 0; e < h->ne; ++e) {
       const int t = int(e % 6);
       const int64_t cell = e / 6;
-      const int k = int(cell / (int64_t(h->nx) * h->ny));
-      const int64_t rem = cell - int64_t(k) * h->nx * h->ny;
+      const int kl = int(cell / (int64_t(h->nx) * h->ny)), k = kl + h->kz0;
+      const int64_t rem = cell - int64_t(kl) * h->nx * h->ny;
       const int j = int(rem / h->nx), i = int(rem - int64_t(j) * h->nx);
       const float o[3] = {float(i) * dx, float(j) * dy, float(k) * dz}, hh[3] = {dx, dy, dz};
       for (int n = 0; n < h->NP; ++n)
@@ -541,7 +570,8 @@ void fill_ic(Handle* h, int which, int kind, const double* params, int nparams) 
   a.kind = kind;
   a.h[0] = h->lx / h->nx;
   a.h[1] = h->ly / h->ny;
-  a.h[2] = h->lz / h->nz;
+  a.h[2] = h->hz();
+  a.kz0 = h->kz0;
   a.L[0] = h->lx;
   a.L[1] = h->ly;
   a.L[2] = h->lz;
@@ -572,11 +602,13 @@ void destroy(Handle* h) {
   cudaFree(h->uscalar);
   cudaFree(h->derr);
   cudaFree(h->tcimg);
+  if (h->nccl) nccl_release(h);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
 
-Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, int prec) {
+Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, int prec, const SlabPlan* slab,
+               int nparts, int part) {
   if (!m || !ph) throw ArgError("null descriptor");
   if (m->dim != 2 && m->dim != 3) throw ArgError("mesh dim must be 2 or 3");
   if (P < 1 || P > 5) throw ArgError("order P must be in 1..5");
@@ -604,10 +636,23 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   h->nx = m->nx;
   h->ny = m->ny;
   h->nz = m->dim == 3 ? m->nz : 1;
+  h->nzg = h->nz;
   h->lx = m->lx;
   h->ly = m->ly;
   h->lz = m->lz;
   for (int k = 0; k < 2 * m->dim; ++k) h->bc[k] = m->bc[k];
+  if (slab) {  // local z layers: [ghost lo] owned [ghost hi]
+    h->nparts = nparts;
+    h->part = part;
+    h->glo = slab->glo;
+    h->ghi = slab->ghi;
+    h->nb_lo = slab->nb_lo;
+    h->nb_hi = slab->nb_hi;
+    h->nz = slab->cz1 - slab->cz0 + slab->glo + slab->ghi;
+    h->kz0 = slab->cz0 - slab->glo;
+    h->bc[4] = slab->bc_lo;
+    h->bc[5] = slab->bc_hi;
+  }
   h->NC = ph->kind == MXM_DG_PHYS_ADVECTION ? 1
         : ph->kind == MXM_DG_PHYS_EULER     ? (m->dim == 3 ? 5 : 4)
         : ph->kind == MXM_DG_PHYS_MAXWELL   ? 6
@@ -618,6 +663,8 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   h->ntypes = m->dim == 3 ? 6 : 2;
   h->ncell = int64_t(h->nx) * h->ny * h->nz;
   h->ne = h->ncell * h->ntypes;
+  h->cbeg = int64_t(h->nx) * h->ny * h->glo;
+  h->cend = h->ncell - int64_t(h->nx) * h->ny * h->ghi;
   if (h->ne > (int64_t(1) << 31) / 64) throw ArgError("mesh too large for 32-bit cell indexing");
   h->rbytes = prec == MXM_DG_PREC_F64 ? 8 : 4;
   // split-BF16 tensor-core contraction for the 3D orders it is built for
@@ -629,7 +676,7 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   h->NP = h->ref.NP;
   h->NFP = h->ref.NFP;
   if (h->dim == 3) {
-    h->k3 = build_kuhn3d(h->ref, h->lx / h->nx, h->ly / h->ny, h->lz / h->nz);
+    h->k3 = build_kuhn3d(h->ref, h->lx / h->nx, h->ly / h->ny, h->hz());
     h->Ahost = shared_operator(h->ref);
     h->K = 3 * h->NP + 4 * h->NFP;
     fill_tab3<double>(h.get(), h->t3d);
@@ -777,12 +824,12 @@ int mxm_dg_node_xyz(void* handle, double* out) {
   API_BEGIN
   const int dim = h->dim, NP = h->NP;
   if (dim == 3) {
-    const double hh[3] = {h->lx / h->nx, h->ly / h->ny, h->lz / h->nz};
+    const double hh[3] = {h->lx / h->nx, h->ly / h->ny, h->hz()};
     for (int64_t e = 0; e < h->ne; ++e) {
       const int t = int(e % 6);
       const int64_t cell = e / 6;
-      const int k = int(cell / (int64_t(h->nx) * h->ny));
-      const int64_t rem = cell - int64_t(k) * h->nx * h->ny;
+      const int kl = int(cell / (int64_t(h->nx) * h->ny)), k = kl + h->kz0;
+      const int64_t rem = cell - int64_t(kl) * h->nx * h->ny;
       const int j = int(rem / h->nx), i = int(rem - int64_t(j) * h->nx);
       const int c[3] = {i, j, k};
       for (int n = 0; n < NP; ++n)
@@ -832,9 +879,10 @@ static void download_component(Handle* h, int c, float* f32, double* f64) {
   std::vector<unsigned char> buf(h->qbytes());
   CK(cudaMemcpyAsync(buf.data(), h->q[0], h->qbytes(), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  const size_t nn = size_t(h->ne) * h->NP;
+  const size_t nn = size_t(h->own_ne()) * h->NP, n0 = size_t(h->own_e0()) * h->NP;  // owned elements
   for (size_t k = 0; k < nn; ++k) {
-    const double v = h->rbytes == 8 ? ((const double*)buf.data())[k * h->NC + c] : ((const float*)buf.data())[k * h->NC + c];
+    const size_t at = (n0 + k) * h->NC + c;
+    const double v = h->rbytes == 8 ? ((const double*)buf.data())[at] : ((const float*)buf.data())[at];
     if (f32) f32[k] = float(v);
     if (f64) f64[k] = v;
   }
@@ -928,11 +976,14 @@ int mxm_dg_reduce_conserved(void* handle, int which, int c, int kind, double* ou
   if (which < 0 || which > 2 || c < 0 || c >= h->NC || kind < 0 || kind > 4)
     throw mxm::ArgError("which 0..2, component in range, kind 0..4");
   const double scale = mxm::reduce_scale(h, kind);
+  const size_t off = size_t(h->own_e0()) * h->NP * h->NC;  // owned elements only
   cudaError_t e = h->rbytes == 8
-                      ? mxm::launch_reduce<double>(h->P, h->dim, h->NC, (const double*)h->q[which], (const double*)h->w,
-                                                   h->ne, c, kind, scale, h->partial, h->npartial, h->dscalar, h->stream)
-                      : mxm::launch_reduce<float>(h->P, h->dim, h->NC, (const float*)h->q[which], (const float*)h->w,
-                                                  h->ne, c, kind, scale, h->partial, h->npartial, h->dscalar, h->stream);
+                      ? mxm::launch_reduce<double>(h->P, h->dim, h->NC, (const double*)h->q[which] + off,
+                                                   (const double*)h->w, h->own_ne(), c, kind, scale, h->partial,
+                                                   h->npartial, h->dscalar, h->stream)
+                      : mxm::launch_reduce<float>(h->P, h->dim, h->NC, (const float*)h->q[which] + off,
+                                                  (const float*)h->w, h->own_ne(), c, kind, scale, h->partial,
+                                                  h->npartial, h->dscalar, h->stream);
   if (e != cudaSuccess) throw mxm::CudaError(e, "reduction launch");
   CK(cudaMemcpyAsync(out, h->dscalar, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
@@ -973,15 +1024,18 @@ int mxm_dg_reduce_conserved_noalloc(void* handle, int which, int c, int kind, in
     }
     scratch = g_static_scratch[h->device];
   }
-  const int64_t want = (h->ne + 255) / 256;
+  const int64_t want = (h->own_ne() + 255) / 256;
   const int nb = nblocks > 0 ? nblocks : int(want < h->npartial ? want : h->npartial);
   const double scale = mxm::reduce_scale(h, kind);
   double* result = scratch + mxm::kStaticPartials;
+  const size_t off = size_t(h->own_e0()) * h->NP * h->NC;
   cudaError_t e = h->rbytes == 8
-                      ? mxm::launch_reduce<double>(h->P, h->dim, h->NC, (const double*)h->q[which], (const double*)h->w,
-                                                   h->ne, c, kind, scale, scratch, nb, result, h->stream)
-                      : mxm::launch_reduce<float>(h->P, h->dim, h->NC, (const float*)h->q[which], (const float*)h->w,
-                                                  h->ne, c, kind, scale, scratch, nb, result, h->stream);
+                      ? mxm::launch_reduce<double>(h->P, h->dim, h->NC, (const double*)h->q[which] + off,
+                                                   (const double*)h->w, h->own_ne(), c, kind, scale, scratch, nb,
+                                                   result, h->stream)
+                      : mxm::launch_reduce<float>(h->P, h->dim, h->NC, (const float*)h->q[which] + off,
+                                                  (const float*)h->w, h->own_ne(), c, kind, scale, scratch, nb,
+                                                  result, h->stream);
   if (e != cudaSuccess) throw mxm::CudaError(e, "reduction launch");
   CK(cudaMemcpyAsync(out, result, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));

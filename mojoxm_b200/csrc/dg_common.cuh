@@ -166,7 +166,9 @@ struct Stage3DArgs {
   // step); cdt = c dt is rounded once from FP64.
   R b, cdt;
   int nx, ny, nz;
-  int ncell;
+  // cells cbeg .. ncell-1 are computed (all cells, or the owned layers of a
+  // z-slab whose ghost layers are filled by the halo exchange)
+  int cbeg, ncell;
   int bc[6];
   int rhs_only;
   int* err;  // device error word (bounded waits that gave up set bit 0)
@@ -196,7 +198,8 @@ struct LimArgs {
   R* q;
   R* avg;          // [Ne][NC]
   const R* w;      // [NP] node weights
-  int64_t ne;
+  int64_t ne;      // cell means over elements 0 .. ne-1
+  int64_t e0, e1;  // theta and its application over elements e0 .. e1-1 (3D)
   int nx, ny, nz;  // cells (nz = 1 in 2D)
   int bc[6];
   R eps2;

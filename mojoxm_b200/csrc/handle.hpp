@@ -38,6 +38,14 @@ struct Handle {
   double lx = 1, ly = 1, lz = 1;
   int bc[6] = {0, 0, 0, 0, 0, 0};
   int64_t ncell = 0, ne = 0;
+  // z-slab decomposition (mxm_dg_create_slab): the local z layers are
+  // [ghost lo] owned layers [ghost hi]; cells cbeg .. cend-1 are owned and
+  // computed, the ghost layers are filled by the halo exchange.  A plain
+  // handle is one part with no ghosts (cbeg = 0, cend = ncell).
+  int nparts = 1, part = 0, glo = 0, ghi = 0, nb_lo = -1, nb_hi = -1;
+  int nzg = 1, kz0 = 0;  // global z cells; global z index of local layer 0
+  int64_t cbeg = 0, cend = 0;
+  struct NcclLink* nccl = nullptr;  // halo transport of a multi-process slab
   size_t rbytes = 8;
   int device = 0, nsm = 148;
   cudaStream_t stream = nullptr;
@@ -65,6 +73,9 @@ struct Handle {
   KuhnTab2<float> t2f{};
   std::string err;
   size_t qcount() const { return size_t(ne) * NP * NC; }
+  int64_t own_e0() const { return cbeg * ntypes; }
+  int64_t own_ne() const { return (cend - cbeg) * ntypes; }
+  double hz() const { return lz / nzg; }  // cell size along z (global)
   size_t qbytes() const { return qcount() * rbytes; }
 };
 
@@ -74,9 +85,27 @@ extern std::string g_create_err;
 
 // Solver operations shared by the C ABI, the batch and the server (capi.cu);
 // they throw CudaError / ArgError.
-Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, int prec);
+// One part of a z-slab decomposition: global z cells [cz0, cz1) owned, ghost
+// layers below/above (glo, ghi) and the local BC codes of the z faces.
+struct SlabPlan {
+  int cz0, cz1, glo, ghi, bc_lo, bc_hi, nb_lo, nb_hi;
+};
+SlabPlan slab_plan(int nz, int bc_lo, int bc_hi, int nparts, int part);
+
+Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, int prec,
+               const SlabPlan* slab = nullptr, int nparts = 1, int part = 0);
 void destroy(Handle* h);
 void step_n(Handle* h, double dt, int n);
+// stage kernel of Shu-Osher stage s without exchange or limiter, and the
+// buffers it reads and writes
+void stage_only(Handle* h, int s, double dt);
+int stage_in(int s);
+int stage_out(int s);
+void limit_buf(Handle* h, void* qv);
+// NCCL halo transport (slab.cu): exchange the ghost layers of state buffer
+// `which` on the handle's stream; release the link
+void nccl_exchange(Handle* h, int which);
+void nccl_release(Handle* h);
 void fill_ic(Handle* h, int which, int kind, const double* params, int nparams);
 // 2D GLM-MHD psi damping after each step: whether h has it, and its factor
 bool glm_damped(const Handle* h);

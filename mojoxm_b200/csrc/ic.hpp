@@ -10,6 +10,7 @@ constexpr int kMaxIcNC = 17;  // components of the widest physics (two-fluid)
 struct IcArgs {
   int64_t ne;
   int dim, P, NP, NC, nx, ny, nz, kind;
+  int kz0;                  // global z index of local layer 0 (slab parts)
   double h[3], L[3];
   double prm[32];
   double gamma, c;          // Euler gamma, Maxwell wave speed (from the physics)

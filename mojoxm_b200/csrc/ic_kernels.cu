@@ -29,8 +29,9 @@ __global__ void ic_kernel(IcArgs a, R* q) {
   int ci, cj, ck = 0;
   if (a.dim == 3) {
     const int64_t nxy = int64_t(a.nx) * a.ny;
-    ck = int(cell / nxy);
-    const int64_t rem = cell - int64_t(ck) * nxy;
+    const int kl = int(cell / nxy);
+    ck = kl + a.kz0;
+    const int64_t rem = cell - int64_t(kl) * nxy;
     cj = int(rem / a.nx);
     ci = int(rem - int64_t(cj) * a.nx);
   } else {

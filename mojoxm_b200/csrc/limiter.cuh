@@ -37,11 +37,11 @@ __global__ void __launch_bounds__(32 * EPB) theta_apply_kernel(LimArgs<R> a, Kuh
   constexpr int NTYPE = DIM == 3 ? 6 : 2, NFACE = DIM + 1, VALS = NP * NC;
   __shared__ R sq[EPB][VALS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t e = int64_t(blockIdx.x) * EPB + warp;
-  const bool valid = e < a.ne;
+  const int64_t eb = a.e0 + int64_t(blockIdx.x) * EPB, e = eb + warp;
+  const bool valid = e < a.e1;
   // contiguous block load of the EPB elements
-  const int64_t base = int64_t(blockIdx.x) * EPB * VALS;
-  const int64_t nvals = (a.ne - int64_t(blockIdx.x) * EPB) * VALS;
+  const int64_t base = eb * VALS;
+  const int64_t nvals = (a.e1 - eb) * VALS;
   for (int idx = threadIdx.x; idx < EPB * VALS; idx += 32 * EPB)
     if (idx < nvals) (&sq[0][0])[idx] = a.q[base + idx];
   __syncthreads();

@@ -35,7 +35,8 @@ cudaError_t lim_np(const LimArgs<R>& a, const KuhnTab3<R>& t3, const KuhnTab2<R>
     // elements per block: their staged states stay within 40 KB of static shared memory
     constexpr size_t kElem = sizeof(R) * NP * NC;
     constexpr int EPB = kElem * 8 <= 40960 ? 8 : (kElem * 4 <= 40960 ? 4 : 2);
-    theta_apply_kernel<R, DIM, NP, NC, EPB><<<int((a.ne + EPB - 1) / EPB), 32 * EPB, 0, st>>>(a, t3, t2);
+    if (a.e1 > a.e0)
+      theta_apply_kernel<R, DIM, NP, NC, EPB><<<int((a.e1 - a.e0 + EPB - 1) / EPB), 32 * EPB, 0, st>>>(a, t3, t2);
   }
   return cudaGetLastError();
 }

@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
   const R* Aop = ASMEM ? sA : args.A;
 
   const int tid = threadIdx.x;
-  const int ngroups = (args.ncell + EC - 1) / EC;
+  const int ngroups = (args.ncell - args.cbeg + EC - 1) / EC;
   if (tid == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
   __syncthreads();
 
   auto issue = [&](int grp, int buf) {
-    const int c0 = grp * EC, nc = min(EC, args.ncell - c0);
+    const int c0 = args.cbeg + grp * EC, nc = min(EC, args.ncell - c0);
     const uint32_t bytes = uint32_t(nc) * 6u * NP * NC * sizeof(R);
     fence_proxy_async();
     mbar_arrive_expect_tx(&bar[buf], bytes);
@@ -86,8 +86,9 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
   // (whole tiles of the usual shapes; a partial last tile may take plain loads)
   auto tile_bulk = [&](int g) -> bool {
     const size_t per_cube = size_t(6) * NP * NC * sizeof(R);
-    const size_t start = reinterpret_cast<uintptr_t>(args.q_in) + size_t(g) * EC * per_cube;
-    const size_t bytes = size_t(min(EC, args.ncell - g * EC)) * per_cube;
+    const int cg = args.cbeg + g * EC;
+    const size_t start = reinterpret_cast<uintptr_t>(args.q_in) + size_t(cg) * per_cube;
+    const size_t bytes = size_t(min(EC, args.ncell - cg)) * per_cube;
     return start % 16 == 0 && bytes % 16 == 0;
   };
   uint32_t par = 0u;  // bit b: phase parity of tile buffer b
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
 
   const int nwork = tab->n_face_work;
   for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x, buf ^= 1) {
-    const int cell0 = grp * EC;
+    const int cell0 = args.cbeg + grp * EC;
     const int nhere = min(EC, args.ncell - cell0);
     const int ne_here = 6 * nhere;
     R* q = sQ + buf * QV;
@@ -262,9 +263,9 @@ __global__ void wavespeed3d_kernel(Stage3DArgs<R> args, KuhnTab3<R> tab, Phys ph
   constexpr int NC = Phys::NC, NP = ntet(P), NFP = ntri(P);
   const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double best = 0.0;
-  if (tid < int64_t(args.ncell) * 6 * 4 * NFP) {
-    const int64_t e = tid / (4 * NFP);
-    const int fm = int(tid - e * 4 * NFP), lf = fm / NFP, m = fm - lf * NFP;
+  if (tid < int64_t(args.ncell - args.cbeg) * 6 * 4 * NFP) {
+    const int64_t el = tid / (4 * NFP), e = int64_t(args.cbeg) * 6 + el;
+    const int fm = int(tid - el * 4 * NFP), lf = fm / NFP, m = fm - lf * NFP;
     const int t = int(e % 6);
     const int cell = int(e / 6), nxy = args.nx * args.ny;
     const int ck = cell / nxy, rem = cell - ck * nxy, cj = rem / args.nx, ci = rem - cj * args.nx;

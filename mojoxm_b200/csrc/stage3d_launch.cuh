@@ -46,7 +46,7 @@ cudaError_t launch3_p(const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phy
     cudaError_t e = persistent_blocks_per_sm((const void*)kern, C::NT, C::kSmem, &bps);
     if (e != cudaSuccess) return e;
   }
-  const int ngroups = (a.ncell + C::EC - 1) / C::EC;
+  const int ngroups = (a.ncell - a.cbeg + C::EC - 1) / C::EC;
   int nblk = nsm * bps;
   if (nblk > ngroups) nblk = ngroups;
   if (nblk < 1) nblk = 1;
@@ -71,7 +71,7 @@ cudaError_t launch_stage3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& ta
 template <class R, class Phys>
 cudaError_t launch_wavespeed3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phys& ph,
                                unsigned long long* out, cudaStream_t st) {
-  const int64_t n = int64_t(a.ncell) * 6 * 4 * ntri(P);
+  const int64_t n = int64_t(a.ncell - a.cbeg) * 6 * 4 * ntri(P);
   const int nb = int((n + 255) / 256);
   switch (P) {
     case 1: wavespeed3d_kernel<R, Phys, 1><<<nb, 256, 0, st>>>(a, tab, ph, out); break;

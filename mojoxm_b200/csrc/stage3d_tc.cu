@@ -15,7 +15,7 @@ cudaError_t launch_tc_p(const Stage3DArgs<float>& a, const KuhnTab3<float>& tab,
     cudaError_t e = persistent_blocks_per_sm((const void*)kern, NT, S::SMEM, &bps);
     if (e != cudaSuccess) return e;
   }
-  const int ngroups = (a.ncell + S::EC - 1) / S::EC;
+  const int ngroups = (a.ncell - a.cbeg + S::EC - 1) / S::EC;
   int nblk = nsm * bps;
   if (nblk > ngroups) nblk = ngroups;
   if (nblk < 1) nblk = 1;

@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
   int* sMd = sNb + EC * 6;                                 // [EC][6] face mode | code << 8
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int ngroups = (args.ncell + EC - 1) / EC;
+  const int ngroups = (args.ncell - args.cbeg + EC - 1) / EC;
   if (tid == 0) {
     for (int k = 0; k < 4; ++k) mbar_init(&bar[k], 1);
     fence_mbar_init();
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
     bulk_g2s(sAhi, a_image, uint32_t(2 * S::A_BYTES), &bar[3]);
   }
   auto issue = [&](int grp, int buf) {
-    const int c0 = grp * EC, nc = min(EC, args.ncell - c0);
+    const int c0 = args.cbeg + grp * EC, nc = min(EC, args.ncell - c0);
     const uint32_t bytes = uint32_t(nc) * 6u * NP * NC * 4u;
     fence_proxy_async();
     mbar_arrive_expect_tx(&bar[buf], bytes);
@@ -215,8 +215,9 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
   // last, partial tile of an odd-sized span takes plain loads).
   auto tile_bulk = [&](int g) -> bool {
     const size_t per_cube = size_t(6) * NP * NC * 4;
-    const size_t start = reinterpret_cast<uintptr_t>(args.q_in) + size_t(g) * EC * per_cube;
-    const size_t bytes = size_t(min(EC, args.ncell - g * EC)) * per_cube;
+    const int cg = args.cbeg + g * EC;
+    const size_t start = reinterpret_cast<uintptr_t>(args.q_in) + size_t(cg) * per_cube;
+    const size_t bytes = size_t(min(EC, args.ncell - cg)) * per_cube;
     return start % 16 == 0 && bytes % 16 == 0;
   };
   int buf = 0;
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
   // Fbar.  The cube-face treatment runs at the same time on threads from
   // NT/2 on.
   auto fbar_phase = [&](int g, const float* qt) {
-    const int ncg = min(EC, args.ncell - g * EC);
+    const int ncg = min(EC, args.ncell - args.cbeg - g * EC);
     for (int w = tid; w < ncg * 24; w += NT) {
       const int el = w >> 2, lf = w & 3, t = el % 6;
       float F[3 * NC];
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
     }
     for (int w = tid - NT / 2; w >= 0 && w < ncg * 6; w += NT / 2) {
       const int cl = w / 6, dd = w - cl * 6;
-      cube_dirs3(g * EC + cl, args.nx, args.ny, args.nz, args.bc, sNb + cl * 6, sMd + cl * 6, dd);
+      cube_dirs3(args.cbeg + g * EC + cl, args.nx, args.ny, args.nz, args.bc, sNb + cl * 6, sMd + cl * 6, dd);
     }
   };
   // With two state buffers the next tile's copy lands while this tile is
@@ -257,7 +258,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
   bool fb_ready = false;
 
   for (int grp = blockIdx.x; grp < ngroups && !failed; grp += gridDim.x, buf ^= (S::QB - 1)) {
-    const int cell0 = grp * EC;
+    const int cell0 = args.cbeg + grp * EC;
     const int nc_here = min(EC, args.ncell - cell0);
     const int ne_here = 6 * nc_here;
     float* q = sQ + buf * QV;

@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol():
     L = M.lib()
     for name in header_functions():
         assert hasattr(L, name), name
-    assert L.mxm_dg_version() == 20000
+    assert L.mxm_dg_version() == 20100
 
 
 def test_bad_arguments_return_einval():
