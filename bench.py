@@ -17,7 +17,10 @@ algorithm; the Mojo reference itself cannot be built on this image) on the
 host cores with all threads, on a bounded sample of the same workload.
 Multi-GPU (torchrun): every rank advances its own replica of the workload
 (independent solves, no collective on the data path); `value` is the sum of
-all ranks' DOF over the max-over-ranks device time.
+all ranks' DOF over the max-over-ranks device time.  Side legs in the same
+line: the batched 2D engine, the Maxwell cavity, the 3D MHD Alfven wave, the
+served stream, and (`slab`) the headline mesh split into z-slabs on one GPU
+with its halo exchange.
 """
 from __future__ import annotations
 
@@ -60,6 +63,7 @@ def parse():
     ap.add_argument("--serve-slots", type=int, default=8, help="solves running at once in the served leg")
     ap.add_argument("--cavity", type=int, default=1, help="run the 24^3x6 P=4 Maxwell cavity leg (1/0)")
     ap.add_argument("--mhd", type=int, default=1, help="run the 3D ideal-MHD Alfven-wave leg (1/0)")
+    ap.add_argument("--slab-parts", type=int, default=4, help="z-slab decomposition leg on one GPU (0 = skip)")
     return ap.parse_args()
 
 
@@ -464,6 +468,50 @@ def mhd_alfven(M, nx=64, P=3, steps=30, precision="mixed"):
             "rel_l2_vs_f64": float(np.sqrt(((qa - q64) ** 2).sum() / (q64 ** 2).sum())), "steps": 3 + steps}
 
 
+def slab_decomposed(M, a, parts, steps=20):
+    """The headline mesh split into `parts` z-slabs on this GPU, stepped as one
+    in-process group (ghost layers by device copies, ordered by events): the
+    cost of the halo exchange against the undecomposed solve, and a check
+    that the owned results stay bit-identical to it."""
+    import time
+    mesh = M.Mesh(a.n, a.n, a.n, 1.0, 1.0, 1.0)
+    ph = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_RUSANOV)
+    dt = dt_for(a.n, a.P)
+    ic = [1.0, 0.2, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0]
+    ps = [M.Solver(mesh, ph, P=a.P, precision=a.precision, nparts=parts, part=r) for r in range(parts)]
+    for s in ps:
+        s.fill_ic(M.IC_SINE_WAVE, ic)
+    grp = M.SlabGroup(ps)
+    grp.step_n(dt, 3)
+    grp.synchronize()
+    t0 = time.perf_counter()
+    grp.step_n(dt, steps)
+    grp.synchronize()
+    el = time.perf_counter() - t0
+    one = M.Solver(mesh, ph, P=a.P, precision=a.precision)
+    one.fill_ic(M.IC_SINE_WAVE, ic)
+    one.step_n(dt, 3)
+    one.synchronize()
+    t0 = time.perf_counter()
+    one.step_n(dt, steps)
+    one.synchronize()
+    el1 = time.perf_counter() - t0
+    ref = one.download_state().reshape(-1)
+    n = one.NP * one.NC
+    got = np.concatenate([s.download_state().reshape(-1)[s.owned_e0 * n:(s.owned_e0 + s.owned_ne) * n] for s in ps])
+    layer_bytes = ps[0].slab_layout()["layer"] * (8 if a.precision == "f64" else 4)
+    ghosts = sum(sum(s.ghosts) for s in ps)
+    dof = one.dof_count()
+    grp.close()
+    for s in ps + [one]:
+        s.close()
+    return {"workload": f"{workload_name(a)}, split into {parts} z-slabs on one GPU", "parts": parts,
+            "value": 3 * dof * steps / el, "unit": UNIT, "ms_per_step": el * 1e3 / steps,
+            "single_domain_ms_per_step": el1 * 1e3 / steps, "overhead": el / el1 - 1.0,
+            "exchange_bytes_per_stage": ghosts * layer_bytes, "bit_identical_to_single_domain": bool(np.array_equal(got, ref)),
+            "timing": "host wall clock around synchronized steps (both runs)"}
+
+
 def served(M, nreq, lam, seed=7, largest=False, slots=8, precision=None):
     """Served stream: Poisson arrivals at `lam`/s of 2D/3D Euler, 2D
     shallow-water dam breaks and 3D Maxwell plane waves, 2k-400k elements
@@ -647,6 +695,7 @@ def main():
             bat["speedup_vs_f64"] = bat["value"] / b64["value"]
         cav = maxwell_cavity(M) if a.cavity else None
         mhd = mhd_alfven(M) if a.mhd else None
+        slab = slab_decomposed(M, a, a.slab_parts) if a.slab_parts > 0 else None
         srv = served(M, a.serve_requests, a.serve_lambda, largest=a.serve_largest,
                      slots=a.serve_slots) if a.serve_requests > 0 else None
         if srv is not None:  # the same stream with every request in FP64
@@ -673,7 +722,7 @@ def main():
             "plain_f64": plain,
             "measured_gemm_peaks": fpp,
             "batched": bat,
-            "maxwell_cavity": cav, "mhd_alfven": mhd,
+            "maxwell_cavity": cav, "mhd_alfven": mhd, "slab": slab,
             "served": srv,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": qbytes,
                     "entry": "mxm_dg_advance_host (pinned host state in/out, 1 SSPRK3 step per call)"},

@@ -147,6 +147,9 @@ int mxm_dg_state_ptr(void* handle, int which, void** dptr);
 int mxm_dg_node_xyz_ptr(void* handle, void** dptr);
 /* Host copies of node coordinates in FP64 [Ne*NP*dim]. */
 int mxm_dg_node_xyz(void* handle, double* host);
+/* The Float32 coordinates of mxm_dg_node_xyz_ptr on the host (the values
+ * the reference's VTU frames store as points). */
+int mxm_dg_node_xyz_f32(void* handle, float* host);
 /* Copy a whole state buffer from/to caller-owned host memory; `nbytes` must
  * equal Ne*NP*NC*real_bytes.  Synchronous. */
 int mxm_dg_upload_state(void* handle, int which, const void* host, size_t nbytes);

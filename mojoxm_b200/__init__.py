@@ -38,7 +38,7 @@ EXPORTED = [
     "mxm_dg_slab_plan", "mxm_dg_create_slab", "mxm_dg_slab_info", "mxm_dg_slab_layout", "mxm_dg_slab_stage",
     "mxm_dg_nccl_unique_id", "mxm_dg_slab_connect_nccl", "mxm_dg_group_create", "mxm_dg_group_step_n",
     "mxm_dg_group_synchronize", "mxm_dg_group_last_error", "mxm_dg_group_destroy",
-    "mxm_dg_version", "mxm_dg_create", "mxm_dg_destroy", "mxm_dg_sizes", "mxm_dg_dof_count",
+    "mxm_dg_version", "mxm_dg_node_xyz_f32", "mxm_dg_create", "mxm_dg_destroy", "mxm_dg_sizes", "mxm_dg_dof_count",
     "mxm_dg_state_bytes_per_step", "mxm_dg_state_ptr", "mxm_dg_node_xyz_ptr", "mxm_dg_node_xyz",
     "mxm_dg_upload_state", "mxm_dg_download_state", "mxm_dg_download_component", "mxm_dg_download_component_f64",
     "mxm_dg_enable_limiter", "mxm_dg_step_ssprk3", "mxm_dg_step_n", "mxm_dg_rk_stage", "mxm_dg_eval_rhs",
@@ -95,6 +95,7 @@ def lib():
         L.mxm_dg_state_ptr.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
         L.mxm_dg_node_xyz_ptr.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
         L.mxm_dg_node_xyz.argtypes = [vp, dp]
+        L.mxm_dg_node_xyz_f32.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
         L.mxm_dg_upload_state.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t]
         L.mxm_dg_download_state.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t]
         L.mxm_dg_download_component.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
@@ -429,6 +430,12 @@ class Solver:
     def node_xyz(self):
         out = np.zeros((self.num_elements, self.NP, self.mesh.dim))
         self._c(lib().mxm_dg_node_xyz(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    def node_xyz_f32(self):
+        """Float32 node coordinates as the reference builds elem_node_xyz."""
+        out = np.zeros((self.num_elements, self.NP, self.mesh.dim), np.float32)
+        self._c(lib().mxm_dg_node_xyz_f32(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return out
 
     def node_xyz_ptr(self):

@@ -495,7 +495,7 @@ double reduce_scale(const Handle* h, int kind) {
 }
 
 // Float32 node coordinates exactly as the reference builds elem_node_xyz.
-void build_xyz(Handle* h) {
+std::vector<float> xyz_f32(const Handle* h) {
   std::vector<float> x(size_t(h->ne) * h->NP * h->dim);
   if (h->dim == 3) {
     // local_mesh.mojo:568-580 (rel coords in Float32) and :814-827
@@ -540,6 +540,11 @@ void build_xyz(Handle* h) {
       }
     }
   }
+  return x;
+}
+
+void build_xyz(Handle* h) {
+  const std::vector<float> x = xyz_f32(h);
   CK(cudaMalloc(&h->xyz, x.size() * sizeof(float)));
   CK(cudaMemcpy(h->xyz, x.data(), x.size() * sizeof(float), cudaMemcpyHostToDevice));
 }
@@ -817,6 +822,14 @@ int mxm_dg_node_xyz_ptr(void* handle, void** dptr) {
   API_BEGIN
   if (!h->xyz) mxm::build_xyz(h);
   *dptr = h->xyz;
+  API_END
+}
+
+int mxm_dg_node_xyz_f32(void* handle, float* out) {
+  API_BEGIN
+  if (!out) throw mxm::ArgError("out must be non-null");
+  const std::vector<float> x = mxm::xyz_f32(h);
+  std::memcpy(out, x.data(), x.size() * sizeof(float));
   API_END
 }
 
