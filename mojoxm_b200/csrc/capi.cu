@@ -2,6 +2,7 @@
 // device state, operators and scratch, and dispatches the sm_100a kernels.
 // Mirrors the reference's Solver[PhysT, P] (src/solver.mojo:538-1092) and
 // the 2D stage helpers (src/local_mesh_2d_gpu_*.mojo, src/ssprk3.mojo:56-78).
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -182,7 +183,7 @@ Mhd2D<R, GLM> make_mhd2d(const double* p) {
 
 template <class R>
 cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double b, double c,
-                         double dt, int rhs_only) {
+                         double dt, int rhs_only, int64_t c0, int64_t c1) {
   const double* p = h->phys.p;
   const R cdt = R(c * dt);
   if (h->dim == 3) {
@@ -197,8 +198,8 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
     ar.nx = h->nx;
     ar.ny = h->ny;
     ar.nz = h->nz;
-    ar.cbeg = int(h->cbeg);
-    ar.ncell = int(h->cend);
+    ar.cbeg = int(c0);
+    ar.ncell = int(c1);
     for (int k = 0; k < 6; ++k) ar.bc[k] = h->bc[k];
     ar.rhs_only = rhs_only;
     ar.err = h->derr;
@@ -389,10 +390,13 @@ cudaError_t wavespeed_launch(Handle* h, const void* qi, unsigned long long* out)
 }
 
 // One Shu-Osher stage q_out = (1 - b) q_a + b q_b + c dt L(q_in).
+// Cells c0 .. c1-1 (default: the owned cells).
 void stage(Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double b, double c, double dt,
-           int rhs_only) {
-  cudaError_t e = h->rbytes == 8 ? stage_launch<double>(h, qi, qa, qb, qo, b, c, dt, rhs_only)
-                                 : stage_launch<float>(h, qi, qa, qb, qo, b, c, dt, rhs_only);
+           int rhs_only, int64_t c0 = -1, int64_t c1 = -1) {
+  if (c0 < 0) c0 = h->cbeg;
+  if (c1 < 0) c1 = h->cend;
+  cudaError_t e = h->rbytes == 8 ? stage_launch<double>(h, qi, qa, qb, qo, b, c, dt, rhs_only, c0, c1)
+                                 : stage_launch<float>(h, qi, qa, qb, qo, b, c, dt, rhs_only, c0, c1);
   if (e != cudaSuccess) throw CudaError(e, "stage kernel launch");
 }
 
@@ -431,11 +435,25 @@ void limit_buf(Handle* h, void* qv) {
 // reads q, q1, q2 and writes q1, q2, q.
 int stage_in(int s) { return s; }
 int stage_out(int s) { return s == 0 ? 1 : (s == 1 ? 2 : 0); }
-void stage_only(Handle* h, int s, double dt) {
+void stage_only(Handle* h, int s, double dt, int64_t c0, int64_t c1) {
   void *q0 = h->q[0], *q1 = h->q[1], *q2 = h->q[2];
-  if (s == 0) stage(h, q0, q0, q0, q1, 0.0, 1.0, dt, 0);
-  else if (s == 1) stage(h, q1, q0, q1, q2, 0.25, 0.25, dt, 0);
-  else stage(h, q2, q0, q2, q0, 2.0 / 3.0, 2.0 / 3.0, dt, 0);
+  if (s == 0) stage(h, q0, q0, q0, q1, 0.0, 1.0, dt, 0, c0, c1);
+  else if (s == 1) stage(h, q1, q0, q1, q2, 0.25, 0.25, dt, 0, c0, c1);
+  else stage(h, q2, q0, q2, q0, 2.0 / 3.0, 2.0 / 3.0, dt, 0, c0, c1);
+}
+
+// Owned cells split for overlap: the interior cells (no face on a ghost
+// layer) run while the ghost layers are exchanged; the boundary layers
+// after.  lo/hi: the bottom and top owned layers when they face a ghost
+// layer (empty ranges have c1 <= c0).
+void slab_ranges(const Handle* h, int64_t in[2], int64_t lo[2], int64_t hi[2]) {
+  const int64_t nxy = int64_t(h->nx) * h->ny;
+  in[0] = h->cbeg + (h->glo ? nxy : 0);
+  in[1] = h->cend - (h->ghi ? nxy : 0);
+  lo[0] = h->cbeg;
+  lo[1] = h->glo ? std::min(h->cbeg + nxy, h->cend) : h->cbeg;
+  hi[0] = h->ghi ? std::max(h->cend - nxy, lo[1]) : h->cend;
+  hi[1] = h->cend;
 }
 
 // A slab part exchanges the ghost layers of the stage's input first and,
@@ -444,15 +462,26 @@ void stage_only(Handle* h, int s, double dt) {
 // stage before its kernel (src/solver.mojo:1038-1068).
 void rk_stage(Handle* h, int s, double dt) {
   const bool halo = h->glo || h->ghi;
-  if (halo) {
+  if (!halo) {
+    stage_only(h, s, dt);
+  } else {
     if (!h->nccl)
       throw ArgError("a slab part with ghost layers steps through mxm_dg_group_step_n, or by itself after "
                      "mxm_dg_slab_connect_nccl");
-    nccl_exchange(h, stage_in(s));
+    // the exchange runs on the part's second stream beside the interior cells
+    int64_t in[2], lo[2], hi[2];
+    slab_ranges(h, in, lo, hi);
+    CK(cudaEventRecord(h->ev_in, h->stream));
+    CK(cudaStreamWaitEvent(h->comm, h->ev_in, 0));
+    nccl_exchange(h, stage_in(s), h->comm);
+    CK(cudaEventRecord(h->ev_x, h->comm));
+    if (in[1] > in[0]) stage_only(h, s, dt, in[0], in[1]);
+    CK(cudaStreamWaitEvent(h->stream, h->ev_x, 0));
+    if (lo[1] > lo[0]) stage_only(h, s, dt, lo[0], lo[1]);
+    if (hi[1] > hi[0]) stage_only(h, s, dt, hi[0], hi[1]);
   }
-  stage_only(h, s, dt);
   if (h->lim_on) {
-    if (halo) nccl_exchange(h, stage_out(s));
+    if (halo) nccl_exchange(h, stage_out(s), h->stream);
     limit_buf(h, h->q[stage_out(s)]);
   }
 }
@@ -608,6 +637,9 @@ void destroy(Handle* h) {
   cudaFree(h->derr);
   cudaFree(h->tcimg);
   if (h->nccl) nccl_release(h);
+  if (h->ev_in) cudaEventDestroy(h->ev_in);
+  if (h->ev_x) cudaEventDestroy(h->ev_x);
+  if (h->comm) cudaStreamDestroy(h->comm);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -698,6 +730,11 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   Handle* raw = h.get();
   try {
+    if (raw->glo || raw->ghi) {  // a slab part: exchange stream and its events
+      CK(cudaStreamCreateWithFlags(&raw->comm, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&raw->ev_in, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&raw->ev_x, cudaEventDisableTiming));
+    }
     for (auto& b : raw->q) {
       cudaError_t e = cudaMalloc(&b, raw->qbytes());
       if (e != cudaSuccess) throw CudaError(e, "cudaMalloc(state)");

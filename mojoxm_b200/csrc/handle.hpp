@@ -46,6 +46,8 @@ struct Handle {
   int nzg = 1, kz0 = 0;  // global z cells; global z index of local layer 0
   int64_t cbeg = 0, cend = 0;
   struct NcclLink* nccl = nullptr;  // halo transport of a multi-process slab
+  cudaStream_t comm = nullptr;       // a slab part's exchange stream
+  cudaEvent_t ev_in = nullptr, ev_x = nullptr;  // input written / ghosts landed
   size_t rbytes = 8;
   int device = 0, nsm = 148;
   cudaStream_t stream = nullptr;
@@ -98,13 +100,14 @@ void destroy(Handle* h);
 void step_n(Handle* h, double dt, int n);
 // stage kernel of Shu-Osher stage s without exchange or limiter, and the
 // buffers it reads and writes
-void stage_only(Handle* h, int s, double dt);
+void stage_only(Handle* h, int s, double dt, int64_t c0 = -1, int64_t c1 = -1);
+void slab_ranges(const Handle* h, int64_t in[2], int64_t lo[2], int64_t hi[2]);
 int stage_in(int s);
 int stage_out(int s);
 void limit_buf(Handle* h, void* qv);
 // NCCL halo transport (slab.cu): exchange the ghost layers of state buffer
 // `which` on the handle's stream; release the link
-void nccl_exchange(Handle* h, int which);
+void nccl_exchange(Handle* h, int which, cudaStream_t st);
 void nccl_release(Handle* h);
 void fill_ic(Handle* h, int which, int kind, const double* params, int nparams);
 // 2D GLM-MHD psi damping after each step: whether h has it, and its factor

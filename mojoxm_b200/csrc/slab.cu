@@ -122,14 +122,14 @@ struct NcclLink {
 // in the order (from lo: the up message, from hi: the down message), so the
 // messages of a pair of parts that neighbour each other on both sides (two
 // periodic parts) match in NCCL's per-pair issue order.
-void nccl_exchange(Handle* h, int which) {
+void nccl_exchange(Handle* h, int which, cudaStream_t st) {
   const NcclApi& api = nccl_api();
   const size_t bytes = layer_vals(h) * h->rbytes;
   nck(api.group_start(), "ncclGroupStart");
-  if (h->ghi) nck(api.send(layer_ptr(h, which, owned_hi_layer(h)), bytes, ncclUint8, h->nb_hi, h->nccl->comm, h->stream), "ncclSend");
-  if (h->glo) nck(api.send(layer_ptr(h, which, owned_lo_layer(h)), bytes, ncclUint8, h->nb_lo, h->nccl->comm, h->stream), "ncclSend");
-  if (h->glo) nck(api.recv(layer_ptr(h, which, ghost_lo_layer(h)), bytes, ncclUint8, h->nb_lo, h->nccl->comm, h->stream), "ncclRecv");
-  if (h->ghi) nck(api.recv(layer_ptr(h, which, ghost_hi_layer(h)), bytes, ncclUint8, h->nb_hi, h->nccl->comm, h->stream), "ncclRecv");
+  if (h->ghi) nck(api.send(layer_ptr(h, which, owned_hi_layer(h)), bytes, ncclUint8, h->nb_hi, h->nccl->comm, st), "ncclSend");
+  if (h->glo) nck(api.send(layer_ptr(h, which, owned_lo_layer(h)), bytes, ncclUint8, h->nb_lo, h->nccl->comm, st), "ncclSend");
+  if (h->glo) nck(api.recv(layer_ptr(h, which, ghost_lo_layer(h)), bytes, ncclUint8, h->nb_lo, h->nccl->comm, st), "ncclRecv");
+  if (h->ghi) nck(api.recv(layer_ptr(h, which, ghost_hi_layer(h)), bytes, ncclUint8, h->nb_hi, h->nccl->comm, st), "ncclRecv");
   nck(api.group_end(), "ncclGroupEnd");
 }
 
@@ -163,32 +163,71 @@ struct Group {
   // keeps a part from rewriting layers its neighbours are still copying
   void exchange(int which) {
     barrier();
+    for (int r = 0; r < int(parts.size()); ++r) {
+      CK(cudaSetDevice(parts[r]->device));
+      pull(r, which, parts[r]->stream);
+    }
+    barrier();
+  }
+  // copy the neighbours' boundary layers of `which` into part r's ghost layers on stream st
+  void pull(int r, int which, cudaStream_t st) {
+    Handle* h = parts[r];
+    const size_t bytes = layer_vals(h) * h->rbytes;
+    if (h->glo) {
+      const Handle* lo = parts[h->nb_lo];
+      CK(cudaMemcpyPeerAsync(layer_ptr(h, which, ghost_lo_layer(h)), h->device,
+                             layer_ptr(lo, which, owned_hi_layer(lo)), lo->device, bytes, st));
+    }
+    if (h->ghi) {
+      const Handle* hi = parts[h->nb_hi];
+      CK(cudaMemcpyPeerAsync(layer_ptr(h, which, ghost_hi_layer(h)), h->device,
+                             layer_ptr(hi, which, owned_lo_layer(hi)), hi->device, bytes, st));
+    }
+  }
+  // One stage with the exchange of its input overlapped: each part's
+  // exchange stream waits for its own and its neighbours' last writes, pulls
+  // its ghost layers while the main stream computes the interior cells; the
+  // boundary layers wait for the part's own copies and for the neighbours'
+  // copies out of this part (which must finish before it writes again).
+  void stage_overlapped(int s, double dt) {
     const int n = int(parts.size());
+    for (int r = 0; r < n; ++r) {
+      CK(cudaSetDevice(parts[r]->device));
+      CK(cudaEventRecord(parts[r]->ev_in ? parts[r]->ev_in : ev[r], parts[r]->stream));
+    }
+    auto ev_in = [&](int r) { return parts[r]->ev_in ? parts[r]->ev_in : ev[r]; };
+    for (int r = 0; r < n; ++r) {
+      Handle* h = parts[r];
+      if (!h->comm) continue;  // no ghost layers
+      CK(cudaSetDevice(h->device));
+      CK(cudaStreamWaitEvent(h->comm, ev_in(r), 0));
+      for (int nb : {h->nb_lo, h->nb_hi})
+        if (nb >= 0 && nb != r) CK(cudaStreamWaitEvent(h->comm, ev_in(nb), 0));
+      pull(r, stage_in(s), h->comm);
+      CK(cudaEventRecord(h->ev_x, h->comm));
+    }
+    int64_t in[2], lo[2], hi[2];
     for (int r = 0; r < n; ++r) {
       Handle* h = parts[r];
       CK(cudaSetDevice(h->device));
-      const size_t bytes = layer_vals(h) * h->rbytes;
-      if (h->glo) {
-        const Handle* lo = parts[h->nb_lo];
-        CK(cudaMemcpyPeerAsync(layer_ptr(h, which, ghost_lo_layer(h)), h->device,
-                               layer_ptr(lo, which, owned_hi_layer(lo)), lo->device, bytes, h->stream));
-      }
-      if (h->ghi) {
-        const Handle* hi = parts[h->nb_hi];
-        CK(cudaMemcpyPeerAsync(layer_ptr(h, which, ghost_hi_layer(h)), h->device,
-                               layer_ptr(hi, which, owned_lo_layer(hi)), hi->device, bytes, h->stream));
-      }
+      slab_ranges(h, in, lo, hi);
+      if (in[1] > in[0]) stage_only(h, s, dt, in[0], in[1]);
     }
-    barrier();
+    for (int r = 0; r < n; ++r) {
+      Handle* h = parts[r];
+      CK(cudaSetDevice(h->device));
+      if (h->comm) CK(cudaStreamWaitEvent(h->stream, h->ev_x, 0));
+      for (int nb : {h->nb_lo, h->nb_hi})
+        if (nb >= 0 && nb != r && parts[nb]->comm) CK(cudaStreamWaitEvent(h->stream, parts[nb]->ev_x, 0));
+      slab_ranges(h, in, lo, hi);
+      if (lo[1] > lo[0]) stage_only(h, s, dt, lo[0], lo[1]);
+      if (hi[1] > hi[0]) stage_only(h, s, dt, hi[0], hi[1]);
+    }
   }
   void step_n(double dt, int nsteps) {
     for (int k = 0; k < nsteps; ++k)
       for (int s = 0; s < 3; ++s) {
-        exchange(stage_in(s));
-        for (Handle* h : parts) {
-          CK(cudaSetDevice(h->device));
-          stage_only(h, s, dt);
-        }
+        stage_overlapped(s, dt);
         if (parts[0]->lim_on) {
           exchange(stage_out(s));
           for (Handle* h : parts) {
