@@ -1154,7 +1154,15 @@ int mxm_dg_time_steps(void* handle, double dt, int nsteps, double* ms) {
 
 int mxm_dg_launches_per_step(void* handle, int32_t* n) {
   API_BEGIN
-  *n = 3 * (1 + (h->lim_on ? 2 : 0));
+  // a slab part launches its stage as interior + boundary layers; the 2D
+  // GLM stack adds one psi-damping launch per step
+  int per_stage = 1;
+  if (h->glo || h->ghi) {
+    int64_t in[2], lo[2], hi[2];
+    mxm::slab_ranges(h, in, lo, hi);
+    per_stage = int(in[1] > in[0]) + int(lo[1] > lo[0]) + int(hi[1] > hi[0]);
+  }
+  *n = 3 * (per_stage + (h->lim_on ? 2 : 0)) + (mxm::glm_damped(h) ? 1 : 0);
   API_END
 }
 

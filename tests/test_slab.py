@@ -211,6 +211,8 @@ def test_slab_owned_diagnostics_and_layout():
         plan = halo.SlabPlan.of(7, 0, 0, 3, s.part)
         assert s.slab_layout() == halo.layer_offsets(plan, per_layer)
         assert s.owned_layers == (plan.cz0, plan.cz1) and s.ghosts == (plan.ghost_lo, plan.ghost_hi)
+        # interior cells (when a part owns more than two layers) + the two boundary layers
+        assert s.launches_per_step() == 3 * (2 + int(plan.cz1 - plan.cz0 > 2))
     grp.close()
 
 
