@@ -180,6 +180,11 @@ int mxm_dg_limit(void* handle, int which);
  * download d_q into q_out_host (the same layout).  Pinned host memory gives
  * asynchronous copies; pageable memory works too. */
 int mxm_dg_advance_host(void* handle, const void* q_host, void* q_out_host, int nsteps, double dt);
+/* The same, returning once enqueued: q_out_host holds the result after
+ * mxm_dg_synchronize.  Successive calls pipeline (one call's download runs
+ * beside the next call's upload and steps); the host buffers must stay
+ * valid until the synchronize and should be pinned (mxm_dg_host_alloc). */
+int mxm_dg_advance_host_async(void* handle, const void* q_host, void* q_out_host, int nsteps, double dt);
 
 /* ---- diagnostics (FP64 device reductions) -------------------------------- */
 /* Max over all face nodes of the signal speed numerical_flux/boundary_flux

@@ -38,7 +38,7 @@ EXPORTED = [
     "mxm_dg_slab_plan", "mxm_dg_create_slab", "mxm_dg_slab_info", "mxm_dg_slab_layout", "mxm_dg_slab_stage",
     "mxm_dg_nccl_unique_id", "mxm_dg_slab_connect_nccl", "mxm_dg_group_create", "mxm_dg_group_step_n",
     "mxm_dg_group_synchronize", "mxm_dg_group_last_error", "mxm_dg_group_destroy",
-    "mxm_dg_version", "mxm_dg_node_xyz_f32", "mxm_dg_create", "mxm_dg_destroy", "mxm_dg_sizes", "mxm_dg_dof_count",
+    "mxm_dg_version", "mxm_dg_node_xyz_f32", "mxm_dg_advance_host_async", "mxm_dg_create", "mxm_dg_destroy", "mxm_dg_sizes", "mxm_dg_dof_count",
     "mxm_dg_state_bytes_per_step", "mxm_dg_state_ptr", "mxm_dg_node_xyz_ptr", "mxm_dg_node_xyz",
     "mxm_dg_upload_state", "mxm_dg_download_state", "mxm_dg_download_component", "mxm_dg_download_component_f64",
     "mxm_dg_enable_limiter", "mxm_dg_step_ssprk3", "mxm_dg_step_n", "mxm_dg_rk_stage", "mxm_dg_eval_rhs",
@@ -107,6 +107,7 @@ def lib():
         L.mxm_dg_eval_rhs.argtypes = [vp, vp, vp]
         L.mxm_dg_limit.argtypes = [vp, ctypes.c_int]
         L.mxm_dg_advance_host.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double]
+        L.mxm_dg_advance_host_async.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double]
         L.mxm_dg_max_wavespeed.argtypes = [vp, dp]
         L.mxm_dg_reduce_conserved.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
         L.mxm_dg_reduce_conserved_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
@@ -490,6 +491,12 @@ class Solver:
         out = np.empty_like(a) if out is None else out
         self._c(lib().mxm_dg_advance_host(self.h, a.ctypes.data, out.ctypes.data, nsteps, dt))
         return out
+
+    def advance_host_async(self, q_host, nsteps, dt, out):
+        """Enqueue upload + steps + download; `q_host` and `out` (pinned, e.g.
+        PinnedArray) must stay alive until synchronize()."""
+        assert q_host.flags["C_CONTIGUOUS"] and out.flags["C_CONTIGUOUS"] and out.nbytes == q_host.nbytes
+        self._c(lib().mxm_dg_advance_host_async(self.h, q_host.ctypes.data, out.ctypes.data, nsteps, dt))
 
     def synchronize(self):
         self._c(lib().mxm_dg_synchronize(self.h))

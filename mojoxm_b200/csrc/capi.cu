@@ -640,6 +640,13 @@ void destroy(Handle* h) {
   if (h->ev_in) cudaEventDestroy(h->ev_in);
   if (h->ev_x) cudaEventDestroy(h->ev_x);
   if (h->comm) cudaStreamDestroy(h->comm);
+  if (h->h2d) cudaStreamSynchronize(h->h2d);
+  if (h->d2h) cudaStreamSynchronize(h->d2h);
+  for (cudaEvent_t e : {h->e_tail, h->e_in, h->e_res, h->e_out_free})
+    if (e) cudaEventDestroy(e);
+  if (h->h2d) cudaStreamDestroy(h->h2d);
+  if (h->d2h) cudaStreamDestroy(h->d2h);
+  cudaFree(h->out_stage);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -1004,6 +1011,36 @@ int mxm_dg_advance_host(void* handle, const void* q_host, void* q_out_host, int 
   API_END
 }
 
+// Pipelined host entry: the upload of this call's state waits only for the
+// work already enqueued on the handle; the result leaves through a device
+// staging buffer on its own stream, so one call's download overlaps the next
+// call's upload (PCIe is full duplex) and its steps.
+int mxm_dg_advance_host_async(void* handle, const void* q_host, void* q_out_host, int nsteps, double dt) {
+  API_BEGIN
+  if (!q_host || !q_out_host || nsteps < 0) throw mxm::ArgError("host buffers must be non-null, nsteps >= 0");
+  if (!h->h2d) {
+    CK(cudaStreamCreateWithFlags(&h->h2d, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&h->d2h, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&h->e_tail, &h->e_in, &h->e_res, &h->e_out_free})
+      CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    CK(cudaMalloc(&h->out_stage, h->qbytes()));
+    CK(cudaEventRecord(h->e_out_free, h->d2h));
+  }
+  CK(cudaEventRecord(h->e_tail, h->stream));  // every use of q so far
+  CK(cudaStreamWaitEvent(h->h2d, h->e_tail, 0));
+  CK(cudaMemcpyAsync(h->q[0], q_host, h->qbytes(), cudaMemcpyHostToDevice, h->h2d));
+  CK(cudaEventRecord(h->e_in, h->h2d));
+  CK(cudaStreamWaitEvent(h->stream, h->e_in, 0));
+  mxm::step_n(h, dt, nsteps);
+  CK(cudaStreamWaitEvent(h->stream, h->e_out_free, 0));  // the previous result has left the staging buffer
+  CK(cudaMemcpyAsync(h->out_stage, h->q[0], h->qbytes(), cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaEventRecord(h->e_res, h->stream));
+  CK(cudaStreamWaitEvent(h->d2h, h->e_res, 0));
+  CK(cudaMemcpyAsync(q_out_host, h->out_stage, h->qbytes(), cudaMemcpyDeviceToHost, h->d2h));
+  CK(cudaEventRecord(h->e_out_free, h->d2h));
+  API_END
+}
+
 int mxm_dg_max_wavespeed(void* handle, double* out) {
   API_BEGIN
   CK(cudaMemsetAsync(h->uscalar, 0, sizeof(unsigned long long), h->stream));
@@ -1124,6 +1161,8 @@ int mxm_dg_host_free(void* host) {
 int mxm_dg_synchronize(void* handle) {
   API_BEGIN
   CK(cudaStreamSynchronize(h->stream));
+  if (h->h2d) CK(cudaStreamSynchronize(h->h2d));
+  if (h->d2h) CK(cudaStreamSynchronize(h->d2h));
   CK(cudaGetLastError());
   int derr = 0;
   CK(cudaMemcpy(&derr, h->derr, sizeof(int), cudaMemcpyDeviceToHost));
