@@ -642,10 +642,11 @@ void destroy(Handle* h) {
   if (h->comm) cudaStreamDestroy(h->comm);
   if (h->h2d) cudaStreamSynchronize(h->h2d);
   if (h->d2h) cudaStreamSynchronize(h->d2h);
-  for (cudaEvent_t e : {h->e_tail, h->e_in, h->e_res, h->e_out_free})
+  for (cudaEvent_t e : {h->e_in_free, h->e_in, h->e_res, h->e_out_free})
     if (e) cudaEventDestroy(e);
   if (h->h2d) cudaStreamDestroy(h->h2d);
   if (h->d2h) cudaStreamDestroy(h->d2h);
+  cudaFree(h->in_stage);
   cudaFree(h->out_stage);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -1011,26 +1012,30 @@ int mxm_dg_advance_host(void* handle, const void* q_host, void* q_out_host, int 
   API_END
 }
 
-// Pipelined host entry: the upload of this call's state waits only for the
-// work already enqueued on the handle; the result leaves through a device
-// staging buffer on its own stream, so one call's download overlaps the next
-// call's upload (PCIe is full duplex) and its steps.
+// Pipelined host entry: the state arrives in a device staging buffer on an
+// upload stream and leaves from another on a download stream; the handle's
+// stream only copies it in and out on the device (two 3 TB/s copies), so one
+// call's upload runs beside the previous call's steps and download (PCIe is
+// full duplex) and the pipeline moves at the PCIe rate of one direction.
 int mxm_dg_advance_host_async(void* handle, const void* q_host, void* q_out_host, int nsteps, double dt) {
   API_BEGIN
   if (!q_host || !q_out_host || nsteps < 0) throw mxm::ArgError("host buffers must be non-null, nsteps >= 0");
   if (!h->h2d) {
     CK(cudaStreamCreateWithFlags(&h->h2d, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&h->d2h, cudaStreamNonBlocking));
-    for (cudaEvent_t* e : {&h->e_tail, &h->e_in, &h->e_res, &h->e_out_free})
+    for (cudaEvent_t* e : {&h->e_in_free, &h->e_in, &h->e_res, &h->e_out_free})
       CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    CK(cudaMalloc(&h->in_stage, h->qbytes()));
     CK(cudaMalloc(&h->out_stage, h->qbytes()));
+    CK(cudaEventRecord(h->e_in_free, h->h2d));
     CK(cudaEventRecord(h->e_out_free, h->d2h));
   }
-  CK(cudaEventRecord(h->e_tail, h->stream));  // every use of q so far
-  CK(cudaStreamWaitEvent(h->h2d, h->e_tail, 0));
-  CK(cudaMemcpyAsync(h->q[0], q_host, h->qbytes(), cudaMemcpyHostToDevice, h->h2d));
+  CK(cudaStreamWaitEvent(h->h2d, h->e_in_free, 0));  // the previous input has left the staging buffer
+  CK(cudaMemcpyAsync(h->in_stage, q_host, h->qbytes(), cudaMemcpyHostToDevice, h->h2d));
   CK(cudaEventRecord(h->e_in, h->h2d));
   CK(cudaStreamWaitEvent(h->stream, h->e_in, 0));
+  CK(cudaMemcpyAsync(h->q[0], h->in_stage, h->qbytes(), cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaEventRecord(h->e_in_free, h->stream));
   mxm::step_n(h, dt, nsteps);
   CK(cudaStreamWaitEvent(h->stream, h->e_out_free, 0));  // the previous result has left the staging buffer
   CK(cudaMemcpyAsync(h->out_stage, h->q[0], h->qbytes(), cudaMemcpyDeviceToDevice, h->stream));

@@ -50,8 +50,8 @@ struct Handle {
   // host pipeline of mxm_dg_advance_host_async: copy streams, the result's
   // device staging buffer and the events that order them
   cudaStream_t h2d = nullptr, d2h = nullptr;
-  void* out_stage = nullptr;
-  cudaEvent_t e_tail = nullptr, e_in = nullptr, e_res = nullptr, e_out_free = nullptr;
+  void *in_stage = nullptr, *out_stage = nullptr;
+  cudaEvent_t e_in_free = nullptr, e_in = nullptr, e_res = nullptr, e_out_free = nullptr;
   cudaEvent_t ev_in = nullptr, ev_x = nullptr;  // input written / ghosts landed
   size_t rbytes = 8;
   int device = 0, nsm = 148;
