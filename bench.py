@@ -641,7 +641,7 @@ def main():
     pin_in = M.PinnedArray(s.shape, s.dtype)
     pin_out = M.PinnedArray(s.shape, s.dtype)
     pin_in.array[:] = s.download_state(0)
-    e2e_steps = max(2, min(a.steps, 10))
+    e2e_steps = max(2, min(a.steps, 30))
     s.advance_host_async(pin_in.array, 1, dt, pin_out.array)  # warm (allocates the pipeline)
     s.synchronize()
     barrier()
