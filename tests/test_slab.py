@@ -191,6 +191,26 @@ def test_group_bit_identical_to_plain(prec, nparts, case):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name,prec,bcs", [
+    ("maxwell", "mixed", (0, 0, 1, 1, 1, 1)),
+    ("mhd", "f32", (0,) * 6),
+    ("shallow_water", "f64", (1, 1, 0, 0, 1, 1)),
+    ("advection", "mixed", (3, 2, 0, 0, 3, 2)),
+    ("two_fluid", "f32", (0,) * 6),
+])
+def test_group_bit_identical_other_physics(name, prec, bcs):
+    ph = dgcases.two_fluid() if name == "two_fluid" else dgcases.PHYSICS_3D[name]()
+    plain, parts, _ = _plain_and_parts(ph, bcs, 2, prec, 3, n=(2, 2, 6), lim=True)
+    grp = M.SlabGroup(parts)
+    grp.step_n(5e-4, 3)
+    grp.synchronize()
+    plain.step_n(5e-4, 3)
+    got = np.concatenate([_owned(s) for s in parts])
+    assert np.array_equal(got, plain.download_state(0).reshape(-1))
+    grp.close()
+
+
+@pytest.mark.gpu
 def test_slab_owned_diagnostics_and_layout():
     ph, bcs, _ = _case("periodic")
     plain, parts, per_layer = _plain_and_parts(ph, bcs, 2, "f64", 3, n=(4, 2, 7))
