@@ -524,6 +524,38 @@ double reduce_scale(const Handle* h, int kind) {
 }
 
 // Float32 node coordinates exactly as the reference builds elem_node_xyz.
+// Device memory of a handle is stream-ordered (cudaMallocAsync /
+// cudaFreeAsync on the handle's stream): cudaFree waits for the whole
+// device, which would stall a server that creates and destroys solves while
+// others run.  The device's default pool keeps freed memory for the next
+// solve (its release threshold is raised once per device).
+namespace {
+std::mutex g_pool_mu;
+bool g_pool_ready[64] = {};
+}  // namespace
+
+void dev_alloc(Handle* h, void** p, size_t bytes) {
+  if (h->device >= 0 && h->device < 64) {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    if (!g_pool_ready[h->device]) {
+      cudaMemPool_t pool;
+      CK(cudaDeviceGetDefaultMemPool(&pool, h->device));
+      uint64_t keep = UINT64_MAX;
+      CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+      g_pool_ready[h->device] = true;
+    }
+  }
+  const cudaError_t e = cudaMallocAsync(p, bytes, h->stream);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    throw CudaError(e, "cudaMallocAsync");
+  }
+}
+
+void dev_free(Handle* h, void* p) {
+  if (p) cudaFreeAsync(p, h->stream);
+}
+
 std::vector<float> xyz_f32(const Handle* h) {
   std::vector<float> x(size_t(h->ne) * h->NP * h->dim);
   if (h->dim == 3) {
@@ -574,8 +606,9 @@ std::vector<float> xyz_f32(const Handle* h) {
 
 void build_xyz(Handle* h) {
   const std::vector<float> x = xyz_f32(h);
-  CK(cudaMalloc(&h->xyz, x.size() * sizeof(float)));
-  CK(cudaMemcpy(h->xyz, x.data(), x.size() * sizeof(float), cudaMemcpyHostToDevice));
+  dev_alloc(h, reinterpret_cast<void**>(&h->xyz), x.size() * sizeof(float));
+  CK(cudaMemcpyAsync(h->xyz, x.data(), x.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
 }
 
 // Device IC fill of state buffer `which` (asynchronous on the handle's stream).
@@ -626,16 +659,10 @@ void destroy(Handle* h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  for (auto& b : h->q) cudaFree(b);
-  cudaFree(h->A);
-  cudaFree(h->w);
-  cudaFree(h->avg);
-  cudaFree(h->xyz);
-  cudaFree(h->partial);
-  cudaFree(h->dscalar);
-  cudaFree(h->uscalar);
-  cudaFree(h->derr);
-  cudaFree(h->tcimg);
+  for (void* p : {h->q[0], h->q[1], h->q[2], h->A, h->w, h->avg, static_cast<void*>(h->xyz),
+                  static_cast<void*>(h->partial), static_cast<void*>(h->dscalar), static_cast<void*>(h->uscalar),
+                  static_cast<void*>(h->derr), h->tcimg})
+    dev_free(h, p);
   if (h->nccl) nccl_release(h);
   if (h->ev_in) cudaEventDestroy(h->ev_in);
   if (h->ev_x) cudaEventDestroy(h->ev_x);
@@ -646,8 +673,8 @@ void destroy(Handle* h) {
     if (e) cudaEventDestroy(e);
   if (h->h2d) cudaStreamDestroy(h->h2d);
   if (h->d2h) cudaStreamDestroy(h->d2h);
-  cudaFree(h->in_stage);
-  cudaFree(h->out_stage);
+  dev_free(h, h->in_stage);
+  dev_free(h, h->out_stage);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -744,8 +771,7 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
       CK(cudaEventCreateWithFlags(&raw->ev_x, cudaEventDisableTiming));
     }
     for (auto& b : raw->q) {
-      cudaError_t e = cudaMalloc(&b, raw->qbytes());
-      if (e != cudaSuccess) throw CudaError(e, "cudaMalloc(state)");
+      dev_alloc(raw, &b, raw->qbytes());
       CK(cudaMemsetAsync(b, 0, raw->qbytes(), raw->stream));
     }
     // fused operators, k-major per type, in the handle's real type
@@ -753,26 +779,28 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
     for (int i = 0; i < raw->NP; ++i)
       for (int k = 0; k < raw->K; ++k) At[size_t(k) * raw->NP + i] = raw->Ahost[size_t(i) * raw->K + k];
     auto upload = [&](void** dst, const std::vector<double>& src) {
-      CK(cudaMalloc(dst, src.size() * raw->rbytes));
+      dev_alloc(raw, dst, src.size() * raw->rbytes);
       if (raw->rbytes == 8) {
-        CK(cudaMemcpy(*dst, src.data(), src.size() * 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(*dst, src.data(), src.size() * 8, cudaMemcpyHostToDevice, raw->stream));
       } else {
         std::vector<float> f(src.begin(), src.end());
-        CK(cudaMemcpy(*dst, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(*dst, f.data(), f.size() * 4, cudaMemcpyHostToDevice, raw->stream));
+        CK(cudaStreamSynchronize(raw->stream));  // f goes out of scope
       }
     };
     upload(&raw->A, At);
     upload(&raw->w, raw->ref.w);
     if (raw->use_tc) {
       auto img = tc_operator_image(raw->Ahost, raw->NP, raw->K, 3 * raw->NP);
-      CK(cudaMalloc(&raw->tcimg, img.size()));
-      CK(cudaMemcpy(raw->tcimg, img.data(), img.size(), cudaMemcpyHostToDevice));
+      dev_alloc(raw, &raw->tcimg, img.size());
+      CK(cudaMemcpyAsync(raw->tcimg, img.data(), img.size(), cudaMemcpyHostToDevice, raw->stream));
+      CK(cudaStreamSynchronize(raw->stream));  // img goes out of scope
     }
-    CK(cudaMalloc(&raw->avg, size_t(raw->ne) * raw->NC * raw->rbytes));
-    CK(cudaMalloc(&raw->partial, raw->npartial * sizeof(double)));
-    CK(cudaMalloc(&raw->dscalar, 4 * sizeof(double)));
-    CK(cudaMalloc(&raw->uscalar, 4 * sizeof(unsigned long long)));
-    CK(cudaMalloc(&raw->derr, sizeof(int)));
+    dev_alloc(raw, &raw->avg, size_t(raw->ne) * raw->NC * raw->rbytes);
+    dev_alloc(raw, reinterpret_cast<void**>(&raw->partial), raw->npartial * sizeof(double));
+    dev_alloc(raw, reinterpret_cast<void**>(&raw->dscalar), 4 * sizeof(double));
+    dev_alloc(raw, reinterpret_cast<void**>(&raw->uscalar), 4 * sizeof(unsigned long long));
+    dev_alloc(raw, reinterpret_cast<void**>(&raw->derr), sizeof(int));
     CK(cudaMemsetAsync(raw->derr, 0, sizeof(int), raw->stream));
     CK(cudaStreamSynchronize(raw->stream));
   } catch (...) {
@@ -1025,8 +1053,9 @@ int mxm_dg_advance_host_async(void* handle, const void* q_host, void* q_out_host
     CK(cudaStreamCreateWithFlags(&h->d2h, cudaStreamNonBlocking));
     for (cudaEvent_t* e : {&h->e_in_free, &h->e_in, &h->e_res, &h->e_out_free})
       CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-    CK(cudaMalloc(&h->in_stage, h->qbytes()));
-    CK(cudaMalloc(&h->out_stage, h->qbytes()));
+    mxm::dev_alloc(h, &h->in_stage, h->qbytes());
+    mxm::dev_alloc(h, &h->out_stage, h->qbytes());
+    CK(cudaStreamSynchronize(h->stream));  // the copy streams use them next
     CK(cudaEventRecord(h->e_in_free, h->h2d));
     CK(cudaEventRecord(h->e_out_free, h->d2h));
   }
