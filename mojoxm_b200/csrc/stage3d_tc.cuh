@@ -91,15 +91,6 @@ struct TcShape {
   static constexpr size_t SMEM = OFF_C + CD_BYTES;
   static constexpr bool BULK = (6 * NP * NC * 4) % 16 == 0;
   static_assert(O_BYTES <= 2 * B_BYTES, "staging tile must fit the operand buffer");
-  // q_a of a tile lands in the lo half of the operand buffer (free once the
-  // face MMAs completed), in the leading columns k < 8 floor(3NP / 8): those
-  // are rewritten by the next tile's volume phase before any MMA reads them.
-  // The trailing K padding is never rewritten and must keep finite bf16
-  // values (it meets zero operator columns; a NaN pattern there would poison
-  // the accumulator), so the copy must not reach it; the staging tile sO
-  // stays in the hi half.
-  static constexpr size_t QA_OFF = B_BYTES;
-  static constexpr bool QA_SMEM = O_BYTES <= B_BYTES && Q_BYTES <= size_t(3 * NP / 8) * M * 16;
 };
 
 // Blocks per SM the register allocation must allow: what fits in shared
@@ -127,7 +118,6 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
   extern __shared__ __align__(1024) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);  // [0..1] q tiles, [2] mma, [3] A image
   uint32_t* tslot = reinterpret_cast<uint32_t*>(smem + 32);
-  uint64_t* bar_qa = reinterpret_cast<uint64_t*>(smem + 48);  // q_a tile copy
   KuhnTab3<float>* tab = reinterpret_cast<KuhnTab3<float>*>(smem + S::HDR);
   unsigned char* sAhi = smem + S::OFF_A;
   unsigned char* sAlo = sAhi + S::A_BYTES;
@@ -144,7 +134,6 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
   const int ngroups = (args.ncell - args.cbeg + EC - 1) / EC;
   if (tid == 0) {
     for (int k = 0; k < 4; ++k) mbar_init(&bar[k], 1);
-    mbar_init(bar_qa, 1);
     fence_mbar_init();
   }
   if (warp == 0) {
@@ -187,8 +176,8 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
   };
   // bit b: phase parity / copy in flight of tile buffer b (scalars, so they
   // stay in registers)
-  uint32_t par = 0u, pend = 0u, mma_parity = 0u, qa_par = 0u;
-  bool mma_pending = false, qa_pending = false;
+  uint32_t par = 0u, pend = 0u, mma_parity = 0u;
+  bool mma_pending = false;
   // One half of K: make the operand writes visible to the tensor-core
   // (async) proxy, let one thread issue nks K-steps (hi*hi + hi*lo + lo*hi)
   // against operator K-steps [ka0, ka0 + nks) (mma_issue), and wait
@@ -478,16 +467,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
     // ... and q_a of this thread's first epilogue node (global memory when
     // q_a is not the tile's own state)
     const bool a_in = args.q_a == args.q_in, b_in = args.q_b == args.q_in;
-    // q_a (when it is not the tile's own state) comes by bulk copy into the
-    // operand buffer once the face MMAs are done, else by plain loads
-    const float* qa_src = args.q_a + size_t(cell0) * 6 * NP * NC;
-    const uint32_t qa_bytes = uint32_t(ne_here) * NP * NC * 4u;
-    const bool qa_bulk = S::QA_SMEM && !args.rhs_only && !a_in && reinterpret_cast<uintptr_t>(qa_src) % 16 == 0 &&
-                         qa_bytes % 16 == 0;
-    const float* sQa = reinterpret_cast<const float*>(sBhi + S::QA_OFF);
-    // (register prefetch of the first node's q_a only for shapes without the
-    // shared-memory copy: it would cost registers the copy makes unneeded)
-    const bool pre_a = !S::QA_SMEM && !args.rhs_only && !a_in && tid < ne_here * NP;
+    const bool pre_a = !args.rhs_only && !a_in && tid < ne_here * NP;
     float pa[NC];
     if (pre_a) {
       const size_t base = (size_t(cell0) * 6 * NP + tid) * NC;
@@ -497,14 +477,6 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
     if (!mma_wait()) {
       failed = true;
       break;
-    }
-    if (qa_bulk) {
-      if (tid == 0) {
-        fence_proxy_async();
-        mbar_arrive_expect_tx(bar_qa, qa_bytes);
-        bulk_g2s(const_cast<float*>(sQa), qa_src, qa_bytes, bar_qa);
-      }
-      qa_pending = true;
     }
     {  // warp w reads TMEM lanes [32 (w % 4), +32) (rows (c, el)), columns
        // [16 (w / 4), +16) of every 32 (16 at a time: bounded registers)
@@ -521,14 +493,6 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
     }
     tc_fence_before();
     __syncthreads();
-    if (qa_bulk) {
-      if (!block_wait_bounded(bar_qa, qa_par, kWaitLimitNs)) {
-        failed = true;
-        break;
-      }
-      qa_par ^= 1u;
-      qa_pending = false;
-    }
     // ---- epilogue per node: source, RK combine, floor, store
     for (int idx = tid; idx < ne_here * NP; idx += NT) {
       const int el = idx / NP, i = idx - el * NP;
@@ -543,7 +507,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
         if (args.rhs_only) {
           out[c] = rhs;
         } else {
-          const float va = a_in ? ql[c] : (qa_bulk ? sQa[idx * NC + c] : (pre_a && idx == tid ? pa[c] : args.q_a[base + c]));
+          const float va = a_in ? ql[c] : (pre_a && idx == tid ? pa[c] : args.q_a[base + c]);
           const float vb = b_in ? ql[c] : args.q_b[base + c];
           out[c] = va + args.b * (vb - va) + args.cdt * rhs;
         }
@@ -561,7 +525,6 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
       for (int b = 0; b < 2; ++b)
         if ((pend >> b) & 1u) mbar_wait_bounded(&bar[b], (par >> b) & 1u, kWaitLimitNs);
       if (mma_pending) mbar_wait_bounded(&bar[2], mma_parity, kWaitLimitNs);
-      if (qa_pending) mbar_wait_bounded(bar_qa, qa_par, kWaitLimitNs);
     }
   }
   tc_fence_before();
