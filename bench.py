@@ -17,7 +17,9 @@ algorithm; the Mojo reference itself cannot be built on this image) on the
 host cores with all threads, on a bounded sample of the same workload.
 Multi-GPU (torchrun): every rank advances its own replica of the workload
 (independent solves, no collective on the data path); `value` is the sum of
-all ranks' DOF over the max-over-ranks device time.  Side legs in the same
+all ranks' DOF over the max-over-ranks device time.  `--decomp slab` instead
+splits one n x n x (n N) mesh into N z-slabs, one per GPU, whose ghost
+layers move over NCCL every stage (weak scaling).  Side legs in the same
 line: the batched 2D engine, the Maxwell cavity, the 3D MHD Alfven wave, the
 served stream, and (`slab`) the headline mesh split into z-slabs on one GPU
 with its halo exchange.
@@ -64,6 +66,9 @@ def parse():
     ap.add_argument("--cavity", type=int, default=1, help="run the 24^3x6 P=4 Maxwell cavity leg (1/0)")
     ap.add_argument("--mhd", type=int, default=1, help="run the 3D ideal-MHD Alfven-wave leg (1/0)")
     ap.add_argument("--slab-parts", type=int, default=4, help="z-slab decomposition leg on one GPU (0 = skip)")
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
+                    help="under torchrun: independent replicas (default), or one n x n x (n*N) mesh split into "
+                         "z-slabs, one per GPU, ghost layers over NCCL (weak scaling)")
     return ap.parse_args()
 
 
@@ -617,11 +622,30 @@ def main():
 
     M.set_device(local)
     phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_RUSANOV, False)
-    s = M.Solver(M.Mesh(a.n, a.n, a.n, 1.0, 1.0, 1.0), phys, P=a.P, precision=a.precision)
-    q0 = smooth_wave_state(s.node_xyz())
-    s.upload_state(q0)
+    slab = a.decomp == "slab" and world > 1
+
+    def make(prec):
+        """This rank's solve: a replica of the n^3 mesh, or its z-slab of the
+        n x n x (n*world) mesh with the ghost layers connected over NCCL."""
+        if not slab:
+            return M.Solver(M.Mesh(a.n, a.n, a.n, 1.0, 1.0, 1.0), phys, P=a.P, precision=prec)
+        h = M.Solver(M.Mesh(a.n, a.n, a.n * world, 1.0, 1.0, float(world)), phys, P=a.P, precision=prec,
+                     nparts=world, part=rank)
+        uid = [M.nccl_unique_id() if rank == 0 else None]
+        dist.broadcast_object_list(uid, src=0)
+        h.connect_nccl(uid[0])
+        return h
+
+    s = make(a.precision)
+    q0_local = smooth_wave_state(s.node_xyz())  # global positions: the wave is periodic in z with period 1
+    s.upload_state(q0_local)
+    q0 = q0_local  # the n^3 state of the accuracy check
+    if slab:
+        tmp = M.Solver(M.Mesh(a.n, a.n, a.n, 1.0, 1.0, 1.0), phys, P=a.P, precision="f64")
+        q0 = smooth_wave_state(tmp.node_xyz())
+        tmp.close()
     dt = dt_for(a.n, a.P)
-    dof = s.dof_count()
+    dof = s.owned_ne * s.NP * s.NC  # owned DOF (all of them for a replica)
 
     def barrier():
         s.synchronize()
@@ -640,7 +664,7 @@ def main():
     # end to end through the host-buffer entry (pinned in/out, copies timed)
     pin_in = M.PinnedArray(s.shape, s.dtype)
     pin_out = M.PinnedArray(s.shape, s.dtype)
-    pin_in.array[:] = s.download_state(0)
+    pin_in.array[:] = s.download_state(0)  # the rank's whole state buffer (ghost layers included)
     e2e_steps = max(2, min(a.steps, 30))
     s.advance_host_async(pin_in.array, 1, dt, pin_out.array)  # warm (allocates the pipeline)
     s.synchronize()
@@ -660,8 +684,8 @@ def main():
     # the plain FP64 kernels on the same workload (the ratio's denominator)
     plain = None
     if a.precision != "f64":
-        s64 = M.Solver(M.Mesh(a.n, a.n, a.n, 1.0, 1.0, 1.0), phys, P=a.P, precision="f64")
-        s64.upload_state(q0)
+        s64 = make("f64")
+        s64.upload_state(q0_local)
         s64.step_n(dt, max(3, a.warmup))
         barrier()
         ms64 = s64.time_steps(dt, a.steps)
@@ -709,9 +733,12 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": DTYPE[a.precision], "data": "synthetic",
-            "config": {"workload": workload_name(a), "elements": s.num_elements, "NP": s.NP, "NC": s.NC,
+            "config": {"workload": workload_name(a) + (f"; one {a.n}x{a.n}x{a.n * world} mesh in {world} z-slabs"
+                                                      if slab else ""),
+                       "elements": s.owned_ne, "NP": s.NP, "NC": s.NC,
                        "accuracy": acc,
-                       "dof_per_stage": dof, "dt": dt, "parallelism": f"replicas x{world}",
+                       "dof_per_stage": dof, "dt": dt,
+                       "parallelism": f"z-slabs x{world}, ghost layers over NCCL" if slab else f"replicas x{world}",
                        "l2": "inputs larger than L2: 3 state buffers of "
                              f"{qbytes / 1e6:.0f} MB each (L2 126 MB), no flush"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
