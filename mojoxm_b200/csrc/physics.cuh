@@ -327,9 +327,9 @@ struct EulerD {
       q[4] = R(pm / g1);
       return;
     }
-    const double ke = 0.5 * m2 * (1.0 / rho);
-    const double p = g1 * (double(q[4]) - ke);
-    if (!(p > pm)) q[4] = R(ke + pm / g1);
+    // p > pm  <=>  g1 (E rho - m2 / 2) > pm rho  (rho > 0): the test needs no
+    // FP64 division; the floored energy is formed as before
+    if (!(g1 * (double(q[4]) * rho - 0.5 * m2) > pm * rho)) q[4] = R(0.5 * m2 * (1.0 / rho) + pm / g1);
   }
 };
 
