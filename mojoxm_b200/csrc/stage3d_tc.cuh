@@ -71,9 +71,13 @@ struct TcShape {
   static constexpr size_t FB_BYTES = size_t(EB) * 3 * NC * 4;
   static constexpr size_t FN_BYTES = size_t(EB) * 4 * NC * 4;  // Fbar . n per (element, face)
   static constexpr size_t CD_BYTES = size_t(EC) * 12 * 4;  // per cube: 6 neighbour cubes + 6 face modes
+  // per face-work entry: normal, scale, the inner neighbour's scale, packed
+  // indices; per (entry, face node): own / neighbour node, neighbour's slot
+  static constexpr size_t FR_BYTES = 24 * 8 * 4, FM_BYTES = size_t(24) * NFP * 4;
   static constexpr size_t HDR = 128;
   static constexpr size_t TAB = (sizeof(KuhnTab3<float>) + 127) / 128 * 128;
-  static constexpr size_t FIXED = HDR + TAB + 2 * A_BYTES + 2 * B_BYTES + FB_BYTES + FN_BYTES + CD_BYTES;
+  static constexpr size_t FIXED = HDR + TAB + 2 * A_BYTES + 2 * B_BYTES + FB_BYTES + FN_BYTES + CD_BYTES + 16 +
+                                  FR_BYTES + FM_BYTES;
   // State tile buffers: two (prefetch the next tile during this one) unless
   // a single buffer lets more blocks share an SM (228 KB of shared memory
   // per SM, 1 KB reserved per block on sm_100a; at most 4 blocks of 256
@@ -88,7 +92,9 @@ struct TcShape {
   static constexpr size_t OFF_F = OFF_Q + QB * Q_BYTES;
   static constexpr size_t OFF_N = OFF_F + FB_BYTES;
   static constexpr size_t OFF_C = OFF_N + FN_BYTES;
-  static constexpr size_t SMEM = OFF_C + CD_BYTES;
+  static constexpr size_t OFF_R = (OFF_C + CD_BYTES + 15) / 16 * 16;
+  static constexpr size_t OFF_M = OFF_R + FR_BYTES;
+  static constexpr size_t SMEM = OFF_M + FM_BYTES;
   static constexpr bool BULK = (6 * NP * NC * 4) % 16 == 0;
   static_assert(O_BYTES <= 2 * B_BYTES, "staging tile must fit the operand buffer");
 };
@@ -129,6 +135,8 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
   float* sFn = reinterpret_cast<float*>(smem + S::OFF_N);  // [EB][4][NC] Fbar . n of each face
   int* sNb = reinterpret_cast<int*>(smem + S::OFF_C);      // [EC][6] neighbour cube per direction
   int* sMd = sNb + EC * 6;                                 // [EC][6] face mode | code << 8
+  float* sFR = reinterpret_cast<float*>(smem + S::OFF_R);  // [work][8] face records
+  int* sFM = reinterpret_cast<int*>(smem + S::OFF_M);      // [work][NFP] face-node indices
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ngroups = (args.ncell - args.cbeg + EC - 1) / EC;
@@ -144,6 +152,25 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
     const int* src = reinterpret_cast<const int*>(&tabp);
     int* dst = reinterpret_cast<int*>(tab);
     for (int k = tid; k < int(sizeof(KuhnTab3<float>) / 4); k += NT) dst[k] = src[k];
+  }
+  // face records, decoded once per block from the topology table: bits
+  // t | lf << 3 | nb_t << 5 | nb_lf << 8 | (axis + 1) << 10 | (dir > 0) << 12 | (side == 0) << 13
+  for (int w = tid; w < tabp.n_face_work; w += NT) {
+    const int tl = tabp.face_work[w], t = tl >> 2, lf = tl & 3;
+    const int ax = tabp.axis[t][lf], nbt = tabp.nb_t[t][lf], lf2 = tabp.nb_lf[t][lf];
+    float* r = sFR + w * 8;
+    r[0] = tabp.normal[t][lf][0];
+    r[1] = tabp.normal[t][lf][1];
+    r[2] = tabp.normal[t][lf][2];
+    r[3] = tabp.fscale[t][lf];
+    r[4] = ax < 0 ? tabp.fscale[nbt][lf2] : 0.f;
+    r[5] = __int_as_float(t | (lf << 3) | ((nbt & 7) << 5) | ((lf2 & 3) << 8) | ((ax + 1) << 10) |
+                          ((tabp.dir[t][lf] > 0 ? 1 : 0) << 12) | ((tabp.side[t][lf] == 0 ? 1 : 0) << 13));
+  }
+  for (int idx = tid; idx < tabp.n_face_work * NFP; idx += NT) {
+    const int w = idx / NFP, m = idx - w * NFP;
+    const int tl = tabp.face_work[w], t = tl >> 2, lf = tl & 3;
+    sFM[idx] = int(tabp.own_node[lf][m]) | (int(tabp.nb_node[t][lf][m]) << 8) | (int(tabp.nb_m[t][lf][m]) << 16);
   }
   // zero the flux tiles once: padding rows / k columns stay zero for good
   for (int k = tid; k < int(2 * S::B_BYTES / 16); k += NT) reinterpret_cast<uint4*>(sBhi)[k] = make_uint4(0, 0, 0, 0);
@@ -359,24 +386,26 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
     auto face_item = [&](int idx, int& e1, int& k1, float* v1, int& e2, int& k2, float* v2) -> int {
       const int cl = idx % EC, rest = idx / EC, m = rest % NFP, wk = rest / NFP;
       if (cl >= nc_here) return 0;
-      const int tl = tab->face_work[wk], t = tl >> 2, lf = tl & 3;
-      const int el = cl * 6 + t, ax = tab->axis[t][lf];
-      const bool own_left = tab->side[t][lf] == 0;
-      const int nbt = tab->nb_t[t][lf];
+      const float4 fr = *reinterpret_cast<const float4*>(sFR + wk * 8);
+      const float2 fr2 = *reinterpret_cast<const float2*>(sFR + wk * 8 + 4);
+      const int bits = __float_as_int(fr2.y), nm = sFM[wk * NFP + m];
+      const int t = bits & 7, lf = (bits >> 3) & 3, nbt = (bits >> 5) & 7, ax = ((bits >> 10) & 3) - 1;
+      const int el = cl * 6 + t;
+      const bool own_left = (bits >> 13) & 1;
       int mode = FACE_INTERIOR, code = 0, nbcube = 0;
       if (ax >= 0) {
-        const int dd = 2 * ax + (tab->dir[t][lf] > 0 ? 1 : 0);
+        const int dd = 2 * ax + ((bits >> 12) & 1);
         const int md = sMd[cl * 6 + dd];
         mode = md & 0xff;
         code = md >> 8;
         nbcube = sNb[cl * 6 + dd];
       }
-      const float* qo = &q[(el * NP + tab->own_node[lf][m]) * NC];
-      float nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1], nz = tab->normal[t][lf][2];
-      float scale = tab->fscale[t][lf];
+      const float* qo = &q[(el * NP + (nm & 255)) * NC];
+      float nx = fr.x, ny = fr.y, nz = fr.z;
+      float scale = fr.w;
       float qn[NC], qg[NC];
       if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
-        const int nbn = tab->nb_node[t][lf][m];
+        const int nbn = (nm >> 8) & 255;
         if (ax < 0) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) qn[c] = q[((cl * 6 + nbt) * NP + nbn) * NC + c];
@@ -417,13 +446,13 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
       k1 = lf * NFP + m;
       if (ax >= 0) return 1;
       // the other tet of this inner face: same flux and normal, its own scale and Fbar
-      const int el2 = cl * 6 + nbt, lf2 = tab->nb_lf[t][lf];
-      const float s2 = tab->fscale[nbt][lf2];
+      const int el2 = cl * 6 + nbt, lf2 = (bits >> 8) & 3;
+      const float s2 = fr2.x;
       const float* Fn2 = &sFn[(el2 * 4 + lf2) * NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) v2[c] = s2 * (f[c] - Fn2[c]);
       e2 = el2;
-      k2 = lf2 * NFP + tab->nb_m[t][lf][m];
+      k2 = lf2 * NFP + (nm >> 16);
       return 2;
     };
     const int nface_items = EC * nwork * NFP;
