@@ -76,8 +76,8 @@ struct TcShape {
   static constexpr size_t FR_BYTES = 24 * 8 * 4, FM_BYTES = size_t(24) * NFP * 4;
   static constexpr size_t HDR = 128;
   static constexpr size_t TAB = (sizeof(KuhnTab3<float>) + 127) / 128 * 128;
-  static constexpr size_t FIXED = HDR + TAB + 2 * A_BYTES + 2 * B_BYTES + FB_BYTES + FN_BYTES + CD_BYTES + 16 +
-                                  FR_BYTES + FM_BYTES;
+  static constexpr size_t FIXED0 = HDR + TAB + 2 * A_BYTES + 2 * B_BYTES + FB_BYTES + FN_BYTES + CD_BYTES;
+  static constexpr size_t FIXED1 = FIXED0 + 16 + FR_BYTES + FM_BYTES;
   // State tile buffers: two (prefetch the next tile during this one) unless
   // a single buffer lets more blocks share an SM (228 KB of shared memory
   // per SM, 1 KB reserved per block on sm_100a; at most 4 blocks of 256
@@ -85,7 +85,15 @@ struct TcShape {
   static constexpr size_t blocks_for(size_t s) {
     return size_t(228 * 1024) / (s + 1024) < 4 ? size_t(228 * 1024) / (s + 1024) : 4;
   }
-  static constexpr int QB = blocks_for(FIXED + Q_BYTES) > blocks_for(FIXED + 2 * Q_BYTES) ? 1 : 2;
+  static constexpr int qb_for(size_t fixed) {
+    return blocks_for(fixed + Q_BYTES) > blocks_for(fixed + 2 * Q_BYTES) ? 1 : 2;
+  }
+  // the face records only where they cost neither a block per SM nor the
+  // second state buffer
+  static constexpr bool FREC = qb_for(FIXED1) >= qb_for(FIXED0) &&
+                               blocks_for(FIXED1 + qb_for(FIXED1) * Q_BYTES) >= blocks_for(FIXED0 + qb_for(FIXED0) * Q_BYTES);
+  static constexpr size_t FIXED = FREC ? FIXED1 : FIXED0;
+  static constexpr int QB = qb_for(FIXED);
   static constexpr size_t OFF_A = HDR + TAB;
   static constexpr size_t OFF_B = OFF_A + 2 * A_BYTES;
   static constexpr size_t OFF_Q = OFF_B + 2 * B_BYTES;
@@ -94,7 +102,7 @@ struct TcShape {
   static constexpr size_t OFF_C = OFF_N + FN_BYTES;
   static constexpr size_t OFF_R = (OFF_C + CD_BYTES + 15) / 16 * 16;
   static constexpr size_t OFF_M = OFF_R + FR_BYTES;
-  static constexpr size_t SMEM = OFF_M + FM_BYTES;
+  static constexpr size_t SMEM = FREC ? OFF_M + FM_BYTES : OFF_C + CD_BYTES;
   static constexpr bool BULK = (6 * NP * NC * 4) % 16 == 0;
   static_assert(O_BYTES <= 2 * B_BYTES, "staging tile must fit the operand buffer");
 };
@@ -155,6 +163,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
   }
   // face records, decoded once per block from the topology table: bits
   // t | lf << 3 | nb_t << 5 | nb_lf << 8 | (axis + 1) << 10 | (dir > 0) << 12 | (side == 0) << 13
+  if constexpr (S::FREC) {
   for (int w = tid; w < tabp.n_face_work; w += NT) {
     const int tl = tabp.face_work[w], t = tl >> 2, lf = tl & 3;
     const int ax = tabp.axis[t][lf], nbt = tabp.nb_t[t][lf], lf2 = tabp.nb_lf[t][lf];
@@ -171,6 +180,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
     const int w = idx / NFP, m = idx - w * NFP;
     const int tl = tabp.face_work[w], t = tl >> 2, lf = tl & 3;
     sFM[idx] = int(tabp.own_node[lf][m]) | (int(tabp.nb_node[t][lf][m]) << 8) | (int(tabp.nb_m[t][lf][m]) << 16);
+  }
   }
   // zero the flux tiles once: padding rows / k columns stay zero for good
   for (int k = tid; k < int(2 * S::B_BYTES / 16); k += NT) reinterpret_cast<uint4*>(sBhi)[k] = make_uint4(0, 0, 0, 0);
@@ -386,26 +396,41 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
     auto face_item = [&](int idx, int& e1, int& k1, float* v1, int& e2, int& k2, float* v2) -> int {
       const int cl = idx % EC, rest = idx / EC, m = rest % NFP, wk = rest / NFP;
       if (cl >= nc_here) return 0;
-      const float4 fr = *reinterpret_cast<const float4*>(sFR + wk * 8);
-      const float2 fr2 = *reinterpret_cast<const float2*>(sFR + wk * 8 + 4);
-      const int bits = __float_as_int(fr2.y), nm = sFM[wk * NFP + m];
-      const int t = bits & 7, lf = (bits >> 3) & 3, nbt = (bits >> 5) & 7, ax = ((bits >> 10) & 3) - 1;
+      int t, lf, nbt, ax, own_n, bits = 0, nm = 0;
+      bool own_left;
+      float nx, ny, nz, scale, s2r = 0.f;
+      if constexpr (S::FREC) {
+        const float4 fr = *reinterpret_cast<const float4*>(sFR + wk * 8);
+        const float2 fr2 = *reinterpret_cast<const float2*>(sFR + wk * 8 + 4);
+        bits = __float_as_int(fr2.y);
+        nm = sFM[wk * NFP + m];
+        t = bits & 7, lf = (bits >> 3) & 3, nbt = (bits >> 5) & 7, ax = ((bits >> 10) & 3) - 1;
+        own_left = (bits >> 13) & 1;
+        own_n = nm & 255;
+        nx = fr.x, ny = fr.y, nz = fr.z, scale = fr.w, s2r = fr2.x;
+      } else {
+        const int tl = tab->face_work[wk];
+        t = tl >> 2, lf = tl & 3;
+        ax = tab->axis[t][lf];
+        own_left = tab->side[t][lf] == 0;
+        nbt = tab->nb_t[t][lf];
+        own_n = tab->own_node[lf][m];
+        nx = tab->normal[t][lf][0], ny = tab->normal[t][lf][1], nz = tab->normal[t][lf][2];
+        scale = tab->fscale[t][lf];
+      }
       const int el = cl * 6 + t;
-      const bool own_left = (bits >> 13) & 1;
       int mode = FACE_INTERIOR, code = 0, nbcube = 0;
       if (ax >= 0) {
-        const int dd = 2 * ax + ((bits >> 12) & 1);
+        const int dd = 2 * ax + (S::FREC ? ((bits >> 12) & 1) : (tab->dir[t][lf] > 0 ? 1 : 0));
         const int md = sMd[cl * 6 + dd];
         mode = md & 0xff;
         code = md >> 8;
         nbcube = sNb[cl * 6 + dd];
       }
-      const float* qo = &q[(el * NP + (nm & 255)) * NC];
-      float nx = fr.x, ny = fr.y, nz = fr.z;
-      float scale = fr.w;
+      const float* qo = &q[(el * NP + own_n) * NC];
       float qn[NC], qg[NC];
       if (mode == FACE_INTERIOR || mode == FACE_MIXED) {
-        const int nbn = (nm >> 8) & 255;
+        const int nbn = S::FREC ? (nm >> 8) & 255 : int(tab->nb_node[t][lf][m]);
         if (ax < 0) {
 #pragma unroll
           for (int c = 0; c < NC; ++c) qn[c] = q[((cl * 6 + nbt) * NP + nbn) * NC + c];
@@ -446,13 +471,13 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
       k1 = lf * NFP + m;
       if (ax >= 0) return 1;
       // the other tet of this inner face: same flux and normal, its own scale and Fbar
-      const int el2 = cl * 6 + nbt, lf2 = (bits >> 8) & 3;
-      const float s2 = fr2.x;
+      const int el2 = cl * 6 + nbt, lf2 = S::FREC ? (bits >> 8) & 3 : int(tab->nb_lf[t][lf]);
+      const float s2 = S::FREC ? s2r : tab->fscale[nbt][lf2];
       const float* Fn2 = &sFn[(el2 * 4 + lf2) * NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) v2[c] = s2 * (f[c] - Fn2[c]);
       e2 = el2;
-      k2 = lf2 * NFP + (nm >> 16);
+      k2 = lf2 * NFP + (S::FREC ? (nm >> 16) : int(tab->nb_m[t][lf][m]));
       return 2;
     };
     const int nface_items = EC * nwork * NFP;
