@@ -315,6 +315,8 @@ int mxm_dg_slab_connect_nccl(void* handle, const unsigned char* id128);
 int mxm_dg_group_create(void* const* handles, int n, void** group);
 int mxm_dg_group_step_n(void* group, double dt, int nsteps);
 int mxm_dg_group_synchronize(void* group);
+/* `nsteps` group steps timed with CUDA events that bracket every part's work. */
+int mxm_dg_group_time_steps(void* group, double dt, int nsteps, double* ms);
 int mxm_dg_group_last_error(void* group, char* buf, int len);
 int mxm_dg_group_destroy(void* group);
 

@@ -37,7 +37,7 @@ PREC = {"f64": 0, "f32": 1, "mixed": 2}
 EXPORTED = [
     "mxm_dg_slab_plan", "mxm_dg_create_slab", "mxm_dg_slab_info", "mxm_dg_slab_layout", "mxm_dg_slab_stage",
     "mxm_dg_nccl_unique_id", "mxm_dg_slab_connect_nccl", "mxm_dg_group_create", "mxm_dg_group_step_n",
-    "mxm_dg_group_synchronize", "mxm_dg_group_last_error", "mxm_dg_group_destroy",
+    "mxm_dg_group_synchronize", "mxm_dg_group_last_error", "mxm_dg_group_destroy", "mxm_dg_group_time_steps",
     "mxm_dg_version", "mxm_dg_node_xyz_f32", "mxm_dg_advance_host_async", "mxm_dg_create", "mxm_dg_destroy", "mxm_dg_sizes", "mxm_dg_dof_count",
     "mxm_dg_state_bytes_per_step", "mxm_dg_state_ptr", "mxm_dg_node_xyz_ptr", "mxm_dg_node_xyz",
     "mxm_dg_upload_state", "mxm_dg_download_state", "mxm_dg_download_component", "mxm_dg_download_component_f64",
@@ -153,6 +153,7 @@ def lib():
         L.mxm_dg_group_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
         L.mxm_dg_group_step_n.argtypes = [vp, ctypes.c_double, ctypes.c_int]
         L.mxm_dg_group_synchronize.argtypes = [vp]
+        L.mxm_dg_group_time_steps.argtypes = [vp, ctypes.c_double, ctypes.c_int, dp]
         L.mxm_dg_group_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
         L.mxm_dg_group_destroy.argtypes = [vp]
         _lib = L
@@ -595,6 +596,12 @@ class SlabGroup:
 
     def synchronize(self):
         self._c(lib().mxm_dg_group_synchronize(self.g))
+
+    def time_steps(self, dt, nsteps):
+        """Device time (ms) of `nsteps` group steps (CUDA events)."""
+        v = ctypes.c_double()
+        self._c(lib().mxm_dg_group_time_steps(self.g, dt, nsteps, ctypes.byref(v)))
+        return v.value
 
     def close(self):
         if getattr(self, "g", None):

@@ -408,6 +408,55 @@ int mxm_dg_group_step_n(void* group, double dt, int nsteps) {
   }
 }
 
+// Device time of `nsteps` group steps: every part's stream starts after an
+// event on part 0's stream and part 0's stream waits for every part at the
+// end, so the two timing events bracket all parts' work.
+int mxm_dg_group_time_steps(void* group, double dt, int nsteps, double* ms) {
+  Group* g = (Group*)group;
+  if (!g || !ms || nsteps < 0) return MXM_DG_EINVAL;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  try {
+    Handle* h0 = g->parts[0];
+    CK(cudaSetDevice(h0->device));
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    g->barrier();  // part 0's stream waits for its neighbours' work so far
+    for (size_t r = 1; r < g->parts.size(); ++r) {
+      CK(cudaSetDevice(g->parts[r]->device));
+      CK(cudaEventRecord(g->ev[r], g->parts[r]->stream));
+      CK(cudaSetDevice(h0->device));
+      CK(cudaStreamWaitEvent(h0->stream, g->ev[r], 0));
+    }
+    CK(cudaSetDevice(h0->device));
+    CK(cudaEventRecord(t0, h0->stream));
+    for (size_t r = 1; r < g->parts.size(); ++r) {
+      CK(cudaSetDevice(g->parts[r]->device));
+      CK(cudaStreamWaitEvent(g->parts[r]->stream, t0, 0));
+    }
+    g->step_n(dt, nsteps);
+    for (size_t r = 1; r < g->parts.size(); ++r) {
+      CK(cudaSetDevice(g->parts[r]->device));
+      CK(cudaEventRecord(g->ev[r], g->parts[r]->stream));
+      CK(cudaSetDevice(h0->device));
+      CK(cudaStreamWaitEvent(h0->stream, g->ev[r], 0));
+    }
+    CK(cudaSetDevice(h0->device));
+    CK(cudaEventRecord(t1, h0->stream));
+    CK(cudaEventSynchronize(t1));
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, t0, t1));
+    *ms = f;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return MXM_DG_OK;
+  } catch (std::exception& ex) {
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    g->err = ex.what();
+    return MXM_DG_ECUDA;
+  }
+}
+
 int mxm_dg_group_synchronize(void* group) {
   Group* g = (Group*)group;
   if (!g) return MXM_DG_EINVAL;
