@@ -14,7 +14,10 @@ kernels over the whole mesh; the metric counts Ne*NP*NC DOF per stage
 
 --impl reference times the CPU oracle (the C++ restatement of the reference
 algorithm; the Mojo reference itself cannot be built on this image) on the
-host cores with all threads, on a bounded sample of the same workload.
+host cores with all threads, on the same workload (same mesh, order, flux,
+initial state and dt; FP32 like the reference's own runs): W warm-up and K
+timed SSPRK3 steps.  The `cpu_baseline` object of the product's line is the
+same oracle run on the same workload for a few seconds.
 Multi-GPU (torchrun): every rank advances its own replica of the workload
 (independent solves, no collective on the data path); `value` is the sum of
 all ranks' DOF over the max-over-ranks device time.  `--decomp slab` instead
@@ -43,6 +46,56 @@ sys.path.insert(0, ROOT)
 GAMMA = 1.4
 METRIC = "DOF·stage/s at fixed L2 err vs plain FP64 on B200"
 UNIT = "DOF·stage/s"
+
+
+# ---- replica bookkeeping (one process per GPU under torchrun) --------------
+# The DG hot path exchanges no data between GPUs in replica mode: every rank
+# advances its own solve.  What crosses ranks is bookkeeping only -- each
+# rank's device time (the job time is the maximum over ranks) and its unit
+# counts (summed) -- over the gloo process group the bench opens; without a
+# process group the helpers act on the local values.
+
+def _dist():
+    try:
+        import torch.distributed as dist
+
+        if dist.is_available() and dist.is_initialized():
+            return dist
+    except ImportError:
+        pass
+    return None
+
+
+def rank_world():
+    d = _dist()
+    return (d.get_rank(), d.get_world_size()) if d else (0, 1)
+
+
+def shard(items, rank=None, world=None):
+    """Items of this rank: every world-th item starting at rank (round robin,
+    so ranks get work of similar size when items come from one distribution)."""
+    if rank is None or world is None:
+        rank, world = rank_world()
+    return [it for k, it in enumerate(items) if k % world == rank]
+
+
+def _reduce(value, op):
+    d = _dist()
+    if d is None:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64)
+    d.all_reduce(t, op=op(d))
+    return float(t.item())
+
+
+def max_over_ranks(value):
+    return _reduce(value, lambda d: d.ReduceOp.MAX)
+
+
+def sum_over_ranks(value):
+    return _reduce(value, lambda d: d.ReduceOp.SUM)
 
 
 def parse():
@@ -291,39 +344,78 @@ def traffic_per_launch(a):
         return None
 
 
-def cpu_baseline(a, seconds):
-    """Oracle (C++ restatement, OpenMP) on a bounded sample of the workload."""
+def cpu_model():
+    """The host CPU's model name (first entry of /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
+
+
+def omp_threads():
+    """Threads the oracle's OpenMP loops use: OMP_NUM_THREADS if set, else
+    the CPUs this process may run on."""
+    env = os.environ.get("OMP_NUM_THREADS", "")
+    if env.isdigit() and int(env) > 0:
+        return int(env)
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(a, seconds, steps=None, warmup=1):
+    """The oracle (C++ restatement of the reference's algorithm, OpenMP over
+    elements) on the benchmark's own workload: the same n^3 x 6 mesh, order,
+    flux and initial state, in the reference's arithmetic (Float32, or FP64
+    for --precision f64).  `steps` SSPRK3 steps are timed after `warmup`;
+    without `steps` the count is chosen from one warm step so the timed
+    part lasts about `seconds` (at least 3 steps, at most --steps)."""
     import oracle
 
     oracle.build()
-    n = 8
+    n = a.n
     o = oracle.Oracle3D(a.P, n, 1.0, dict(kind=1, flux=0, entropy_fix=0, p=[GAMMA, 1e-6, 1e-6, 0, 0, 0, 0, 0, 0, 0, 0]),
                         real="f64" if a.precision == "f64" else "f32")
     o.set(smooth_wave_state(o.node_xyz()))
     dt = dt_for(n, a.P)
-    o.step(dt, 1)
-    steps, t0 = 0, time.perf_counter()
-    while True:
-        o.step(dt, 1)
-        steps += 1
-        el = time.perf_counter() - t0
-        if el >= seconds or steps >= 200:
-            break
+    t0 = time.perf_counter()
+    o.step(dt, max(1, warmup))
+    t_warm = (time.perf_counter() - t0) / max(1, warmup)
+    if steps is None:
+        steps = int(max(3, min(a.steps, round(seconds / max(t_warm, 1e-9)))))
+    t0 = time.perf_counter()
+    o.step(dt, steps)
+    el = time.perf_counter() - t0
     dof = o.Ne * o.NP * o.NC
-    return dict(value=3 * dof * steps / el, unit=UNIT, cores=os.cpu_count(), kind="port",
-                sample=f"oracle {'FP64' if a.precision == 'f64' else 'FP32'} restatement, {n}^3x6 = {6 * n ** 3} tets "
-                       f"P={a.P} Rusanov, {steps} SSPRK3 steps "
-                       f"in {el:.1f} s, OpenMP {os.cpu_count()} threads")
+    thr = omp_threads()
+    return dict(value=3 * dof * steps / el, unit=UNIT, cores=thr, kind="port", cpu_model=cpu_model(),
+                ms_per_step=el * 1e3 / steps, steps=steps, warmup=max(1, warmup), same_workload=True,
+                sample=f"oracle {'FP64' if a.precision == 'f64' else 'FP32'} restatement on the full workload: "
+                       f"{n}^3x6 = {6 * n ** 3} tets P={a.P} Rusanov, same initial state and dt, "
+                       f"{steps} timed SSPRK3 steps after {max(1, warmup)} in {el:.1f} s, OpenMP {thr} threads "
+                       f"on {cpu_model()}")
 
 
 def run_reference(a, rank, world):
+    """The reference arm: the oracle on the host cores, on the benchmark's own
+    workload (same mesh, order, flux, state, dt), W warm-up and K timed
+    SSPRK3 steps.  Rank 0 alone runs it; other ranks exit without work."""
     if rank != 0:
         return
-    cb = cpu_baseline(a, a.cpu_seconds)
+    cb = cpu_baseline(a, a.cpu_seconds, steps=a.steps, warmup=max(1, a.warmup))
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": a.gpus,
-            "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if a.precision == "f64" else "f32", "data": "synthetic",
-            "config": {"workload": workload_name(a), "sample": cb["sample"]},
+            "config": {"workload": workload_name(a).split(", FP")[0] + (", FP64" if a.precision == "f64" else ", FP32"),
+                       "elements": 6 * a.n ** 3, "sample": cb["sample"]},
             "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -611,7 +703,6 @@ def main():
         return
 
     import mojoxm_b200 as M
-    from mojoxm_b200 import replicas
 
     M.set_device(local)
     phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_RUSANOV, False)
@@ -651,8 +742,8 @@ def main():
     with clock_sampler(local) as clk:
         ms = s.time_steps(dt, a.steps)  # CUDA events on the solver's stream
     barrier()
-    ms_max = replicas.max_over_ranks(ms)  # job time = slowest replica
-    value = replicas.sum_over_ranks(3 * dof * a.steps) / (ms_max * 1e-3)
+    ms_max = max_over_ranks(ms)  # job time = slowest replica
+    value = sum_over_ranks(3 * dof * a.steps) / (ms_max * 1e-3)
 
     # end to end through the host-buffer entry (pinned in/out, copies timed)
     pin_in = M.PinnedArray(s.shape, s.dtype)
@@ -668,8 +759,8 @@ def main():
     s.synchronize()
     el = time.perf_counter() - t0
     barrier()
-    el = replicas.max_over_ranks(el)
-    e2e_value = replicas.sum_over_ranks(3 * dof * e2e_steps) / el
+    el = max_over_ranks(el)
+    e2e_value = sum_over_ranks(3 * dof * e2e_steps) / el
     qbytes = int(np.prod(s.shape)) * np.dtype(s.dtype).itemsize
     pin_in.free()
     pin_out.free()
@@ -683,9 +774,9 @@ def main():
         barrier()
         ms64 = s64.time_steps(dt, a.steps)
         barrier()
-        ms64 = replicas.max_over_ranks(ms64)
+        ms64 = max_over_ranks(ms64)
         s64.close()
-        v64 = replicas.sum_over_ranks(3 * dof * a.steps) / (ms64 * 1e-3)
+        v64 = sum_over_ranks(3 * dof * a.steps) / (ms64 * 1e-3)
         plain = {"value": v64, "ms_per_step": ms64 / a.steps, "speedup": value / v64,
                  "contraction_tflops": 2 * (3 * s.NP + 4 * s.NFP) * dof * 3 * a.steps / (ms64 * 1e-3) / 1e12}
 
@@ -714,7 +805,7 @@ def main():
             bat["speedup_vs_f64"] = bat["value"] / b64["value"]
         cav = maxwell_cavity(M) if a.cavity else None
         mhd = mhd_alfven(M) if a.mhd else None
-        slab = slab_decomposed(M, a, a.slab_parts) if a.slab_parts > 0 else None
+        slab_leg = slab_decomposed(M, a, a.slab_parts) if a.slab_parts > 0 else None
         srv = served(M, a.serve_requests, a.serve_lambda, largest=a.serve_largest,
                      slots=a.serve_slots) if a.serve_requests > 0 else None
         if srv is not None:  # the same stream with every request in FP64
@@ -744,7 +835,7 @@ def main():
             "plain_f64": plain,
             "measured_gemm_peaks": fpp,
             "batched": bat,
-            "maxwell_cavity": cav, "mhd_alfven": mhd, "slab": slab,
+            "maxwell_cavity": cav, "mhd_alfven": mhd, "slab": slab_leg,
             "served": srv,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": qbytes,
                     "entry": "mxm_dg_advance_host_async (pinned host state in/out every step, 1 SSPRK3 step per "

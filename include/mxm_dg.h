@@ -200,14 +200,18 @@ int mxm_dg_max_wavespeed(void* handle, double* out);
 int mxm_dg_reduce_conserved(void* handle, int which, int c, int kind, double* out);
 /* The same reduction without any device allocation; it has no counterpart
  * in the reference.  Its scratch is a static device array of the library
- * (4096 first-pass partials plus the result slot), so `nblocks`, the number
- * of first-pass blocks, must lie in 0..4096 (0 picks the same count as
- * mxm_dg_reduce_conserved, which makes the two results bit-identical);
- * larger values return MXM_DG_EINVAL with a message.  The first call on a
- * device looks the scratch up (one-time set-up), so make it before any
- * stream capture.  Nothing in the scratch needs to start at zero.  The
- * scratch is shared by all handles on a device: calls whose work overlaps
- * on one device (other host threads, other streams) race on it. */
+ * (4096 first-pass partials plus the result slot), so `nblocks`, an upper
+ * bound on the first-pass blocks, must lie in 0..4096; the count launched is
+ * min(nblocks, ceil(owned elements / 256)) (0 picks the same count as
+ * mxm_dg_reduce_conserved, min(ceil(owned elements / 256), 1024), which
+ * makes the two results bit-identical); larger values return MXM_DG_EINVAL
+ * with a message.  The first call on a device looks the scratch's address
+ * up (one-time set-up) and caches it for the life of the library, which
+ * assumes the device's primary context lives as long as the library does
+ * (no cudaDeviceReset in between); make that first call before any stream
+ * capture.  Nothing in the scratch needs to start at zero.  The scratch is
+ * shared by all handles on a device: calls whose work overlaps on one
+ * device (other host threads, other streams) race on it. */
 int mxm_dg_reduce_conserved_noalloc(void* handle, int which, int c, int kind, int nblocks, double* out);
 
 /* ---- misc ---------------------------------------------------------------- */
@@ -284,6 +288,13 @@ int mxm_dg_fill_ic(void* handle, int which, int kind, const double* params, int 
  * ghost_lo, ghost_hi (0/1), local bc_z_lo, local bc_z_hi, lo neighbour part,
  * hi neighbour part (-1 = none)}.  Needs no GPU. */
 int mxm_dg_slab_plan(int nz, int bc_z_lo, int bc_z_hi, int nparts, int part, int32_t* out8);
+/* Host-only: the point-to-point operations of part `part`'s ghost exchange
+ * in the order the NCCL transport issues them (sends up then down, receives
+ * from below then from above; the counterpart of HaloExchange.exchange's
+ * message schedule, src/halo_exchange.mojo:313-395).  out12 holds *nops
+ * triples {0 send / 1 receive, peer part, local z layer (0 = ghost below
+ * when there is one)}.  Needs no GPU. */
+int mxm_dg_slab_exchange_ops(int nz, int bc_z_lo, int bc_z_hi, int nparts, int part, int32_t* out12, int* nops);
 /* As mxm_dg_create, for part `part` of an nparts-slab decomposition of the
  * global mesh `mesh` (nparts = 1: a plain handle). */
 int mxm_dg_create_slab(const mxm_dg_mesh_desc* mesh, const mxm_dg_physics_desc* phys, int P, int precision,

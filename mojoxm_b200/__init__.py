@@ -35,7 +35,7 @@ BC_INTERIOR, BC_WALL, BC_OUTFLOW, BC_INFLOW = 0, 1, 2, 3
 PREC = {"f64": 0, "f32": 1, "mixed": 2}
 
 EXPORTED = [
-    "mxm_dg_slab_plan", "mxm_dg_create_slab", "mxm_dg_slab_info", "mxm_dg_slab_layout", "mxm_dg_slab_stage",
+    "mxm_dg_slab_plan", "mxm_dg_slab_exchange_ops", "mxm_dg_create_slab", "mxm_dg_slab_info", "mxm_dg_slab_layout", "mxm_dg_slab_stage",
     "mxm_dg_nccl_unique_id", "mxm_dg_slab_connect_nccl", "mxm_dg_group_create", "mxm_dg_group_step_n",
     "mxm_dg_group_synchronize", "mxm_dg_group_last_error", "mxm_dg_group_destroy", "mxm_dg_group_time_steps",
     "mxm_dg_version", "mxm_dg_node_xyz_f32", "mxm_dg_advance_host_async", "mxm_dg_create", "mxm_dg_destroy", "mxm_dg_sizes", "mxm_dg_dof_count",
@@ -143,6 +143,7 @@ def lib():
         L.mxm_dg_server_stats.argtypes = [vp, dp, ctypes.c_int]
         L.mxm_dg_server_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
         L.mxm_dg_slab_plan.argtypes = [ctypes.c_int] * 5 + [i32p]
+        L.mxm_dg_slab_exchange_ops.argtypes = [ctypes.c_int] * 5 + [i32p, ctypes.POINTER(ctypes.c_int)]
         L.mxm_dg_create_slab.argtypes = [ctypes.POINTER(_MeshDesc), ctypes.POINTER(_PhysDesc), ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
         L.mxm_dg_slab_info.argtypes = [vp, i64p]

@@ -98,6 +98,15 @@ struct SlabPlan {
   int cz0, cz1, glo, ghi, bc_lo, bc_hi, nb_lo, nb_hi;
 };
 SlabPlan slab_plan(int nz, int bc_lo, int bc_hi, int nparts, int part);
+// One point-to-point operation of a part's ghost exchange: send (recv = 0)
+// the local z layer `layer` to part `peer`, or receive (recv = 1) into it.
+struct SlabXOp {
+  int recv, peer, layer;
+};
+// The exchange of a part with ghost layers (glo, ghi), neighbours (nb_lo,
+// nb_hi) and local_nz local layers, in the order the NCCL transport issues
+// it; returns the count (at most 4).
+int slab_exchange_ops(int glo, int ghi, int nb_lo, int nb_hi, int local_nz, SlabXOp out[4]);
 
 Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, int prec,
                const SlabPlan* slab = nullptr, int nparts = 1, int part = 0);

@@ -55,6 +55,20 @@ SlabPlan slab_plan(int nz, int bc_lo, int bc_hi, int nparts, int part) {
   return p;
 }
 
+// Every part issues its sends in the order (up: top owned layer to the hi
+// neighbour, down: bottom owned layer to the lo neighbour) and its receives
+// in the order (from lo: the up message, from hi: the down message), so the
+// messages of a pair of parts that neighbour each other on both sides (two
+// periodic parts) match in NCCL's per-pair issue order.
+int slab_exchange_ops(int glo, int ghi, int nb_lo, int nb_hi, int local_nz, SlabXOp out[4]) {
+  int n = 0;
+  if (ghi) out[n++] = SlabXOp{0, nb_hi, local_nz - 2};  // top owned layer
+  if (glo) out[n++] = SlabXOp{0, nb_lo, glo};           // bottom owned layer (local layer 1)
+  if (glo) out[n++] = SlabXOp{1, nb_lo, 0};             // ghost layer below
+  if (ghi) out[n++] = SlabXOp{1, nb_hi, local_nz - 1};  // ghost layer above
+  return n;
+}
+
 namespace {
 
 size_t layer_vals(const Handle* h) { return size_t(h->nx) * h->ny * 6 * h->NP * h->NC; }
@@ -117,19 +131,18 @@ struct NcclLink {
   ncclComm_t comm = nullptr;
 };
 
-// Every part issues its sends in the order (up: top owned layer to the hi
-// neighbour, down: bottom owned layer to the lo neighbour) and its receives
-// in the order (from lo: the up message, from hi: the down message), so the
-// messages of a pair of parts that neighbour each other on both sides (two
-// periodic parts) match in NCCL's per-pair issue order.
+// The part's sends and receives in slab_exchange_ops' order, as one NCCL group.
 void nccl_exchange(Handle* h, int which, cudaStream_t st) {
   const NcclApi& api = nccl_api();
   const size_t bytes = layer_vals(h) * h->rbytes;
+  SlabXOp ops[4];
+  const int n = slab_exchange_ops(h->glo, h->ghi, h->nb_lo, h->nb_hi, h->nz, ops);
   nck(api.group_start(), "ncclGroupStart");
-  if (h->ghi) nck(api.send(layer_ptr(h, which, owned_hi_layer(h)), bytes, ncclUint8, h->nb_hi, h->nccl->comm, st), "ncclSend");
-  if (h->glo) nck(api.send(layer_ptr(h, which, owned_lo_layer(h)), bytes, ncclUint8, h->nb_lo, h->nccl->comm, st), "ncclSend");
-  if (h->glo) nck(api.recv(layer_ptr(h, which, ghost_lo_layer(h)), bytes, ncclUint8, h->nb_lo, h->nccl->comm, st), "ncclRecv");
-  if (h->ghi) nck(api.recv(layer_ptr(h, which, ghost_hi_layer(h)), bytes, ncclUint8, h->nb_hi, h->nccl->comm, st), "ncclRecv");
+  for (int k = 0; k < n; ++k) {
+    char* p = layer_ptr(h, which, ops[k].layer);
+    if (ops[k].recv) nck(api.recv(p, bytes, ncclUint8, ops[k].peer, h->nccl->comm, st), "ncclRecv");
+    else nck(api.send(p, bytes, ncclUint8, ops[k].peer, h->nccl->comm, st), "ncclSend");
+  }
   nck(api.group_end(), "ncclGroupEnd");
 }
 
@@ -281,6 +294,24 @@ int mxm_dg_slab_plan(int nz, int bc_lo, int bc_hi, int nparts, int part, int32_t
   }
 }
 
+int mxm_dg_slab_exchange_ops(int nz, int bc_lo, int bc_hi, int nparts, int part, int32_t* out12, int* nops) {
+  if (!out12 || !nops) return MXM_DG_EINVAL;
+  try {
+    const mxm::SlabPlan p = mxm::slab_plan(nz, bc_lo, bc_hi, nparts, part);
+    mxm::SlabXOp ops[4];
+    const int n = mxm::slab_exchange_ops(p.glo, p.ghi, p.nb_lo, p.nb_hi, p.cz1 - p.cz0 + p.glo + p.ghi, ops);
+    for (int k = 0; k < n; ++k) {
+      out12[3 * k] = ops[k].recv;
+      out12[3 * k + 1] = ops[k].peer;
+      out12[3 * k + 2] = ops[k].layer;
+    }
+    *nops = n;
+    return MXM_DG_OK;
+  } catch (std::exception& ex) {
+    return create_error(ex, MXM_DG_EINVAL);
+  }
+}
+
 int mxm_dg_create_slab(const mxm_dg_mesh_desc* mesh, const mxm_dg_physics_desc* phys, int P, int precision,
                        int nparts, int part, void** out) {
   if (!out) return MXM_DG_EINVAL;
@@ -367,7 +398,12 @@ int mxm_dg_group_create(void* const* handles, int n, void** out) {
       if (h->nccl) throw mxm::ArgError("a part connected to NCCL cannot join an in-process group");
       g->parts.push_back(h);
     }
-    for (Handle* h : g->parts) {  // direct NVLink copies between the parts' GPUs where possible
+    // Direct NVLink copies between the parts' GPUs where possible.  The
+    // parts' state buffers come from each device's default memory pool
+    // (stream-ordered allocation), whose access from other devices is set on
+    // the pool (cudaMemPoolSetAccess); peer access of the contexts covers
+    // cudaMalloc'd memory only, so both are granted.
+    for (Handle* h : g->parts) {
       CK(cudaSetDevice(h->device));
       for (Handle* o : g->parts) {
         int can = 0;
@@ -375,6 +411,13 @@ int mxm_dg_group_create(void* const* handles, int n, void** out) {
           const cudaError_t e = cudaDeviceEnablePeerAccess(o->device, 0);
           if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
           else CK(e);
+          cudaMemPool_t pool;  // o's pool, readable and writable from h's device
+          CK(cudaDeviceGetDefaultMemPool(&pool, o->device));
+          cudaMemAccessDesc ad{};
+          ad.location.type = cudaMemLocationTypeDevice;
+          ad.location.id = h->device;
+          ad.flags = cudaMemAccessFlagsProtReadWrite;
+          CK(cudaMemPoolSetAccess(pool, &ad, 1));
         }
       }
       cudaEvent_t ev;
@@ -390,13 +433,18 @@ int mxm_dg_group_create(void* const* handles, int n, void** out) {
   }
 }
 
+// Arguments every group step entry checks before it launches anything.
+static void group_step_args(const Group* g, int nsteps) {
+  if (nsteps < 0) throw mxm::ArgError("nsteps must be >= 0");
+  for (Handle* h : g->parts)
+    if (h->lim_on != g->parts[0]->lim_on) throw mxm::ArgError("the parts must agree on the limiter");
+}
+
 int mxm_dg_group_step_n(void* group, double dt, int nsteps) {
   Group* g = (Group*)group;
   if (!g) return MXM_DG_EINVAL;
   try {
-    if (nsteps < 0) throw mxm::ArgError("nsteps must be >= 0");
-    for (Handle* h : g->parts)
-      if (h->lim_on != g->parts[0]->lim_on) throw mxm::ArgError("the parts must agree on the limiter");
+    group_step_args(g, nsteps);
     g->step_n(dt, nsteps);
     return MXM_DG_OK;
   } catch (mxm::CudaError& ex) {
@@ -413,9 +461,10 @@ int mxm_dg_group_step_n(void* group, double dt, int nsteps) {
 // end, so the two timing events bracket all parts' work.
 int mxm_dg_group_time_steps(void* group, double dt, int nsteps, double* ms) {
   Group* g = (Group*)group;
-  if (!g || !ms || nsteps < 0) return MXM_DG_EINVAL;
+  if (!g || !ms) return MXM_DG_EINVAL;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   try {
+    group_step_args(g, nsteps);
     Handle* h0 = g->parts[0];
     CK(cudaSetDevice(h0->device));
     CK(cudaEventCreate(&t0));
@@ -449,11 +498,16 @@ int mxm_dg_group_time_steps(void* group, double dt, int nsteps, double* ms) {
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     return MXM_DG_OK;
-  } catch (std::exception& ex) {
+  } catch (mxm::CudaError& ex) {
     if (t0) cudaEventDestroy(t0);
     if (t1) cudaEventDestroy(t1);
     g->err = ex.what();
     return MXM_DG_ECUDA;
+  } catch (std::exception& ex) {
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    g->err = ex.what();
+    return MXM_DG_EINVAL;
   }
 }
 

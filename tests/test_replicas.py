@@ -1,6 +1,6 @@
 """Multi-rank bookkeeping of replica runs, on CPU with gloo (world size 2):
 sharding covers every unit exactly once, the job time is the maximum over
-ranks and unit counts are summed, as bench.py computes them under torchrun."""
+ranks and unit counts are summed (the helpers bench.py uses under torchrun)."""
 import os
 import socket
 
@@ -8,7 +8,7 @@ import pytest
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from mojoxm_b200 import replicas
+import bench as replicas
 
 
 def _free_port():

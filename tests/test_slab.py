@@ -2,13 +2,14 @@
 path: src/partition.mojo:106-228, src/halo_exchange.mojo:187-395).
 
 CPU: the library's slab plan (host-only), and the caller-driven exchange
-schedule of mojoxm_b200.halo over torch.distributed gloo with 2 and 3 ranks,
+schedule of tests/torch_halo.py over torch.distributed gloo with 2 and 3 ranks,
 each rank stepping its slab with the oracle; the gathered owned layers must
 equal the undecomposed oracle solve bit for bit.
 GPU: slab parts stepped as an in-process group against the plain solve (bit
 identical in FP64, FP32 and MIXED, with and without the limiter), the owned
 diagnostics, the layout report and the NCCL transport's set-up.
 """
+import ctypes
 import os
 import socket
 
@@ -19,7 +20,7 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 import mojoxm_b200 as M
-from mojoxm_b200 import halo
+from tests import torch_halo as halo
 from tests import dgcases
 
 P_CPU = 2
@@ -51,6 +52,55 @@ def test_slab_plan_partitions():
         halo.SlabPlan.of(2, 0, 0, 3, 0)  # fewer layers than parts
     with pytest.raises(M.DGError):
         halo.SlabPlan.of(8, 0, 1, 2, 0)  # one z boundary periodic, the other bounded
+
+
+def _exchange_ops(nz, bc_lo, bc_hi, nparts, part):
+    out = (ctypes.c_int32 * 12)()
+    n = ctypes.c_int()
+    assert M.lib().mxm_dg_slab_exchange_ops(nz, bc_lo, bc_hi, nparts, part, out, ctypes.byref(n)) == M.OK
+    return [tuple(out[3 * k:3 * k + 3]) for k in range(n.value)]
+
+
+def test_nccl_exchange_schedule_delivers_every_ghost_layer():
+    """The library's own NCCL exchange order (mxm_dg_slab_exchange_ops, the
+    list nccl_exchange issues), replayed without any transport: sends from
+    part a to part b pair with receives on b from a in issue order, as NCCL
+    point-to-point does.  Every ghost layer must receive exactly the
+    neighbour's owned layer that it stands for (same global z layer), no
+    owned layer may be received into, and no message may be left unpaired."""
+    for nz in range(1, 10):
+        for nparts in range(1, min(nz, 5) + 1):
+            for bc in ((0, 0), (1, 1)):
+                plans = [halo.SlabPlan.of(nz, bc[0], bc[1], nparts, r) for r in range(nparts)]
+                ops = [_exchange_ops(nz, bc[0], bc[1], nparts, r) for r in range(nparts)]
+
+                def glob(r, layer):  # global z layer of part r's local layer
+                    return (plans[r].cz0 - plans[r].ghost_lo + layer) % nz
+
+                sends, recvs = {}, {}
+                for r, lst in enumerate(ops):
+                    assert len(lst) == 2 * (plans[r].ghost_lo + plans[r].ghost_hi)
+                    # a group's sends are issued before its receives
+                    kinds = [k for k, _, _ in lst]
+                    assert kinds == sorted(kinds)
+                    for kind, peer, layer in lst:
+                        assert 0 <= layer < plans[r].local_layers
+                        (recvs if kind else sends).setdefault((r, peer) if not kind else (peer, r), []).append(
+                            (r, layer))
+                assert sorted(sends) == sorted(recvs)
+                got = {}
+                for key in sends:
+                    assert len(sends[key]) == len(recvs[key])
+                    for (a, la), (b, lb) in zip(sends[key], recvs[key]):
+                        owned_a = plans[a].ghost_lo <= la < plans[a].local_layers - plans[a].ghost_hi
+                        ghost_b = (lb == 0 and plans[b].ghost_lo) or (lb == plans[b].local_layers - 1 and plans[b].ghost_hi)
+                        assert owned_a and ghost_b
+                        assert glob(a, la) == glob(b, lb)
+                        assert (b, lb) not in got
+                        got[(b, lb)] = a
+                want = {(r, 0) for r in range(nparts) if plans[r].ghost_lo} | \
+                    {(r, plans[r].local_layers - 1) for r in range(nparts) if plans[r].ghost_hi}
+                assert set(got) == want
 
 
 def test_layer_offsets():

@@ -47,10 +47,30 @@ def test_noalloc_reduction_matches_allocating_entry(dim, prec):
                 rc_b, b = _noalloc(s, c, kind=kind)
                 assert rc_a == M.OK and rc_b == M.OK, M._err(s.h)
                 assert abs(a - b) <= TOL * max(1.0, abs(a)), (kind, c, a, b)
-    # a different first-pass block count still sums the same values
-    rc, b = _noalloc(s, 0, kind=0, nblocks=7)
-    _, a = _alloc(s, 0, kind=0)
-    assert rc == M.OK and abs(a - b) <= 1e-11 * max(1.0, abs(a))
+    s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nblocks", [7, 1500, 4096])
+def test_noalloc_other_block_counts(nblocks):
+    """Block counts other than the default one.  36^3 x 6 = 279,936 elements
+    need 1094 blocks of 256, so the default (capped at 1024 partials) uses
+    1024; nblocks 7 runs the grid-stride loop with 7 blocks, 1500 and 4096
+    are capped at 1094 blocks, a count the allocating entry never uses."""
+    phys = M.Euler(flux_type=M.FLUX_RUSANOV)
+    s = M.Solver(M.Mesh(36, 36, 36), phys, P=1, precision="f64")
+    assert s.Ne == 279936
+    q = random_state(s.shape, phys, seed=5)
+    s.upload_state(q)
+    for _ in range(2):
+        for kind in (0, 1, 2, 3):
+            _, a = _alloc(s, 4, kind=kind)
+            rc, b = _noalloc(s, 4, kind=kind, nblocks=nblocks)
+            assert rc == M.OK, M._err(s.h)
+            if kind == 2:
+                assert a == b
+            else:
+                assert abs(a - b) <= 1e-12 * abs(a), (kind, nblocks, a, b)
     s.close()
 
 

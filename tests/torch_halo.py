@@ -1,4 +1,6 @@
-"""Caller-driven halo exchange of a z-slab decomposition over torch.distributed.
+"""Caller-driven halo exchange of a z-slab decomposition over torch.distributed
+(a test-side driver: the library itself uses no PyTorch; its own transports
+are NCCL point-to-point and the in-process group of slab.cu).
 
 The reference steps one patch per MPI rank and refills the patch's ghost
 ring once per RK stage (HaloExchange.exchange, src/halo_exchange.mojo:
@@ -28,7 +30,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import DGError, lib
+from mojoxm_b200 import DGError, lib
 
 STAGE_IN = (0, 1, 2)   # Shu-Osher stage s reads q, q1, q2 ...
 STAGE_OUT = (1, 2, 0)  # ... and writes q1, q2, q
