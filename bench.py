@@ -421,6 +421,31 @@ def run_reference(a, rank, world):
     print(json.dumps(line))
 
 
+def batch_member(M, rng, precision):
+    """The next member of the batched 2D workload drawn from `rng`: an
+    n x n x 2 triangle mesh, n ~ U{16,32,64,128,256}, P ~ U{1..5}, HLLE flux,
+    BJ limiter (eps 0.1), and with equal odds an isentropic vortex
+    (beta ~ U[2,6], periodic [0,10]^2) or a tanh-smoothed Sod tube (left /
+    right rho, p ~ U[0.1,1], width 8h, outflow x, periodic y), filled on the
+    device.  Returns (solver, "vortex" | "sod", cell size h)."""
+    n = int(rng.choice([16, 32, 64, 128, 256]))
+    P = int(rng.integers(1, 6))
+    phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_HLLE, False)
+    if rng.random() < 0.5:
+        mesh = M.Mesh(n, n, 1, 10.0, 10.0, 1.0, dim=2)
+        s = M.Solver(mesh, phys, P=P, precision=precision)
+        s.fill_ic(M.IC_VORTEX, [rng.uniform(2, 6), 5.0, 5.0, 1.0, 1.0, 0.0, 1.0])
+        kind, h = "vortex", 10.0 / n
+    else:
+        mesh = M.Mesh(n, n, 1, 1.0, 1.0, 1.0, bcs=M.BoundaryConditions(2, 2, 0, 0), dim=2)
+        s = M.Solver(mesh, phys, P=P, precision=precision)
+        rl, pl, rr, pr = rng.uniform(0.1, 1.0, 4)
+        s.fill_ic(M.IC_SOD, [rl, pl, rr, pr, 0.5, 8.0 / n])
+        kind, h = "sod", 1.0 / n
+    s.enable_cell_limiter(True, 0.1)
+    return s, kind, h
+
+
 def batched_2d(M, nsolves, steps, seed=2024, precision="f32", loop=True, ref=None, keep=False):
     """Batched 2D Euler on triangles: `nsolves` independent solves, n x n x 2
     tris with n ~ U{16,32,64,128,256}, P ~ U{1..5}, ICs a seeded mix of
@@ -435,24 +460,9 @@ def batched_2d(M, nsolves, steps, seed=2024, precision="f32", loop=True, ref=Non
     batch = M.Batch()
     solvers, kinds, dts = [], [], []
     for k in range(nsolves):
-        n = int(rng.choice([16, 32, 64, 128, 256]))
-        P = int(rng.integers(1, 6))
-        phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_HLLE, False)
-        if rng.random() < 0.5:
-            mesh = M.Mesh(n, n, 1, 10.0, 10.0, 1.0, dim=2)
-            s = M.Solver(mesh, phys, P=P, precision=precision)
-            s.fill_ic(M.IC_VORTEX, [rng.uniform(2, 6), 5.0, 5.0, 1.0, 1.0, 0.0, 1.0])
-            h = 10.0 / n
-            kinds.append("vortex")
-        else:
-            mesh = M.Mesh(n, n, 1, 1.0, 1.0, 1.0, bcs=M.BoundaryConditions(2, 2, 0, 0), dim=2)
-            s = M.Solver(mesh, phys, P=P, precision=precision)
-            rl, pl, rr, pr = rng.uniform(0.1, 1.0, 4)
-            s.fill_ic(M.IC_SOD, [rl, pl, rr, pr, 0.5, 8.0 / n])
-            h = 1.0 / n
-            kinds.append("sod")
-        s.enable_cell_limiter(True, 0.1)
-        dt = ref["dts"][k] if ref else 0.3 * h / ((2 * P + 1) * s.max_wavespeed())
+        s, kind, h = batch_member(M, rng, precision)
+        kinds.append(kind)
+        dt = ref["dts"][k] if ref else 0.3 * h / ((2 * s.P + 1) * s.max_wavespeed())
         batch.add(s, dt)
         dts.append(dt)
         solvers.append(s)

@@ -59,7 +59,7 @@ def test_noalloc_other_block_counts(nblocks):
     are capped at 1094 blocks, a count the allocating entry never uses."""
     phys = M.Euler(flux_type=M.FLUX_RUSANOV)
     s = M.Solver(M.Mesh(36, 36, 36), phys, P=1, precision="f64")
-    assert s.Ne == 279936
+    assert s.num_elements == 279936
     q = random_state(s.shape, phys, seed=5)
     s.upload_state(q)
     for _ in range(2):
