@@ -80,6 +80,11 @@ extern "C" {
 #define MXM_DG_PREC_F64 0   /* state, geometry and all arithmetic in FP64       */
 #define MXM_DG_PREC_F32 1   /* FP32 state and arithmetic (the reference's path) */
 #define MXM_DG_PREC_MIXED 2 /* FP32 state/flux, split-BF16 tensor-core contractions */
+/* FP32 state/flux, split-TF32 tensor-core contractions (tcgen05 kind::tf32,
+ * hi + lo of 11 significant bits each: the operator carries ~22 bits
+ * against 16 for split-BF16, for long linear runs).  3D P = 2..4; where no
+ * TF32 tile fits (P = 5, P = 1, 2D, two-fluid) the FP32 kernel runs. */
+#define MXM_DG_PREC_MIXED_TF32 3
 
 /* Physics parameters, `p[]` in the field order of the Mojo structs:
  *  ADVECTION (advection.mojo:192-199): p = {vx, vy, vz, inflow_q}

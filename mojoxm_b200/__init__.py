@@ -32,7 +32,7 @@ OK, EINVAL, ENOMEM, ECUDA, ENONFINITE, ETIMEDOUT, ENOTREADY = 0, -1, -2, -3, -4,
 PHYS_ADVECTION, PHYS_EULER, PHYS_MAXWELL, PHYS_SHALLOW_WATER, PHYS_MHD, PHYS_MHD_PLAIN, PHYS_TWO_FLUID = range(7)
 FLUX_RUSANOV, FLUX_ROE, FLUX_HLLE, FLUX_HLLEC, FLUX_HLLC, FLUX_HLL = 0, 1, 2, 3, 4, 5
 BC_INTERIOR, BC_WALL, BC_OUTFLOW, BC_INFLOW = 0, 1, 2, 3
-PREC = {"f64": 0, "f32": 1, "mixed": 2}
+PREC = {"f64": 0, "f32": 1, "mixed": 2, "tf32": 3}
 
 EXPORTED = [
     "mxm_dg_slab_plan", "mxm_dg_slab_exchange_ops", "mxm_dg_create_slab", "mxm_dg_slab_info", "mxm_dg_slab_layout", "mxm_dg_slab_stage",

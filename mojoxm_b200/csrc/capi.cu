@@ -43,26 +43,50 @@ static float bf16_value(uint16_t b) {
   return f;
 }
 
+// Round to TF32 (11 significant bits), to nearest with ties away from zero,
+// as cvt.rna.tf32.f32 does on the device; the low 13 bits are cleared.
+static uint32_t tf32_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) u += 0x1000u;  // finite: round the magnitude
+  return u & 0xffffe000u;
+}
+static float bits_f32(uint32_t u) {
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
 // Shared operator A (NP x K, row-major, FP64) as the tensor-core B operand:
 // N = NP rounded up to 16 rows; the volume columns [0, nvol) padded to
-// kvol = nvol rounded up to 16, then the face columns [nvol, K) from column
-// kvol on, padded to a multiple of 16; K-major no-swizzle core-matrix
-// layout, split into a bfloat16 hi image followed by a lo image
-// (a = hi + lo); padding entries are zero.
-static std::vector<unsigned char> tc_operator_image(const std::vector<double>& A, int NP, int K, int nvol) {
-  const int NN = (NP + 15) / 16 * 16, kvol = (nvol + 15) / 16 * 16;
-  const int KA = kvol + (K - nvol + 15) / 16 * 16;
-  const size_t half = size_t(NN) * KA * 2;
+// kvol = nvol rounded up to the MMA K step (16 for split-BF16, 8 for
+// split-TF32), then the face columns [nvol, K) from column kvol on, padded
+// likewise; K-major no-swizzle core-matrix layout, split into a hi image
+// followed by a lo image (a = hi + lo, bfloat16 or TF32 in 32-bit words);
+// padding entries are zero.
+static std::vector<unsigned char> tc_operator_image(const std::vector<double>& A, int NP, int K, int nvol, int kind) {
+  const int ks = kind == TC_TF32 ? 8 : 16, elem = kind == TC_TF32 ? 4 : 2;
+  const int NN = (NP + 15) / 16 * 16, kvol = (nvol + ks - 1) / ks * ks;
+  const int KA = kvol + (K - nvol + ks - 1) / ks * ks;
+  const size_t half = size_t(NN) * KA * elem;
   std::vector<unsigned char> img(2 * half, 0);
   for (int i = 0; i < NP; ++i)
     for (int k = 0; k < K; ++k) {
       const double v = A[size_t(i) * K + k];
-      const uint16_t hi = bf16_bits(float(v));
-      const uint16_t lo = bf16_bits(float(v - double(bf16_value(hi))));
       const int col = k < nvol ? k : kvol + (k - nvol);
-      const size_t off = umma_tile_offset(i, col, NN);
-      std::memcpy(&img[off], &hi, 2);
-      std::memcpy(&img[half + off], &lo, 2);
+      if (kind == TC_TF32) {
+        const uint32_t hi = tf32_bits(float(v));
+        const uint32_t lo = tf32_bits(float(v - double(bits_f32(hi))));
+        const size_t off = umma_k_off<OpTF32>(i, col, NN);
+        std::memcpy(&img[off], &hi, 4);
+        std::memcpy(&img[half + off], &lo, 4);
+      } else {
+        const uint16_t hi = bf16_bits(float(v));
+        const uint16_t lo = bf16_bits(float(v - double(bf16_value(hi))));
+        const size_t off = umma_k_off<OpBF16>(i, col, NN);
+        std::memcpy(&img[off], &hi, 2);
+        std::memcpy(&img[half + off], &lo, 2);
+      }
     }
   return img;
 }
@@ -209,7 +233,7 @@ cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* 
       if constexpr (std::is_same<R, float>::value &&
                     std::decay<decltype(ph)>::type::NC <= 16) {
         if (h->use_tc)
-          return launch_stage3d_tc(h->P, ar, t, ph, (const unsigned char*)h->tcimg, h->nsm, h->stream);
+          return launch_stage3d_tc(h->P, h->tc_kind, ar, t, ph, (const unsigned char*)h->tcimg, h->nsm, h->stream);
       }
       return launch_stage3d<R>(h->P, ar, t, ph, h->nsm, h->stream);
     };
@@ -684,8 +708,8 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   if (!m || !ph) throw ArgError("null descriptor");
   if (m->dim != 2 && m->dim != 3) throw ArgError("mesh dim must be 2 or 3");
   if (P < 1 || P > 5) throw ArgError("order P must be in 1..5");
-  if (prec != MXM_DG_PREC_F64 && prec != MXM_DG_PREC_F32 && prec != MXM_DG_PREC_MIXED)
-    throw ArgError("precision must be MXM_DG_PREC_F64, MXM_DG_PREC_F32 or MXM_DG_PREC_MIXED");
+  if (prec != MXM_DG_PREC_F64 && prec != MXM_DG_PREC_F32 && prec != MXM_DG_PREC_MIXED && prec != MXM_DG_PREC_MIXED_TF32)
+    throw ArgError("precision must be MXM_DG_PREC_F64, MXM_DG_PREC_F32, MXM_DG_PREC_MIXED or MXM_DG_PREC_MIXED_TF32");
   if (ph->kind < 0 || ph->kind > MXM_DG_PHYS_TWO_FLUID) throw ArgError("unknown physics kind");
   if (ph->kind == MXM_DG_PHYS_TWO_FLUID && m->dim != 3) throw ArgError("two-fluid physics is 3D only");
   if (ph->kind == MXM_DG_PHYS_MHD_PLAIN && m->dim != 2) throw ArgError("MHD_PLAIN physics is 2D only");
@@ -739,9 +763,12 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
   h->cend = h->ncell - int64_t(h->nx) * h->ny * h->ghi;
   if (h->ne > (int64_t(1) << 31) / 64) throw ArgError("mesh too large for 32-bit cell indexing");
   h->rbytes = prec == MXM_DG_PREC_F64 ? 8 : 4;
-  // split-BF16 tensor-core contraction for the 3D orders it is built for
-  // (a 128-row tile needs at least 8 element slots: NC <= 16)
-  h->use_tc = prec == MXM_DG_PREC_MIXED && m->dim == 3 && P >= 2 && P <= 5 && h->NC <= 16;
+  // split-BF16 / split-TF32 tensor-core contraction for the 3D orders it is
+  // built for (a 128-row tile needs at least 8 element slots: NC <= 16; the
+  // TF32 operands of P = 5 exceed a block's shared memory)
+  h->tc_kind = prec == MXM_DG_PREC_MIXED_TF32 ? TC_TF32 : TC_BF16;
+  h->use_tc = (prec == MXM_DG_PREC_MIXED || prec == MXM_DG_PREC_MIXED_TF32) && m->dim == 3 && P >= 2 && P <= 5 &&
+              h->NC <= 16 && tc_shape_fits(P, h->NC, h->tc_kind);
   if (m->dim == 3 && !h->use_tc && stage3d_smem_need(P, h->NC, h->rbytes) > kMaxSmemPerBlock)
     throw ArgError("this order, component count and precision exceed the stage tile's shared memory");
   h->ref = build_refops(h->dim, P);
@@ -791,7 +818,7 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
     upload(&raw->A, At);
     upload(&raw->w, raw->ref.w);
     if (raw->use_tc) {
-      auto img = tc_operator_image(raw->Ahost, raw->NP, raw->K, 3 * raw->NP);
+      auto img = tc_operator_image(raw->Ahost, raw->NP, raw->K, 3 * raw->NP, raw->tc_kind);
       dev_alloc(raw, &raw->tcimg, img.size());
       CK(cudaMemcpyAsync(raw->tcimg, img.data(), img.size(), cudaMemcpyHostToDevice, raw->stream));
       CK(cudaStreamSynchronize(raw->stream));  // img goes out of scope

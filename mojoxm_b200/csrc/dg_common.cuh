@@ -212,11 +212,16 @@ cudaError_t launch_stage3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& ta
 template <class R, class Phys>
 cudaError_t launch_wavespeed3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phys& ph,
                                unsigned long long* out, cudaStream_t st);
-// Tensor-core (split-BF16 tcgen05) 3D stage for FP32 state, P = 2..5;
-// `img` is the operator image built by tc_operator_image().
+// Tensor-core 3D stage for FP32 state, P = 2..5: split-BF16 (kind
+// TC_BF16, tcgen05 kind::f16) or split-TF32 (TC_TF32, kind::tf32) operands;
+// `img` is the operator image built by tc_operator_image() for that kind.
+constexpr int TC_BF16 = 0, TC_TF32 = 1;
 template <class Phys>
-cudaError_t launch_stage3d_tc(int P, const Stage3DArgs<float>& a, const KuhnTab3<float>& tab, const Phys& ph,
-                              const unsigned char* img, int nsm, cudaStream_t st);
+cudaError_t launch_stage3d_tc(int P, int kind, const Stage3DArgs<float>& a, const KuhnTab3<float>& tab,
+                              const Phys& ph, const unsigned char* img, int nsm, cudaStream_t st);
+// Whether the tensor-core stage of (P, components, kind) fits one block's
+// shared memory.
+bool tc_shape_fits(int P, int NC, int kind);
 template <class R, class Phys>
 cudaError_t launch_stage2d(int P, const Stage2DArgs<R>& a, const KuhnTab2<R>& tab, const Phys& ph, int nsm,
                            cudaStream_t st);

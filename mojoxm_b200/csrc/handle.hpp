@@ -65,7 +65,8 @@ struct Handle {
   double* dscalar = nullptr;
   unsigned long long* uscalar = nullptr;
   int* derr = nullptr;  // device error word written by bounded waits
-  bool use_tc = false;  // MIXED precision: tensor-core contraction
+  bool use_tc = false;  // MIXED / MIXED_TF32 precision: tensor-core contraction
+  int tc_kind = 0;      // TC_BF16 or TC_TF32 operands
   void* tcimg = nullptr;  // operator image (bf16 hi | lo) in the UMMA layout
   int npartial = 1024;
   bool lim_on = false;

@@ -1,38 +1,66 @@
-// Launch + explicit instantiation of the tensor-core (split-BF16) 3D stage
-// kernel for P = 2..5; P = 1 uses the FP32 SIMT kernel.
+// Launch + explicit instantiation of the tensor-core 3D stage kernel
+// (split-BF16 or split-TF32 operands) for P = 2..5 where the shape fits
+// shared memory; P = 1 uses the FP32 SIMT kernel.
 #include "stage3d_tc.cuh"
 
 namespace mxm {
 
-template <class Phys, int P>
+template <class Phys, int P, class Op>
 cudaError_t launch_tc_p(const Stage3DArgs<float>& a, const KuhnTab3<float>& tab, const Phys& ph,
                         const unsigned char* img, int nsm, cudaStream_t st) {
-  using S = TcShape<P, Phys::NC>;
-  constexpr int NT = 256;
-  auto kern = stage3d_tc_kernel<Phys, P, NT>;
-  static int bps = -1;
-  if (bps < 0) {
-    cudaError_t e = persistent_blocks_per_sm((const void*)kern, NT, S::SMEM, &bps);
-    if (e != cudaSuccess) return e;
+  using S = TcShape<P, Phys::NC, Op>;
+  if constexpr (!S::FITS) {
+    return cudaErrorInvalidValue;  // the create call refuses these shapes
+  } else {
+    constexpr int NT = 256;
+    auto kern = stage3d_tc_kernel<Phys, P, NT, Op>;
+    static int bps = -1;
+    if (bps < 0) {
+      cudaError_t e = persistent_blocks_per_sm((const void*)kern, NT, S::SMEM, &bps);
+      if (e != cudaSuccess) return e;
+    }
+    const int ngroups = (a.ncell - a.cbeg + S::EC - 1) / S::EC;
+    int nblk = nsm * bps;
+    if (nblk > ngroups) nblk = ngroups;
+    if (nblk < 1) nblk = 1;
+    kern<<<nblk, NT, S::SMEM, st>>>(a, tab, ph, img);
+    return cudaGetLastError();
   }
-  const int ngroups = (a.ncell - a.cbeg + S::EC - 1) / S::EC;
-  int nblk = nsm * bps;
-  if (nblk > ngroups) nblk = ngroups;
-  if (nblk < 1) nblk = 1;
-  kern<<<nblk, NT, S::SMEM, st>>>(a, tab, ph, img);
-  return cudaGetLastError();
+}
+
+template <class Phys, class Op>
+cudaError_t launch_tc_kind(int P, const Stage3DArgs<float>& a, const KuhnTab3<float>& tab, const Phys& ph,
+                           const unsigned char* img, int nsm, cudaStream_t st) {
+  switch (P) {
+    case 2: return launch_tc_p<Phys, 2, Op>(a, tab, ph, img, nsm, st);
+    case 3: return launch_tc_p<Phys, 3, Op>(a, tab, ph, img, nsm, st);
+    case 4: return launch_tc_p<Phys, 4, Op>(a, tab, ph, img, nsm, st);
+    case 5: return launch_tc_p<Phys, 5, Op>(a, tab, ph, img, nsm, st);
+  }
+  return cudaErrorInvalidValue;
 }
 
 template <class Phys>
-cudaError_t launch_stage3d_tc(int P, const Stage3DArgs<float>& a, const KuhnTab3<float>& tab, const Phys& ph,
-                              const unsigned char* img, int nsm, cudaStream_t st) {
-  switch (P) {
-    case 2: return launch_tc_p<Phys, 2>(a, tab, ph, img, nsm, st);
-    case 3: return launch_tc_p<Phys, 3>(a, tab, ph, img, nsm, st);
-    case 4: return launch_tc_p<Phys, 4>(a, tab, ph, img, nsm, st);
-    case 5: return launch_tc_p<Phys, 5>(a, tab, ph, img, nsm, st);
-  }
-  return cudaErrorInvalidValue;
+cudaError_t launch_stage3d_tc(int P, int kind, const Stage3DArgs<float>& a, const KuhnTab3<float>& tab,
+                              const Phys& ph, const unsigned char* img, int nsm, cudaStream_t st) {
+  return kind == TC_TF32 ? launch_tc_kind<Phys, OpTF32>(P, a, tab, ph, img, nsm, st)
+                         : launch_tc_kind<Phys, OpBF16>(P, a, tab, ph, img, nsm, st);
+}
+
+bool tc_shape_fits(int P, int NC, int kind) {
+  auto fits = [&](auto op) -> bool {
+    using O = decltype(op);
+    switch (NC) {
+      case 1: return P == 2 ? TcShape<2, 1, O>::FITS : P == 3 ? TcShape<3, 1, O>::FITS : P == 4 ? TcShape<4, 1, O>::FITS : TcShape<5, 1, O>::FITS;
+      case 3: return P == 2 ? TcShape<2, 3, O>::FITS : P == 3 ? TcShape<3, 3, O>::FITS : P == 4 ? TcShape<4, 3, O>::FITS : TcShape<5, 3, O>::FITS;
+      case 5: return P == 2 ? TcShape<2, 5, O>::FITS : P == 3 ? TcShape<3, 5, O>::FITS : P == 4 ? TcShape<4, 5, O>::FITS : TcShape<5, 5, O>::FITS;
+      case 6: return P == 2 ? TcShape<2, 6, O>::FITS : P == 3 ? TcShape<3, 6, O>::FITS : P == 4 ? TcShape<4, 6, O>::FITS : TcShape<5, 6, O>::FITS;
+      case 9: return P == 2 ? TcShape<2, 9, O>::FITS : P == 3 ? TcShape<3, 9, O>::FITS : P == 4 ? TcShape<4, 9, O>::FITS : TcShape<5, 9, O>::FITS;
+    }
+    return false;
+  };
+  if (P < 2 || P > 5) return false;
+  return kind == TC_TF32 ? fits(OpTF32{}) : fits(OpBF16{});
 }
 
 using TA = AdvectionD<float>;
@@ -43,9 +71,9 @@ using TEC = EulerD<float, FLUX_HLLEC>;
 using TM = MaxwellD<float>;
 using TS = ShallowWaterD<float>;
 using TH = MhdD<float>;
-#define MXM_INST_TC(PH)                                                                                           \
-  template cudaError_t launch_stage3d_tc<PH>(int, const Stage3DArgs<float>&, const KuhnTab3<float>&, const PH&, \
-                                             const unsigned char*, int, cudaStream_t);
+#define MXM_INST_TC(PH)                                                                                      \
+  template cudaError_t launch_stage3d_tc<PH>(int, int, const Stage3DArgs<float>&, const KuhnTab3<float>&,    \
+                                             const PH&, const unsigned char*, int, cudaStream_t);
 MXM_INST_TC(TA)
 MXM_INST_TC(TER)
 MXM_INST_TC(TEO)

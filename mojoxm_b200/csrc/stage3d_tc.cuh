@@ -38,34 +38,26 @@
 namespace mxm {
 
 __host__ __device__ constexpr int rup16(int x) { return (x + 15) / 16 * 16; }
+__host__ __device__ constexpr int rupk(int x, int k) { return (x + k - 1) / k * k; }
 __host__ __device__ constexpr int tmem_cols_for(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : (n <= 128 ? 128 : 256)); }
 
-// MN-major, no-swizzle operand tile of `rows` x KP bf16:
-// byte (k/8)*(rows*16) + (row/8)*128 + (k%8)*16 + (row%8)*2
-__host__ __device__ constexpr uint32_t umma_mn_offset(int row, int k, int rows) {
-  return uint32_t((k >> 3) * rows * 16 + (row >> 3) * 128 + (k & 7) * 16 + (row & 7) * 2);
-}
-
-__host__ __device__ constexpr uint32_t umma_idesc_bf16_f32_amn(int M, int N) {
-  return umma_idesc_bf16_f32(M, N) | (1u << 15);  // A operand MN-major
-}
-
 // The K dimension is split into the volume columns (3 NP, padded to KV) and
-// the face columns (4 NFP, padded to KF); both halves reuse one operand
-// buffer of KB = max(KV, KF) columns, and the operator image stores the
-// face columns from KV on (tc_operator_image's `kvol`).
-template <int P, int NC>
+// the face columns (4 NFP, padded to KF), each padded to the operand kind's
+// MMA K step; both halves reuse one operand buffer of KB = max(KV, KF)
+// columns, and the operator image stores the face columns from KV on
+// (tc_operator_image's `kvol`).
+template <int P, int NC, class Op = OpBF16>
 struct TcShape {
   static constexpr int NP = ntet(P), NFP = ntri(P), K = 3 * NP + 4 * NFP;
-  static constexpr int KV = rup16(3 * NP), KF = rup16(4 * NFP), KA = KV + KF;
+  static constexpr int KV = rupk(3 * NP, Op::KSTEP), KF = rupk(4 * NFP, Op::KSTEP), KA = KV + KF;
   static constexpr int KB = KV > KF ? KV : KF;
   static constexpr int NN = rup16(NP), M = 128;
   static constexpr int EBP = (M / NC) / 8 * 8;      // element slots per component (multiple of 8)
   static constexpr int EC = EBP / 6, EB = 6 * EC;   // whole cubes in a tile
   static constexpr int NPO = NP | 1;                // odd row stride of the accumulator staging tile
   static constexpr int NCOLS = tmem_cols_for(NN);
-  static constexpr size_t A_BYTES = size_t(NN) * KA * 2;  // one of hi / lo
-  static constexpr size_t B_BYTES = size_t(M) * KB * 2;
+  static constexpr size_t A_BYTES = size_t(NN) * KA * Op::ELEM;  // one of hi / lo
+  static constexpr size_t B_BYTES = size_t(M) * KB * Op::ELEM;
   static constexpr size_t Q_BYTES = size_t(EB) * NP * NC * 4;
   static constexpr size_t O_BYTES = size_t(M) * NPO * 4;   // aliases the operand buffer (free by then)
   static constexpr size_t FB_BYTES = size_t(EB) * 3 * NC * 4;
@@ -105,29 +97,34 @@ struct TcShape {
   static constexpr size_t SMEM = FREC ? OFF_M + FM_BYTES : OFF_C + CD_BYTES;
   static constexpr bool BULK = (6 * NP * NC * 4) % 16 == 0;
   static_assert(O_BYTES <= 2 * B_BYTES, "staging tile must fit the operand buffer");
+  static constexpr bool FITS = SMEM + 1024 <= size_t(227 * 1024);
 };
 
 // Blocks per SM the register allocation must allow: what fits in shared
 // memory, at most three for register-light fluxes and two for the Roe /
 // HLLE / HLLEC solvers (capping those at three blocks' registers spills).
-template <class Phys, int P>
+template <class Phys, int P, class Op>
 __host__ __device__ constexpr int tc_min_blocks() {
-  return int(TcShape<P, Phys::NC>::blocks_for(TcShape<P, Phys::NC>::SMEM)) < (Phys::kLightFlux ? 3 : 2)
-             ? int(TcShape<P, Phys::NC>::blocks_for(TcShape<P, Phys::NC>::SMEM))
+  return int(TcShape<P, Phys::NC, Op>::blocks_for(TcShape<P, Phys::NC, Op>::SMEM)) < (Phys::kLightFlux ? 3 : 2)
+             ? int(TcShape<P, Phys::NC, Op>::blocks_for(TcShape<P, Phys::NC, Op>::SMEM))
              : (Phys::kLightFlux ? 3 : 2);
 }
 
-template <class Phys, int P, int NT>
-__global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kernel(Stage3DArgs<float> args, KuhnTab3<float> tabp, Phys ph,
+template <class Phys, int P, int NT, class Op>
+__global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_kernel(Stage3DArgs<float> args, KuhnTab3<float> tabp, Phys ph,
                                                          const unsigned char* __restrict__ a_image) {
   constexpr int NC = Phys::NC;
-  using S = TcShape<P, NC>;
+  using S = TcShape<P, NC, Op>;
   constexpr int NP = S::NP, NFP = S::NFP, KV = S::KV, KF = S::KF, NN = S::NN, M = S::M, NPO = S::NPO;
   constexpr int EC = S::EC, EB = S::EB, EBP = S::EBP, QV = EB * NP * NC;
-  constexpr uint32_t LBO_A = NN * 16, LBO_B = M * 16, SBO = 128;
-  constexpr uint32_t CSTRIDE = EBP * 16;  // byte step between the rows of consecutive components
-  constexpr uint32_t IDESC = umma_idesc_bf16_f32_amn(M, NN);
-  static_assert(NN % 16 == 0 && NN <= 256 && KV % 16 == 0 && KF % 16 == 0 && EC >= 1 && EBP * NC <= M,
+  // LBO of the K-major operator image and of the MN-major flux tile; the
+  // start-address step of one MMA K step in each
+  constexpr uint32_t LBO_A = NN * 16, LBO_B = (M / Op::CM) * 128, SBO = 128;
+  constexpr uint32_t KSTEP_A = (Op::KSTEP / Op::CM) * LBO_A, KSTEP_B = (Op::KSTEP / 8) * LBO_B;
+  constexpr uint32_t CSTRIDE = (EBP / Op::CM) * 128;  // byte step between the rows of consecutive components
+  constexpr uint32_t IDESC = umma_idesc_f32acc_amn<Op>(M, NN);
+  static_assert(NN % 16 == 0 && NN <= 256 && KV % Op::KSTEP == 0 && KF % Op::KSTEP == 0 && EC >= 1 &&
+                    EBP * NC <= M && EBP % Op::CM == 0,
                 "UMMA shape");
   extern __shared__ __align__(1024) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);  // [0..1] q tiles, [2] mma, [3] A image
@@ -202,14 +199,9 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
   };
   // store the NC operand values v[c] of row (c, el), column k as bf16 hi / lo
   auto put = [&](int el, int k, const float* v) {
-    const uint32_t off = umma_mn_offset(el, k, M);
+    const uint32_t off = umma_mn_off<Op>(el, k, M);
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      __nv_bfloat16 h, l;
-      split_bf16(v[c], h, l);
-      *reinterpret_cast<__nv_bfloat16*>(sBhi + off + c * CSTRIDE) = h;
-      *reinterpret_cast<__nv_bfloat16*>(sBlo + off + c * CSTRIDE) = l;
-    }
+    for (int c = 0; c < NC; ++c) Op::put1(sBhi + off + c * CSTRIDE, sBlo + off + c * CSTRIDE, v[c]);
   };
   // bit b: phase parity / copy in flight of tile buffer b (scalars, so they
   // stay in registers)
@@ -229,12 +221,12 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
       const uint32_t ah = smem_u32(sAhi), al = smem_u32(sAlo), bh = smem_u32(sBhi), bl = smem_u32(sBlo);
 #pragma unroll 1
       for (int ks = 0; ks < nks; ++ks) {
-        const uint32_t oa = uint32_t(ka0 + ks) * 2 * LBO_A, ob = uint32_t(ks) * 2 * LBO_B;
+        const uint32_t oa = uint32_t(ka0 + ks) * KSTEP_A, ob = uint32_t(ks) * KSTEP_B;
         const uint64_t dAh = umma_desc(ah + oa, LBO_A, SBO), dAl = umma_desc(al + oa, LBO_A, SBO);
         const uint64_t dBh = umma_desc(bh + ob, LBO_B, SBO), dBl = umma_desc(bl + ob, LBO_B, SBO);
-        tc_mma_bf16(tmem, dBh, dAh, IDESC, (ka0 + ks) > 0 ? 1u : 0u);
-        tc_mma_bf16(tmem, dBh, dAl, IDESC, 1u);
-        tc_mma_bf16(tmem, dBl, dAh, IDESC, 1u);
+        Op::mma(tmem, dBh, dAh, IDESC, (ka0 + ks) > 0 ? 1u : 0u);
+        Op::mma(tmem, dBh, dAl, IDESC, 1u);
+        Op::mma(tmem, dBl, dAh, IDESC, 1u);
       }
       tc_commit(&bar[2]);
     }
@@ -377,15 +369,12 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
       const float* iJb = tab->invJ[t1];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const uint32_t off = umma_mn_offset(el, d * NP + j, M);
+        const uint32_t off = umma_mn_off<Op>(el, d * NP + j, M);
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           const float va = iJa[d * 3 + 0] * Fa[c] + iJa[d * 3 + 1] * Fa[NC + c] + iJa[d * 3 + 2] * Fa[2 * NC + c];
           const float vb = iJb[d * 3 + 0] * Fb[c] + iJb[d * 3 + 1] * Fb[NC + c] + iJb[d * 3 + 2] * Fb[2 * NC + c];
-          uint32_t h, l;
-          split_bf16x2(va, vb, h, l);
-          *reinterpret_cast<uint32_t*>(sBhi + off + c * CSTRIDE) = h;
-          *reinterpret_cast<uint32_t*>(sBlo + off + c * CSTRIDE) = l;
+          Op::put2(sBhi + off + c * CSTRIDE, sBlo + off + c * CSTRIDE, va, vb);
         }
       }
     }
@@ -533,10 +522,11 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P>()) stage3d_tc_kerne
       break;
     }
     {  // warp w reads TMEM lanes [32 (w % 4), +32) (rows (c, el)), columns
-       // [16 (w / 4), +16) of every 32 (16 at a time: bounded registers)
+       // [16 (w / 4), +16) of every 16 (NT / 128) (16 at a time: bounded
+       // registers)
       const int row = (warp & 3) * 32 + lane;
 #pragma unroll
-      for (int c0 = (warp >> 2) * 16; c0 < NN; c0 += 32) {
+      for (int c0 = (warp >> 2) * 16; c0 < NN; c0 += 16 * (NT / 128)) {
         float v[16];
         tmem_ld16(tmem + (uint32_t((warp & 3) * 32) << 16) + c0, v);
         tmem_ld_wait();

@@ -102,4 +102,101 @@ __device__ __forceinline__ void split_bf16x2(float a, float b, uint32_t& hi, uin
   lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
+// x = hi + lo with hi, lo rounded to TF32 (11 significant bits, round to
+// nearest, ties away from zero: cvt.rna.tf32.f32); x - hi is exact in FP32,
+// so hi + lo carries 22 significant bits of x.
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = to_tf32(x);
+  lo = to_tf32(x - __uint_as_float(hi));
+}
+
+__device__ __forceinline__ void tc_mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+// Operand kinds of the split-precision contraction.  Both keep a value as
+// hi + lo and form hi*hi + hi*lo + lo*hi in FP32 (three MMAs into one
+// accumulator).  ELEM: bytes per operand element; KSTEP: K of one MMA;
+// CM: elements in the 16 contiguous bytes of a core-matrix row; FMT: the
+// A / B format code of the instruction descriptor.
+//  * OpBF16 (kind::f16): 8 + 8 significant bits, relative error ~2^-16;
+//  * OpTF32 (kind::tf32): 11 + 11 significant bits, relative error ~2^-22,
+//    twice the shared memory per operand.
+struct OpBF16 {
+  static constexpr int ELEM = 2, KSTEP = 16, CM = 8;
+  static constexpr uint32_t FMT = 1;
+  __device__ static void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    tc_mma_bf16(d, a, b, idesc, acc);
+  }
+  // one value: hi at ph, lo at pl
+  __device__ static void put1(unsigned char* ph, unsigned char* pl, float v) {
+    __nv_bfloat16 h, l;
+    split_bf16(v, h, l);
+    *reinterpret_cast<__nv_bfloat16*>(ph) = h;
+    *reinterpret_cast<__nv_bfloat16*>(pl) = l;
+  }
+  // two MN-adjacent values (rows r, r + 1 of one k; r even)
+  __device__ static void put2(unsigned char* ph, unsigned char* pl, float a, float b) {
+    uint32_t h, l;
+    split_bf16x2(a, b, h, l);
+    *reinterpret_cast<uint32_t*>(ph) = h;
+    *reinterpret_cast<uint32_t*>(pl) = l;
+  }
+};
+struct OpTF32 {
+  static constexpr int ELEM = 4, KSTEP = 8, CM = 4;
+  static constexpr uint32_t FMT = 2;
+  __device__ static void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    tc_mma_tf32(d, a, b, idesc, acc);
+  }
+  __device__ static void put1(unsigned char* ph, unsigned char* pl, float v) {
+    uint32_t h, l;
+    split_tf32(v, h, l);
+    *reinterpret_cast<uint32_t*>(ph) = h;
+    *reinterpret_cast<uint32_t*>(pl) = l;
+  }
+  __device__ static void put2(unsigned char* ph, unsigned char* pl, float a, float b) {
+    uint2 h, l;
+    split_tf32(a, h.x, l.x);
+    split_tf32(b, h.y, l.y);
+    *reinterpret_cast<uint2*>(ph) = h;
+    *reinterpret_cast<uint2*>(pl) = l;
+  }
+};
+
+// Instruction descriptor: FP32 accumulator, A and B of format Op::FMT, A
+// (the M side) MN-major, B K-major.
+template <class Op>
+__host__ __device__ constexpr uint32_t umma_idesc_f32acc_amn(int M, int N) {
+  return (1u << 4) | (Op::FMT << 7) | (Op::FMT << 10) | (1u << 15) | (uint32_t(N >> 3) << 17) |
+         (uint32_t(M >> 4) << 24);
+}
+
+// No-swizzle core-matrix layouts (8 rows of 16 bytes per core matrix):
+// MN-major `rows` x K tile: CM consecutive rows of one k in 16 bytes, the 8
+// k of a core matrix 16 bytes apart, core matrices along the rows 128 bytes
+// apart (SBO), along K rows/CM * 128 bytes apart (LBO);
+template <class Op>
+__host__ __device__ constexpr uint32_t umma_mn_off(int row, int k, int rows) {
+  return uint32_t((k >> 3) * (rows / Op::CM) * 128 + (row / Op::CM) * 128 + (k & 7) * 16 + (row % Op::CM) * Op::ELEM);
+}
+// K-major `nn` x K tile: CM consecutive k of one row in 16 bytes, the 8 rows
+// of a core matrix 16 bytes apart, core matrices along the rows 128 bytes
+// apart (SBO), along K nn/8 * 128 bytes apart (LBO).
+template <class Op>
+__host__ __device__ constexpr uint32_t umma_k_off(int n, int k, int nn) {
+  return uint32_t((k / Op::CM) * (nn >> 3) * 128 + (n >> 3) * 128 + (n & 7) * 16 + (k % Op::CM) * Op::ELEM);
+}
+
 }  // namespace mxm

@@ -87,10 +87,10 @@ def test_c2_rhs_and_stage_vs_oracle(oracle_mod, prec):
     s.close()
 
 
-C3_RHS = {"f64": (1e-13, 2e-13), "mixed": (2e-5, 5e-5)}
+C3_RHS = {"f64": (1e-13, 2e-13), "mixed": (2e-5, 5e-5), "tf32": (2e-6, 5e-6)}
 
 
-@pytest.mark.parametrize("prec", ["f64", "mixed"])
+@pytest.mark.parametrize("prec", ["f64", "mixed", "tf32"])
 def test_c3_maxwell_rhs_vs_oracle(oracle_mod, prec):
     n, P = 24, 4
     bcs = (1, 1, 1, 1, 0, 0)
