@@ -12,7 +12,9 @@ cudaError_t launch_tc_p(const Stage3DArgs<float>& a, const KuhnTab3<float>& tab,
   if constexpr (!S::FITS) {
     return cudaErrorInvalidValue;  // the create call refuses these shapes
   } else {
-    constexpr int NT = 256;
+    // 256 threads per block; a shape that fits one block per SM (the
+    // split-TF32 P4 tiles) takes 512 so that the SM still holds 16 warps
+    constexpr int NT = S::blocks_for(S::SMEM) == 1 ? 512 : 256;
     auto kern = stage3d_tc_kernel<Phys, P, NT, Op>;
     static int bps = -1;
     if (bps < 0) {

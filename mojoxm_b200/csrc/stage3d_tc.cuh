@@ -8,8 +8,9 @@
 //     RHS^T[(c,el), i] = sum_k  B^T[(c,el), k] * A[i, k]
 // so one 128-row MMA tile covers the (component, element) pairs of a tile
 // against the shared operator A (N = NP rounded up to 16, K = 3NP + 4NFP
-// rounded up to 16).  Operands are split x = hi + lo in bfloat16 and the
-// product is hi*hi + hi*lo + lo*hi (three MMAs into one FP32 accumulator).
+// rounded up to the MMA K step).  Operands are split x = hi + lo in
+// bfloat16 (kind::f16) or TF32 (kind::tf32) and the product is
+// hi*hi + hi*lo + lo*hi (three MMAs into one FP32 accumulator).
 //
 // Accuracy: before splitting, every element subtracts its own constant flux
 // Fbar = F(q at node 0) from its volume fluxes and Fbar.n from its face
@@ -19,8 +20,9 @@
 // cancellation error of the O(|F|/h) terms -- shrink to the flux variation
 // across the element.
 //
-// Layout: the (c,el) x K operand is MN-major (8 consecutive rows of one k in
-// 16 bytes).  Work is mapped element-fastest: 8 consecutive threads take 8
+// Layout: the (c,el) x K operand is MN-major for split-BF16 (8 consecutive
+// rows of one k in 16 bytes) and K-major for split-TF32 (4 consecutive k of
+// one row in 16 bytes).  Work is mapped element-fastest: 8 consecutive threads take 8
 // consecutive elements at the same node, so a warp's operand stores land in
 // one or two 128-byte core matrices.  Faces are walked through a per-cube
 // work list (every cube-boundary face, and each face inside the cube once,
@@ -117,12 +119,14 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
   using S = TcShape<P, NC, Op>;
   constexpr int NP = S::NP, NFP = S::NFP, KV = S::KV, KF = S::KF, NN = S::NN, M = S::M, NPO = S::NPO;
   constexpr int EC = S::EC, EB = S::EB, EBP = S::EBP, QV = EB * NP * NC;
-  // LBO of the K-major operator image and of the MN-major flux tile; the
-  // start-address step of one MMA K step in each
-  constexpr uint32_t LBO_A = NN * 16, LBO_B = (M / Op::CM) * 128, SBO = 128;
-  constexpr uint32_t KSTEP_A = (Op::KSTEP / Op::CM) * LBO_A, KSTEP_B = (Op::KSTEP / 8) * LBO_B;
-  constexpr uint32_t CSTRIDE = (EBP / Op::CM) * 128;  // byte step between the rows of consecutive components
-  constexpr uint32_t IDESC = umma_idesc_f32acc_amn<Op>(M, NN);
+  // LBO of the K-major operator image and of the flux tile (MN-major for
+  // split-BF16, K-major for split-TF32); the start-address step of one MMA
+  // K step in each
+  constexpr uint32_t LBO_A = NN * 16, LBO_B = umma_a_lbo<Op>(M), SBO = 128;
+  constexpr uint32_t KSTEP_A = (Op::KSTEP / Op::CM) * LBO_A, KSTEP_B = umma_a_kstep<Op>(M);
+  // byte step between the rows of consecutive components (EBP rows apart)
+  constexpr uint32_t CSTRIDE = (EBP / (Op::A_MN ? Op::CM : 8)) * 128;
+  constexpr uint32_t IDESC = umma_idesc_f32acc<Op>(M, NN);
   static_assert(NN % 16 == 0 && NN <= 256 && KV % Op::KSTEP == 0 && KF % Op::KSTEP == 0 && EC >= 1 &&
                     EBP * NC <= M && EBP % Op::CM == 0,
                 "UMMA shape");
@@ -199,7 +203,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
   };
   // store the NC operand values v[c] of row (c, el), column k as bf16 hi / lo
   auto put = [&](int el, int k, const float* v) {
-    const uint32_t off = umma_mn_off<Op>(el, k, M);
+    const uint32_t off = umma_a_off<Op>(el, k, M);
 #pragma unroll
     for (int c = 0; c < NC; ++c) Op::put1(sBhi + off + c * CSTRIDE, sBlo + off + c * CSTRIDE, v[c]);
   };
@@ -369,12 +373,17 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
       const float* iJb = tab->invJ[t1];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const uint32_t off = umma_mn_off<Op>(el, d * NP + j, M);
+        const uint32_t off = umma_a_off<Op>(el, d * NP + j, M);
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           const float va = iJa[d * 3 + 0] * Fa[c] + iJa[d * 3 + 1] * Fa[NC + c] + iJa[d * 3 + 2] * Fa[2 * NC + c];
           const float vb = iJb[d * 3 + 0] * Fb[c] + iJb[d * 3 + 1] * Fb[NC + c] + iJb[d * 3 + 2] * Fb[2 * NC + c];
-          Op::put2(sBhi + off + c * CSTRIDE, sBlo + off + c * CSTRIDE, va, vb);
+          if constexpr (Op::A_MN) {
+            Op::put2(sBhi + off + c * CSTRIDE, sBlo + off + c * CSTRIDE, va, vb);
+          } else {  // K-major: row el + 1 lies 16 bytes on, in the same core matrix (el even)
+            Op::put1(sBhi + off + c * CSTRIDE, sBlo + off + c * CSTRIDE, va);
+            Op::put1(sBhi + off + 16 + c * CSTRIDE, sBlo + off + 16 + c * CSTRIDE, vb);
+          }
         }
       }
     }
@@ -474,7 +483,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
     // [0, KV).  While those MMAs run, each thread evaluates its first face
     // item into registers; the operand columns are overwritten only after
     // the MMAs completed.
-    mma_issue(0, KV / 16);
+    mma_issue(0, KV / Op::KSTEP);
     int e1 = 0, k1 = 0, e2 = 0, k2 = 0;
     float v1[NC], v2[NC];
     const int nfirst = tid < nface_items ? face_item(tid, e1, k1, v1, e2, k2, v2) : 0;
@@ -490,7 +499,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
       if (n == 2) put(e2, k2, v2);
     }
     // face half of K: operand columns [0, KF) against operator columns [KV, KV + KF)
-    mma_issue(KV / 16, KF / 16);
+    mma_issue(KV / Op::KSTEP, KF / Op::KSTEP);
     // while the face MMAs run: the next tile's wait and Fbar phase (its
     // copy was issued a whole tile earlier) ...
     fb_ready = false;

@@ -130,11 +130,14 @@ __device__ __forceinline__ void tc_mma_tf32(uint32_t tmem_d, uint64_t adesc, uin
 // accumulator).  ELEM: bytes per operand element; KSTEP: K of one MMA;
 // CM: elements in the 16 contiguous bytes of a core-matrix row; FMT: the
 // A / B format code of the instruction descriptor.
+// A_MN: whether the flux tile (the MMA's A operand) is stored MN-major.
 //  * OpBF16 (kind::f16): 8 + 8 significant bits, relative error ~2^-16;
+//    MN-major flux tile (two elements of one k share a 4-byte word);
 //  * OpTF32 (kind::tf32): 11 + 11 significant bits, relative error ~2^-22,
-//    twice the shared memory per operand.
+//    twice the shared memory per operand; both operands K-major.
 struct OpBF16 {
   static constexpr int ELEM = 2, KSTEP = 16, CM = 8;
+  static constexpr bool A_MN = true;
   static constexpr uint32_t FMT = 1;
   __device__ static void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     tc_mma_bf16(d, a, b, idesc, acc);
@@ -156,6 +159,7 @@ struct OpBF16 {
 };
 struct OpTF32 {
   static constexpr int ELEM = 4, KSTEP = 8, CM = 4;
+  static constexpr bool A_MN = false;
   static constexpr uint32_t FMT = 2;
   __device__ static void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     tc_mma_tf32(d, a, b, idesc, acc);
@@ -176,10 +180,10 @@ struct OpTF32 {
 };
 
 // Instruction descriptor: FP32 accumulator, A and B of format Op::FMT, A
-// (the M side) MN-major, B K-major.
+// (the M side) MN-major when Op::A_MN, B K-major.
 template <class Op>
-__host__ __device__ constexpr uint32_t umma_idesc_f32acc_amn(int M, int N) {
-  return (1u << 4) | (Op::FMT << 7) | (Op::FMT << 10) | (1u << 15) | (uint32_t(N >> 3) << 17) |
+__host__ __device__ constexpr uint32_t umma_idesc_f32acc(int M, int N) {
+  return (1u << 4) | (Op::FMT << 7) | (Op::FMT << 10) | ((Op::A_MN ? 1u : 0u) << 15) | (uint32_t(N >> 3) << 17) |
          (uint32_t(M >> 4) << 24);
 }
 
@@ -197,6 +201,20 @@ __host__ __device__ constexpr uint32_t umma_mn_off(int row, int k, int rows) {
 template <class Op>
 __host__ __device__ constexpr uint32_t umma_k_off(int n, int k, int nn) {
   return uint32_t((k / Op::CM) * (nn >> 3) * 128 + (n >> 3) * 128 + (n & 7) * 16 + (k % Op::CM) * Op::ELEM);
+}
+// The flux tile (`rows` x K, the MMA's A operand) in Op's layout, its LBO
+// and the start-address step of one MMA K step.
+template <class Op>
+__host__ __device__ constexpr uint32_t umma_a_off(int row, int k, int rows) {
+  return Op::A_MN ? umma_mn_off<Op>(row, k, rows) : umma_k_off<Op>(row, k, rows);
+}
+template <class Op>
+__host__ __device__ constexpr uint32_t umma_a_lbo(int rows) {
+  return Op::A_MN ? uint32_t(rows / Op::CM) * 128 : uint32_t(rows / 8) * 128;
+}
+template <class Op>
+__host__ __device__ constexpr uint32_t umma_a_kstep(int rows) {
+  return Op::A_MN ? uint32_t(Op::KSTEP / 8) * umma_a_lbo<Op>(rows) : uint32_t(Op::KSTEP / Op::CM) * umma_a_lbo<Op>(rows);
 }
 
 }  // namespace mxm

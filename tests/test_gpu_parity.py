@@ -156,7 +156,7 @@ TOL_MIXED_P = {2: TOL_MIXED, 3: TOL_MIXED, 4: TOL_MIXED, 5: 2e-3}
 # arithmetic in the fluxes (the FP32 SIMT kernel's own level on these
 # random states) rather than of the operand split.  P = 5 runs the FP32
 # kernel (its TF32 operands exceed a block's shared memory).
-TOL_TF32 = {2: 5e-5, 3: 5e-5, 4: 5e-5, 5: 5e-5}
+TOL_TF32 = {2: 5e-6, 3: 5e-6, 4: 5e-6, 5: 5e-6}
 
 
 @pytest.mark.parametrize("prec", ["mixed", "tf32"])
