@@ -9,10 +9,11 @@
 // only, BC self-neighbours skipped, applied to every component.
 //
 // B200 form: pass 1 computes cell means with one thread per (element,
-// component) over coalesced loads; pass 2 stages a group of elements' nodal
-// values in shared memory with contiguous loads, reduces theta per element
-// with warp shuffles, and writes the limited values back contiguously only
-// for elements with theta < 1.
+// component) over coalesced loads; pass 2 (3D) stages a group of elements'
+// nodal values in shared memory with contiguous loads, reduces theta per
+// element with warp shuffles, and writes the limited values back
+// contiguously only for elements with theta < 1; pass 2 (2D) runs
+// node-parallel over a chunk of elements (theta2d_block).
 #pragma once
 #include "dg_common.cuh"
 
@@ -125,90 +126,103 @@ __global__ void __launch_bounds__(32 * EPB) theta_apply_kernel(LimArgs<R> a, Kuh
   }
 }
 
-// 2D theta + apply for one element (component 0 decides theta, faces whose
-// neighbour resolves to the element itself -- BC faces -- do not constrain,
-// theta scales every component's deviation from its cell mean), on the
-// element's values `row` (NP nodes x NC, node stride NC).  Same arithmetic
-// as the reference's 2D kernels; *changed = 1 when the row was rewritten.
-template <class R, int NP, int NC>
-__device__ __forceinline__ void theta2d_elem_row(R* row, const R* avg, int64_t e, const KuhnTab2<R>& tab, int nx,
-                                                 int ny, const int* bc, R eps2, int* changed) {
-  const int t = int(e & 1);
-  const int64_t cell = e >> 1;
-  const int cj = int(cell / nx), ci = int(cell - int64_t(cj) * nx);
-  const R own = avg[e * NC];
-  R lo = own, hi = own;
-#pragma unroll
-  for (int lf = 0; lf < 3; ++lf) {
-    const int ax = tab.axis[t][lf], dir = tab.dir[t][lf];
-    int code;
-    const int mode = face_mode(ax, dir, ax == 0 ? ci : cj, ax == 0 ? nx : ny, bc, code);
-    if (mode != FACE_INTERIOR && mode != FACE_MIXED) continue;
-    const int ni = wrapi(ci + tab.off[t][lf][0], nx), nj = wrapi(cj + tab.off[t][lf][1], ny);
-    const int64_t nb = (int64_t(nj) * nx + ni) * 2 + tab.nb_t[t][lf];
-    if (nb == e) continue;
-    const R v = avg[nb * NC];
-    if (v < lo) lo = v;
-    if (v > hi) hi = v;
-  }
-  R th = R(1);
-  const R tiny = R(1.0e-30);
-#pragma unroll 4
-  for (int n = 0; n < NP; ++n) {
-    const R dl = row[n * NC] - own;
-    const R da = dl >= R(0) ? dl : -dl;
-    if (da <= tiny) continue;
-    R pD = hi - own;
-    if (pD < R(0)) pD = R(0);
-    R nD = own - lo;
-    if (nD < R(0)) nD = R(0);
-    const R D = dl > R(0) ? pD : nD;
-    const R D2 = D * D, d2 = da * da, Dd = D * da;
-    const R al = (D2 + R(2) * Dd + eps2) / (D2 + R(2) * d2 + Dd + eps2);
-    if (al < th) th = al;
-  }
-  *changed = th < R(1) ? 1 : 0;
-  if (!(th < R(1))) return;
-  R bm[NC];
-#pragma unroll
-  for (int c = 0; c < NC; ++c) bm[c] = avg[e * NC + c];
-  for (int n = 0; n < NP; ++n)
-#pragma unroll
-    for (int c = 0; c < NC; ++c) row[n * NC + c] = bm[c] + th * (row[n * NC + c] - bm[c]);
-}
-
-// A block of 128 threads limits 128 consecutive elements: their values are
-// staged into shared memory with coalesced loads (row stride VALS | 1, so
-// the per-element reads hit distinct banks), each thread runs
-// theta2d_elem_row on its element's row, and rows that changed go back with coalesced
-// stores.  kLim2dBlock elements per block; dynamic shared memory
-// lim2d_smem_bytes<R, NP, NC>().
+// A block of kLim2dBlock threads limits up to kLim2dBlock consecutive
+// elements, node-parallel: (1) one thread per element resolves its cell
+// mean and the neighbours' bounds (component 0; BC faces skipped); (2) one
+// thread per (element, node) evaluates the Barth-Jespersen / Venkatakrishnan
+// ratio of its node and folds it into the element's theta with a shared
+// atomic minimum on the value's bits (non-negative IEEE values order like
+// their unsigned bit patterns, and a minimum is exact in any order, so theta
+// equals the reference's sequential minimum bit for bit); (3) one thread per
+// value rewrites the values of elements with theta < 1.  Loads and stores
+// run over consecutive values of the chunk.  The arithmetic is the
+// reference's 2D limiter (src/local_mesh_2d_gpu_limiter.mojo:74-153): theta
+// from component 0, faces whose neighbour resolves to the element itself
+// (BC faces) do not constrain, theta scales every component's deviation from
+// its cell mean.  Dynamic shared memory lim2d_smem_bytes<R, NP, NC>().
 constexpr int kLim2dBlock = 128;
 template <class R, int NP, int NC>
 constexpr size_t lim2d_smem_bytes() {
-  return size_t(kLim2dBlock) * ((NP * NC) | 1) * sizeof(R) + kLim2dBlock * sizeof(int);
+  return size_t(kLim2dBlock) * (3 * sizeof(R) + sizeof(unsigned long long));
 }
+
+template <class R>
+struct ThetaBits;  // theta as an unsigned integer of the same width
+template <>
+struct ThetaBits<float> {
+  using U = unsigned int;
+  __device__ static U to(float v) { return __float_as_uint(v); }
+  __device__ static float from(U u) { return __uint_as_float(u); }
+};
+template <>
+struct ThetaBits<double> {
+  using U = unsigned long long;
+  __device__ static U to(double v) { return (unsigned long long)__double_as_longlong(v); }
+  __device__ static double from(U u) { return __longlong_as_double((long long)u); }
+};
 
 template <class R, int NP, int NC>
 __device__ __forceinline__ void theta2d_block(R* q, const R* avg, int64_t e0, int ne, const KuhnTab2<R>& tab, int nx,
                                               int ny, const int* bc, R eps2, unsigned char* smem) {
-  constexpr int VALS = NP * NC, VS = VALS | 1;
-  R* sq = reinterpret_cast<R*>(smem);
-  int* changed = reinterpret_cast<int*>(smem + size_t(kLim2dBlock) * VS * sizeof(R));
+  constexpr int VALS = NP * NC;
+  using TB = ThetaBits<R>;
+  using U = typename TB::U;
+  U* s_th = reinterpret_cast<U*>(smem);  // 8-byte aligned first
+  R* s_own = reinterpret_cast<R*>(smem + size_t(kLim2dBlock) * sizeof(unsigned long long));
+  R* s_lo = s_own + kLim2dBlock;
+  R* s_hi = s_lo + kLim2dBlock;
   const int tid = threadIdx.x;
+  if (tid < ne) {  // the element's cell mean and its interior neighbours' bounds
+    const int64_t e = e0 + tid;
+    const int t = int(e & 1);
+    const int64_t cell = e >> 1;
+    const int cj = int(cell / nx), ci = int(cell - int64_t(cj) * nx);
+    const R own = avg[e * NC];
+    R lo = own, hi = own;
+#pragma unroll
+    for (int lf = 0; lf < 3; ++lf) {
+      const int ax = tab.axis[t][lf], dir = tab.dir[t][lf];
+      int code;
+      const int mode = face_mode(ax, dir, ax == 0 ? ci : cj, ax == 0 ? nx : ny, bc, code);
+      if (mode != FACE_INTERIOR && mode != FACE_MIXED) continue;
+      const int ni = wrapi(ci + tab.off[t][lf][0], nx), nj = wrapi(cj + tab.off[t][lf][1], ny);
+      const int64_t nb = (int64_t(nj) * nx + ni) * 2 + tab.nb_t[t][lf];
+      if (nb == e) continue;
+      const R v = avg[nb * NC];
+      if (v < lo) lo = v;
+      if (v > hi) hi = v;
+    }
+    s_own[tid] = own;
+    s_lo[tid] = lo;
+    s_hi[tid] = hi;
+    s_th[tid] = TB::to(R(1));
+  }
+  __syncthreads();
   R* base = q + e0 * VALS;
-  for (int idx = tid; idx < ne * VALS; idx += blockDim.x) {
-    const int el = idx / VALS;
-    sq[el * VS + (idx - el * VALS)] = base[idx];
+  const R tiny = R(1.0e-30);
+  for (int idx = tid; idx < ne * NP; idx += blockDim.x) {
+    const int el = idx / NP;
+    const R own = s_own[el];
+    const R dl = base[size_t(idx) * NC] - own;  // component 0 of node idx - el NP of element el
+    const R da = dl >= R(0) ? dl : -dl;
+    if (da <= tiny) continue;
+    R pD = s_hi[el] - own;
+    if (pD < R(0)) pD = R(0);
+    R nD = own - s_lo[el];
+    if (nD < R(0)) nD = R(0);
+    const R D = dl > R(0) ? pD : nD;
+    const R D2 = D * D, d2 = da * da, Dd = D * da;
+    const R al = (D2 + R(2) * Dd + eps2) / (D2 + R(2) * d2 + Dd + eps2);
+    if (al < R(1)) atomicMin(&s_th[el], TB::to(al));
   }
   __syncthreads();
-  if (tid < ne) {  // the element's cell means and its neighbours' from global memory
-    theta2d_elem_row<R, NP, NC>(sq + tid * VS, avg, e0 + tid, tab, nx, ny, bc, eps2, changed + tid);
-  }
-  __syncthreads();
   for (int idx = tid; idx < ne * VALS; idx += blockDim.x) {
     const int el = idx / VALS;
-    if (changed[el]) base[idx] = sq[el * VS + (idx - el * VALS)];
+    const R th = TB::from(s_th[el]);
+    if (!(th < R(1))) continue;
+    const int c = (idx - el * VALS) % NC;
+    const R bm = avg[(e0 + el) * NC + c];
+    base[idx] = bm + th * (base[idx] - bm);
   }
 }
 
