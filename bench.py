@@ -112,10 +112,14 @@ def parse():
                     help="SSPRK3 steps of the accuracy check vs the FP64 path (0 = skip)")
     ap.add_argument("--batch-solves", type=int, default=512, help="batched 2D leg: solves (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=10)
-    ap.add_argument("--serve-requests", type=int, default=32, help="served leg: requests (0 = skip)")
+    ap.add_argument("--serve-requests", type=int, default=500, help="served leg: requests (0 = skip)")
     ap.add_argument("--serve-lambda", type=float, default=200.0)
-    ap.add_argument("--serve-largest", action="store_true", help="add the 48^3x6 limited Sod P5 request")
+    ap.add_argument("--serve-largest", type=int, default=1, help="add the 48^3x6 limited Sod P5 request (1/0)")
     ap.add_argument("--serve-slots", type=int, default=8, help="solves running at once in the served leg")
+    ap.add_argument("--serve-low-seconds", type=float, default=25.0,
+                    help="served leg at half the measured capacity: seconds of arrivals (0 = skip)")
+    ap.add_argument("--serve-f64-requests", type=int, default=100,
+                    help="requests of the stream replayed in FP64 for the plain comparison (0 = skip)")
     ap.add_argument("--cavity", type=int, default=1, help="run the 24^3x6 P=4 Maxwell cavity leg (1/0)")
     ap.add_argument("--mhd", type=int, default=1, help="run the 3D ideal-MHD Alfven-wave leg (1/0)")
     ap.add_argument("--slab-parts", type=int, default=4, help="z-slab decomposition leg on one GPU (0 = skip)")
@@ -620,20 +624,26 @@ def slab_decomposed(M, a, parts, steps=20):
             "timing": "CUDA events (the group's events bracket all parts' streams)"}
 
 
-def served(M, nreq, lam, seed=7, largest=False, slots=8, precision=None):
-    """Served stream: Poisson arrivals at `lam`/s of 2D/3D Euler, 2D
-    shallow-water dam breaks and 3D Maxwell plane waves, 2k-400k elements
-    (log-uniform), P in 2..5, 50-500 SSPRK3 steps, seeded ICs, admitted by a
-    150 GB HBM budget; `largest` adds the 3D limited Sod at P=5 on 48^3 x 6
-    tets (50 steps).  `precision` replaces every request's precision (the
-    plain FP64 comparison replays the same stream in "f64")."""
+SERVED_KINDS = ("euler2d_vortex", "euler3d_wave", "dam_break", "maxwell3d_plane_wave", "euler3d_sod_limited")
+
+
+def served_requests(M, nreq, seed=7, largest=True, precision=None):
+    """The served stream's requests, drawn from `seed`: 2D Euler vortices,
+    3D Euler smooth waves, 2D shallow-water dam breaks (h_left ~ U[1,3],
+    h_right = 1), 3D Maxwell plane waves and 3D limited Sod tubes (HLLEC,
+    BJ limiter, outflow x, walls y/z, left / right rho, p ~ U[0.1, 1]), each
+    with 2k-400k elements (log-uniform), P in 2..5 and 50-500 SSPRK3 steps;
+    `largest` adds, at a seeded position, the 3D limited Sod at P = 5 on
+    48^3 x 6 = 663,552 tets (50 steps).  `precision` replaces every
+    request's own (the FP64 comparison).  Returns [(kind, submit args)]."""
     rng = np.random.default_rng(seed)
     reqs = []
     for k in range(nreq):
-        kind = int(rng.integers(0, 4))
+        kind = int(rng.integers(0, len(SERVED_KINDS)))
         E = float(np.exp(rng.uniform(np.log(2e3), np.log(4e5))))
         P = int(rng.integers(2, 6))
         nsteps = int(rng.integers(50, 501))
+        lim = None
         if kind == 0:  # 2D Euler vortex
             n = max(4, int(round(np.sqrt(E / 2))))
             mesh = M.Mesh(n, n, 1, 10.0, 10.0, 1.0, dim=2)
@@ -653,26 +663,38 @@ def served(M, nreq, lam, seed=7, largest=False, slots=8, precision=None):
             hl = rng.uniform(1, 3)
             ic, prm, lam_est, h = M.IC_DAM_BREAK, [hl, 1.0, 0.5, 2.0 / n], 2 * np.sqrt(9.81 * hl), 1.0 / n
             prec = "f32"
-        else:  # 3D Maxwell plane wave
+        elif kind == 3:  # 3D Maxwell plane wave
             n = max(2, int(round((E / 6) ** (1 / 3))))
             mesh = M.Mesh(n, n, n)
             phys = M.Maxwell(1.0, *([0.0] * 12))
             ic, prm, lam_est, h = M.IC_PLANE_WAVE, [1.0, 1.0], 1.0, 1.0 / n
             prec = "mixed"
+        else:  # 3D limited Sod tube
+            n = max(2, int(round((E / 6) ** (1 / 3))))
+            mesh = M.Mesh(n, n, n, bcs=M.BoundaryConditions(2, 2, 1, 1, 1, 1))
+            phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_HLLEC, False)
+            rl, pl, rr, pr = rng.uniform(0.1, 1.0, 4)
+            ic, prm, h = M.IC_SOD, [rl, pl, rr, pr, 0.5, 1.0 / n], 1.0 / n
+            lam_est = np.sqrt(GAMMA * max(pl, pr) / min(rl, rr)) + 1.0
+            prec, lim = "mixed", 0.1
         dt = 0.1 * h / (lam_est * (2 * P + 1))
-        reqs.append((mesh, phys, P, precision or prec, ic, prm, dt, nsteps, None))
+        reqs.append((SERVED_KINDS[kind], (mesh, phys, P, precision or prec, ic, prm, dt, nsteps, lim)))
     if largest:
         mesh = M.Mesh(48, 48, 48, bcs=M.BoundaryConditions(2, 2, 1, 1, 1, 1))
         phys = M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_HLLEC, False)
-        reqs.append((mesh, phys, 5, precision or "f32", M.IC_SOD, [1.0, 1.0, 0.125, 0.1, 0.5, 1.0 / 48], 0.1 / 48 / (2.5 * 11),
-                     50, 0.1))
-    gaps = rng.exponential(1.0 / lam, len(reqs))
-    # warm-up (untimed): one tiny request of every (physics, order, precision)
-    # the stream uses, so module loading and first-launch set-up of each
-    # kernel happen before the timed stream
-    warm, seen = M.Server(hbm_budget_bytes=150e9, max_active=slots, steps_per_chunk=10), set()
-    wids = []
-    for mesh, phys, P, prec, ic, prm, dt, nsteps, lim in reqs:
+        big = ("largest_euler3d_sod_limited_P5",
+               (mesh, phys, 5, precision or "mixed", M.IC_SOD, [1.0, 1.0, 0.125, 0.1, 0.5, 1.0 / 48],
+                0.1 / 48 / (2.5 * 11), 50, 0.1))
+        reqs.insert(int(rng.integers(0, len(reqs) + 1)), big)
+    return reqs
+
+
+def _warm_server(M, reqs, slots):
+    """One tiny request of every (dim, physics, order, precision, limiter,
+    boundaries) the stream uses, so module loading and first-launch set-up
+    of each kernel happen before the timed stream."""
+    warm, seen, wids = M.Server(hbm_budget_bytes=150e9, max_active=slots, steps_per_chunk=10), set(), []
+    for _, (mesh, phys, P, prec, ic, prm, dt, nsteps, lim) in reqs:
         key = (mesh.dim, phys.kind, phys.flux_type, P, prec, lim is not None, tuple(mesh.bcs.as_list()))
         if key in seen:
             continue
@@ -682,25 +704,109 @@ def served(M, nreq, lam, seed=7, largest=False, slots=8, precision=None):
     for i in wids:
         warm.wait(i, timeout_s=300)
     warm.close()
+
+
+def run_stream(M, reqs, lam, slots, seed=11, warm=True, keep=True):
+    """Submit `reqs` with Poisson gaps at `lam`/s to a server with a 150 GB
+    HBM budget and `slots` concurrent solves; return the server's latency
+    and throughput figures, each kind's latencies, and the slot occupancy and
+    admitted bytes sampled every 20 ms from the first submit to the last
+    result (time-weighted means, maxima and a series of at most 60 points).
+    keep: every result is copied to a host array (released once its
+    latency is read); otherwise results stay on the device and the latency
+    ends when the solve's last kernel has finished."""
+    if warm:
+        _warm_server(M, reqs, slots)
+    gaps = np.random.default_rng(seed).exponential(1.0 / lam, len(reqs))
     srv = M.Server(hbm_budget_bytes=150e9, max_active=slots, steps_per_chunk=10)
+    samples, stop = [], threading.Event()
+
+    def sampler():
+        while not stop.is_set():
+            st = srv.stats()
+            samples.append((time.perf_counter(), st["running"], st["queued"], st["bytes_in_use"]))
+            stop.wait(0.02)
+
     t0 = time.perf_counter()
+    th = threading.Thread(target=sampler, daemon=True)
+    th.start()
     ids, t_next = [], 0.0
-    for r, g in zip(reqs, gaps):
+    for (_, r), g in zip(reqs, gaps):
         t_next += g
         delay = t_next - (time.perf_counter() - t0)
         if delay > 0:
             time.sleep(delay)
-        ids.append(srv.submit(*r))
+        ids.append(srv.submit(*r, keep_result=keep))
+    lat = []
     for i in ids:
-        srv.wait(i, timeout_s=900)
+        lat.append(srv.wait(i, timeout_s=1800))
+        srv._out.pop(i, None)  # the host copy is not needed past this point
+    stop.set()
+    th.join(timeout=5)
     st = srv.stats()
     srv.close()
-    return {"workload": f"{len(reqs)} requests, Poisson arrivals at {lam:g}/s: 2D/3D Euler, 2D dam break, 3D Maxwell "
-                        f"plane wave; 2k-400k elements, P 2..5, 50-500 steps" + ("; + 48^3x6 limited Sod P5" if largest else ""),
-            "requests": len(reqs), "lambda_per_s": lam, "solves_per_s": st["solves_per_s"], "p50_ms": st["p50_ms"],
+    by_kind = {}
+    for (kind, _), l in zip(reqs, lat):
+        by_kind.setdefault(kind, []).append(l)
+    kinds = {k: {"n": len(v), "p50_ms": float(np.percentile(v, 50)), "max_ms": float(np.max(v))}
+             for k, v in sorted(by_kind.items())}
+    occ = {}
+    if len(samples) > 1:
+        t = np.array([x[0] for x in samples]) - t0
+        run = np.array([x[1] for x in samples])
+        que = np.array([x[2] for x in samples])
+        byt = np.array([x[3] for x in samples])
+        w = np.diff(t, append=t[-1])
+        tw = max(float(w.sum()), 1e-9)
+        step = max(1, len(t) // 60)
+        occ = {"samples": len(t), "mean_running": float((run * w).sum() / tw), "max_running": float(run.max()),
+               "mean_queued": float((que * w).sum() / tw), "max_queued": float(que.max()),
+               "mean_admitted_bytes": float((byt * w).sum() / tw), "max_admitted_bytes": float(byt.max()),
+               "series_t_s_running_queued_gb": [[round(float(t[i]), 2), int(run[i]), int(que[i]),
+                                                 round(float(byt[i]) / 1e9, 3)] for i in range(0, len(t), step)]}
+    return {"requests": len(reqs), "lambda_per_s": lam, "results_to_host": keep,
+            "solves_per_s": st["solves_per_s"], "p50_ms": st["p50_ms"],
             "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "dof_stage_per_s": st["dof_stage_per_s"],
             "completed": st["completed"], "failed": st["failed"], "peak_concurrent": st["peak_concurrent"],
-            "peak_admitted_bytes": st["peak_bytes"], "hbm_budget_bytes": 150e9, "slots": slots, "seed": seed}
+            "peak_admitted_bytes": st["peak_bytes"], "latency_by_kind": kinds, "occupancy": occ}
+
+
+def served(M, a):
+    """The served configuration: `--serve-requests` requests (+ the largest
+    member) at `--serve-lambda`/s, over the server's capacity; the same kinds
+    at half the measured capacity (a stable queue; `--serve-low-seconds` of
+    arrivals); and the plain FP64 comparison replaying the first
+    `--serve-f64-requests` requests of the stream in FP64 beside the same
+    subset in the stream's precisions."""
+    reqs = served_requests(M, a.serve_requests, seed=7, largest=a.serve_largest)
+    # 500 arrivals within a few seconds: results stay on the device so the
+    # host does not hold every outstanding request's state at once
+    out = run_stream(M, reqs, a.serve_lambda, a.serve_slots, keep=False)
+    out["workload"] = (f"{len(reqs)} requests, Poisson arrivals at {a.serve_lambda:g}/s: 2D/3D Euler, 2D dam break, "
+                       "3D Maxwell plane wave, 3D limited Sod (HLLEC + limiter); 2k-400k elements, P 2..5, "
+                       "50-500 steps" + ("; + 48^3x6 limited Sod P5" if a.serve_largest else "") +
+                       "; HBM budget 150 GB")
+    out["slots"] = a.serve_slots
+    out["hbm_budget_bytes"] = 150e9
+    out["over_capacity"] = bool(a.serve_lambda > out["solves_per_s"])
+    cap = out["solves_per_s"]
+    if a.serve_low_seconds > 0 and cap > 0:
+        lam_low = 0.5 * cap
+        n_low = max(20, int(lam_low * a.serve_low_seconds))
+        low = run_stream(M, served_requests(M, n_low, seed=8, largest=False), lam_low, a.serve_slots, seed=12,
+                         warm=False)
+        low["note"] = "arrival rate half the capacity measured on the stream above: the queue stays stable"
+        out["sub_capacity"] = low
+    if a.serve_f64_requests > 0:
+        sub = reqs[:a.serve_f64_requests]
+        fast = run_stream(M, sub, a.serve_lambda, a.serve_slots, warm=False)
+        sub64 = [(k, (r[0], r[1], r[2], "f64") + tuple(r[4:])) for k, r in sub]
+        slow = run_stream(M, sub64, a.serve_lambda, a.serve_slots)
+        out["plain_f64"] = {"requests": len(sub), "stream_precisions": {k: fast[k] for k in (
+            "solves_per_s", "dof_stage_per_s", "p50_ms", "p99_ms")},
+            "f64": {k: slow[k] for k in ("solves_per_s", "dof_stage_per_s", "p50_ms", "p99_ms")}}
+        out["speedup_vs_f64"] = fast["dof_stage_per_s"] / slow["dof_stage_per_s"]
+    return out
 
 
 def main():
@@ -824,13 +930,7 @@ def main():
         cav = maxwell_cavity(M) if a.cavity else None
         mhd = mhd_alfven(M) if a.mhd else None
         slab_leg = slab_decomposed(M, a, a.slab_parts) if a.slab_parts > 0 else None
-        srv = served(M, a.serve_requests, a.serve_lambda, largest=a.serve_largest,
-                     slots=a.serve_slots) if a.serve_requests > 0 else None
-        if srv is not None:  # the same stream with every request in FP64
-            s64 = served(M, a.serve_requests, a.serve_lambda, largest=a.serve_largest, slots=a.serve_slots,
-                         precision="f64")
-            srv["plain_f64"] = {k: s64[k] for k in ("solves_per_s", "dof_stage_per_s", "p50_ms", "p99_ms")}
-            srv["speedup_vs_f64"] = srv["dof_stage_per_s"] / s64["dof_stage_per_s"]
+        srv = served(M, a) if a.serve_requests > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

@@ -396,7 +396,7 @@ int mxm_dg_server_wait(void* server, int64_t request_id, double timeout_s, doubl
 /* out[0] completed, [1] failed, [2] p50 ms, [3] p99 ms, [4] mean ms,
  * [5] solves/s and [6] DOF·stage/s from the first submit to the last
  * completion, [7] peak admitted bytes, [8] peak concurrent solves,
- * [9] queued now, [10] running now. */
+ * [9] queued now, [10] running now, [11] admitted bytes now. */
 int mxm_dg_server_stats(void* server, double* out, int n);
 int mxm_dg_server_last_error(void* server, char* buf, int len);
 

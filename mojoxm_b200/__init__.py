@@ -765,9 +765,12 @@ class Server:
         lib().mxm_dg_server_last_error(self.h, buf, 1024)
         return buf.value.decode(errors="replace")
 
-    def submit(self, mesh: Mesh, physics, P, precision, ic_kind, ic_params, dt, nsteps, limiter_eps=None):
+    def submit(self, mesh: Mesh, physics, P, precision, ic_kind, ic_params, dt, nsteps, limiter_eps=None,
+               keep_result=True):
+        """Queue one solve; its final state lands in a host array (result())
+        unless keep_result is False (the server then copies nothing back)."""
         shape = state_shape(mesh, physics, P)
-        out = np.empty(shape, dtype=np.float64 if precision == "f64" else np.float32)
+        out = np.empty(shape, dtype=np.float64 if precision == "f64" else np.float32) if keep_result else None
         p = np.ascontiguousarray(ic_params, dtype=np.float64)
         md, pd = mesh.desc(), _phys_desc(physics)
         rid = ctypes.c_int64()
@@ -775,7 +778,7 @@ class Server:
                                         p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), p.size,
                                         0 if limiter_eps is None else 1,
                                         0.1 if limiter_eps is None else limiter_eps, dt, nsteps,
-                                        out.ctypes.data, ctypes.byref(rid))
+                                        None if out is None else out.ctypes.data, ctypes.byref(rid))
         if rc != OK:
             raise DGError(rc, self._errmsg())
         self._out[rid.value] = out
@@ -803,10 +806,10 @@ class Server:
         return self._out[rid]
 
     def stats(self):
-        v = np.zeros(11)
-        _check(lib().mxm_dg_server_stats(self.h, v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 11))
+        v = np.zeros(12)
+        _check(lib().mxm_dg_server_stats(self.h, v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 12))
         keys = ["completed", "failed", "p50_ms", "p99_ms", "mean_ms", "solves_per_s", "dof_stage_per_s",
-                "peak_bytes", "peak_concurrent", "queued", "running"]
+                "peak_bytes", "peak_concurrent", "queued", "running", "bytes_in_use"]
         return dict(zip(keys, v.tolist()))
 
     def close(self):

@@ -405,10 +405,11 @@ int mxm_dg_server_stats(void* server, double* out, int n) {
   for (double v : lat) mean += v;
   mean = lat.empty() ? 0 : mean / lat.size();
   const double span = lat.empty() ? 0 : std::chrono::duration<double>(s->t_last_done - s->t_first_submit).count();
-  const double v[11] = {double(lat.size()), double(failed), pct(0.5), pct(0.99), mean,
+  const double v[12] = {double(lat.size()), double(failed), pct(0.5), pct(0.99), mean,
                         span > 0 ? lat.size() / span : 0.0, span > 0 ? s->dof_stages_done / span : 0.0,
-                        s->peak_bytes, double(s->peak_active), double(s->queue.size()), double(s->active.size())};
-  for (int i = 0; i < n && i < 11; ++i) out[i] = v[i];
+                        s->peak_bytes, double(s->peak_active), double(s->queue.size()), double(s->active.size()),
+                        s->bytes_in_use};
+  for (int i = 0; i < n && i < 12; ++i) out[i] = v[i];
   return MXM_DG_OK;
 }
 
