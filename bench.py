@@ -112,6 +112,7 @@ def parse():
                     help="SSPRK3 steps of the accuracy check vs the FP64 path (0 = skip)")
     ap.add_argument("--batch-solves", type=int, default=512, help="batched 2D leg: solves (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--batch3d-solves", type=int, default=64, help="batched 3D tensor-core leg: solves (0 = skip)")
     ap.add_argument("--serve-requests", type=int, default=500, help="served leg: requests (0 = skip)")
     ap.add_argument("--serve-lambda", type=float, default=200.0)
     ap.add_argument("--serve-largest", type=int, default=1, help="add the 48^3x6 limited Sod P5 request (1/0)")
@@ -498,7 +499,10 @@ def batched_2d(M, nsolves, steps, seed=2024, precision="f32", loop=True, ref=Non
         out["rel_l2_vs_f64_steps"] = 3 + steps
     if loop:
         # the same solves advanced one at a time through their own handles
-        # (per-solve launches on per-solve streams), 2 steps, wall clock
+        # (per-solve launches on per-solve streams), 2 steps after an untimed
+        # one, wall clock
+        for i, s in enumerate(solvers):
+            s.step_n(batch.dts[i], 1)
         for s in solvers:
             s.synchronize()
         t0 = time.perf_counter()
@@ -516,6 +520,58 @@ def batched_2d(M, nsolves, steps, seed=2024, precision="f32", loop=True, ref=Non
     else:
         for s in solvers:
             s.close()
+    return out
+
+
+def batched_3d(M, nsolves, steps, seed=2025):
+    """Batched 3D Euler on the tensor-core stage: `nsolves` independent solves
+    of uneven size and order (n^3 x 6 tets, n ~ U{4..16}, P ~ U{2..5}),
+    split-BF16, half smooth density waves (Rusanov, periodic) and half
+    limited Sod tubes (HLLEC, BJ limiter, outflow x, walls y/z), advanced
+    as one batch (one tensor-core launch per (flux, order) group and stage,
+    the limited solves' limiter passes, all in one CUDA graph), against the
+    same solves stepped one after another through their own handles."""
+    rng = np.random.default_rng(seed)
+    batch, solvers = M.Batch(), []
+    for _ in range(nsolves):
+        n, P = int(rng.integers(4, 17)), int(rng.integers(2, 6))
+        if rng.random() < 0.5:
+            s = M.Solver(M.Mesh(n, n, n), M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_RUSANOV, False), P=P, precision="mixed")
+            s.fill_ic(M.IC_SINE_WAVE, [1, 0.2, 1, 1, 1, 1, 1, 1, 1])
+            lam = np.sqrt(3) + 1.5
+        else:
+            s = M.Solver(M.Mesh(n, n, n, bcs=M.BoundaryConditions(2, 2, 1, 1, 1, 1)),
+                         M.Euler(GAMMA, 1e-6, 1e-6, M.FLUX_HLLEC, False), P=P, precision="mixed")
+            rl, pl, rr, pr = rng.uniform(0.1, 1.0, 4)
+            s.fill_ic(M.IC_SOD, [rl, pl, rr, pr, 0.5, 1.0 / n])
+            s.enable_cell_limiter(True, 0.1)
+            lam = np.sqrt(GAMMA * max(pl, pr) / min(rl, rr)) + 1.0
+        batch.add(s, 0.1 / n / (lam * (2 * P + 1)))
+        solvers.append(s)
+    dof = batch.dof_count()
+    batch.step(3)
+    batch.synchronize()
+    ms = batch.time_steps(steps)
+    batch.synchronize()
+    value = 3 * dof * steps / (ms * 1e-3)
+    for i, s in enumerate(solvers):  # one untimed step: the single-solve kernels load
+        s.step_n(batch.dts[i], 1)
+    for s in solvers:
+        s.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(2):
+        for i, s in enumerate(solvers):
+            s.step_n(batch.dts[i], 1)
+    for s in solvers:
+        s.synchronize()
+    loop_s = (time.perf_counter() - t0) / 2
+    out = {"workload": f"{nsolves} independent 3D Euler solves (split-BF16 tensor-core stage; smooth waves and "
+                       "limited Sod tubes), n^3x6 tets with n in 4..16, P in 2..5", "solves": nsolves, "dof": dof,
+           "value": value, "unit": UNIT, "ms_per_step": ms / steps, "launches_per_step": batch.launches_per_step(),
+           "per_solve_loop_value": 3 * dof / loop_s, "speedup_vs_per_solve_loop": value / (3 * dof / loop_s)}
+    batch.close()
+    for s in solvers:
+        s.close()
     return out
 
 
@@ -927,6 +983,7 @@ def main():
             bat["plain_f64_value"] = b64["value"]
             bat["plain_f64_ms_per_step"] = b64["ms_per_step"]
             bat["speedup_vs_f64"] = bat["value"] / b64["value"]
+        bat3 = batched_3d(M, a.batch3d_solves, a.batch_steps) if a.batch3d_solves > 0 else None
         cav = maxwell_cavity(M) if a.cavity else None
         mhd = mhd_alfven(M) if a.mhd else None
         slab_leg = slab_decomposed(M, a, a.slab_parts) if a.slab_parts > 0 else None
@@ -952,7 +1009,7 @@ def main():
             "cpu_baseline": cb,
             "plain_f64": plain,
             "measured_gemm_peaks": fpp,
-            "batched": bat,
+            "batched": bat, "batched_3d": bat3,
             "maxwell_cavity": cav, "mhd_alfven": mhd, "slab": slab_leg,
             "served": srv,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": qbytes,

@@ -661,9 +661,12 @@ class DiagnosticsWriter:  # src/diagnostics.mojo:96-229
 
 
 class Batch:
-    """Many independent 2D solves advanced together (mxm_dg_batch_*): one
-    persistent stage launch per physics group and stage, the SSPRK3 step
-    captured as a CUDA graph, tile sizes autotuned per (group, P)."""
+    """Many independent solves advanced together (mxm_dg_batch_*), the SSPRK3
+    step captured as a CUDA graph: 2D solves in one persistent stage launch
+    per physics group and stage (tile sizes autotuned per (group, P)); 3D
+    tensor-core solves (precision "mixed" / "tf32") in one launch per
+    (physics, order, operand kind) and stage; other 3D solves by their own
+    launches in the same graph."""
 
     def __init__(self):
         h = ctypes.c_void_p()

@@ -1,9 +1,18 @@
-// Batched engine of the C ABI (mxm_dg_batch_*): many independent 2D solves
-// of uneven mesh size and order advanced together, one persistent stage
-// launch per physics group and stage, the whole SSPRK3 step (counter resets,
-// stage kernels, limiter passes) captured once in a CUDA graph and replayed.
-// Tile sizes (cells per tile) per (group, P) come from an autotuner that
-// times the batched stage kernel on the batch's own solves.
+// Batched engine of the C ABI (mxm_dg_batch_*): many independent solves of
+// uneven mesh size and order advanced together, the whole SSPRK3 step
+// (counter resets, stage kernels, limiter passes) captured once in a CUDA
+// graph and replayed.
+//  * 2D solves: one persistent stage launch per physics group and stage;
+//    tile sizes (cells per tile) per (group, P) come from an autotuner that
+//    times the batched stage kernel on the batch's own solves.
+//  * 3D solves on the tensor-core stage (MIXED, MIXED_TF32): one launch per
+//    (physics, order, operand kind) group and stage over the tiles of all
+//    its solves (stage3d_tc_kernel's batched form); their limiter passes are
+//    the single-solve ones, one pair per limited solve.
+//  * other 3D solves (FP32 / FP64 SIMT stage): their single-solve launches,
+//    in the same graph.
+// Every solve gets its single-solve arithmetic, so batched results are
+// bit-identical to the same solves stepped alone.
 //
 // The reference has no batching: each 2D solve runs its own driver loop
 // (examples/euler_sod_2d_gpu.mojo, src/ssprk3.mojo:56-78).  Member solves are
@@ -27,6 +36,13 @@ namespace mxm {
 struct BatchGroup {
   mxm_dg_physics_desc phys{};
   int NC = 0;
+  int dim = 2;
+  // 3D: tc = batched tensor-core tiles of order P and operand kind `kind`;
+  // otherwise the members' single-solve launches
+  bool tc = false;
+  int P = 0, kind = 0;
+  Stage3DArgs<float>* d_margs = nullptr;  // [3][members]: stage arguments
+  KuhnTab3<float>* d_tabs = nullptr;      // [members]
   std::vector<int> members;  // indices into Batch::members
   int ec[6] = {0, 0, 0, 0, 0, 0};
   int4* d_items = nullptr;
@@ -40,8 +56,19 @@ struct BatchGroup {
   const void* A[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
+// The limited 3D members of one component count: their cell-mean and theta
+// passes as one launch each per stage, over chunks of kLim3Chunk elements.
+struct Lim3Group {
+  int NC = 0;
+  std::vector<int> members;
+  void* d_desc = nullptr;  // LimDesc3<R>[members]
+  int4* d_items = nullptr;
+  int nitems = 0;
+};
+
 struct Batch {
   int device = 0, nsm = 148;
+  std::vector<Lim3Group> lim3;
   cudaStream_t stream = nullptr;
   size_t rbytes = 0;
   std::vector<Handle*> members;
@@ -75,12 +102,142 @@ void release_graph(Batch* b) {
   b->built = false;
 }
 
+void free_lim3(Batch* b) {
+  for (auto& lg : b->lim3) {
+    cudaFree(lg.d_desc);
+    cudaFree(lg.d_items);
+  }
+  b->lim3.clear();
+}
+
+// component counts the batched 3D limiter is built for (the 17-component
+// two-fluid state keeps its single-solve limiter launches)
+bool lim3_batched_nc(int nc) { return nc == 1 || nc == 3 || nc == 5 || nc == 6 || nc == 9; }
+
+template <class R>
+void build_lim3(Batch* b) {
+  free_lim3(b);
+  for (size_t i = 0; i < b->members.size(); ++i) {
+    const Handle* h = b->members[i];
+    if (h->dim != 3 || !h->lim_on || !lim3_batched_nc(h->NC)) continue;
+    Lim3Group* lg = nullptr;
+    for (auto& x : b->lim3)
+      if (x.NC == h->NC) lg = &x;
+    if (!lg) {
+      b->lim3.emplace_back();
+      lg = &b->lim3.back();
+      lg->NC = h->NC;
+    }
+    lg->members.push_back(int(i));
+  }
+  for (auto& lg : b->lim3) {
+    std::vector<LimDesc3<R>> desc(lg.members.size());
+    std::vector<int4> items;
+    for (size_t j = 0; j < lg.members.size(); ++j) {
+      const Handle* h = b->members[lg.members[j]];
+      LimDesc3<R>& d = desc[j];
+      std::memset(&d, 0, sizeof(d));
+      d.a.avg = (R*)h->avg;
+      d.a.w = (const R*)h->w;
+      d.a.ne = h->ne;
+      d.a.e0 = 0;
+      d.a.e1 = h->ne;
+      d.a.nx = h->nx; d.a.ny = h->ny; d.a.nz = h->nz;
+      for (int k = 0; k < 6; ++k) d.a.bc[k] = h->bc[k];
+      if (sizeof(R) == 4) {
+        const float ef = float(h->lim_eps);  // as the single-solve limiter: eps2 = eps*eps in FP32
+        d.a.eps2 = R(ef * ef);
+      } else {
+        d.a.eps2 = R(h->lim_eps * h->lim_eps);
+      }
+      for (int k = 0; k < 3; ++k) d.qs[k] = (R*)h->q[k];
+      d.tab = sizeof(R) == 8 ? reinterpret_cast<const KuhnTab3<R>&>(h->t3d) : reinterpret_cast<const KuhnTab3<R>&>(h->t3f);
+      d.P = h->P;
+      for (int64_t e0 = 0; e0 < h->ne; e0 += kLim3Chunk)
+        items.push_back(make_int4(int(j), int(e0), int(std::min<int64_t>(kLim3Chunk, h->ne - e0)), 0));
+    }
+    lg.nitems = int(items.size());
+    CK(cudaMalloc(&lg.d_desc, desc.size() * sizeof(LimDesc3<R>)));
+    CK(cudaMemcpy(lg.d_desc, desc.data(), desc.size() * sizeof(LimDesc3<R>), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&lg.d_items, items.size() * sizeof(int4)));
+    CK(cudaMemcpy(lg.d_items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  }
+}
+
+template <class R, int NC>
+cudaError_t lim3_launch_nc(const Lim3Group& lg, int which, cudaStream_t st) {
+  const LimBatch3<R> lb{(const LimDesc3<R>*)lg.d_desc, lg.d_items, lg.nitems, which};
+  avg3d_batch_kernel<R, NC><<<lg.nitems, 256, 0, st>>>(lb);
+  theta3d_batch_kernel<R, NC><<<lg.nitems, 32 * kLim3Epb, 0, st>>>(lb);
+  return cudaGetLastError();
+}
+
+template <class R>
+cudaError_t lim3_launch(const Lim3Group& lg, int which, cudaStream_t st) {
+  if (lg.nitems <= 0) return cudaSuccess;
+  switch (lg.NC) {
+    case 1: return lim3_launch_nc<R, 1>(lg, which, st);
+    case 3: return lim3_launch_nc<R, 3>(lg, which, st);
+    case 5: return lim3_launch_nc<R, 5>(lg, which, st);
+    case 6: return lim3_launch_nc<R, 6>(lg, which, st);
+    case 9: return lim3_launch_nc<R, 9>(lg, which, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
 void free_group(BatchGroup& g) {
   cudaFree(g.d_items);
   cudaFree(g.d_litems);
   cudaFree(g.d_counter);
+  cudaFree(g.d_margs);
+  cudaFree(g.d_tabs);
   g.d_items = g.d_litems = nullptr;
   g.d_counter = nullptr;
+  g.d_margs = nullptr;
+  g.d_tabs = nullptr;
+}
+
+// During the capture of the step the 3D members' single-solve launches go to
+// the batch stream (the members are idle while the batch owns them).
+struct StreamSwap {
+  std::vector<std::pair<Handle*, cudaStream_t>> saved;
+  StreamSwap(Batch* b) {
+    for (Handle* h : b->members)
+      if (h->dim == 3) {
+        saved.emplace_back(h, h->stream);
+        h->stream = b->stream;
+      }
+  }
+  ~StreamSwap() {
+    for (auto& p : saved) p.first->stream = p.second;
+  }
+};
+
+// Tiles {member of the group, first cell, cells, 0} and per-stage arguments
+// of a 3D tensor-core group.
+void build_tc3(Batch* b, BatchGroup& g) {
+  const int ng = int(g.members.size());
+  const Handle* h0 = b->members[g.members[0]];
+  const int ec = tc_tile_cubes(g.P, h0->NC, g.kind);
+  if (ec < 1) throw ArgError("no tensor-core tile for this order and component count");
+  std::vector<int4> items;
+  std::vector<Stage3DArgs<float>> margs(size_t(3) * ng);
+  std::vector<KuhnTab3<float>> tabs(ng);
+  for (int j = 0; j < ng; ++j) {
+    Handle* h = b->members[g.members[j]];
+    for (int64_t c0 = h->cbeg; c0 < h->cend; c0 += ec)
+      items.push_back(make_int4(j, int(c0), int(std::min<int64_t>(ec, h->cend - c0)), 0));
+    for (int st = 0; st < 3; ++st) margs[size_t(st) * ng + j] = tc_stage_args(h, st, b->dt[g.members[j]], b->derr);
+    tabs[j] = h->t3f;
+  }
+  g.ec[g.P] = ec;
+  g.nitems = int(items.size());
+  CK(cudaMalloc(&g.d_items, std::max<size_t>(1, items.size()) * sizeof(int4)));
+  CK(cudaMemcpy(g.d_items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&g.d_margs, margs.size() * sizeof(Stage3DArgs<float>)));
+  CK(cudaMemcpy(g.d_margs, margs.data(), margs.size() * sizeof(Stage3DArgs<float>), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&g.d_tabs, tabs.size() * sizeof(KuhnTab3<float>)));
+  CK(cudaMemcpy(g.d_tabs, tabs.data(), tabs.size() * sizeof(KuhnTab3<float>), cudaMemcpyHostToDevice));
 }
 
 template <class R>
@@ -200,6 +357,7 @@ void autotune(Batch* b) {
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   for (auto& g : b->groups) {
+    if (g.dim == 3) continue;  // 3D tiles are fixed by the tensor-core shape
     if (!g.d_counter) CK(cudaMalloc(&g.d_counter, 3 * sizeof(int)));
     for (int P = 1; P <= 5; ++P) {
       bool any = false;
@@ -250,6 +408,10 @@ void build(Batch* b) {
   upload_solves<R>(b);
   for (auto& g : b->groups) {
     free_group(g);
+    if (g.dim == 3) {
+      if (g.tc) build_tc3(b, g);
+      continue;
+    }
     layout(b, g, g.ec);
     std::vector<int4> items = make_items(b, g, g.ec, 0);
     g.nitems = int(items.size());
@@ -271,19 +433,53 @@ void build(Batch* b) {
     g.grid = grid_for<R>(b, g, g.smem, g.nitems);
   }
   for (auto& g : b->groups)
-    if (g.nlitems > 0) CK(prepare_lim2d_batch<R>(g.NC));
+    if (g.dim == 2 && g.nlitems > 0) CK(prepare_lim2d_batch<R>(g.NC));
+  build_lim3<R>(b);
+  // first-use set-up of the batched 3D kernels (kernel attributes,
+  // occupancy) before the capture: an empty batch launches nothing
+  for (auto& g : b->groups)
+    if (g.dim == 3 && g.tc) {
+      const Tc3Batch none{g.d_margs, g.d_tabs, g.d_items, 0};
+      CK(launch_tc_group(b->members[g.members[0]], none, b->stream));
+    }
   // one SSPRK3 step as a graph
+  StreamSwap swap(b);
   CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t cap = cudaSuccess;
   for (auto& g : b->groups)
-    if (cap == cudaSuccess) cap = cudaMemsetAsync(g.d_counter, 0, 3 * sizeof(int), b->stream);
+    if (cap == cudaSuccess && g.dim == 2) cap = cudaMemsetAsync(g.d_counter, 0, 3 * sizeof(int), b->stream);
   for (int s = 0; s < 3 && cap == cudaSuccess; ++s) {
     for (auto& g : b->groups) {
       if (cap != cudaSuccess) break;
-      cap = launch_group_stage<R>(b, g, g.d_items, g.nitems, s, g.grid, g.smem);
+      if (g.dim == 2) {
+        cap = launch_group_stage<R>(b, g, g.d_items, g.nitems, s, g.grid, g.smem);
+      } else if (g.tc) {
+        const Tc3Batch bat{g.d_margs + size_t(s) * g.members.size(), g.d_tabs, g.d_items, g.nitems};
+        cap = launch_tc_group(b->members[g.members[0]], bat, b->stream);
+      } else {
+        try {
+          for (int m : g.members) stage_only(b->members[m], s, b->dt[m]);
+        } catch (CudaError& ex) {
+          cap = ex.e;
+        }
+      }
+    }
+    // 3D limiter passes: batched per component count; the two-fluid state
+    // keeps its single-solve launches
+    for (auto& lg : b->lim3)
+      if (cap == cudaSuccess) cap = lim3_launch<R>(lg, stage_out(s), b->stream);
+    for (auto& g : b->groups) {
+      if (cap != cudaSuccess || g.dim != 3) continue;
+      try {
+        for (int m : g.members)
+          if (b->members[m]->lim_on && !lim3_batched_nc(b->members[m]->NC))
+            limit_buf(b->members[m], b->members[m]->q[stage_out(s)]);
+      } catch (CudaError& ex) {
+        cap = ex.e;
+      }
     }
     for (auto& g : b->groups) {
-      if (cap != cudaSuccess || g.nlitems == 0) continue;
+      if (cap != cudaSuccess || g.dim != 2 || g.nlitems == 0) continue;
       LimBatch2DArgs<R> la;
       la.solves = (const SolveDesc2<R>*)b->d_solves;
       la.items = g.d_litems;
@@ -378,6 +574,7 @@ int mxm_dg_batch_destroy(void* batch) {
   cudaStreamSynchronize(b->stream);
   mxm::release_graph(b);
   for (auto& g : b->groups) mxm::free_group(g);
+  mxm::free_lim3(b);
   cudaFree(b->d_solves);
   cudaFree(b->derr);
   cudaStreamDestroy(b->stream);
@@ -389,7 +586,7 @@ int mxm_dg_batch_add(void* batch, void* solver, double dt, int32_t* index) {
   BATCH_BEGIN
   mxm::Handle* h = (mxm::Handle*)solver;
   if (!h) throw mxm::ArgError("null solver handle");
-  if (h->dim != 2) throw mxm::ArgError("batched solves are 2D (triangle meshes)");
+  if (h->nparts > 1) throw mxm::ArgError("slab parts step through their group, not a batch");
   if (h->device != b->device) throw mxm::ArgError("solver lives on another device than the batch");
   if (!(dt > 0.0)) throw mxm::ArgError("dt must be positive");
   if (b->rbytes && h->rbytes != b->rbytes) throw mxm::ArgError("all solves of a batch share one precision");
@@ -399,13 +596,25 @@ int mxm_dg_batch_add(void* batch, void* solver, double dt, int32_t* index) {
   const int id = int(b->members.size());
   b->members.push_back(h);
   b->dt.push_back(dt);
+  // groups: 2D by physics; 3D tensor-core by (physics, order, operand
+  // kind); the other 3D solves by physics
+  const bool tc = h->dim == 3 && h->use_tc;
   int gi = -1;
-  for (size_t k = 0; k < b->groups.size(); ++k)
-    if (std::memcmp(&b->groups[k].phys, &h->phys, sizeof(h->phys)) == 0) gi = int(k);
+  for (size_t k = 0; k < b->groups.size(); ++k) {
+    const mxm::BatchGroup& g = b->groups[k];
+    if (g.dim == h->dim && g.tc == tc && std::memcmp(&g.phys, &h->phys, sizeof(h->phys)) == 0 &&
+        (!tc || (g.P == h->P && g.kind == h->tc_kind)))
+      gi = int(k);
+  }
   if (gi < 0) {
     b->groups.emplace_back();
-    b->groups.back().phys = h->phys;
-    b->groups.back().NC = h->NC;
+    mxm::BatchGroup& g = b->groups.back();
+    g.phys = h->phys;
+    g.NC = h->NC;
+    g.dim = h->dim;
+    g.tc = tc;
+    g.P = tc ? h->P : 0;
+    g.kind = tc ? h->tc_kind : 0;
     gi = int(b->groups.size()) - 1;
   }
   b->groups[gi].members.push_back(id);
@@ -491,12 +700,27 @@ int mxm_dg_batch_launches_per_step(void* batch, int32_t* n) {
   if (!n) throw mxm::ArgError("n non-null");
   // per stage: one stage kernel per group, plus the two limiter passes of a
   // group with limited members
+  // 3D: one batched launch per tensor-core group and stage, one launch per
+  // other solve and stage, two limiter launches per component count of the
+  // limited solves and stage (two per two-fluid limited solve and stage)
   int k = 0;
+  std::vector<int> lim_nc;
   for (auto& g : b->groups) {
+    if (g.dim == 3) {
+      k += g.tc ? 3 : 3 * int(g.members.size());
+      for (int m : g.members) {
+        const mxm::Handle* h = b->members[m];
+        if (!h->lim_on) continue;
+        if (!mxm::lim3_batched_nc(h->NC)) k += 6;
+        else if (std::find(lim_nc.begin(), lim_nc.end(), h->NC) == lim_nc.end()) lim_nc.push_back(h->NC);
+      }
+      continue;
+    }
     bool lim = false;
     for (int m : g.members) lim = lim || b->members[m]->lim_on;
     k += 3 * (lim ? 3 : 1);
   }
+  k += 6 * int(lim_nc.size());
   for (const mxm::Handle* h : b->members) k += mxm::glm_damped(h) ? 1 : 0;  // psi damping
   *n = k;
   BATCH_END

@@ -205,76 +205,109 @@ Mhd2D<R, GLM> make_mhd2d(const double* p) {
   return ph;
 }
 
+// Build the 3D physics functor of the handle's descriptor in real type R
+// and call f(ph); the parameter layout is the one mxm_dg_physics_desc
+// documents.
+template <class R, class F>
+cudaError_t with_phys3d(const Handle* h, F&& f) {
+  const double* p = h->phys.p;
+  switch (h->phys.kind) {
+    case MXM_DG_PHYS_ADVECTION: {
+      AdvectionD<R> ph{R(p[0]), R(p[1]), R(p[2]), R(p[3])};
+      return f(ph);
+    }
+    case MXM_DG_PHYS_EULER: {
+      auto mk = [&](auto ph) {
+        ph.gamma = R(p[0]); ph.rho_min = R(p[1]); ph.p_min = R(p[2]);
+        ph.gx = R(p[3]); ph.gy = R(p[4]); ph.gz = R(p[5]);
+        for (int k = 0; k < 5; ++k) ph.inflow[k] = R(p[6 + k]);
+        ph.entropy_fix = h->phys.entropy_fix;
+        return f(ph);
+      };
+      switch (h->phys.flux_type) {
+        case MXM_DG_FLUX_RUSANOV: return mk(EulerD<R, FLUX_RUSANOV>{});
+        case MXM_DG_FLUX_ROE: return mk(EulerD<R, FLUX_ROE>{});
+        case MXM_DG_FLUX_HLLE: return mk(EulerD<R, FLUX_HLLE>{});
+        case MXM_DG_FLUX_HLLEC: return mk(EulerD<R, FLUX_HLLEC>{});
+      }
+      return cudaErrorInvalidValue;
+    }
+    case MXM_DG_PHYS_MAXWELL: {
+      MaxwellD<R> ph;
+      ph.c = R(p[0]);
+      for (int k = 0; k < 3; ++k) { ph.J[k] = R(p[1 + k]); ph.M[k] = R(p[4 + k]); }
+      for (int k = 0; k < 6; ++k) ph.inflow[k] = R(p[7 + k]);
+      return f(ph);
+    }
+    case MXM_DG_PHYS_SHALLOW_WATER: {
+      ShallowWaterD<R> ph;
+      ph.g = R(p[0]); ph.h_min = R(p[1]);
+      for (int k = 0; k < 3; ++k) ph.inflow[k] = R(p[2 + k]);
+      return f(ph);
+    }
+    case MXM_DG_PHYS_MHD: return f(make_mhd<R>(p));
+    case MXM_DG_PHYS_TWO_FLUID: return f(make_two_fluid<R>(p));
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class R>
+Stage3DArgs<R> stage3d_args(const Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double b,
+                            double c, double dt, int rhs_only, int64_t c0, int64_t c1) {
+  Stage3DArgs<R> ar;
+  ar.q_in = (const R*)qi;
+  ar.q_a = (const R*)qa;
+  ar.q_b = (const R*)qb;
+  ar.q_out = (R*)qo;
+  ar.A = (const R*)h->A;
+  ar.b = R(b);
+  ar.cdt = R(c * dt);
+  ar.nx = h->nx;
+  ar.ny = h->ny;
+  ar.nz = h->nz;
+  ar.cbeg = int(c0);
+  ar.ncell = int(c1);
+  for (int k = 0; k < 6; ++k) ar.bc[k] = h->bc[k];
+  ar.rhs_only = rhs_only;
+  ar.err = h->derr;
+  return ar;
+}
+
+// Shu-Osher stage s (q, q1, q2 routing as stage_only) of a tensor-core
+// handle as the batched 3D launch takes it.
+Stage3DArgs<float> tc_stage_args(const Handle* h, int s, double dt, int* err) {
+  void *q0 = h->q[0], *q1 = h->q[1], *q2 = h->q[2];
+  Stage3DArgs<float> a = s == 0 ? stage3d_args<float>(h, q0, q0, q0, q1, 0.0, 1.0, dt, 0, h->cbeg, h->cend)
+                       : s == 1 ? stage3d_args<float>(h, q1, q0, q1, q2, 0.25, 0.25, dt, 0, h->cbeg, h->cend)
+                                : stage3d_args<float>(h, q2, q0, q2, q0, 2.0 / 3.0, 2.0 / 3.0, dt, 0, h->cbeg, h->cend);
+  a.err = err;
+  return a;
+}
+
+cudaError_t launch_tc_group(const Handle* h0, const Tc3Batch& bat, cudaStream_t st) {
+  return with_phys3d<float>(h0, [&](const auto& ph) -> cudaError_t {
+    if constexpr (std::decay<decltype(ph)>::type::NC <= 16)
+      return launch_stage3d_tc_batch(h0->P, h0->tc_kind, bat, ph, (const unsigned char*)h0->tcimg, h0->nsm, st);
+    return cudaErrorInvalidValue;
+  });
+}
+
 template <class R>
 cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double b, double c,
                          double dt, int rhs_only, int64_t c0, int64_t c1) {
   const double* p = h->phys.p;
   const R cdt = R(c * dt);
   if (h->dim == 3) {
-    Stage3DArgs<R> ar;
-    ar.q_in = (const R*)qi;
-    ar.q_a = (const R*)qa;
-    ar.q_b = (const R*)qb;
-    ar.q_out = (R*)qo;
-    ar.A = (const R*)h->A;
-    ar.b = R(b);
-    ar.cdt = cdt;
-    ar.nx = h->nx;
-    ar.ny = h->ny;
-    ar.nz = h->nz;
-    ar.cbeg = int(c0);
-    ar.ncell = int(c1);
-    for (int k = 0; k < 6; ++k) ar.bc[k] = h->bc[k];
-    ar.rhs_only = rhs_only;
-    ar.err = h->derr;
+    const Stage3DArgs<R> ar = stage3d_args<R>(h, qi, qa, qb, qo, b, c, dt, rhs_only, c0, c1);
     const KuhnTab3<R>& t = tab3<R>(h);
     // MIXED precision routes the 3D stage through the tensor-core kernel
-    auto go = [&](const auto& ph) -> cudaError_t {
-      if constexpr (std::is_same<R, float>::value &&
-                    std::decay<decltype(ph)>::type::NC <= 16) {
+    return with_phys3d<R>(h, [&](const auto& ph) -> cudaError_t {
+      if constexpr (std::is_same<R, float>::value && std::decay<decltype(ph)>::type::NC <= 16) {
         if (h->use_tc)
           return launch_stage3d_tc(h->P, h->tc_kind, ar, t, ph, (const unsigned char*)h->tcimg, h->nsm, h->stream);
       }
       return launch_stage3d<R>(h->P, ar, t, ph, h->nsm, h->stream);
-    };
-    switch (h->phys.kind) {
-      case MXM_DG_PHYS_ADVECTION: {
-        AdvectionD<R> ph{R(p[0]), R(p[1]), R(p[2]), R(p[3])};
-        return go(ph);
-      }
-      case MXM_DG_PHYS_EULER: {
-        auto mk = [&](auto ph) {
-          ph.gamma = R(p[0]); ph.rho_min = R(p[1]); ph.p_min = R(p[2]);
-          ph.gx = R(p[3]); ph.gy = R(p[4]); ph.gz = R(p[5]);
-          for (int k = 0; k < 5; ++k) ph.inflow[k] = R(p[6 + k]);
-          ph.entropy_fix = h->phys.entropy_fix;
-          return go(ph);
-        };
-        switch (h->phys.flux_type) {
-          case MXM_DG_FLUX_RUSANOV: return mk(EulerD<R, FLUX_RUSANOV>{});
-          case MXM_DG_FLUX_ROE: return mk(EulerD<R, FLUX_ROE>{});
-          case MXM_DG_FLUX_HLLE: return mk(EulerD<R, FLUX_HLLE>{});
-          case MXM_DG_FLUX_HLLEC: return mk(EulerD<R, FLUX_HLLEC>{});
-        }
-        return cudaErrorInvalidValue;
-      }
-      case MXM_DG_PHYS_MAXWELL: {
-        MaxwellD<R> ph;
-        ph.c = R(p[0]);
-        for (int k = 0; k < 3; ++k) { ph.J[k] = R(p[1 + k]); ph.M[k] = R(p[4 + k]); }
-        for (int k = 0; k < 6; ++k) ph.inflow[k] = R(p[7 + k]);
-        return go(ph);
-      }
-      case MXM_DG_PHYS_SHALLOW_WATER: {
-        ShallowWaterD<R> ph;
-        ph.g = R(p[0]); ph.h_min = R(p[1]);
-        for (int k = 0; k < 3; ++k) ph.inflow[k] = R(p[2 + k]);
-        return go(ph);
-      }
-      case MXM_DG_PHYS_MHD: return go(make_mhd<R>(p));
-      case MXM_DG_PHYS_TWO_FLUID: return go(make_two_fluid<R>(p));
-    }
-    return cudaErrorInvalidValue;
+    });
   }
   Stage2DArgs<R> ar;
   ar.q_in = (const R*)qi;

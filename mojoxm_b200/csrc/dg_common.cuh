@@ -212,6 +212,21 @@ cudaError_t launch_stage3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& ta
 template <class R, class Phys>
 cudaError_t launch_wavespeed3d(int P, const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phys& ph,
                                unsigned long long* out, cudaStream_t st);
+// Batched tensor-core 3D stage: the tiles of many solves of one physics,
+// order and operand kind in one launch.  items[t] = {solve, first cell,
+// cells, 0}, the tiles of one solve consecutive; margs[solve] are the
+// solve's arguments of the stage launched (q_in / q_a / q_b / q_out, b,
+// c dt, mesh, boundaries), tabs[solve] its metric table.
+struct Tc3Batch {
+  const Stage3DArgs<float>* margs;
+  const KuhnTab3<float>* tabs;
+  const int4* items;
+  int nitems;
+};
+template <class Phys>
+cudaError_t launch_stage3d_tc_batch(int P, int kind, const Tc3Batch& bat, const Phys& ph, const unsigned char* img,
+                                    int nsm, cudaStream_t st);
+
 // Tensor-core 3D stage for FP32 state, P = 2..5: split-BF16 (kind
 // TC_BF16, tcgen05 kind::f16) or split-TF32 (TC_TF32, kind::tf32) operands;
 // `img` is the operator image built by tc_operator_image() for that kind.

@@ -120,6 +120,12 @@ void slab_ranges(const Handle* h, int64_t in[2], int64_t lo[2], int64_t hi[2]);
 int stage_in(int s);
 int stage_out(int s);
 void limit_buf(Handle* h, void* qv);
+// Batched 3D tensor-core stages: stage s's arguments of a handle (its error
+// word replaced by `err`), the launch of a batch of tiles of handles of h0's
+// physics, order and operand kind, and the cubes per tile of that shape.
+Stage3DArgs<float> tc_stage_args(const Handle* h, int s, double dt, int* err);
+cudaError_t launch_tc_group(const Handle* h0, const Tc3Batch& bat, cudaStream_t st);
+int tc_tile_cubes(int P, int NC, int kind);
 // NCCL halo transport (slab.cu): exchange the ghost layers of state buffer
 // `which` on the handle's stream; release the link
 void nccl_exchange(Handle* h, int which, cudaStream_t st);

@@ -32,13 +32,17 @@ __global__ void cell_avg_kernel(LimArgs<R> a) {
   a.avg[tid] = s;
 }
 
-// One warp per element; EPB elements per block of 32*EPB threads.
+// Theta + apply of elements eb .. eb + EPB - 1 (those below a.e1), one
+// warp per element, in a block of 32*EPB threads; `sqf` is the block's
+// staging space of EPB * NP * NC values.  Every thread must call it (it
+// synchronises the block once).
 template <class R, int DIM, int NP, int NC, int EPB>
-__global__ void __launch_bounds__(32 * EPB) theta_apply_kernel(LimArgs<R> a, KuhnTab3<R> t3, KuhnTab2<R> t2) {
+__device__ __forceinline__ void theta_apply_group(const LimArgs<R>& a, const KuhnTab3<R>& t3, const KuhnTab2<R>& t2,
+                                                  int64_t eb, R* sqf) {
   constexpr int NTYPE = DIM == 3 ? 6 : 2, NFACE = DIM + 1, VALS = NP * NC;
-  __shared__ R sq[EPB][VALS];
+  R (*sq)[VALS] = reinterpret_cast<R (*)[VALS]>(sqf);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t eb = a.e0 + int64_t(blockIdx.x) * EPB, e = eb + warp;
+  const int64_t e = eb + warp;
   const bool valid = e < a.e1;
   // contiguous block load of the EPB elements
   const int64_t base = eb * VALS;
@@ -123,6 +127,83 @@ __global__ void __launch_bounds__(32 * EPB) theta_apply_kernel(LimArgs<R> a, Kuh
     const int c = idx % NC;
     const R bm = a.avg[e * NC + c];
     qe[idx] = bm + th * (sq[warp][idx] - bm);
+  }
+}
+
+// One warp per element; EPB elements per block of 32*EPB threads.
+template <class R, int DIM, int NP, int NC, int EPB>
+__global__ void __launch_bounds__(32 * EPB) theta_apply_kernel(LimArgs<R> a, KuhnTab3<R> t3, KuhnTab2<R> t2) {
+  __shared__ R sq[EPB * NP * NC];
+  theta_apply_group<R, DIM, NP, NC, EPB>(a, t3, t2, a.e0 + int64_t(blockIdx.x) * EPB, sq);
+}
+
+// ---- batched 3D limiter: the cell-mean and theta passes of many limited
+// solves (any order) in one launch each, over chunks of elements.
+template <class R>
+struct LimDesc3 {
+  LimArgs<R> a;  // q unused: the buffer is qs[which]
+  R* qs[3];
+  KuhnTab3<R> tab;
+  int P;
+};
+template <class R>
+struct LimBatch3 {
+  const LimDesc3<R>* solves;
+  const int4* items;  // {solve, first element, elements, 0}
+  int nitems, which;
+};
+constexpr int kLim3Chunk = 128, kLim3Epb = 8;
+
+template <class R, int NP, int NC>
+__device__ __forceinline__ void avg3d_chunk(const LimDesc3<R>& d, R* q, int64_t e0, int ne) {
+  for (int idx = threadIdx.x; idx < ne * NC; idx += blockDim.x) {
+    const int64_t e = e0 + idx / NC;
+    const int c = idx % NC;
+    const R* qe = q + e * NP * NC + c;
+    R s = R(0);
+#pragma unroll
+    for (int n = 0; n < NP; ++n) s += __ldg(&d.a.w[n]) * qe[n * NC];
+    d.a.avg[e * NC + c] = s;
+  }
+}
+
+template <class R, int NC>
+__global__ void avg3d_batch_kernel(LimBatch3<R> lb) {
+  const int4 it = lb.items[blockIdx.x];
+  const LimDesc3<R>& d = lb.solves[it.x];
+  R* q = d.qs[lb.which];
+  switch (d.P) {
+    case 1: avg3d_chunk<R, ntet(1), NC>(d, q, it.y, it.z); break;
+    case 2: avg3d_chunk<R, ntet(2), NC>(d, q, it.y, it.z); break;
+    case 3: avg3d_chunk<R, ntet(3), NC>(d, q, it.y, it.z); break;
+    case 4: avg3d_chunk<R, ntet(4), NC>(d, q, it.y, it.z); break;
+    default: avg3d_chunk<R, ntet(5), NC>(d, q, it.y, it.z); break;
+  }
+}
+
+template <class R, int NP, int NC>
+__device__ __forceinline__ void theta3d_chunk(const LimDesc3<R>& d, R* q, int64_t e0, int ne, R* sq) {
+  LimArgs<R> a = d.a;
+  a.q = q;
+  a.e1 = e0 + ne;
+  for (int g = 0; g < ne; g += kLim3Epb) {
+    theta_apply_group<R, 3, NP, NC, kLim3Epb>(a, d.tab, KuhnTab2<R>{}, e0 + g, sq);
+    __syncthreads();  // the staging space is reused by the next group
+  }
+}
+
+template <class R, int NC>
+__global__ void __launch_bounds__(32 * kLim3Epb) theta3d_batch_kernel(LimBatch3<R> lb) {
+  __shared__ R sq[kLim3Epb * ntet(5) * NC];
+  const int4 it = lb.items[blockIdx.x];
+  const LimDesc3<R>& d = lb.solves[it.x];
+  R* q = d.qs[lb.which];
+  switch (d.P) {
+    case 1: theta3d_chunk<R, ntet(1), NC>(d, q, it.y, it.z, sq); break;
+    case 2: theta3d_chunk<R, ntet(2), NC>(d, q, it.y, it.z, sq); break;
+    case 3: theta3d_chunk<R, ntet(3), NC>(d, q, it.y, it.z, sq); break;
+    case 4: theta3d_chunk<R, ntet(4), NC>(d, q, it.y, it.z, sq); break;
+    default: theta3d_chunk<R, ntet(5), NC>(d, q, it.y, it.z, sq); break;
   }
 }
 

@@ -5,39 +5,44 @@
 
 namespace mxm {
 
-template <class Phys, int P, class Op>
-cudaError_t launch_tc_p(const Stage3DArgs<float>& a, const KuhnTab3<float>& tab, const Phys& ph,
+template <class Phys, int P, class Op, bool BATCH>
+cudaError_t launch_tc_p(const Stage3DArgs<float>& a, const Tc3Batch& bat, const KuhnTab3<float>& tab, const Phys& ph,
                         const unsigned char* img, int nsm, cudaStream_t st) {
   using S = TcShape<P, Phys::NC, Op>;
   if constexpr (!S::FITS) {
     return cudaErrorInvalidValue;  // the create call refuses these shapes
   } else {
     // 256 threads per block; a shape that fits one block per SM (the
-    // split-TF32 P4 tiles) takes 512 so that the SM still holds 16 warps
+    // split-TF32 P4 tiles, split-BF16 P5) takes 512 so that the SM still
+    // holds 16 warps.  Batched launches keep the current solve's arguments
+    // behind the tile's shared memory.
     constexpr int NT = S::blocks_for(S::SMEM) == 1 ? 512 : 256;
-    auto kern = stage3d_tc_kernel<Phys, P, NT, Op>;
+    constexpr size_t smem = BATCH ? S::BATCH_SMEM : S::SMEM;
+    static_assert(sizeof(Stage3DArgs<float>) <= 256, "batched arguments slot");
+    auto kern = stage3d_tc_kernel<Phys, P, NT, Op, BATCH>;
     static int bps = -1;
     if (bps < 0) {
-      cudaError_t e = persistent_blocks_per_sm((const void*)kern, NT, S::SMEM, &bps);
+      cudaError_t e = persistent_blocks_per_sm((const void*)kern, NT, smem, &bps);
       if (e != cudaSuccess) return e;
     }
-    const int ngroups = (a.ncell - a.cbeg + S::EC - 1) / S::EC;
+    const int ntiles = BATCH ? bat.nitems : (a.ncell - a.cbeg + S::EC - 1) / S::EC;
+    if (ntiles <= 0) return cudaSuccess;
     int nblk = nsm * bps;
-    if (nblk > ngroups) nblk = ngroups;
+    if (nblk > ntiles) nblk = ntiles;
     if (nblk < 1) nblk = 1;
-    kern<<<nblk, NT, S::SMEM, st>>>(a, tab, ph, img);
+    kern<<<nblk, NT, smem, st>>>(a, tab, ph, img, bat);
     return cudaGetLastError();
   }
 }
 
-template <class Phys, class Op>
-cudaError_t launch_tc_kind(int P, const Stage3DArgs<float>& a, const KuhnTab3<float>& tab, const Phys& ph,
-                           const unsigned char* img, int nsm, cudaStream_t st) {
+template <class Phys, class Op, bool BATCH>
+cudaError_t launch_tc_kind(int P, const Stage3DArgs<float>& a, const Tc3Batch& bat, const KuhnTab3<float>& tab,
+                           const Phys& ph, const unsigned char* img, int nsm, cudaStream_t st) {
   switch (P) {
-    case 2: return launch_tc_p<Phys, 2, Op>(a, tab, ph, img, nsm, st);
-    case 3: return launch_tc_p<Phys, 3, Op>(a, tab, ph, img, nsm, st);
-    case 4: return launch_tc_p<Phys, 4, Op>(a, tab, ph, img, nsm, st);
-    case 5: return launch_tc_p<Phys, 5, Op>(a, tab, ph, img, nsm, st);
+    case 2: return launch_tc_p<Phys, 2, Op, BATCH>(a, bat, tab, ph, img, nsm, st);
+    case 3: return launch_tc_p<Phys, 3, Op, BATCH>(a, bat, tab, ph, img, nsm, st);
+    case 4: return launch_tc_p<Phys, 4, Op, BATCH>(a, bat, tab, ph, img, nsm, st);
+    case 5: return launch_tc_p<Phys, 5, Op, BATCH>(a, bat, tab, ph, img, nsm, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -45,8 +50,33 @@ cudaError_t launch_tc_kind(int P, const Stage3DArgs<float>& a, const KuhnTab3<fl
 template <class Phys>
 cudaError_t launch_stage3d_tc(int P, int kind, const Stage3DArgs<float>& a, const KuhnTab3<float>& tab,
                               const Phys& ph, const unsigned char* img, int nsm, cudaStream_t st) {
-  return kind == TC_TF32 ? launch_tc_kind<Phys, OpTF32>(P, a, tab, ph, img, nsm, st)
-                         : launch_tc_kind<Phys, OpBF16>(P, a, tab, ph, img, nsm, st);
+  const Tc3Batch none{nullptr, nullptr, nullptr, 0};
+  return kind == TC_TF32 ? launch_tc_kind<Phys, OpTF32, false>(P, a, none, tab, ph, img, nsm, st)
+                         : launch_tc_kind<Phys, OpBF16, false>(P, a, none, tab, ph, img, nsm, st);
+}
+
+template <class Phys>
+cudaError_t launch_stage3d_tc_batch(int P, int kind, const Tc3Batch& bat, const Phys& ph, const unsigned char* img,
+                                    int nsm, cudaStream_t st) {
+  static const Stage3DArgs<float> a0{};
+  static const KuhnTab3<float> t0{};
+  return kind == TC_TF32 ? launch_tc_kind<Phys, OpTF32, true>(P, a0, bat, t0, ph, img, nsm, st)
+                         : launch_tc_kind<Phys, OpBF16, true>(P, a0, bat, t0, ph, img, nsm, st);
+}
+
+int tc_tile_cubes(int P, int NC, int kind) {
+  auto ec = [&](auto op) -> int {
+    using O = decltype(op);
+    switch (NC) {
+      case 1: return P == 2 ? TcShape<2, 1, O>::EC : P == 3 ? TcShape<3, 1, O>::EC : P == 4 ? TcShape<4, 1, O>::EC : TcShape<5, 1, O>::EC;
+      case 3: return P == 2 ? TcShape<2, 3, O>::EC : P == 3 ? TcShape<3, 3, O>::EC : P == 4 ? TcShape<4, 3, O>::EC : TcShape<5, 3, O>::EC;
+      case 5: return P == 2 ? TcShape<2, 5, O>::EC : P == 3 ? TcShape<3, 5, O>::EC : P == 4 ? TcShape<4, 5, O>::EC : TcShape<5, 5, O>::EC;
+      case 6: return P == 2 ? TcShape<2, 6, O>::EC : P == 3 ? TcShape<3, 6, O>::EC : P == 4 ? TcShape<4, 6, O>::EC : TcShape<5, 6, O>::EC;
+      case 9: return P == 2 ? TcShape<2, 9, O>::EC : P == 3 ? TcShape<3, 9, O>::EC : P == 4 ? TcShape<4, 9, O>::EC : TcShape<5, 9, O>::EC;
+    }
+    return 0;
+  };
+  return kind == TC_TF32 ? ec(OpTF32{}) : ec(OpBF16{});
 }
 
 bool tc_shape_fits(int P, int NC, int kind) {
@@ -75,7 +105,9 @@ using TS = ShallowWaterD<float>;
 using TH = MhdD<float>;
 #define MXM_INST_TC(PH)                                                                                      \
   template cudaError_t launch_stage3d_tc<PH>(int, int, const Stage3DArgs<float>&, const KuhnTab3<float>&,    \
-                                             const PH&, const unsigned char*, int, cudaStream_t);
+                                             const PH&, const unsigned char*, int, cudaStream_t);            \
+  template cudaError_t launch_stage3d_tc_batch<PH>(int, int, const Tc3Batch&, const PH&, const unsigned char*, \
+                                                   int, cudaStream_t);
 MXM_INST_TC(TA)
 MXM_INST_TC(TER)
 MXM_INST_TC(TEO)

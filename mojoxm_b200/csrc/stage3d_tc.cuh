@@ -100,6 +100,8 @@ struct TcShape {
   static constexpr bool BULK = (6 * NP * NC * 4) % 16 == 0;
   static_assert(O_BYTES <= 2 * B_BYTES, "staging tile must fit the operand buffer");
   static constexpr bool FITS = SMEM + 1024 <= size_t(227 * 1024);
+  // batched launches: the current solve's stage arguments behind the tile
+  static constexpr size_t OFF_ARGS = (SMEM + 15) / 16 * 16, BATCH_SMEM = OFF_ARGS + 256;
 };
 
 // Blocks per SM the register allocation must allow: what fits in shared
@@ -112,9 +114,18 @@ __host__ __device__ constexpr int tc_min_blocks() {
              : (Phys::kLightFlux ? 3 : 2);
 }
 
-template <class Phys, int P, int NT, class Op>
-__global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_kernel(Stage3DArgs<float> args, KuhnTab3<float> tabp, Phys ph,
-                                                         const unsigned char* __restrict__ a_image) {
+// BATCH: the tiles of many solves of one physics, order and operand kind
+// (Tc3Batch: per-tile {solve, first cell, cells}, grouped by solve; per
+// solve its stage arguments and metric table).  Each block takes a
+// contiguous range of tiles; when the solve changes, the block reloads the
+// solve's arguments (into shared memory, `args` then refers there), table
+// and face records.  A solve's tiles get exactly the arithmetic of the
+// single-solve launch, so batched results are bit-identical to it.
+// Single-solve launches pass `args0` / `tabp` and leave `bat` empty.
+template <class Phys, int P, int NT, class Op, bool BATCH>
+__global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_kernel(
+    Stage3DArgs<float> args0, const __grid_constant__ KuhnTab3<float> tabp, Phys ph,
+    const unsigned char* __restrict__ a_image, const __grid_constant__ Tc3Batch bat) {
   constexpr int NC = Phys::NC;
   using S = TcShape<P, NC, Op>;
   constexpr int NP = S::NP, NFP = S::NFP, KV = S::KV, KF = S::KF, NN = S::NN, M = S::M, NPO = S::NPO;
@@ -147,8 +158,36 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
   float* sFR = reinterpret_cast<float*>(smem + S::OFF_R);  // [work][8] face records
   int* sFM = reinterpret_cast<int*>(smem + S::OFF_M);      // [work][NFP] face-node indices
 
+  // the stage arguments: the kernel parameter, or the current solve's copy
+  // in shared memory (batched launches)
+  Stage3DArgs<float>* sArgs = reinterpret_cast<Stage3DArgs<float>*>(smem + S::OFF_ARGS);
+  const Stage3DArgs<float>& args = BATCH ? *sArgs : args0;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int ngroups = (args.ncell - args.cbeg + EC - 1) / EC;
+  const int ngroups = BATCH ? bat.nitems : (args0.ncell - args0.cbeg + EC - 1) / EC;
+  // tiles of this block: every gridDim.x-th from blockIdx.x (one solve), or
+  // a contiguous range (batched)
+  const int t_first = BATCH ? int(int64_t(blockIdx.x) * ngroups / gridDim.x) : int(blockIdx.x);
+  const int t_end = BATCH ? int(int64_t(blockIdx.x + 1) * ngroups / gridDim.x) : ngroups;
+  auto next_tile = [&](int g) -> int {
+    if constexpr (BATCH) return g + 1 < t_end ? g + 1 : ngroups;
+    else return g + int(gridDim.x);
+  };
+  auto tile_member = [&](int g) -> int {
+    if constexpr (BATCH) return bat.items[g].x;
+    else return 0;
+  };
+  auto tile_cell0 = [&](int g) -> int {
+    if constexpr (BATCH) return bat.items[g].y;
+    else return args0.cbeg + g * EC;
+  };
+  auto tile_cells = [&](int g) -> int {
+    if constexpr (BATCH) return bat.items[g].z;
+    else return min(EC, args0.ncell - args0.cbeg - g * EC);
+  };
+  auto tile_qin = [&](int g) -> const float* {
+    if constexpr (BATCH) return bat.margs[bat.items[g].x].q_in;
+    else return args0.q_in;
+  };
   if (tid == 0) {
     for (int k = 0; k < 4; ++k) mbar_init(&bar[k], 1);
     fence_mbar_init();
@@ -157,32 +196,36 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
     tmem_alloc(tslot, S::NCOLS);
     tmem_relinquish();
   }
+  // the solve's metric table into shared memory and its face records,
+  // decoded from the table: bits
+  // t | lf << 3 | nb_t << 5 | nb_lf << 8 | (axis + 1) << 10 | (dir > 0) << 12 | (side == 0) << 13
+  auto load_table = [&](const KuhnTab3<float>& tsrc) {
   {
-    const int* src = reinterpret_cast<const int*>(&tabp);
+    const int* src = reinterpret_cast<const int*>(&tsrc);
     int* dst = reinterpret_cast<int*>(tab);
     for (int k = tid; k < int(sizeof(KuhnTab3<float>) / 4); k += NT) dst[k] = src[k];
   }
-  // face records, decoded once per block from the topology table: bits
-  // t | lf << 3 | nb_t << 5 | nb_lf << 8 | (axis + 1) << 10 | (dir > 0) << 12 | (side == 0) << 13
   if constexpr (S::FREC) {
-  for (int w = tid; w < tabp.n_face_work; w += NT) {
-    const int tl = tabp.face_work[w], t = tl >> 2, lf = tl & 3;
-    const int ax = tabp.axis[t][lf], nbt = tabp.nb_t[t][lf], lf2 = tabp.nb_lf[t][lf];
+  for (int w = tid; w < tsrc.n_face_work; w += NT) {
+    const int tl = tsrc.face_work[w], t = tl >> 2, lf = tl & 3;
+    const int ax = tsrc.axis[t][lf], nbt = tsrc.nb_t[t][lf], lf2 = tsrc.nb_lf[t][lf];
     float* r = sFR + w * 8;
-    r[0] = tabp.normal[t][lf][0];
-    r[1] = tabp.normal[t][lf][1];
-    r[2] = tabp.normal[t][lf][2];
-    r[3] = tabp.fscale[t][lf];
-    r[4] = ax < 0 ? tabp.fscale[nbt][lf2] : 0.f;
+    r[0] = tsrc.normal[t][lf][0];
+    r[1] = tsrc.normal[t][lf][1];
+    r[2] = tsrc.normal[t][lf][2];
+    r[3] = tsrc.fscale[t][lf];
+    r[4] = ax < 0 ? tsrc.fscale[nbt][lf2] : 0.f;
     r[5] = __int_as_float(t | (lf << 3) | ((nbt & 7) << 5) | ((lf2 & 3) << 8) | ((ax + 1) << 10) |
-                          ((tabp.dir[t][lf] > 0 ? 1 : 0) << 12) | ((tabp.side[t][lf] == 0 ? 1 : 0) << 13));
+                          ((tsrc.dir[t][lf] > 0 ? 1 : 0) << 12) | ((tsrc.side[t][lf] == 0 ? 1 : 0) << 13));
   }
-  for (int idx = tid; idx < tabp.n_face_work * NFP; idx += NT) {
+  for (int idx = tid; idx < tsrc.n_face_work * NFP; idx += NT) {
     const int w = idx / NFP, m = idx - w * NFP;
-    const int tl = tabp.face_work[w], t = tl >> 2, lf = tl & 3;
-    sFM[idx] = int(tabp.own_node[lf][m]) | (int(tabp.nb_node[t][lf][m]) << 8) | (int(tabp.nb_m[t][lf][m]) << 16);
+    const int tl = tsrc.face_work[w], t = tl >> 2, lf = tl & 3;
+    sFM[idx] = int(tsrc.own_node[lf][m]) | (int(tsrc.nb_node[t][lf][m]) << 8) | (int(tsrc.nb_m[t][lf][m]) << 16);
   }
   }
+  };
+  if constexpr (!BATCH) load_table(tabp);
   // zero the flux tiles once: padding rows / k columns stay zero for good
   for (int k = tid; k < int(2 * S::B_BYTES / 16); k += NT) reinterpret_cast<uint4*>(sBhi)[k] = make_uint4(0, 0, 0, 0);
   tc_fence_before();
@@ -195,11 +238,11 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
     bulk_g2s(sAhi, a_image, uint32_t(2 * S::A_BYTES), &bar[3]);
   }
   auto issue = [&](int grp, int buf) {
-    const int c0 = args.cbeg + grp * EC, nc = min(EC, args.ncell - c0);
+    const int c0 = tile_cell0(grp), nc = tile_cells(grp);
     const uint32_t bytes = uint32_t(nc) * 6u * NP * NC * 4u;
     fence_proxy_async();
     mbar_arrive_expect_tx(&bar[buf], bytes);
-    bulk_g2s(sQ + buf * QV, args.q_in + size_t(c0) * 6 * NP * NC, bytes, &bar[buf]);
+    bulk_g2s(sQ + buf * QV, tile_qin(grp) + size_t(c0) * 6 * NP * NC, bytes, &bar[buf]);
   };
   // store the NC operand values v[c] of row (c, el), column k as bf16 hi / lo
   auto put = [&](int el, int k, const float* v) {
@@ -248,18 +291,18 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
   // last, partial tile of an odd-sized span takes plain loads).
   auto tile_bulk = [&](int g) -> bool {
     const size_t per_cube = size_t(6) * NP * NC * 4;
-    const int cg = args.cbeg + g * EC;
-    const size_t start = reinterpret_cast<uintptr_t>(args.q_in) + size_t(cg) * per_cube;
-    const size_t bytes = size_t(min(EC, args.ncell - cg)) * per_cube;
+    const size_t start = reinterpret_cast<uintptr_t>(tile_qin(g)) + size_t(tile_cell0(g)) * per_cube;
+    const size_t bytes = size_t(tile_cells(g)) * per_cube;
     return start % 16 == 0 && bytes % 16 == 0;
   };
   int buf = 0;
   bool failed = !block_wait_bounded(&bar[3], 0, kWaitLimitNs);
-  if (int(blockIdx.x) < ngroups && !failed && tile_bulk(blockIdx.x)) {
-    if (tid == 0) issue(blockIdx.x, 0);
+  if (t_first < t_end && !failed && tile_bulk(t_first)) {
+    if (tid == 0) issue(t_first, 0);
     pend |= 1u;
   }
-  const int nwork = tab->n_face_work;
+  const int nwork = BATCH ? (bat.nitems > 0 ? bat.tabs[bat.items[0].x].n_face_work : 0) : tab->n_face_work;
+  int cur_member = -1;  // batched: the solve whose arguments and table are loaded
   // ---- per-element constant flux Fbar = F(q at node 0) and the cube-face
   // treatment of tile g (state tile qt): one thread per (element, face); each
   // evaluates the element's flux at node 0 (4x redundant, but the phase's
@@ -267,7 +310,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
   // Fbar.  The cube-face treatment runs at the same time on threads from
   // NT/2 on.
   auto fbar_phase = [&](int g, const float* qt) {
-    const int ncg = min(EC, args.ncell - args.cbeg - g * EC);
+    const int ncg = tile_cells(g), cg0 = tile_cell0(g);
     for (int w = tid; w < ncg * 24; w += NT) {
       const int el = w >> 2, lf = w & 3, t = el % 6;
       float F[3 * NC];
@@ -282,7 +325,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
     }
     for (int w = tid - NT / 2; w >= 0 && w < ncg * 6; w += NT / 2) {
       const int cl = w / 6, dd = w - cl * 6;
-      cube_dirs3(args.cbeg + g * EC + cl, args.nx, args.ny, args.nz, args.bc, sNb + cl * 6, sMd + cl * 6, dd);
+      cube_dirs3(cg0 + cl, args.nx, args.ny, args.nz, args.bc, sNb + cl * 6, sMd + cl * 6, dd);
     }
   };
   // With two state buffers the next tile's copy lands while this tile is
@@ -290,19 +333,33 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
   // (fb_ready: sF, sFn, sNb, sMd and the tile wait are done for grp).
   bool fb_ready = false;
 
-  for (int grp = blockIdx.x; grp < ngroups && !failed; grp += gridDim.x, buf ^= (S::QB - 1)) {
-    const int cell0 = args.cbeg + grp * EC;
-    const int nc_here = min(EC, args.ncell - cell0);
+  for (int grp = t_first; grp < t_end && !failed; grp = next_tile(grp), buf ^= (S::QB - 1)) {
+    if constexpr (BATCH) {  // a new solve: its arguments, table and face records
+      const int m = tile_member(grp);
+      if (m != cur_member) {
+        __syncthreads();  // every thread is done with the previous solve's tile
+        {
+          const int* src = reinterpret_cast<const int*>(&bat.margs[m]);
+          int* dst = reinterpret_cast<int*>(sArgs);
+          for (int k = tid; k < int(sizeof(Stage3DArgs<float>) / 4); k += NT) dst[k] = src[k];
+        }
+        load_table(bat.tabs[m]);
+        __syncthreads();
+        cur_member = m;
+      }
+    }
+    const int cell0 = tile_cell0(grp);
+    const int nc_here = tile_cells(grp);
     const int ne_here = 6 * nc_here;
     float* q = sQ + buf * QV;
     if (fb_ready) {
       __syncthreads();  // every thread is done with the previous tile (its buffer, sO)
-      if (S::QB == 2 && grp + int(gridDim.x) < ngroups && tile_bulk(grp + gridDim.x)) {
-        if (tid == 0) issue(grp + gridDim.x, buf ^ 1);
+      if (S::QB == 2 && next_tile(grp) < ngroups && tile_bulk(next_tile(grp))) {
+        if (tid == 0) issue(next_tile(grp), buf ^ 1);
         pend |= 1u << (buf ^ 1);
       }
     } else if (tile_bulk(grp)) {
-      if (S::QB == 1 && grp != int(blockIdx.x)) {  // single buffer: load this tile now
+      if (S::QB == 1 && grp != t_first) {  // single buffer: load this tile now
         __syncthreads();                            // every thread is done with the previous tile
         if (tid == 0) issue(grp, 0);
         pend |= 1u;
@@ -313,8 +370,8 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
       }
       par ^= 1u << buf;
       pend &= ~(1u << buf);
-      if (S::QB == 2 && grp + int(gridDim.x) < ngroups && tile_bulk(grp + gridDim.x)) {
-        if (tid == 0) issue(grp + gridDim.x, buf ^ 1);
+      if (S::QB == 2 && next_tile(grp) < ngroups && tile_bulk(next_tile(grp))) {
+        if (tid == 0) issue(next_tile(grp), buf ^ 1);
         pend |= 1u << (buf ^ 1);
       }
     } else {
@@ -504,8 +561,9 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
     // copy was issued a whole tile earlier) ...
     fb_ready = false;
     if (S::QB == 2) {
-      const int nxt = grp + int(gridDim.x);
-      if (nxt < ngroups && tile_bulk(nxt)) {
+      // (a tile of another solve waits for the solve's table instead)
+      const int nxt = next_tile(grp);
+      if (nxt < ngroups && tile_bulk(nxt) && tile_member(nxt) == tile_member(grp)) {
         if (!block_wait_bounded(&bar[buf ^ 1], (par >> (buf ^ 1)) & 1u, kWaitLimitNs)) {
           failed = true;
           break;
@@ -571,7 +629,10 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
     }
   }
   if (failed) {
-    if (tid == 0 && args.err) atomicOr(args.err, 2);
+    // (batched: every solve's arguments carry the batch's error word; the
+    // shared copy may not be loaded yet when the operator image wait gave up)
+    int* errp = BATCH ? (bat.nitems > 0 ? bat.margs[bat.items[0].x].err : nullptr) : args0.err;
+    if (tid == 0 && errp) atomicOr(errp, 2);
     // let copies and the MMA batch still in flight land before the shared
     // tiles and the accumulator are released (each wait bounded)
     if (tid == 0) {

@@ -60,19 +60,83 @@ def test_batch_members_match_alone(prec):
 
 
 @pytest.mark.gpu
-def test_batch_rejects_3d_and_mixed_precision():
+def test_batch_rejects_mixed_state_widths_and_repeats():
     batch = M.Batch()
-    s3 = M.Solver(M.Mesh(2, 2, 2), C.PHYSICS_3D["euler_rusanov"](), P=2, precision="f32")
-    with pytest.raises(M.DGError):
-        batch.add(s3, 1e-3)
     a = M.Solver(M.Mesh(4, 4, dim=2), C.PHYSICS_2D["euler_hlle"](), P=2, precision="f32")
     b = M.Solver(M.Mesh(4, 4, dim=2), C.PHYSICS_2D["euler_hlle"](), P=2, precision="f64")
+    s3 = M.Solver(M.Mesh(2, 2, 2), C.PHYSICS_3D["euler_rusanov"](), P=2, precision="f64")
     batch.add(a, 1e-3)
     with pytest.raises(M.DGError):
-        batch.add(b, 1e-3)
+        batch.add(b, 1e-3)  # FP64 state beside FP32 state
+    with pytest.raises(M.DGError):
+        batch.add(s3, 1e-3)
     with pytest.raises(M.DGError):
         batch.add(a, 1e-3)  # already a member
     batch.close()
+
+
+# 3D members: (n cubes, P, physics, precision, limiter, bcs).  Tensor-core
+# members of one (physics, order, operand kind) share one batched launch;
+# the uneven meshes make tiles of several solves meet inside one block's
+# tile range, and the last tile of every solve partial.
+CASES_3D = [
+    ((3, 4, 2), 3, "euler_rusanov", "mixed", False, "periodic"),
+    ((5, 3, 3), 3, "euler_rusanov", "mixed", False, "walls"),
+    ((2, 2, 3), 3, "euler_rusanov", "mixed", False, "periodic"),
+    ((4, 3, 2), 3, "euler_hllec", "mixed", True, "outflow_x_wall_yz"),
+    ((3, 3, 3), 2, "euler_hllec", "mixed", True, "walls"),
+    ((3, 2, 2), 4, "maxwell", "tf32", False, "walls"),
+    ((2, 3, 2), 4, "maxwell", "tf32", False, "periodic"),
+    ((3, 2, 2), 5, "euler_hlle", "mixed", False, "inflow_outflow"),
+    ((3, 3, 2), 2, "mhd", "mixed", True, "periodic"),
+    ((2, 2, 2), 1, "euler_rusanov", "mixed", False, "periodic"),  # P1: the FP32 SIMT stage
+    ((3, 2, 2), 3, "shallow_water", "f32", False, "walls"),       # FP32 SIMT stage
+]
+
+
+@pytest.mark.gpu
+def test_batch_3d_members_match_alone():
+    """3D members (split-BF16 and split-TF32 tensor-core stages, limited and
+    not, and FP32 SIMT members) beside 2D members in one batch: every member
+    ends where the same solve stepped alone ends, bit for bit."""
+    batch = M.Batch()
+    pairs = []
+    for k, (n, P, name, prec, lim, bcn) in enumerate(CASES_3D):
+        phys = C.PHYSICS_3D[name]()
+        bcs = M.BoundaryConditions(*C.BCS_3D[bcn])
+        L = (1.0, 0.9, 1.1)
+        a = M.Solver(M.Mesh(*n, *L, bcs=bcs), phys, P=P, precision=prec)
+        b = M.Solver(M.Mesh(*n, *L, bcs=bcs), phys, P=P, precision=prec)
+        q = C.random_state(a.shape, phys, seed=300 + k)
+        for s in (a, b):
+            s.upload_state(q)
+            if lim:
+                s.enable_cell_limiter(True, 0.05)
+        dt = 2e-4 * (1 + k % 3) / (2 * P + 1)
+        batch.add(a, dt)
+        pairs.append((a, b, dt))
+    s2, phys2 = _make("f32", 6, 3, "euler_hlle", True, "walls")  # a 2D member too
+    t2, _ = _make("f32", 6, 3, "euler_hlle", True, "walls")
+    q2 = C.random_state(s2.shape, phys2, seed=399)
+    s2.upload_state(q2)
+    t2.upload_state(q2)
+    batch.add(s2, 1e-3)
+    pairs.append((s2, t2, 1e-3))
+    nsteps = 3
+    batch.step(nsteps)
+    batch.synchronize()
+    for a, b, dt in pairs:
+        b.step_n(dt, nsteps)
+        qa, qb = a.download_state(), b.download_state()
+        assert np.isfinite(qa).all()
+        assert np.array_equal(qa, qb), (a.P, a.precision, np.abs(qa - qb).max())
+    for k, (n, P, name, prec, lim, bcn) in enumerate(CASES_3D):
+        tc = P >= 2 and prec in ("mixed", "tf32")
+        assert (batch.tile_cells(k) > 0) == tc
+    batch.close()
+    for a, b, _ in pairs:
+        a.close()
+        b.close()
 
 
 @pytest.mark.gpu
