@@ -106,7 +106,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=32, help="cubes per axis")
     ap.add_argument("--P", type=int, default=3)
-    ap.add_argument("--precision", default="mixed", choices=["f64", "f32", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["f64", "f32", "mixed", "tf32"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--l2-steps", type=int, default=100,
                     help="SSPRK3 steps of the accuracy check vs the FP64 path (0 = skip)")
@@ -178,10 +178,11 @@ def dt_for(n, P, cfl=0.1):
 def workload_name(a):
     return (f"3D Euler smooth density wave, periodic [0,1]^3 Kuhn mesh {a.n}^3x6 = {6 * a.n ** 3} tets, "
             f"P={a.P}, Rusanov, " + {"f64": "FP64", "f32": "FP32",
-                                     "mixed": "FP32 state + split-BF16 tcgen05 contraction"}[a.precision])
+                                     "mixed": "FP32 state + split-BF16 tcgen05 contraction",
+                                     "tf32": "FP32 state + split-TF32 tcgen05 contraction"}[a.precision])
 
 
-DTYPE = {"f64": "f64", "f32": "f32", "mixed": "f32+bf16x3"}
+DTYPE = {"f64": "f64", "f32": "f32", "mixed": "f32+bf16x3", "tf32": "f32+tf32x3"}
 
 
 class NvmlClockSampler:
@@ -1003,7 +1004,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic_per_launch(a),
                          "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                         "kernel": "stage3d_tc_kernel" if a.precision == "mixed" else "stage3d_kernel",
+                         "kernel": "stage3d_tc_kernel" if a.precision in ("mixed", "tf32") else "stage3d_kernel",
                          "alg_bytes_per_launch": alg_bytes,
                          "contraction_tflops": nsm_flops / avg_launch_s / 1e12},
             "cpu_baseline": cb,
