@@ -69,6 +69,11 @@ struct Lim3Group {
 struct Batch {
   int device = 0, nsm = 148;
   std::vector<Lim3Group> lim3;
+  // the groups' stage launches of one stage run side by side on these
+  // streams (fork / join by events inside the captured step)
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> ev_side;
+  cudaEvent_t ev_fork = nullptr;
   cudaStream_t stream = nullptr;
   size_t rbytes = 0;
   std::vector<Handle*> members;
@@ -333,9 +338,9 @@ Batch2DArgs<R> stage_args(const Batch* b, const BatchGroup& g, const int4* items
 
 template <class R>
 cudaError_t launch_group_stage(const Batch* b, const BatchGroup& g, const int4* items, int nitems, int stage,
-                               int grid, size_t smem) {
+                               int grid, size_t smem, cudaStream_t st = nullptr) {
   const Batch2DArgs<R> a = stage_args<R>(b, g, items, nitems, stage);
-  return launch_stage2d_batch<R>(g.phys, a, grid, smem, b->stream);
+  return launch_stage2d_batch<R>(g.phys, a, grid, smem, st ? st : b->stream);
 }
 
 template <class R>
@@ -442,6 +447,19 @@ void build(Batch* b) {
       const Tc3Batch none{g.d_margs, g.d_tabs, g.d_items, 0};
       CK(launch_tc_group(b->members[g.members[0]], none, b->stream));
     }
+  // side streams for the groups of a stage (a group's launch underfills the
+  // GPU when its solves are few or small; groups of one stage are
+  // independent)
+  const int nside = int(std::min<size_t>(b->groups.size(), 8));
+  while (int(b->side.size()) < nside) {
+    cudaStream_t st;
+    cudaEvent_t ev;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    b->side.push_back(st);
+    b->ev_side.push_back(ev);
+  }
+  if (!b->ev_fork) CK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
   // one SSPRK3 step as a graph
   StreamSwap swap(b);
   CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -449,19 +467,33 @@ void build(Batch* b) {
   for (auto& g : b->groups)
     if (cap == cudaSuccess && g.dim == 2) cap = cudaMemsetAsync(g.d_counter, 0, 3 * sizeof(int), b->stream);
   for (int s = 0; s < 3 && cap == cudaSuccess; ++s) {
+    // fork: the batched group launches of the stage on the side streams
+    const bool fork = nside > 1;
+    if (fork) {
+      cap = cudaEventRecord(b->ev_fork, b->stream);
+      for (int i = 0; i < nside && cap == cudaSuccess; ++i) cap = cudaStreamWaitEvent(b->side[i], b->ev_fork, 0);
+    }
+    int gi = 0;
     for (auto& g : b->groups) {
       if (cap != cudaSuccess) break;
+      cudaStream_t st = fork ? b->side[gi++ % nside] : b->stream;
       if (g.dim == 2) {
-        cap = launch_group_stage<R>(b, g, g.d_items, g.nitems, s, g.grid, g.smem);
+        cap = launch_group_stage<R>(b, g, g.d_items, g.nitems, s, g.grid, g.smem, st);
       } else if (g.tc) {
         const Tc3Batch bat{g.d_margs + size_t(s) * g.members.size(), g.d_tabs, g.d_items, g.nitems};
-        cap = launch_tc_group(b->members[g.members[0]], bat, b->stream);
-      } else {
+        cap = launch_tc_group(b->members[g.members[0]], bat, st);
+      } else {  // single-solve launches on the batch stream
         try {
           for (int m : g.members) stage_only(b->members[m], s, b->dt[m]);
         } catch (CudaError& ex) {
           cap = ex.e;
         }
+      }
+    }
+    if (fork) {  // join before the limiter passes
+      for (int i = 0; i < nside && cap == cudaSuccess; ++i) {
+        cap = cudaEventRecord(b->ev_side[i], b->side[i]);
+        if (cap == cudaSuccess) cap = cudaStreamWaitEvent(b->stream, b->ev_side[i], 0);
       }
     }
     // 3D limiter passes: batched per component count; the two-fluid state
@@ -575,6 +607,11 @@ int mxm_dg_batch_destroy(void* batch) {
   mxm::release_graph(b);
   for (auto& g : b->groups) mxm::free_group(g);
   mxm::free_lim3(b);
+  for (size_t i = 0; i < b->side.size(); ++i) {
+    cudaStreamDestroy(b->side[i]);
+    cudaEventDestroy(b->ev_side[i]);
+  }
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   cudaFree(b->d_solves);
   cudaFree(b->derr);
   cudaStreamDestroy(b->stream);

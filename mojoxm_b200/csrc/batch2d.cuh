@@ -195,7 +195,7 @@ __device__ __forceinline__ void avg_chunk(const SolveDesc2<R>* sd, int which, in
     const R* q = qb + e * NP * NC + c;
     R s = R(0);
 #pragma unroll
-    for (int n = 0; n < NP; ++n) s += __ldg(&sd->w[n]) * q[n * NC];
+    for (int n = 0; n < NP; ++n) s = fma(__ldg(&sd->w[n]), q[n * NC], s);
     sd->avg[e * NC + c] = s;
   }
 }

@@ -28,7 +28,7 @@ __global__ void cell_avg_kernel(LimArgs<R> a) {
   const R* q = a.q + e * NP * NC + c;
   R s = R(0);
 #pragma unroll
-  for (int n = 0; n < NP; ++n) s += __ldg(&a.w[n]) * q[n * NC];
+  for (int n = 0; n < NP; ++n) s = fma(__ldg(&a.w[n]), q[n * NC], s);
   a.avg[tid] = s;
 }
 
@@ -162,7 +162,7 @@ __device__ __forceinline__ void avg3d_chunk(const LimDesc3<R>& d, R* q, int64_t 
     const R* qe = q + e * NP * NC + c;
     R s = R(0);
 #pragma unroll
-    for (int n = 0; n < NP; ++n) s += __ldg(&d.a.w[n]) * qe[n * NC];
+    for (int n = 0; n < NP; ++n) s = fma(__ldg(&d.a.w[n]), qe[n * NC], s);
     d.a.avg[e * NC + c] = s;
   }
 }
@@ -281,6 +281,7 @@ __device__ __forceinline__ void theta2d_block(R* q, const R* avg, int64_t e0, in
   __syncthreads();
   R* base = q + e0 * VALS;
   const R tiny = R(1.0e-30);
+#pragma unroll 4
   for (int idx = tid; idx < ne * NP; idx += blockDim.x) {
     const int el = idx / NP;
     const R own = s_own[el];
@@ -297,6 +298,7 @@ __device__ __forceinline__ void theta2d_block(R* q, const R* avg, int64_t e0, in
     if (al < R(1)) atomicMin(&s_th[el], TB::to(al));
   }
   __syncthreads();
+#pragma unroll 4
   for (int idx = tid; idx < ne * VALS; idx += blockDim.x) {
     const int el = idx / VALS;
     const R th = TB::from(s_th[el]);
