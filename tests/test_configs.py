@@ -159,14 +159,21 @@ def test_reduced_precision_steps_track_f64(P, prec):
 @pytest.mark.parametrize("prec", ["f32", "mixed"])
 @pytest.mark.parametrize("P", [3, 4, 5])
 def test_reduced_precision_l2_after_100_steps(P, prec):
-    """Relative L2 against the FP64 kernels after 100 SSPRK3 steps of the
-    Euler smooth wave: <= 1e-6 at P3, <= 2e-6 at P4/P5 on this coarse 8^3
-    mesh (measured 0.7e-6 at P3; 1.2e-6 FP32 and 1.6e-6 split-BF16 at P4/P5:
-    FP32 state rounding, a random walk of ~0.7e-6 after 300 stages, plus the
-    FP32 flux and the 16-bit hi+lo operator).  Without exact stage weights
-    (the reference's a q_a + b q_b with a = 1/3 and b = 2/3 rounded
-    separately to FP32 sums to 1 + 3e-8) every variant drifts to ~3e-6."""
-    n = 8
+    """Regression bound on a coarse 8^3 mesh: relative L2 against the FP64
+    kernels after 100 SSPRK3 steps of the Euler smooth wave <= 2e-6
+    (measured 0.7e-6 at P3; 1.2e-6 FP32 and 1.6e-6 split-BF16 at P4/P5).
+    The error is FP32 state rounding, a random walk of ~0.7e-6 after 300
+    stages, plus the FP32 flux and, for split-BF16, the 16-bit hi+lo
+    operator.  Without exact stage weights (the reference's a q_a + b q_b
+    with a = 1/3 and b = 2/3 rounded separately to FP32 sums to 1 + 3e-8)
+    every variant drifts to ~3e-6.  The 1e-6 target is checked at the
+    configuration sizes below."""
+    err = _l2_after_100_steps(8, P, prec)
+    print(f"8^3 P{P} {prec}: rel L2 vs FP64 after 100 steps {err:.2e}")
+    assert err <= 2e-6, err
+
+
+def _l2_after_100_steps(n, P, prec):
     phys = C.euler(M.FLUX_RUSANOV)
     mesh = M.Mesh(n, n, n)
     s64 = M.Solver(mesh, phys, P=P, precision="f64")
@@ -181,8 +188,27 @@ def test_reduced_precision_l2_after_100_steps(P, prec):
     s.step_n(dt, 100)
     err = rel_l2(s.download_state().astype(np.float64), q64)
     s.close()
-    print(f"P{P} {prec}: rel L2 vs FP64 after 100 steps {err:.2e}")
-    assert err <= (1e-6 if P == 3 else 2e-6), err
+    return err
+
+
+# The 1e-6 target after 100 steps, at the sizes the Euler configurations
+# run: P3 on the 32^3 headline mesh (measured 7.0e-7 split-BF16, 7.4e-7
+# FP32), P4 on 24^3 (9.3e-7, 8.1e-7), P5 on 16^3.  P5 misses it (1.20e-6
+# split-BF16, 1.32e-6 FP32): the FP32 state alone, with FP64 fluxes and
+# operator, is 0.7e-6 from FP64 after 300 roundings and the FP32 fluxes add
+# the rest.  That case is an expected failure, strict, so that the miss
+# stays visible here and a fix would show up as an unexpected pass.
+P5_MISS = pytest.mark.xfail(strict=True, reason="FP32-state floor: P5 on 16^3 is 1.2e-6 to 1.3e-6 after 100 "
+                                                "steps against the 1e-6 target")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["mixed", "f32"])
+@pytest.mark.parametrize("P,n", [(3, 32), (4, 24), pytest.param(5, 16, marks=P5_MISS)])
+def test_l2_target_at_config_sizes(P, n, prec):
+    err = _l2_after_100_steps(n, P, prec)
+    print(f"{n}^3 P{P} {prec}: rel L2 vs FP64 after 100 steps {err:.2e}")
+    assert err <= 1e-6, err
 
 
 def alfven_case():
