@@ -237,12 +237,17 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
     mbar_arrive_expect_tx(&bar[3], uint32_t(2 * S::A_BYTES));
     bulk_g2s(sAhi, a_image, uint32_t(2 * S::A_BYTES), &bar[3]);
   }
+  // the tile's state into shared memory; the tile's q_a (read by the
+  // epilogue when it is not the tile's own state) into L2 at the same time
   auto issue = [&](int grp, int buf) {
     const int c0 = tile_cell0(grp), nc = tile_cells(grp);
     const uint32_t bytes = uint32_t(nc) * 6u * NP * NC * 4u;
     fence_proxy_async();
     mbar_arrive_expect_tx(&bar[buf], bytes);
-    bulk_g2s(sQ + buf * QV, tile_qin(grp) + size_t(c0) * 6 * NP * NC, bytes, &bar[buf]);
+    const float* qin = tile_qin(grp);
+    bulk_g2s(sQ + buf * QV, qin + size_t(c0) * 6 * NP * NC, bytes, &bar[buf]);
+    const Stage3DArgs<float>& ta = BATCH ? bat.margs[bat.items[grp].x] : args0;
+    if (!ta.rhs_only && ta.q_a != qin) bulk_prefetch_l2(ta.q_a + size_t(c0) * 6 * NP * NC, bytes);
   };
   // store the NC operand values v[c] of row (c, el), column k as bf16 hi / lo
   auto put = [&](int el, int k, const float* v) {

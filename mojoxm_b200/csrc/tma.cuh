@@ -33,6 +33,12 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                : "memory");
 }
 
+// Bring `bytes` of global memory at src into L2 ahead of their use (no
+// completion to wait for); src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_test_parity(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
