@@ -112,6 +112,9 @@ __global__ void __launch_bounds__(NT) stage2d_batch_kernel(Batch2DArgs<R> ba, Ph
     fence_proxy_async();
     mbar_arrive_expect_tx(&bar[b], bytes);
     bulk_g2s(sQ + size_t(b) * ba.qv, src, bytes, &bar[b]);
+    // stages 1 and 2 combine with q (the step's start state): that span of
+    // the item into L2 an item ahead of its epilogue
+    if (ba.stage > 0) bulk_prefetch_l2(ba.solves[item.x].q[0] + size_t(item.y) * 2 * np * NC, bytes);
   };
   if (tid == 0) {
     const int it = atomicAdd(ba.counter, 1);

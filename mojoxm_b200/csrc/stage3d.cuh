@@ -81,6 +81,9 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
     fence_proxy_async();
     mbar_arrive_expect_tx(&bar[buf], bytes);
     bulk_g2s(sQ + buf * QV, args.q_in + size_t(c0) * 6 * NP * NC, bytes, &bar[buf]);
+    // the tile's q_a (read by the epilogue when it is not the tile's own
+    // state) into L2 a tile ahead of its use
+    if (!args.rhs_only && args.q_a != args.q_in) bulk_prefetch_l2(args.q_a + size_t(c0) * 6 * NP * NC, bytes);
   };
   // bulk copy when the tile span starts and ends on 16-byte boundaries
   // (whole tiles of the usual shapes; a partial last tile may take plain loads)
