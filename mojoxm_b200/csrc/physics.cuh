@@ -314,6 +314,21 @@ struct EulerD {
   // near vacuum E and the kinetic energy cancel, and an FP32 difference
   // would decide the floor on rounding noise.
   __device__ void limit(R* q) const {  // euler.mojo:758-792
+    if constexpr (sizeof(R) == 4) {
+      // Fast accept in FP32 for the common case far from the floors: with
+      // rho above rho_min, a = E rho and b = |m|^2 / 2 rounded in FP32 (each
+      // within a few ulps, b a sum of non-negative terms) and d = a - b,
+      // |d - (E rho - |m|^2 / 2)| <= 4 * 2^-24 (a + b); when (gamma - 1) d
+      // clears p_min rho by (gamma - 1) 1e-6 (a + b) plus 0.1 % of p_min rho
+      // (the products' own rounding), the FP64 test below passes and would
+      // leave q unchanged.  NaNs fail the comparisons and take the FP64 path.
+      const float r = q[0];
+      if (r > rho_min) {
+        const float a = q[4] * r, bb = 0.5f * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        const float g1 = gamma - 1.0f;
+        if (g1 * (a - bb) > 1.001f * (p_min * r) + 1.0e-6f * g1 * (a + bb)) return;
+      }
+    }
     const double rho = double(q[0]), g1 = double(gamma) - 1.0, pm = double(p_min);
     if (!(rho > double(rho_min))) {
       q[0] = rho_min; q[1] = R(0); q[2] = R(0); q[3] = R(0);
