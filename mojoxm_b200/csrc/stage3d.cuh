@@ -27,6 +27,8 @@
 //  * q_a / q_b equal to q_in (SSPRK3 stages 1-3) are read from the tile, so
 //    each stage moves the algorithmic minimum of state bytes.
 #pragma once
+#include <type_traits>
+
 #include "dg_common.cuh"
 #include "physics.cuh"
 #include "tma.cuh"
@@ -41,13 +43,56 @@ struct Stage3DShape {
   static constexpr int BSTR = stage3d_bstr(P, NC, int(sizeof(R)));
 };
 
-template <class R, class Phys, int P, int EC, int RI, int NT, bool ASMEM>
+// Rows a lane holds after ks_fold over a group of 2M lanes: the row set
+// halves (rounded up) at every level.
+constexpr int ks_rows(int n, int m) { return m >= 1 ? ks_rows((n + 1) / 2, m / 2) : n; }
+
+// K-split contraction: the 2M lanes of one aligned group each summed every
+// 2M-th K column of the same RI x NC tile.  A butterfly that halves the row
+// set at every level (lanes with bit m set keep the upper rows) leaves this
+// lane the complete sums of rows base .. base + cnt - 1 in acc[0 .. cnt).
+// Every sum adds the same partials in the same tree order on every run.
+template <int M, int N, int RI, int NC, class R>
+__device__ __forceinline__ void ks_fold(R (&acc)[RI][NC], unsigned gmask, int lane, int& base, int& cnt) {
+  if constexpr (M >= 1) {
+    constexpr int LO = (N + 1) / 2;
+    const bool hi = (lane & M) != 0;
+#pragma unroll
+    for (int j = 0; j < LO; ++j) {
+      const bool has_up = j + LO < N;
+      const int ju = has_up ? j + LO : 0;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const R up = has_up ? acc[ju][c] : R(0);
+        const R send = hi ? acc[j][c] : up;
+        const R keep = hi ? up : acc[j][c];
+        acc[j][c] = keep + __shfl_xor_sync(gmask, send, M);
+      }
+    }
+    if (hi) {
+      base += LO;
+      cnt = cnt > LO ? cnt - LO : 0;
+    } else {
+      cnt = cnt < LO ? cnt : LO;
+    }
+    ks_fold<M / 2, LO, RI, NC, R>(acc, gmask, lane, base, cnt);
+  }
+}
+
+template <class R, class Phys, int P, int EC, int RI, int KS, int NT, bool ASMEM>
 __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTab3<R> tabp, Phys ph) {
   constexpr int NC = Phys::NC;
   using S = Stage3DShape<P, NC, R>;
   constexpr int NP = S::NP, NFP = S::NFP, K = S::K, BSTR = S::BSTR;
   constexpr int EB = 6 * EC, G = NP / RI, QV = EB * NP * NC;
   static_assert(NP % RI == 0, "row tile must divide NP");
+  static_assert(KS >= 1 && KS <= 16 && (KS & (KS - 1)) == 0 && NT % KS == 0, "K split: power of two within a warp");
+  // operator rows read from shared memory as 16-byte vectors where the row
+  // tile and the operator's offset in shared memory allow it
+  constexpr size_t kAOff = 16 + (sizeof(KuhnTab3<R>) + 15) / 16 * 16 + sizeof(R) * (2 * size_t(QV) + size_t(EB) * BSTR);
+  constexpr int AV = 16 / int(sizeof(R));
+  constexpr bool AVEC = ASMEM && NP % AV == 0 && RI % AV == 0 && kAOff % 16 == 0;
+  using RV = typename std::conditional<sizeof(R) == 8, double2, float4>::type;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);                       // [2]
   KuhnTab3<R>* tab = reinterpret_cast<KuhnTab3<R>*>(smem_raw + 16);            // topology
@@ -205,10 +250,14 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
       }
     }
     __syncthreads();
-    // ---- contraction rhs = A B, source, RK combine, floor, store
+    // ---- contraction rhs = A B, source, RK combine, floor, store.  A work
+    // is an RI x NC tile of one element; KS consecutive lanes share it, each
+    // summing every KS-th K column, and ks_fold hands each lane its rows.
     const bool a_in = args.q_a == args.q_in, b_in = args.q_b == args.q_in;
-    for (int w = tid; w < ne_here * G; w += NT) {
-      const int el = w / G, g = w - el * G;
+    constexpr int RO = ks_rows(RI, KS / 2);
+    for (int w = tid; w < ne_here * G * KS; w += NT) {
+      const int wk = w / KS, s = w - wk * KS;
+      const int el = wk / G, g = wk - el * G;
       const int i0 = g * RI;
       R acc[RI][NC];
 #pragma unroll
@@ -217,10 +266,27 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
         for (int c = 0; c < NC; ++c) acc[r][c] = R(0);
       const R* b = &sB[el * BSTR];
 #pragma unroll 4
-      for (int k = 0; k < K; ++k) {
+      for (int k = s; k < K; k += KS) {
         R av[RI], bv[NC];
+        if constexpr (AVEC) {
 #pragma unroll
-        for (int r = 0; r < RI; ++r) av[r] = ASMEM ? Aop[k * NP + i0 + r] : __ldg(&Aop[k * NP + i0 + r]);
+          for (int r = 0; r < RI; r += AV) {
+            const RV v = *reinterpret_cast<const RV*>(&Aop[k * NP + i0 + r]);
+            if constexpr (sizeof(R) == 8) {
+              av[r] = R(v.x);
+              av[r + 1] = R(v.y);
+            } else {
+              const float4 f = *reinterpret_cast<const float4*>(&v);
+              av[r] = R(f.x);
+              av[r + 1] = R(f.y);
+              av[r + 2] = R(f.z);
+              av[r + 3] = R(f.w);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < RI; ++r) av[r] = ASMEM ? Aop[k * NP + i0 + r] : __ldg(&Aop[k * NP + i0 + r]);
+        }
 #pragma unroll
         for (int c = 0; c < NC; ++c) bv[c] = b[k * NC + c];
 #pragma unroll
@@ -228,10 +294,17 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
 #pragma unroll
           for (int c = 0; c < NC; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
       }
+      int rbase = 0, rcnt = RI;
+      if constexpr (KS > 1) {
+        const int lane = tid & 31;
+        const unsigned gmask = ((1u << KS) - 1u) << (lane & ~(KS - 1));
+        ks_fold<KS / 2, RI, RI, NC, R>(acc, gmask, lane, rbase, rcnt);
+      }
       const size_t e = size_t(cell0) * 6 + el;
 #pragma unroll
-      for (int r = 0; r < RI; ++r) {
-        const int i = i0 + r;
+      for (int r = 0; r < RO; ++r) {
+        if (r >= rcnt) break;
+        const int i = i0 + rbase + r;
         const size_t base = (e * NP + i) * NC;
         const R* ql = &q[(el * NP + i) * NC];
         R src[NC];

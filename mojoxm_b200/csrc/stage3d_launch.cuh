@@ -12,6 +12,15 @@ constexpr int ri_capped(int base, int NP, int NC, int cap) {
   return 1;
 }
 
+// K-split width of the contraction: the largest power of two (at most 16)
+// that keeps every work of a tile within one pass of the block and at least
+// 8 K columns per lane.
+constexpr int ks_pick(int works, int nt, int K) {
+  int ks = 1;
+  while (ks < 16 && works * ks * 2 <= nt && K / (ks * 2) >= 8) ks *= 2;
+  return ks;
+}
+
 template <class R, int P, int NC>
 struct Cfg3 {
   using S = Stage3DShape<P, NC, R>;
@@ -30,6 +39,11 @@ struct Cfg3 {
   static constexpr int EC_RAW = kBudget > kFixed ? int((kBudget - kFixed) / kPerCube) : 1;
   static constexpr int EC = EC_RAW > 16 ? 16 : (EC_RAW < 1 ? 1 : EC_RAW);
   static constexpr int NT = 256;
+  // split K only where a tile's works leave most of the block idle: with
+  // 120 of 256 threads busy (FP64 P3) a 2-way split measured -4 %, with 126
+  // (FP32 P4) +9 %, with 42 (FP64 P4) +69 %
+  static constexpr int WORKS = 6 * EC * (S::NP / RI);
+  static constexpr int KS = (sizeof(R) == 8 ? WORKS * 8 < 3 * NT : WORKS * 2 <= NT) ? ks_pick(WORKS, NT, S::K) : 1;
   static constexpr size_t kSmem = stage3d_smem_bytes<R, P, NC, EC, ASMEM>();
   static constexpr bool FITS = kSmem <= kMaxSmemPerBlock;
 };
@@ -40,7 +54,7 @@ cudaError_t launch3_p(const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phy
   if constexpr (!C::FITS) {
     return cudaErrorInvalidConfiguration;  // refused at mxm_dg_create already
   } else {
-  auto kern = stage3d_kernel<R, Phys, P, C::EC, C::RI, C::NT, C::ASMEM>;
+  auto kern = stage3d_kernel<R, Phys, P, C::EC, C::RI, C::KS, C::NT, C::ASMEM>;
   static int bps = -1;
   if (bps < 0) {
     cudaError_t e = persistent_blocks_per_sm((const void*)kern, C::NT, C::kSmem, &bps);
