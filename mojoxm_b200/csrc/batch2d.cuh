@@ -192,14 +192,24 @@ struct LimBatch2DArgs {
 template <class R, int NP, int NC>
 __device__ __forceinline__ void avg_chunk(const SolveDesc2<R>* sd, int which, int e0, int ne) {
   const R* qb = sd->q[which];
+  R* ext = sd->avg + int64_t(2) * sd->ncell * NC;  // component 0's nodal extrema
   for (int idx = threadIdx.x; idx < ne * NC; idx += blockDim.x) {
     const int64_t e = e0 + idx / NC;
     const int c = idx % NC;
     const R* q = qb + e * NP * NC + c;
-    R s = R(0);
+    R s = R(0), lo = q[0], hi = q[0];
 #pragma unroll
-    for (int n = 0; n < NP; ++n) s = fma(__ldg(&sd->w[n]), q[n * NC], s);
+    for (int n = 0; n < NP; ++n) {
+      const R v = q[n * NC];
+      s = fma(__ldg(&sd->w[n]), v, s);
+      lo = fmin(lo, v);
+      hi = fmax(hi, v);
+    }
     sd->avg[e * NC + c] = s;
+    if (c == 0) {
+      ext[e * 2] = lo;
+      ext[e * 2 + 1] = hi;
+    }
   }
 }
 
@@ -226,12 +236,13 @@ __global__ void __launch_bounds__(kLim2dBlock) theta_batch_kernel(LimBatch2DArgs
   const int4 item = la.items[blockIdx.x];
   const SolveDesc2<R>* sd = &la.solves[item.x];
   R* q = sd->q[la.which];
+  const R* ext = sd->avg + int64_t(2) * sd->ncell * NC;
   switch (item.w) {
-    case 1: theta2d_block<R, ntri(1), NC>(q, sd->avg, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
-    case 2: theta2d_block<R, ntri(2), NC>(q, sd->avg, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
-    case 3: theta2d_block<R, ntri(3), NC>(q, sd->avg, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
-    case 4: theta2d_block<R, ntri(4), NC>(q, sd->avg, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
-    default: theta2d_block<R, ntri(5), NC>(q, sd->avg, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
+    case 1: theta2d_block<R, ntri(1), NC>(q, sd->avg, ext, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
+    case 2: theta2d_block<R, ntri(2), NC>(q, sd->avg, ext, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
+    case 3: theta2d_block<R, ntri(3), NC>(q, sd->avg, ext, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
+    case 4: theta2d_block<R, ntri(4), NC>(q, sd->avg, ext, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
+    default: theta2d_block<R, ntri(5), NC>(q, sd->avg, ext, item.y, item.z, sd->tab, sd->nx, sd->ny, sd->bc, sd->eps2, lim_smem); break;
   }
 }
 

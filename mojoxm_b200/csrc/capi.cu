@@ -856,7 +856,9 @@ Handle* create(const mxm_dg_mesh_desc* m, const mxm_dg_physics_desc* ph, int P, 
       CK(cudaMemcpyAsync(raw->tcimg, img.data(), img.size(), cudaMemcpyHostToDevice, raw->stream));
       CK(cudaStreamSynchronize(raw->stream));  // img goes out of scope
     }
-    dev_alloc(raw, &raw->avg, size_t(raw->ne) * raw->NC * raw->rbytes);
+    // cell means, then the nodal extrema of the components that enter theta
+    // (all in 3D, component 0 in 2D)
+    dev_alloc(raw, &raw->avg, size_t(raw->ne) * (raw->NC + 2 * (raw->dim == 3 ? raw->NC : 1)) * raw->rbytes);
     dev_alloc(raw, reinterpret_cast<void**>(&raw->partial), raw->npartial * sizeof(double));
     dev_alloc(raw, reinterpret_cast<void**>(&raw->dscalar), 4 * sizeof(double));
     dev_alloc(raw, reinterpret_cast<void**>(&raw->uscalar), 4 * sizeof(unsigned long long));

@@ -9,11 +9,29 @@
 // only, BC self-neighbours skipped, applied to every component.
 //
 // B200 form: pass 1 computes cell means with one thread per (element,
-// component) over coalesced loads; pass 2 (3D) stages a group of elements'
-// nodal values in shared memory with contiguous loads, reduces theta per
-// element with warp shuffles, and writes the limited values back
-// contiguously only for elements with theta < 1; pass 2 (2D) runs
-// node-parallel over a chunk of elements (theta2d_block).
+// component) over coalesced loads, and beside each mean of a component that
+// enters theta the least and the largest of its nodal values; pass 2 gets
+// theta from those extrema and the neighbours' means without reading the
+// nodal state, and reads and rewrites the values of the elements with
+// theta < 1 only (3D: a warp per element; 2D: a block per chunk of
+// elements, theta2d_block).
+//
+// Why the extrema suffice: the ratio alpha(d) = (D^2 + 2 D d + eps^2) /
+// (D^2 + 2 d^2 + D d + eps^2) of a node with deviation magnitude d from the
+// mean (D the neighbours' bound on that side) is 1 at d = 0, rises to a
+// single maximum and then falls (the numerator of its derivative, D^3 + D
+// eps^2 - 4 D d^2 - 4 D^2 d - 4 d eps^2, is positive at d = 0 and
+// decreasing in d).  So over the nodes of one side it is >= 1 before its
+// crossing of 1 and decreasing after it, and min(1, min over the side's
+// nodes) is min(1, alpha at the side's largest deviation); d = u - mean is
+// monotone in u (also in floating point), so that node is the one with the
+// largest (or, below the mean, the least) value.  theta is then the
+// reference's minimum over every node, up to the rounding of alpha at
+// near-equal deviations.
+//
+// Extrema layout: ext = avg + ne * NC, ext[(e * NCT + c) * 2 + {0, 1}] =
+// {least, largest} nodal value of component c of element e, for the NCT
+// components that enter theta (every component in 3D, component 0 in 2D).
 #pragma once
 #include "dg_common.cuh"
 
@@ -32,25 +50,64 @@ __global__ void cell_avg_kernel(LimArgs<R> a) {
   a.avg[tid] = s;
 }
 
-// Theta + apply of elements eb .. eb + EPB - 1 (those below a.e1), one
-// warp per element, in a block of 32*EPB threads; `sqf` is the block's
-// staging space of EPB * NP * NC values.  Every thread must call it (it
-// synchronises the block once).
-template <class R, int DIM, int NP, int NC, int EPB>
-__device__ __forceinline__ void theta_apply_group(const LimArgs<R>& a, const KuhnTab3<R>& t3, const KuhnTab2<R>& t2,
-                                                  int64_t eb, R* sqf) {
+template <class R, int NP, int NC, int NCT>
+__global__ void cell_avg_kernel(LimArgs<R> a) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (tid >= a.ne * NC) return;
+  const int64_t e = tid / NC;
+  const int c = int(tid - e * NC);
+  const R* q = a.q + e * NP * NC + c;
+  R s = R(0), lo = q[0], hi = q[0];
+#pragma unroll
+  for (int n = 0; n < NP; ++n) {
+    const R v = q[n * NC];
+    s = fma(__ldg(&a.w[n]), v, s);
+    lo = fmin(lo, v);
+    hi = fmax(hi, v);
+  }
+  a.avg[tid] = s;
+  if (c < NCT) {
+    R* x = a.avg + a.ne * NC + (e * NCT + c) * 2;
+    x[0] = lo;
+    x[1] = hi;
+  }
+}
+
+// min(1, alpha at the largest deviation above and below the mean): theta
+// of one component from its mean `own`, the neighbours' bounds lo / hi and
+// the element's least / largest nodal value.  Deviations of magnitude
+// <= 1e-30 do not constrain, as in the reference.
+template <class R>
+__device__ __forceinline__ R theta_from_extrema(R own, R lo, R hi, R umin, R umax, R eps2) {
+  const R tiny = R(1.0e-30);
+  R th = R(1);
+  R pD = hi - own;
+  if (pD < R(0)) pD = R(0);
+  R nD = own - lo;
+  if (nD < R(0)) nD = R(0);
+  const R dp = umax - own;
+  if (dp > tiny) {
+    const R D2 = pD * pD, d2 = dp * dp, Dd = pD * dp;
+    const R al = (D2 + R(2) * Dd + eps2) / (D2 + R(2) * d2 + Dd + eps2);
+    if (al < th) th = al;
+  }
+  const R dn = own - umin;
+  if (dn > tiny) {
+    const R D2 = nD * nD, d2 = dn * dn, Dd = nD * dn;
+    const R al = (D2 + R(2) * Dd + eps2) / (D2 + R(2) * d2 + Dd + eps2);
+    if (al < th) th = al;
+  }
+  return th;
+}
+
+// Theta + apply of element e (< a.e1) by one warp; every lane of the warp
+// calls it with the same e.
+template <class R, int DIM, int NP, int NC>
+__device__ __forceinline__ void theta_apply_elem(const LimArgs<R>& a, const KuhnTab3<R>& t3, const KuhnTab2<R>& t2,
+                                                 int64_t e) {
   constexpr int NTYPE = DIM == 3 ? 6 : 2, NFACE = DIM + 1, VALS = NP * NC;
-  R (*sq)[VALS] = reinterpret_cast<R (*)[VALS]>(sqf);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t e = eb + warp;
-  const bool valid = e < a.e1;
-  // contiguous block load of the EPB elements
-  const int64_t base = eb * VALS;
-  const int64_t nvals = (a.e1 - eb) * VALS;
-  for (int idx = threadIdx.x; idx < EPB * VALS; idx += 32 * EPB)
-    if (idx < nvals) (&sq[0][0])[idx] = a.q[base + idx];
-  __syncthreads();
-  if (!valid) return;
+  constexpr int NCT = DIM == 3 ? NC : 1;  // components entering theta
+  const int lane = threadIdx.x & 31;
   const int t = int(e % NTYPE);
   const int64_t cell = e / NTYPE;
   int cpos[3];
@@ -66,7 +123,7 @@ __device__ __forceinline__ void theta_apply_group(const LimArgs<R>& a, const Kuh
     cpos[2] = 0;
   }
   const int ncells[3] = {a.nx, a.ny, a.nz};
-  // neighbour cell means: lanes 0..NFACE-1 each resolve one face
+  // neighbour elements: lanes 0..NFACE-1 each resolve one face
   int64_t nb = e;
   if (lane < NFACE) {
     const int lf = lane;
@@ -85,36 +142,24 @@ __device__ __forceinline__ void theta_apply_group(const LimArgs<R>& a, const Kuh
       }
     }
   }
-  constexpr int NCT = DIM == 3 ? NC : 1;  // components entering theta
-  R own[NCT], lo[NCT], hi[NCT];
+  int64_t nbs[NFACE];
 #pragma unroll
-  for (int c = 0; c < NCT; ++c) own[c] = lo[c] = hi[c] = a.avg[e * NC + c];
-#pragma unroll
-  for (int lf = 0; lf < NFACE; ++lf) {
-    const int64_t n = __shfl_sync(0xffffffffu, nb, lf);
-    if (DIM == 2 && n == e) continue;  // 2D: BC faces do not constrain
-#pragma unroll
-    for (int c = 0; c < NCT; ++c) {
-      const R v = a.avg[n * NC + c];
-      if (v < lo[c]) lo[c] = v;
-      if (v > hi[c]) hi[c] = v;
-    }
-  }
+  for (int lf = 0; lf < NFACE; ++lf) nbs[lf] = __shfl_sync(0xffffffffu, nb, lf);
+  // lane c < NCT: theta of component c
   R th = R(1);
-  const R tiny = R(1.0e-30);
-  for (int idx = lane; idx < NP * NCT; idx += 32) {
-    const int n = idx / NCT, c = idx - n * NCT;
-    const R dl = sq[warp][n * NC + c] - own[c];
-    const R da = dl >= R(0) ? dl : -dl;
-    if (da <= tiny) continue;
-    R pD = hi[c] - own[c];
-    if (pD < R(0)) pD = R(0);
-    R nD = own[c] - lo[c];
-    if (nD < R(0)) nD = R(0);
-    const R D = dl > R(0) ? pD : nD;
-    const R D2 = D * D, d2 = da * da, Dd = D * da;
-    const R al = (D2 + R(2) * Dd + a.eps2) / (D2 + R(2) * d2 + Dd + a.eps2);
-    if (al < th) th = al;
+  if (lane < NCT) {
+    const int c = lane;
+    const R own = a.avg[e * NC + c];
+    R lo = own, hi = own;
+#pragma unroll
+    for (int lf = 0; lf < NFACE; ++lf) {
+      if (DIM == 2 && nbs[lf] == e) continue;  // 2D: BC faces do not constrain
+      const R v = a.avg[nbs[lf] * NC + c];
+      if (v < lo) lo = v;
+      if (v > hi) hi = v;
+    }
+    const R* x = a.avg + a.ne * NC + (e * NCT + c) * 2;
+    th = theta_from_extrema(own, lo, hi, x[0], x[1], a.eps2);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -126,15 +171,15 @@ __device__ __forceinline__ void theta_apply_group(const LimArgs<R>& a, const Kuh
   for (int idx = lane; idx < VALS; idx += 32) {
     const int c = idx % NC;
     const R bm = a.avg[e * NC + c];
-    qe[idx] = bm + th * (sq[warp][idx] - bm);
+    qe[idx] = bm + th * (qe[idx] - bm);
   }
 }
 
 // One warp per element; EPB elements per block of 32*EPB threads.
 template <class R, int DIM, int NP, int NC, int EPB>
 __global__ void __launch_bounds__(32 * EPB) theta_apply_kernel(LimArgs<R> a, KuhnTab3<R> t3, KuhnTab2<R> t2) {
-  __shared__ R sq[EPB * NP * NC];
-  theta_apply_group<R, DIM, NP, NC, EPB>(a, t3, t2, a.e0 + int64_t(blockIdx.x) * EPB, sq);
+  const int64_t e = a.e0 + int64_t(blockIdx.x) * EPB + (threadIdx.x >> 5);
+  if (e < a.e1) theta_apply_elem<R, DIM, NP, NC>(a, t3, t2, e);
 }
 
 // ---- batched 3D limiter: the cell-mean and theta passes of many limited
@@ -156,14 +201,22 @@ constexpr int kLim3Chunk = 128, kLim3Epb = 8;
 
 template <class R, int NP, int NC>
 __device__ __forceinline__ void avg3d_chunk(const LimDesc3<R>& d, R* q, int64_t e0, int ne) {
+  R* ext = d.a.avg + d.a.ne * NC;
   for (int idx = threadIdx.x; idx < ne * NC; idx += blockDim.x) {
     const int64_t e = e0 + idx / NC;
     const int c = idx % NC;
     const R* qe = q + e * NP * NC + c;
-    R s = R(0);
+    R s = R(0), lo = qe[0], hi = qe[0];
 #pragma unroll
-    for (int n = 0; n < NP; ++n) s = fma(__ldg(&d.a.w[n]), qe[n * NC], s);
+    for (int n = 0; n < NP; ++n) {
+      const R v = qe[n * NC];
+      s = fma(__ldg(&d.a.w[n]), v, s);
+      lo = fmin(lo, v);
+      hi = fmax(hi, v);
+    }
     d.a.avg[e * NC + c] = s;
+    ext[(e * NC + c) * 2] = lo;
+    ext[(e * NC + c) * 2 + 1] = hi;
   }
 }
 
@@ -181,79 +234,55 @@ __global__ void avg3d_batch_kernel(LimBatch3<R> lb) {
   }
 }
 
+// The elements of a chunk, one warp each in turn.
 template <class R, int NP, int NC>
-__device__ __forceinline__ void theta3d_chunk(const LimDesc3<R>& d, R* q, int64_t e0, int ne, R* sq) {
+__device__ __forceinline__ void theta3d_chunk(const LimDesc3<R>& d, R* q, int64_t e0, int ne) {
   LimArgs<R> a = d.a;
   a.q = q;
   a.e1 = e0 + ne;
-  for (int g = 0; g < ne; g += kLim3Epb) {
-    theta_apply_group<R, 3, NP, NC, kLim3Epb>(a, d.tab, KuhnTab2<R>{}, e0 + g, sq);
-    __syncthreads();  // the staging space is reused by the next group
-  }
+  for (int g = threadIdx.x >> 5; g < ne; g += kLim3Epb) theta_apply_elem<R, 3, NP, NC>(a, d.tab, KuhnTab2<R>{}, e0 + g);
 }
 
 template <class R, int NC>
 __global__ void __launch_bounds__(32 * kLim3Epb) theta3d_batch_kernel(LimBatch3<R> lb) {
-  __shared__ R sq[kLim3Epb * ntet(5) * NC];
   const int4 it = lb.items[blockIdx.x];
   const LimDesc3<R>& d = lb.solves[it.x];
   R* q = d.qs[lb.which];
   switch (d.P) {
-    case 1: theta3d_chunk<R, ntet(1), NC>(d, q, it.y, it.z, sq); break;
-    case 2: theta3d_chunk<R, ntet(2), NC>(d, q, it.y, it.z, sq); break;
-    case 3: theta3d_chunk<R, ntet(3), NC>(d, q, it.y, it.z, sq); break;
-    case 4: theta3d_chunk<R, ntet(4), NC>(d, q, it.y, it.z, sq); break;
-    default: theta3d_chunk<R, ntet(5), NC>(d, q, it.y, it.z, sq); break;
+    case 1: theta3d_chunk<R, ntet(1), NC>(d, q, it.y, it.z); break;
+    case 2: theta3d_chunk<R, ntet(2), NC>(d, q, it.y, it.z); break;
+    case 3: theta3d_chunk<R, ntet(3), NC>(d, q, it.y, it.z); break;
+    case 4: theta3d_chunk<R, ntet(4), NC>(d, q, it.y, it.z); break;
+    default: theta3d_chunk<R, ntet(5), NC>(d, q, it.y, it.z); break;
   }
 }
 
 // A block of kLim2dBlock threads limits up to kLim2dBlock consecutive
-// elements, node-parallel: (1) one thread per element resolves its cell
-// mean and the neighbours' bounds (component 0; BC faces skipped); (2) one
-// thread per (element, node) evaluates the Barth-Jespersen / Venkatakrishnan
-// ratio of its node and folds it into the element's theta with a shared
-// atomic minimum on the value's bits (non-negative IEEE values order like
-// their unsigned bit patterns, and a minimum is exact in any order, so theta
-// equals the reference's sequential minimum bit for bit); (3) one thread per
-// value rewrites the values of elements with theta < 1.  Loads and stores
-// run over consecutive values of the chunk.  The arithmetic is the
-// reference's 2D limiter (src/local_mesh_2d_gpu_limiter.mojo:74-153): theta
-// from component 0, faces whose neighbour resolves to the element itself
-// (BC faces) do not constrain, theta scales every component's deviation from
-// its cell mean.  Dynamic shared memory lim2d_smem_bytes<R, NP, NC>().
+// elements: (1) one thread per element resolves its cell mean and the
+// neighbours' bounds (component 0; BC faces skipped) and gets theta from
+// the element's nodal extrema of component 0 (theta_from_extrema); (2) one
+// thread per value rewrites the values of the elements with theta < 1, over
+// consecutive values of the chunk.  The arithmetic is the reference's 2D
+// limiter (src/local_mesh_2d_gpu_limiter.mojo:74-153): theta from component
+// 0, faces whose neighbour resolves to the element itself (BC faces) do not
+// constrain, theta scales every component's deviation from its cell mean.
+// `ext` holds the extrema (one theta component).  Dynamic shared memory
+// lim2d_smem_bytes<R, NP, NC>().
 constexpr int kLim2dBlock = 128;
 template <class R, int NP, int NC>
 constexpr size_t lim2d_smem_bytes() {
-  return size_t(kLim2dBlock) * (3 * sizeof(R) + sizeof(unsigned long long));
+  return size_t(kLim2dBlock) * sizeof(R);
 }
 
-template <class R>
-struct ThetaBits;  // theta as an unsigned integer of the same width
-template <>
-struct ThetaBits<float> {
-  using U = unsigned int;
-  __device__ static U to(float v) { return __float_as_uint(v); }
-  __device__ static float from(U u) { return __uint_as_float(u); }
-};
-template <>
-struct ThetaBits<double> {
-  using U = unsigned long long;
-  __device__ static U to(double v) { return (unsigned long long)__double_as_longlong(v); }
-  __device__ static double from(U u) { return __longlong_as_double((long long)u); }
-};
-
 template <class R, int NP, int NC>
-__device__ __forceinline__ void theta2d_block(R* q, const R* avg, int64_t e0, int ne, const KuhnTab2<R>& tab, int nx,
-                                              int ny, const int* bc, R eps2, unsigned char* smem) {
+__device__ __forceinline__ void theta2d_block(R* q, const R* avg, const R* ext, int64_t e0, int ne,
+                                              const KuhnTab2<R>& tab, int nx, int ny, const int* bc, R eps2,
+                                              unsigned char* smem) {
   constexpr int VALS = NP * NC;
-  using TB = ThetaBits<R>;
-  using U = typename TB::U;
-  U* s_th = reinterpret_cast<U*>(smem);  // 8-byte aligned first
-  R* s_own = reinterpret_cast<R*>(smem + size_t(kLim2dBlock) * sizeof(unsigned long long));
-  R* s_lo = s_own + kLim2dBlock;
-  R* s_hi = s_lo + kLim2dBlock;
+  R* s_th = reinterpret_cast<R*>(smem);
   const int tid = threadIdx.x;
-  if (tid < ne) {  // the element's cell mean and its interior neighbours' bounds
+  bool lim = false;
+  if (tid < ne) {
     const int64_t e = e0 + tid;
     const int t = int(e & 1);
     const int64_t cell = e >> 1;
@@ -273,35 +302,16 @@ __device__ __forceinline__ void theta2d_block(R* q, const R* avg, int64_t e0, in
       if (v < lo) lo = v;
       if (v > hi) hi = v;
     }
-    s_own[tid] = own;
-    s_lo[tid] = lo;
-    s_hi[tid] = hi;
-    s_th[tid] = TB::to(R(1));
+    const R th = theta_from_extrema(own, lo, hi, ext[e * 2], ext[e * 2 + 1], eps2);
+    s_th[tid] = th;
+    lim = th < R(1);
   }
-  __syncthreads();
+  if (!__syncthreads_or(lim)) return;  // no element of the chunk is limited
   R* base = q + e0 * VALS;
-  const R tiny = R(1.0e-30);
-#pragma unroll 4
-  for (int idx = tid; idx < ne * NP; idx += blockDim.x) {
-    const int el = idx / NP;
-    const R own = s_own[el];
-    const R dl = base[size_t(idx) * NC] - own;  // component 0 of node idx - el NP of element el
-    const R da = dl >= R(0) ? dl : -dl;
-    if (da <= tiny) continue;
-    R pD = s_hi[el] - own;
-    if (pD < R(0)) pD = R(0);
-    R nD = own - s_lo[el];
-    if (nD < R(0)) nD = R(0);
-    const R D = dl > R(0) ? pD : nD;
-    const R D2 = D * D, d2 = da * da, Dd = D * da;
-    const R al = (D2 + R(2) * Dd + eps2) / (D2 + R(2) * d2 + Dd + eps2);
-    if (al < R(1)) atomicMin(&s_th[el], TB::to(al));
-  }
-  __syncthreads();
 #pragma unroll 4
   for (int idx = tid; idx < ne * VALS; idx += blockDim.x) {
     const int el = idx / VALS;
-    const R th = TB::from(s_th[el]);
+    const R th = s_th[el];
     if (!(th < R(1))) continue;
     const int c = (idx - el * VALS) % NC;
     const R bm = avg[(e0 + el) * NC + c];
@@ -314,7 +324,7 @@ __global__ void __launch_bounds__(kLim2dBlock) theta2d_kernel(LimArgs<R> a, Kuhn
   extern __shared__ __align__(16) unsigned char lim_smem[];
   const int64_t e0 = int64_t(blockIdx.x) * kLim2dBlock;
   const int ne = int(a.ne - e0 < kLim2dBlock ? a.ne - e0 : kLim2dBlock);
-  theta2d_block<R, NP, NC>(a.q, a.avg, e0, ne, t2, a.nx, a.ny, a.bc, a.eps2, lim_smem);
+  theta2d_block<R, NP, NC>(a.q, a.avg, a.avg + a.ne * NC, e0, ne, t2, a.nx, a.ny, a.bc, a.eps2, lim_smem);
 }
 
 // ---- FP64 reductions: per-block partial sums, then a fixed-order final sum.

@@ -20,7 +20,7 @@ __global__ void reduce_final_kernel(const double* partial, int n, int kind, doub
 template <class R, int DIM, int NP, int NC>
 cudaError_t lim_np(const LimArgs<R>& a, const KuhnTab3<R>& t3, const KuhnTab2<R>& t2, cudaStream_t st) {
   const int64_t n1 = a.ne * NC;
-  cell_avg_kernel<R, NP, NC><<<int((n1 + 255) / 256), 256, 0, st>>>(a);
+  cell_avg_kernel<R, NP, NC, DIM == 3 ? NC : 1><<<int((n1 + 255) / 256), 256, 0, st>>>(a);
   if (DIM == 2) {
     constexpr size_t smem = lim2d_smem_bytes<R, NP, NC>();
     static bool attr = false;
@@ -32,9 +32,7 @@ cudaError_t lim_np(const LimArgs<R>& a, const KuhnTab3<R>& t3, const KuhnTab2<R>
     }
     theta2d_kernel<R, NP, NC><<<int((a.ne + kLim2dBlock - 1) / kLim2dBlock), kLim2dBlock, smem, st>>>(a, t2);
   } else {
-    // elements per block: their staged states stay within 40 KB of static shared memory
-    constexpr size_t kElem = sizeof(R) * NP * NC;
-    constexpr int EPB = kElem * 8 <= 40960 ? 8 : (kElem * 4 <= 40960 ? 4 : 2);
+    constexpr int EPB = 8;  // warps (elements) per block
     if (a.e1 > a.e0)
       theta_apply_kernel<R, DIM, NP, NC, EPB><<<int((a.e1 - a.e0 + EPB - 1) / EPB), 32 * EPB, 0, st>>>(a, t3, t2);
   }

@@ -89,8 +89,8 @@ int nc_of(const mxm_dg_physics_desc& p, int dim) {
                                          : 3;
 }
 
-// device bytes a solve holds: three state buffers, the limiter means, the
-// operator and weights, plus a small fixed allowance
+// device bytes a solve holds: three state buffers, the limiter means and
+// nodal extrema, the operator and weights, plus a small fixed allowance
 size_t footprint(const Request& r, int64_t* dof) {
   const int dim = r.mesh.dim, P = r.P;
   const int64_t ncell = int64_t(r.mesh.nx) * r.mesh.ny * (dim == 3 ? r.mesh.nz : 1);
@@ -101,7 +101,7 @@ size_t footprint(const Request& r, int64_t* dof) {
   const size_t rb = r.prec == MXM_DG_PREC_F64 ? 8 : 4;
   const int K = dim == 3 ? 3 * NP + 4 * NFP : 2 * NP + 3 * NFP;
   *dof = ne * NP * NC;
-  return size_t(3 * ne * NP * NC + ne * NC + K * NP + NP) * rb + (1 << 16);
+  return size_t(3 * ne * NP * NC + ne * (NC + 2 * (dim == 3 ? NC : 1)) + K * NP + NP) * rb + (1 << 16);
 }
 
 void finish(Server* s, Request* r, bool ok) {
