@@ -373,8 +373,9 @@ int mxm_dg_batch_last_error(void* batch, char* buf, int len);
 /* ---- serving loop (no reference counterpart) -----------------------------
  * Continuous batching of independent solves on the calling thread's device:
  * a scheduler thread admits submitted requests in arrival order while their
- * device footprint (three state buffers, limiter means, operator) fits
- * `hbm_budget_bytes` and fewer than `max_active` are running, builds each on
+ * device footprint (three state buffers, limiter means and nodal extrema,
+ * operator) fits `hbm_budget_bytes` and fewer than `max_active` are
+ * running, builds each on
  * its own stream (handle + device IC fill, see mxm_dg_fill_ic) and feeds
  * every running solve chunks of `steps_per_chunk` SSPRK3 steps, so requests
  * that arrive while others run are admitted as memory frees up and their
