@@ -218,6 +218,43 @@ struct StreamSwap {
   }
 };
 
+// Order of a 3D tensor-core group's tiles.  The batched kernel gives block
+// b the contiguous item range [b n / G, (b + 1) n / G) of the launch's G
+// blocks, so that a block rarely changes solve.  Within each solve's span
+// the tiles are laid out so that, at every step k of the blocks' loops, the
+// blocks working on that solve take consecutive tiles (the order of the
+// single-solve kernel, whose blocks take every G-th tile): neighbouring
+// tiles, whose y / z neighbour rows overlap, are then loaded together and
+// stay in L2.  Each tile's arithmetic does not depend on the order.
+void order_tc3_items(const Handle* h0, std::vector<int4>& items) {
+  const int64_t n = int64_t(items.size());
+  int G = 0;
+  if (n < 2 || tc_group_grid(h0, int(n), &G) != cudaSuccess || G < 2) {
+    cudaGetLastError();
+    return;
+  }
+  std::vector<int> owner(size_t(n), 0), step(size_t(n), 0);
+  for (int blk = 0; blk < G; ++blk)
+    for (int64_t p = int64_t(blk) * n / G, hi = int64_t(blk + 1) * n / G, p0 = p; p < hi; ++p) {
+      owner[size_t(p)] = blk;
+      step[size_t(p)] = int(p - p0);
+    }
+  std::vector<int4> out(items.size());
+  std::vector<int64_t> pos;
+  for (int64_t s0 = 0; s0 < n;) {
+    int64_t s1 = s0;
+    while (s1 < n && items[size_t(s1)].x == items[size_t(s0)].x) ++s1;
+    pos.resize(size_t(s1 - s0));
+    for (int64_t p = s0; p < s1; ++p) pos[size_t(p - s0)] = p;
+    std::stable_sort(pos.begin(), pos.end(), [&](int64_t a, int64_t c) {
+      return step[size_t(a)] != step[size_t(c)] ? step[size_t(a)] < step[size_t(c)] : owner[size_t(a)] < owner[size_t(c)];
+    });
+    for (int64_t i = 0; i < s1 - s0; ++i) out[size_t(pos[size_t(i)])] = items[size_t(s0 + i)];
+    s0 = s1;
+  }
+  items.swap(out);
+}
+
 // Tiles {member of the group, first cell, cells, 0} and per-stage arguments
 // of a 3D tensor-core group.
 void build_tc3(Batch* b, BatchGroup& g) {
@@ -235,6 +272,7 @@ void build_tc3(Batch* b, BatchGroup& g) {
     for (int st = 0; st < 3; ++st) margs[size_t(st) * ng + j] = tc_stage_args(h, st, b->dt[g.members[j]], b->derr);
     tabs[j] = h->t3f;
   }
+  order_tc3_items(h0, items);
   g.ec[g.P] = ec;
   g.nitems = int(items.size());
   CK(cudaMalloc(&g.d_items, std::max<size_t>(1, items.size()) * sizeof(int4)));

@@ -292,6 +292,14 @@ cudaError_t launch_tc_group(const Handle* h0, const Tc3Batch& bat, cudaStream_t 
   });
 }
 
+cudaError_t tc_group_grid(const Handle* h0, int ntiles, int* out) {
+  return with_phys3d<float>(h0, [&](const auto& ph) -> cudaError_t {
+    if constexpr (std::decay<decltype(ph)>::type::NC <= 16)
+      return stage3d_tc_batch_grid(h0->P, h0->tc_kind, ph, h0->nsm, ntiles, out);
+    return cudaErrorInvalidValue;
+  });
+}
+
 template <class R>
 cudaError_t stage_launch(Handle* h, const void* qi, const void* qa, const void* qb, void* qo, double b, double c,
                          double dt, int rhs_only, int64_t c0, int64_t c1) {

@@ -226,6 +226,9 @@ struct Tc3Batch {
 template <class Phys>
 cudaError_t launch_stage3d_tc_batch(int P, int kind, const Tc3Batch& bat, const Phys& ph, const unsigned char* img,
                                     int nsm, cudaStream_t st);
+// Blocks that launch_stage3d_tc_batch runs for `ntiles` tiles.
+template <class Phys>
+cudaError_t stage3d_tc_batch_grid(int P, int kind, const Phys& ph, int nsm, int ntiles, int* out);
 
 // Tensor-core 3D stage for FP32 state, P = 2..5: split-BF16 (kind
 // TC_BF16, tcgen05 kind::f16) or split-TF32 (TC_TF32, kind::tf32) operands;

@@ -125,6 +125,7 @@ void limit_buf(Handle* h, void* qv);
 // physics, order and operand kind, and the cubes per tile of that shape.
 Stage3DArgs<float> tc_stage_args(const Handle* h, int s, double dt, int* err);
 cudaError_t launch_tc_group(const Handle* h0, const Tc3Batch& bat, cudaStream_t st);
+cudaError_t tc_group_grid(const Handle* h0, int ntiles, int* out);
 int tc_tile_cubes(int P, int NC, int kind);
 // NCCL halo transport (slab.cu): exchange the ghost layers of state buffer
 // `which` on the handle's stream; release the link

@@ -1,9 +1,42 @@
 // Launch + explicit instantiation of the tensor-core 3D stage kernel
 // (split-BF16 or split-TF32 operands) for P = 2..5 where the shape fits
 // shared memory; P = 1 uses the FP32 SIMT kernel.
+#include <type_traits>
+
 #include "stage3d_tc.cuh"
 
 namespace mxm {
+
+// Threads per block and resident blocks per SM of one instantiation.
+// 256 threads per block; a shape that fits one block per SM (the split-TF32
+// P4 tiles, split-BF16 P5) takes 512 so that the SM still holds 16 warps.
+// Batched launches keep the current solve's arguments behind the tile's
+// shared memory.
+template <class Phys, int P, class Op, bool BATCH>
+struct TcLaunch {
+  using S = TcShape<P, Phys::NC, Op>;
+  static constexpr int NT = S::blocks_for(S::SMEM) == 1 ? 512 : 256;
+  static constexpr size_t smem = BATCH ? S::BATCH_SMEM : S::SMEM;
+  static cudaError_t blocks_per_sm(int* out) {
+    static int bps = -1;
+    if (bps < 0) {
+      cudaError_t e = persistent_blocks_per_sm((const void*)stage3d_tc_kernel<Phys, P, NT, Op, BATCH>, NT, smem, &bps);
+      if (e != cudaSuccess) return e;
+    }
+    *out = bps;
+    return cudaSuccess;
+  }
+  // persistent grid: every resident block, at most one per tile
+  static cudaError_t grid(int nsm, int ntiles, int* out) {
+    int bps = 0;
+    cudaError_t e = blocks_per_sm(&bps);
+    if (e != cudaSuccess) return e;
+    int nblk = nsm * bps;
+    if (nblk > ntiles) nblk = ntiles;
+    *out = nblk < 1 ? 1 : nblk;
+    return cudaSuccess;
+  }
+};
 
 template <class Phys, int P, class Op, bool BATCH>
 cudaError_t launch_tc_p(const Stage3DArgs<float>& a, const Tc3Batch& bat, const KuhnTab3<float>& tab, const Phys& ph,
@@ -12,27 +45,39 @@ cudaError_t launch_tc_p(const Stage3DArgs<float>& a, const Tc3Batch& bat, const 
   if constexpr (!S::FITS) {
     return cudaErrorInvalidValue;  // the create call refuses these shapes
   } else {
-    // 256 threads per block; a shape that fits one block per SM (the
-    // split-TF32 P4 tiles, split-BF16 P5) takes 512 so that the SM still
-    // holds 16 warps.  Batched launches keep the current solve's arguments
-    // behind the tile's shared memory.
-    constexpr int NT = S::blocks_for(S::SMEM) == 1 ? 512 : 256;
-    constexpr size_t smem = BATCH ? S::BATCH_SMEM : S::SMEM;
+    using L = TcLaunch<Phys, P, Op, BATCH>;
     static_assert(sizeof(Stage3DArgs<float>) <= 256, "batched arguments slot");
-    auto kern = stage3d_tc_kernel<Phys, P, NT, Op, BATCH>;
-    static int bps = -1;
-    if (bps < 0) {
-      cudaError_t e = persistent_blocks_per_sm((const void*)kern, NT, smem, &bps);
-      if (e != cudaSuccess) return e;
-    }
     const int ntiles = BATCH ? bat.nitems : (a.ncell - a.cbeg + S::EC - 1) / S::EC;
     if (ntiles <= 0) return cudaSuccess;
-    int nblk = nsm * bps;
-    if (nblk > ntiles) nblk = ntiles;
-    if (nblk < 1) nblk = 1;
-    kern<<<nblk, NT, smem, st>>>(a, tab, ph, img, bat);
+    int nblk = 1;
+    cudaError_t e = L::grid(nsm, ntiles, &nblk);
+    if (e != cudaSuccess) return e;
+    stage3d_tc_kernel<Phys, P, L::NT, Op, BATCH><<<nblk, L::NT, L::smem, st>>>(a, tab, ph, img, bat);
     return cudaGetLastError();
   }
+}
+
+template <class Phys, class Op>
+cudaError_t batch_grid_kind(int P, int nsm, int ntiles, int* out) {
+  auto one = [&](auto pc) -> cudaError_t {
+    constexpr int PP = decltype(pc)::value;
+    if constexpr (!TcShape<PP, Phys::NC, Op>::FITS) return cudaErrorInvalidValue;
+    else return TcLaunch<Phys, PP, Op, true>::grid(nsm, ntiles, out);
+  };
+  switch (P) {
+    case 2: return one(std::integral_constant<int, 2>{});
+    case 3: return one(std::integral_constant<int, 3>{});
+    case 4: return one(std::integral_constant<int, 4>{});
+    case 5: return one(std::integral_constant<int, 5>{});
+  }
+  return cudaErrorInvalidValue;
+}
+
+// Blocks a batched launch of `ntiles` tiles runs (the same rule as the launch).
+template <class Phys>
+cudaError_t stage3d_tc_batch_grid(int P, int kind, const Phys&, int nsm, int ntiles, int* out) {
+  return kind == TC_TF32 ? batch_grid_kind<Phys, OpTF32>(P, nsm, ntiles, out)
+                         : batch_grid_kind<Phys, OpBF16>(P, nsm, ntiles, out);
 }
 
 template <class Phys, class Op, bool BATCH>
@@ -107,7 +152,8 @@ using TH = MhdD<float>;
   template cudaError_t launch_stage3d_tc<PH>(int, int, const Stage3DArgs<float>&, const KuhnTab3<float>&,    \
                                              const PH&, const unsigned char*, int, cudaStream_t);            \
   template cudaError_t launch_stage3d_tc_batch<PH>(int, int, const Tc3Batch&, const PH&, const unsigned char*, \
-                                                   int, cudaStream_t);
+                                                   int, cudaStream_t);                                         \
+  template cudaError_t stage3d_tc_batch_grid<PH>(int, int, const PH&, int, int, int*);
 MXM_INST_TC(TA)
 MXM_INST_TC(TER)
 MXM_INST_TC(TEO)
