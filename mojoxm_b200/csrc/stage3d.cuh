@@ -26,6 +26,10 @@
 //    tile.
 //  * q_a / q_b equal to q_in (SSPRK3 stages 1-3) are read from the tile, so
 //    each stage moves the algorithmic minimum of state bytes.
+//  * Where a tile's contraction works (element x RI-row group) would leave
+//    most of the block idle (one-cube tiles at P4/P5 in FP64), KS lanes of
+//    a warp share a work, each summing every KS-th K column, and a shuffle
+//    butterfly (ks_fold) gives each lane complete rows for the epilogue.
 #pragma once
 #include <type_traits>
 
