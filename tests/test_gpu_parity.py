@@ -142,20 +142,22 @@ def test_reductions_and_wavespeed(oracle_mod):
 
 
 # Mixed precision (FP32 state, split-BF16 tcgen05 contraction) vs the FP64
-# oracle: element-wise RHS error relative to max |RHS|.  Split-BF16 products
-# carry ~16 significant bits; the bound leaves room for the cancellation in
-# the derivative/lift sums.
-TOL_MIXED = 5e-4
-# P = 5: the operator entries (and the cancellation in the sums) are larger;
-# the FP32 SIMT kernel shows the same growth on these random states
-TOL_MIXED_P = {2: TOL_MIXED, 3: TOL_MIXED, 4: TOL_MIXED, 5: 2e-3}
+# oracle: element-wise RHS error relative to max |RHS|.  Split-BF16 keeps
+# 8 + 8 significant bits of each operand and drops the lo x lo product, so
+# each product is off by up to ~2^-16 relative; the derivative and lift sums
+# over K = 3 NP + 4 NFP columns add and partly cancel those errors.  Measured
+# on a B200 for every physics here at P2..P5: 3.2e-6 .. 1.7e-5 (largest:
+# shallow water P4); the bound is about 3x the largest.
+TOL_MIXED = 5e-5
+TOL_MIXED_P = {2: TOL_MIXED, 3: TOL_MIXED, 4: TOL_MIXED, 5: TOL_MIXED}
 
 
 # Split-TF32 (tcgen05 kind::tf32, 11 + 11 significant bits per operand): the
 # contraction is accurate to ~2^-21, so the RHS error is that of FP32
 # arithmetic in the fluxes (the FP32 SIMT kernel's own level on these
 # random states) rather than of the operand split.  P = 5 runs the FP32
-# kernel (its TF32 operands exceed a block's shared memory).
+# kernel (its TF32 operands exceed a block's shared memory).  Measured:
+# 1.3e-7 .. 2.1e-6.
 TOL_TF32 = {2: 5e-6, 3: 5e-6, 4: 5e-6, 5: 5e-6}
 
 
