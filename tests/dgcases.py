@@ -136,6 +136,8 @@ def rel_err(a, b):
 # 278-306).  The bound is that operator discrepancy plus accumulation slack.
 TOL_F64_3D = {1: 1e-12, 2: 1e-12, 3: 1e-12, 4: 2e-12, 5: 5e-12}
 TOL_F64_2D = {1: 1e-12, 2: 1e-12, 3: 1e-11, 4: 2e-10, 5: 1e-8}
-# FP32 product vs FP32 oracle (both mimic the reference's Float32 arithmetic;
-# summation order and fused multiply-adds differ)
-TOL_F32 = 2e-5
+# FP32 product vs FP32 oracle RHS (both mimic the reference's Float32
+# arithmetic; summation order and fused multiply-adds differ).  Measured on a
+# B200 for every 3D physics at P1..P5 and the two-fluid state: 1.7e-7 ..
+# 1.2e-6 (largest: shallow water P5); the bound is about 3x the largest.
+TOL_F32 = 4e-6

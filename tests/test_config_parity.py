@@ -117,6 +117,11 @@ def test_c3_maxwell_rhs_vs_oracle(oracle_mod, prec):
 # the three stages; FP32: against the oracle in FP32 (the reference's own
 # arithmetic), within the FP32 parity bound.
 C4_MEMBERS = 16
+# one limited FP32 SSPRK3 step against the FP32 oracle's: the RHS
+# differences of FP32 summation order pass through three stages and the
+# limiter's theta.  Measured on a B200 over the 16 members: 1.7e-7 ..
+# 5.9e-7; the bound is about 3x the largest.
+C4_TOL_F32 = 2e-6
 
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])
@@ -142,7 +147,7 @@ def test_c4_batched_members_vs_oracle(oracle_mod, prec):
         o.step(dt, 1)
         got, want = s.download_state().astype(np.float64), o.get(0)
         err = C.rel_err(got, want)
-        bound = 50 * C.TOL_F64_2D[s.P] if prec == "f64" else 5 * C.TOL_F32
+        bound = 50 * C.TOL_F64_2D[s.P] if prec == "f64" else C4_TOL_F32
         print(f"C4 {prec} member n={m.nx} P={s.P} {kind}: rel err {err:.2e} (bound {bound:.0e})")
         assert err <= bound, (m.nx, s.P, kind, err)
         worst = max(worst, err)
