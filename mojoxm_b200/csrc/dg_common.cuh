@@ -130,6 +130,25 @@ __device__ __forceinline__ void cube_dirs3(int cell, int nx, int ny, int nz, con
 // maximum first, then the count is the least of the shared-memory, thread
 // and register limits (what the occupancy calculator reports, computed here
 // from the device attributes so the carveout choice cannot lower it).
+// Launch with programmatic stream serialisation: the kernel's blocks may
+// start while the previous kernel of the stream finishes; the kernel itself
+// waits (grid_dep_wait) before it touches that kernel's data.
+template <class... KArgs, class... Args>
+cudaError_t launch_dependent(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t st,
+                             Args&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(unsigned(grid));
+  cfg.blockDim = dim3(unsigned(block));
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<Args&&>(args)...);
+}
+
 inline cudaError_t persistent_blocks_per_sm(const void* kern, int nt, size_t smem, int* bps) {
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;

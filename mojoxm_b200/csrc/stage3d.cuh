@@ -109,6 +109,7 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
   const R* Aop = ASMEM ? sA : args.A;
 
   const int tid = threadIdx.x;
+  grid_dep_launch();  // the next stage may set up as this one's blocks finish
   const int ngroups = (args.ncell - args.cbeg + EC - 1) / EC;
   if (tid == 0) {
     mbar_init(&bar[0], 1);
@@ -145,6 +146,10 @@ __global__ void __launch_bounds__(NT) stage3d_kernel(Stage3DArgs<R> args, KuhnTa
   };
   uint32_t par = 0u;  // bit b: phase parity of tile buffer b
   int buf = 0;
+  // the set-up above overlaps the previous stage's tail; its output (this
+  // stage's q_in / q_a / q_b, and q_out may be a buffer it still reads)
+  // only after it has completed
+  grid_dep_wait();
   if (tid == 0 && int(blockIdx.x) < ngroups && tile_bulk(blockIdx.x)) issue(blockIdx.x, 0);
 
   const int nwork = tab->n_face_work;

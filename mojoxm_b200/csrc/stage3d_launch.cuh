@@ -64,8 +64,7 @@ cudaError_t launch3_p(const Stage3DArgs<R>& a, const KuhnTab3<R>& tab, const Phy
   int nblk = nsm * bps;
   if (nblk > ngroups) nblk = ngroups;
   if (nblk < 1) nblk = 1;
-  kern<<<nblk, C::NT, C::kSmem, st>>>(a, tab, ph);
-  return cudaGetLastError();
+  return launch_dependent(kern, nblk, C::NT, C::kSmem, st, a, tab, ph);
   }
 }
 

@@ -52,8 +52,13 @@ cudaError_t launch_tc_p(const Stage3DArgs<float>& a, const Tc3Batch& bat, const 
     int nblk = 1;
     cudaError_t e = L::grid(nsm, ntiles, &nblk);
     if (e != cudaSuccess) return e;
-    stage3d_tc_kernel<Phys, P, L::NT, Op, BATCH><<<nblk, L::NT, L::smem, st>>>(a, tab, ph, img, bat);
-    return cudaGetLastError();
+    auto kern = stage3d_tc_kernel<Phys, P, L::NT, Op, BATCH>;
+    if constexpr (BATCH) {
+      kern<<<nblk, L::NT, L::smem, st>>>(a, tab, ph, img, bat);
+      return cudaGetLastError();
+    } else {
+      return launch_dependent(kern, nblk, L::NT, L::smem, st, a, tab, ph, img, bat);
+    }
   }
 }
 

@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
   Stage3DArgs<float>* sArgs = reinterpret_cast<Stage3DArgs<float>*>(smem + S::OFF_ARGS);
   const Stage3DArgs<float>& args = BATCH ? *sArgs : args0;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  grid_dep_launch();  // the next stage may set up as this one's blocks finish
   const int ngroups = BATCH ? bat.nitems : (args0.ncell - args0.cbeg + EC - 1) / EC;
   // tiles of this block: every gridDim.x-th from blockIdx.x (one solve), or
   // a contiguous range (batched)
@@ -302,6 +303,10 @@ __global__ void __launch_bounds__(NT, tc_min_blocks<Phys, P, Op>()) stage3d_tc_k
   };
   int buf = 0;
   bool failed = !block_wait_bounded(&bar[3], 0, kWaitLimitNs);
+  // the set-up above overlaps the previous stage's tail; its output (this
+  // stage's q_in / q_a / q_b, and q_out may be a buffer it still reads)
+  // only after it has completed
+  grid_dep_wait();
   if (t_first < t_end && !failed && tile_bulk(t_first)) {
     if (tid == 0) issue(t_first, 0);
     pend |= 1u;

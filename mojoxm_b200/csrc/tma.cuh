@@ -17,6 +17,15 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
+// Programmatic dependent launch.  grid_dep_launch: this block lets the next
+// kernel of the stream (launched with programmatic stream serialisation)
+// start its blocks as SMs free up.  grid_dep_wait: block until the previous
+// kernel of the stream has completed and its writes are visible; every read
+// of its output (and every write the previous kernel may still read) comes
+// after it.  Both return at once when the launch has no such dependency.
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Order this thread's earlier generic-proxy shared accesses before later
 // async-proxy (bulk copy) accesses of the same shared memory.
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
