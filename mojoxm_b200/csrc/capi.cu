@@ -734,12 +734,15 @@ void destroy(Handle* h) {
   if (h->comm) cudaStreamDestroy(h->comm);
   if (h->h2d) cudaStreamSynchronize(h->h2d);
   if (h->d2h) cudaStreamSynchronize(h->d2h);
-  for (cudaEvent_t e : {h->e_in_free, h->e_in, h->e_res, h->e_out_free})
-    if (e) cudaEventDestroy(e);
+  for (int k = 0; k < 2; ++k)
+    for (cudaEvent_t e : {h->e_in_free[k], h->e_in[k], h->e_res[k], h->e_out_free[k]})
+      if (e) cudaEventDestroy(e);
   if (h->h2d) cudaStreamDestroy(h->h2d);
   if (h->d2h) cudaStreamDestroy(h->d2h);
-  dev_free(h, h->in_stage);
-  dev_free(h, h->out_stage);
+  for (int k = 0; k < 2; ++k) {
+    dev_free(h, h->in_stage[k]);
+    dev_free(h, h->out_stage[k]);
+  }
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -1111,7 +1114,8 @@ int mxm_dg_advance_host(void* handle, const void* q_host, void* q_out_host, int 
 }
 
 // Pipelined host entry: the state arrives in a device staging buffer on an
-// upload stream and leaves from another on a download stream; the handle's
+// upload stream and leaves from another on a download stream (two of each,
+// used by alternate calls); the handle's
 // stream only copies it in and out on the device (two 3 TB/s copies), so one
 // call's upload runs beside the previous call's steps and download (PCIe is
 // full duplex) and the pipeline moves at the PCIe rate of one direction.
@@ -1121,27 +1125,36 @@ int mxm_dg_advance_host_async(void* handle, const void* q_host, void* q_out_host
   if (!h->h2d) {
     CK(cudaStreamCreateWithFlags(&h->h2d, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&h->d2h, cudaStreamNonBlocking));
-    for (cudaEvent_t* e : {&h->e_in_free, &h->e_in, &h->e_res, &h->e_out_free})
-      CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-    mxm::dev_alloc(h, &h->in_stage, h->qbytes());
-    mxm::dev_alloc(h, &h->out_stage, h->qbytes());
+    for (int k = 0; k < 2; ++k) {
+      for (cudaEvent_t* e : {&h->e_in_free[k], &h->e_in[k], &h->e_res[k], &h->e_out_free[k]})
+        CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+      mxm::dev_alloc(h, &h->in_stage[k], h->qbytes());
+      mxm::dev_alloc(h, &h->out_stage[k], h->qbytes());
+    }
     CK(cudaStreamSynchronize(h->stream));  // the copy streams use them next
-    CK(cudaEventRecord(h->e_in_free, h->h2d));
-    CK(cudaEventRecord(h->e_out_free, h->d2h));
+    for (int k = 0; k < 2; ++k) {
+      CK(cudaEventRecord(h->e_in_free[k], h->h2d));
+      CK(cudaEventRecord(h->e_out_free[k], h->d2h));
+    }
   }
-  CK(cudaStreamWaitEvent(h->h2d, h->e_in_free, 0));  // the previous input has left the staging buffer
-  CK(cudaMemcpyAsync(h->in_stage, q_host, h->qbytes(), cudaMemcpyHostToDevice, h->h2d));
-  CK(cudaEventRecord(h->e_in, h->h2d));
-  CK(cudaStreamWaitEvent(h->stream, h->e_in, 0));
-  CK(cudaMemcpyAsync(h->q[0], h->in_stage, h->qbytes(), cudaMemcpyDeviceToDevice, h->stream));
-  CK(cudaEventRecord(h->e_in_free, h->stream));
+  // Alternate calls use alternate staging buffers, so this call's upload
+  // waits only for the call before last to have moved its input out of the
+  // buffer (long done), not for the previous call's steps to start.
+  const int k = int(h->pipe_calls & 1);
+  CK(cudaStreamWaitEvent(h->h2d, h->e_in_free[k], 0));
+  CK(cudaMemcpyAsync(h->in_stage[k], q_host, h->qbytes(), cudaMemcpyHostToDevice, h->h2d));
+  CK(cudaEventRecord(h->e_in[k], h->h2d));
+  CK(cudaStreamWaitEvent(h->stream, h->e_in[k], 0));
+  CK(cudaMemcpyAsync(h->q[0], h->in_stage[k], h->qbytes(), cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaEventRecord(h->e_in_free[k], h->stream));
   mxm::step_n(h, dt, nsteps);
-  CK(cudaStreamWaitEvent(h->stream, h->e_out_free, 0));  // the previous result has left the staging buffer
-  CK(cudaMemcpyAsync(h->out_stage, h->q[0], h->qbytes(), cudaMemcpyDeviceToDevice, h->stream));
-  CK(cudaEventRecord(h->e_res, h->stream));
-  CK(cudaStreamWaitEvent(h->d2h, h->e_res, 0));
-  CK(cudaMemcpyAsync(q_out_host, h->out_stage, h->qbytes(), cudaMemcpyDeviceToHost, h->d2h));
-  CK(cudaEventRecord(h->e_out_free, h->d2h));
+  CK(cudaStreamWaitEvent(h->stream, h->e_out_free[k], 0));  // the call before last's result has left this buffer
+  CK(cudaMemcpyAsync(h->out_stage[k], h->q[0], h->qbytes(), cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaEventRecord(h->e_res[k], h->stream));
+  CK(cudaStreamWaitEvent(h->d2h, h->e_res[k], 0));
+  CK(cudaMemcpyAsync(q_out_host, h->out_stage[k], h->qbytes(), cudaMemcpyDeviceToHost, h->d2h));
+  CK(cudaEventRecord(h->e_out_free[k], h->d2h));
+  ++h->pipe_calls;
   API_END
 }
 

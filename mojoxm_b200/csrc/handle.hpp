@@ -49,9 +49,13 @@ struct Handle {
   cudaStream_t comm = nullptr;       // a slab part's exchange stream
   // host pipeline of mxm_dg_advance_host_async: copy streams, the result's
   // device staging buffer and the events that order them
+  // host-buffer pipeline: two staging buffers per direction, used by
+  // alternate calls (slot = pipe_calls & 1)
   cudaStream_t h2d = nullptr, d2h = nullptr;
-  void *in_stage = nullptr, *out_stage = nullptr;
-  cudaEvent_t e_in_free = nullptr, e_in = nullptr, e_res = nullptr, e_out_free = nullptr;
+  void *in_stage[2] = {nullptr, nullptr}, *out_stage[2] = {nullptr, nullptr};
+  cudaEvent_t e_in_free[2] = {nullptr, nullptr}, e_in[2] = {nullptr, nullptr};
+  cudaEvent_t e_res[2] = {nullptr, nullptr}, e_out_free[2] = {nullptr, nullptr};
+  int64_t pipe_calls = 0;
   cudaEvent_t ev_in = nullptr, ev_x = nullptr;  // input written / ghosts landed
   size_t rbytes = 8;
   int device = 0, nsm = 148;
