@@ -188,7 +188,9 @@ int mxm_dg_advance_host(void* handle, const void* q_host, void* q_out_host, int 
 /* The same, returning once enqueued: q_out_host holds the result after
  * mxm_dg_synchronize.  Successive calls pipeline (one call's download runs
  * beside the next call's upload and steps); the host buffers must stay
- * valid until the synchronize and should be pinned (mxm_dg_host_alloc). */
+ * valid until the synchronize and should be pinned (mxm_dg_host_alloc).
+ * The first call allocates four device staging buffers of one state each
+ * (two per direction, used by alternate calls); they live until destroy. */
 int mxm_dg_advance_host_async(void* handle, const void* q_host, void* q_out_host, int nsteps, double dt);
 
 /* ---- diagnostics (FP64 device reductions) -------------------------------- */
